@@ -1,0 +1,316 @@
+"""Benchmark of the B200 PM step (one JSON line on stdout).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+
+Workload (default c2, the single-GPU precision configuration): 512^3 CDM
+particles in a 1000 Mpc/h box, fine mesh 1024^3, coarse mesh 256^3, 8^3 tiles,
+int2 positions and velocities, PP on (pp_range=1), synthetic seeded Zel'dovich
+initial conditions at z_i=49 (Eisenstein-Hu no-wiggle, Philox noise).  A step
+is one pass of the reference main loop body: timestep, update_x,
+ext_pp_force, particle_mesh.  metric = particle-updates/s = Np * steps / time.
+
+value : device time of K steps (CUDA events on the library's stream, state
+        resident in HBM, meshes far larger than the 126 MB L2), max over ranks.
+e2e   : the same steps through the C-ABI as a host that owns the arrays would
+        drive it: per step cube_load_state from pinned host buffers (checkpoint
+        layout), the step, cube_store_state back to pinned host buffers.
+N > 1 : one independent box per rank (replicas, weak scaling), no collective
+        on the data path; barrier and max-over-ranks timing through NCCL.
+--impl reference: the CPU oracle (a restatement of the reference's Fortran
+        step; the Fortran reference cannot be built here) on the host cores, on
+        a bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    "c2": dict(nc=256, nnt=8, box=1000.0, izip=2, pp=True, z_i=49.0,
+               workload="512^3 particles, 1000 Mpc/h, fine 1024^3, coarse 256^3, int2 x/v, PP on (pp_range=1)"),
+    "c1": dict(nc=32, nnt=2, box=200.0, izip=2, pp=False, z_i=49.0,
+               workload="64^3 particles, 200 Mpc/h, fine 128^3, coarse 32^3, int2 x/v, PP off"),
+}
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def make_state(cfg, seed):
+    from cube_nufluid_b200 import ic
+    return ic.zeldovich(cfg["nc"], cfg["nnt"], box=cfg["box"], z_i=cfg["z_i"], seed=seed,
+                        izipx=cfg["izip"], izipv=cfg["izip"])
+
+
+def algorithmic_bytes(cfg, npart):
+    """Per-phase algorithmic bytes of one step (definitions of the survey, sec. 8(d))."""
+    nc = cfg["nc"]
+    nf = 4 * nc
+    Nf, Nc = nf ** 3, nc ** 3
+    bx = bv = 3 * cfg["izip"]
+    kf = 3 * (nf // 2 + 1) ** 3 * 4
+    kc = 3 * (nc // 2 + 1) ** 3 * 4
+    return {
+        "update_x": npart * (2 * bx + 2 * bv + 8),
+        "ext_pp_force": npart * (bx + 2 * bv),
+        "deposit": npart * bx + Nc * 4 + Nf * 4 + Nc * 4,
+        "fine_fft_green": 4 * 8 * Nf + kf,
+        "coarse_fft_green": 4 * 8 * Nc + kc,
+        "kick": npart * (bx + 2 * bv) + Nf * 12 + Nc * 12 + Nc * 12 + Nc * 8,
+    }
+
+
+PHASES = ["update_x", "ext_pp_force", "deposit", "fine_fft_green", "coarse_fft_green", "kick"]
+
+
+def run_ours(args, cfg, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from cube_nufluid_b200 import Cube, make_params, scalars_from_ic
+
+    torch.cuda.set_device(local_rank)
+    st = make_state(cfg, seed=1000 + rank)
+    p = make_params(cfg["nc"], cfg["nnt"], box=cfg["box"], izipx=cfg["izip"], izipv=cfg["izip"],
+                    ext_pp_force=cfg["pp"])
+    cube = Cube(p, np_capacity=st.np)
+    stream = torch.cuda.Stream()
+    cube.L.cube_set_stream(cube.h, stream.cuda_stream)
+    cube.load_state(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    s = scalars_from_ic(st)
+    npart = st.np
+
+    def step():
+        cube.timestep(s)
+        cube.update_x(s)
+        if cfg["pp"]:
+            cube.ext_pp_force(s)
+        cube.particle_mesh(s)
+
+    for _ in range(args.warmup):
+        step()
+    phase_sum = np.zeros(len(PHASES))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = cube.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(args.steps):
+                step()
+                pt = cube.phase_times()
+                phase_sum += np.array([pt[0], pt[1], pt[2], pt[3], pt[4], pt[5]])
+            ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = cube.launch_count() - l0
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+
+    # end to end through the C-ABI with host-resident arrays (pinned)
+    pin = {}
+    for name, a in (("xp", st.xp), ("vp", st.vp), ("pid", st.pid), ("rhoc", st.rhoc), ("vfield", st.vfield)):
+        h = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        h.numpy()[:] = np.ascontiguousarray(a).view(np.uint8).reshape(-1)
+        pin[name] = h
+    xp_h = pin["xp"].numpy().view(st.xp.dtype).reshape(st.xp.shape)
+    vp_h = pin["vp"].numpy().view(st.vp.dtype).reshape(st.vp.shape)
+    pid_h = pin["pid"].numpy().view(np.int32)
+    rhoc_h = pin["rhoc"].numpy().view(np.int32)
+    vf_h = pin["vfield"].numpy().view(np.float32).reshape(st.vfield.shape)
+    import ctypes as C
+
+    def ptr(a):
+        return a.ctypes.data_as(C.c_void_p)
+
+    e2e_steps = max(1, min(args.steps, 3))
+    h2d = xp_h.nbytes + vp_h.nbytes + pid_h.nbytes + rhoc_h.nbytes + vf_h.nbytes
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            cube._check(cube.L.cube_load_state(cube.h, xp_h.shape[0], ptr(xp_h), ptr(vp_h), ptr(pid_h),
+                                               ptr(rhoc_h), ptr(vf_h)))
+            step()
+            n = C.c_int64(0)
+            cube._check(cube.L.cube_store_state(cube.h, C.byref(n), ptr(xp_h), ptr(vp_h), ptr(pid_h),
+                                                ptr(rhoc_h), ptr(vf_h)))
+        e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t2.item())
+    return dict(ms=ms_max, npart=npart, launches=launches, phase_ms=phase_sum / args.steps, clocks=clk.summary(),
+                e2e_ms=e2e_ms, e2e_steps=e2e_steps, h2d=h2d, d2h=h2d, scal=s.as_dict())
+
+
+def cpu_sample(threads: int):
+    """The CPU oracle on a bounded sample: one step (update_x + PP + particle_mesh)
+    of a 64^3-particle box with the workload's method settings."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    from oracle_ref import Oracle
+    from cube_nufluid_b200 import ic, tables, make_params, scalars_from_ic
+
+    st = ic.zeldovich(32, 2, box=200.0, z_i=49.0, seed=7)
+    p = make_params(32, 2, box=200.0, ext_pp_force=True)
+    o = Oracle(p, tables.read_fine_table(), tables.read_coarse_table())
+    o.load(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    s = scalars_from_ic(st)
+    s.dt_old = s.dt = 0.5
+    s.a_mid = s.a
+    t0 = time.perf_counter()
+    o.update_x(s)
+    o.ext_pp_force(s)
+    o.particle_mesh(s, 0)
+    dt = time.perf_counter() - t0
+    return {"value": st.np / dt, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+            "sample": f"1 step (update_x + ext_pp_force + particle_mesh, FP32 reference-order deposit, FP64 FFT) "
+                      f"of a {st.np}-particle box (nc=32, nf=128, 2^3 tiles) on {threads} host thread; "
+                      f"{dt:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=list(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    npart = (2 * cfg["nc"]) ** 3
+    config = {"workload": cfg["workload"], "particles": npart, "nc": cfg["nc"], "nf": 4 * cfg["nc"],
+              "tiles": cfg["nnt"] ** 3, "parallelism": f"replicas x{args.gpus}",
+              "l2": "inputs larger than L2 (meshes of GBs)", "ic": "Zel'dovich z=49, seeded (synthetic)"}
+    metric = "PM step particle-updates/s"
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        base = cpu_sample(1)
+        line = {"impl": "reference", "metric": metric, "value": base["value"], "unit": "particle-updates/s",
+                "n_gpus": args.gpus, "steps": 1, "warmup": 0, "higher_is_better": True, "config": config,
+                "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "particle-updates/s",
+                                              "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "data": "synthetic", "dtype": "f32"}
+        print(json.dumps(line))
+        return
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from cube_nufluid_b200 import build
+    if rank == 0:
+        build.build()
+    if world > 1:
+        dist.barrier()
+    r = run_ours(args, cfg, rank, world, local_rank)
+    value = r["npart"] * world * args.steps / (r["ms"] / 1e3)
+    e2e = r["npart"] * world * r["e2e_steps"] / (r["e2e_ms"] / 1e3)
+    peak, peak_kind = read_peaks()
+    ab = algorithmic_bytes(cfg, r["npart"])
+    phases = {k: float(v) for k, v in zip(PHASES, r["phase_ms"])}
+    dom = max(phases, key=lambda k: phases[k])
+    ach = ab[dom] / (phases[dom] / 1e3) / 1e9
+    phase_gbs = {k: (ab[k] / (phases[k] / 1e3) / 1e9 if phases[k] > 0 else None) for k in PHASES}
+    line = {
+        "metric": metric, "value": value, "unit": "particle-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+        "e2e": {"value": e2e, "unit": "particle-updates/s", "h2d_bytes_per_step": r["h2d"],
+                "d2h_bytes_per_step": r["d2h"], "steps": r["e2e_steps"]},
+        "gpu_launches": int(r["launches"]),
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+                     "frac": ach / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes": ab[dom]},
+        "phases_ms": phases, "phase_gbs": phase_gbs, "clocks": r["clocks"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_sample(1)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,147 @@
+/*
+ * cube_internal.cuh -- device state and launch helpers of the B200 PM step.
+ *
+ * Device layout (one image on one GPU; tiles are only an ordering):
+ *   cell id   c = ((tz*nnt+ty)*nnt+tx)*nt^3 + (lz*nt+ly)*nt + lx
+ *             (Fortran rhoc(lx,ly,lz,tx,ty,tz) order, variables.f90:65)
+ *   particles cell-sorted, each particle stored once (no buffer copies);
+ *             SoA: xp[d][cap], vp[d][cap] (1 or 2 bytes), pid[cap]
+ *   cell_start[c] (int64, exclusive prefix of rhoc), vfield[d][ncells]
+ *   fine mesh nf^3 with row pitch rp = nf+32 floats (128-byte rows), used
+ *             in place as the half spectrum (complex pitch cp = rp/2)
+ *   coarse mesh nc^3, same convention
+ */
+#ifndef CUBE_INTERNAL_CUH
+#define CUBE_INTERNAL_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+#include <vector>
+
+#include "../../include/cube_gpu.h"
+#include "cube_codec.h"
+
+#define CUBE_MAX_RADIX_STAGES 12
+
+struct FftPlan {
+  int n;                          // transform length
+  int nst;                        // number of stages
+  int radix[CUBE_MAX_RADIX_STAGES];
+  float2* tw;                     // device twiddles exp(-2 pi i j/n), j < n
+};
+
+struct MeshLevel {
+  int n;          // mesh points per dimension
+  int rp;         // real row pitch (floats)
+  int cp;         // complex row pitch (float2) = rp/2
+  size_t plane;   // floats per z-plane = n*rp
+  float* rho;     // density, in place as the forward half spectrum
+  float* force;   // [3] force meshes, each n*plane floats, in place as spectra
+  float* kern;    // Green multiplier (imaginary parts, /n^3)
+  int kern_octant;  // 1: kern is [3][(n/2+1)^3] octant; 0: [3][n][n][cp_k]
+  int kern_pitch;   // inner pitch of kern (n/2+1)
+  FftPlan plan;
+};
+
+struct DevScal {
+  unsigned int f2_fine_bits;   // max f^2 as float bits (non-negative floats order as ints)
+  unsigned int f2_coarse_bits;
+  unsigned int vmax_bits[3];
+  unsigned int f2_pp_bits;
+  int err;                     // first error code seen on the device
+  int err_info;
+  unsigned long long n_big;    // re-bin cells needing the block sorter
+  unsigned long long itest1, npairs;
+  unsigned long long moved_far;
+};
+
+struct cube_ctx {
+  cube_params P;
+  int nc, nnt, nt, ncell, ncb, nte, nf, nvbin;
+  int64_t ncells;
+  int izipx, izipv;
+  cube_codec codec;
+  cudaStream_t stream;
+  int own_stream;
+  int64_t np, cap;
+  int state_loaded;
+  // particles (double-buffered for the re-bin)
+  void* xp;  void* vp;  int32_t* pid;
+  void* xp2; void* vp2; int32_t* pid2;
+  int32_t* rhoc;  int32_t* rhoc2;
+  int64_t* cell_start; int64_t* cell_start2;
+  float* vfield; float* vfield2;
+  // re-bin scratch
+  int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
+  int32_t* big_list;
+  double* cell_stats;   // [3][ncells]
+  double* red_tmp;      // scratch for tree sums
+  int64_t* scan_tmp;
+  // meshes
+  MeshLevel fine, coarse;
+  unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator
+  double* dep_partial;            // per-CTA fine mass partial sums
+  int64_t dep_blocks;
+  float* tan_table;               // tanf of each velocity code, index code+nvbin/2
+  DevScal* dscal;                 // device scalars
+  DevScal* hscal;                 // pinned host mirror
+  float2* sbuf;                   // spare spectrum buffer for the forward z pass
+  // timing
+  cudaEvent_t ev[16];
+  float phase_ms[8];
+  long long launches;
+  std::string err;
+};
+
+// ---- error helpers ---------------------------------------------------------
+#define CUBE_CUDA_TRY(ctx, call)                                                   \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      (ctx)->err = std::string(#call) + ": " + cudaGetErrorString(e_);             \
+      return CUBE_ERR_CUDA;                                                        \
+    }                                                                              \
+  } while (0)
+
+#define CUBE_LAUNCH_CHECK(ctx)                                                     \
+  do {                                                                             \
+    (ctx)->launches++;                                                             \
+    cudaError_t e_ = cudaGetLastError();                                           \
+    if (e_ != cudaSuccess) {                                                       \
+      (ctx)->err = std::string("launch: ") + cudaGetErrorString(e_);               \
+      return CUBE_ERR_CUDA;                                                        \
+    }                                                                              \
+  } while (0)
+
+__device__ __forceinline__ void cube_dev_error(DevScal* s, int code, int info) {
+  if (atomicCAS(&s->err, 0, code) == 0) s->err_info = info;
+}
+
+// device-side view of the particle codes
+template <int Z>
+struct CodeT;
+template <>
+struct CodeT<1> { typedef int8_t T; };
+template <>
+struct CodeT<2> { typedef int16_t T; };
+
+__device__ __forceinline__ int64_t cube_cell_of(int gx, int gy, int gz, int nt, int nnt) {
+  const int tx = gx / nt, ty = gy / nt, tz = gz / nt;
+  const int lx = gx - tx * nt, ly = gy - ty * nt, lz = gz - tz * nt;
+  return ((((int64_t)tz * nnt + ty) * nnt + tx) * nt + lz) * (int64_t)nt * nt + (int64_t)ly * nt + lx;
+}
+
+// ---- launchers (implemented in the k_*.cu files) -----------------------------
+int cube_rebin(cube_ctx* ctx, cube_scalars* io);
+int cube_deposit(cube_ctx* ctx, cube_scalars* io);
+int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits);
+int cube_kick(cube_ctx* ctx, cube_scalars* io);
+int cube_pp(cube_ctx* ctx, cube_scalars* io);
+int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table);
+int cube_tree_sum_dev(cube_ctx* ctx, const double* in, int64_t n, double* out_host);
+int cube_exclusive_scan(cube_ctx* ctx, const int32_t* in, int64_t n, int64_t* out);
+int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n);
+int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int ncomp, unsigned int* f2_bits);
+
+#endif

@@ -1,0 +1,191 @@
+/*
+ * k_deposit.cu -- fine and coarse CIC mass deposit (pm.f90:76-107, :192-278).
+ *
+ * One CTA owns a brick of BX x BY x BZ coarse cells and the 4B^3 fine nodes
+ * inside it.  It reads the particles of its cells plus the one-cell layer on
+ * the low side of each dimension (the only outside particles whose CIC cloud
+ * reaches the brick's first node plane), accumulates every weight into
+ * shared memory as a 64-bit fixed-point integer (weight * 2^32, rounded to
+ * nearest), and writes each fine node once as FP32.  Integer accumulation
+ * makes the density independent of particle order: the fine mesh is
+ * bit-identical to the fixed-point mode of the CPU oracle.
+ *
+ * Weights follow the reference expressions in FP32, with the position formed
+ * in FP64 and rounded to FP32 exactly where the reference assigns it to its
+ * real tempx (tile-relative coordinates, as in pm.f90:87 and :255).
+ *
+ * The coarse deposit (ncell coarser, node at the cell centre) is accumulated
+ * from the brick's own particles into a (B+2)^3 shared region and added to a
+ * global 64-bit accumulator with atomics; the nc^3 accumulator stays in L2.
+ */
+#include "cube_internal.cuh"
+
+namespace {
+
+constexpr int BX = 8, BY = 4, BZ = 4;
+constexpr int HX = BX + 1, HY = BY + 1, HZ = BZ + 1;
+constexpr int NHC = HX * HY * HZ;  // cells read (with the low-side layer)
+constexpr int FX = 4 * BX, FY = 4 * BY, FZ = 4 * BZ;
+constexpr int CX = BX + 2, CY = BY + 2, CZ = BZ + 2;
+constexpr double FIX_SCALE = 4294967296.0;  // 2^32
+
+template <int ZX>
+__global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, const int64_t* __restrict__ cell_start,
+                                                 int64_t cap, int nc, int nt, int nnt, float mass,
+                                                 float* __restrict__ rho, int rp, size_t plane,
+                                                 unsigned long long* __restrict__ rho_c_acc,
+                                                 unsigned long long* __restrict__ mass_total) {
+  typedef typename CodeT<ZX>::T TX;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  extern __shared__ unsigned long long smem_u64[];
+  unsigned long long* facc = smem_u64;                 // FX*FY*FZ
+  unsigned long long* cacc = facc + FX * FY * FZ;      // CX*CY*CZ
+  __shared__ int64_t cst[NHC];
+  __shared__ int cpre[NHC + 1];
+
+  const int nbx = nc / BX, nby = nc / BY;
+  const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
+  const int x0 = bx * BX, y0 = by * BY, z0 = bz * BZ;
+
+  for (int i = threadIdx.x; i < FX * FY * FZ; i += blockDim.x) facc[i] = 0ull;
+  for (int i = threadIdx.x; i < CX * CY * CZ; i += blockDim.x) cacc[i] = 0ull;
+  if (threadIdx.x < 32) {
+    // cell table of the (B+1)^3 region in (z,y,x) order; warp 0 builds the prefix
+    int run = 0;
+    for (int base = 0; base < NHC; base += 32) {
+      const int q = base + threadIdx.x;
+      int cnt = 0;
+      if (q < NHC) {
+        const int cx = q % HX - 1, cy = (q / HX) % HY - 1, cz = q / (HX * HY) - 1;
+        const int gx = (x0 + cx + nc) % nc, gy = (y0 + cy + nc) % nc, gz = (z0 + cz + nc) % nc;
+        const int64_t c = cube_cell_of(gx, gy, gz, nt, nnt);
+        const int64_t s0 = cell_start[c];
+        cst[q] = s0;
+        cnt = (int)(cell_start[c + 1] - s0);
+      }
+      int inc = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)threadIdx.x >= o) inc += v;
+      }
+      if (q < NHC) cpre[q] = run + inc - cnt;
+      run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (threadIdx.x == 0) cpre[NHC] = run;
+  }
+  __syncthreads();
+  const int total = cpre[NHC];
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int lo = 0, hi = NHC - 1;  // last q with cpre[q] <= t
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cpre[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const int q = lo;
+    const int64_t ip = cst[q] + (t - cpre[q]);
+    const int cx = q % HX - 1, cy = (q / HX) % HY - 1, cz = q / (HX * HY) - 1;
+    const int cu[3] = {x0 + cx, y0 + cy, z0 + cz};     // unwrapped global coarse cell
+    const int own = (cx >= 0 && cy >= 0 && cz >= 0);
+    int o1[3], c1[3];
+    float dx1[3], dx2[3], cd1[3], cd2[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int g = (cu[d] + nc) % nc;
+      const int l = g % nt;
+      const double fr = cube_xfrac((int32_t)xp[(size_t)d * cap + ip], ZX);
+      // fine: tempx = ncell*(i-1) + ncell*frac (tile-relative), FP64 -> FP32
+      const float tf = (float)cube_dadd(4.0 * (double)l, cube_dmul(4.0, fr));
+      const float f = floorf(tf) + 1.f;
+      dx1[d] = cube_fsub(f, tf);
+      dx2[d] = cube_fsub(1.f, dx1[d]);
+      o1[d] = 4 * (cu[d] - (d == 0 ? x0 : d == 1 ? y0 : z0)) + ((int)f - 1 - 4 * l);
+      // coarse: tempx = (i-1) + frac - 0.5, FP64 -> FP32
+      const float tc = (float)cube_dsub(cube_dadd((double)l, fr), 0.5);
+      const float ci = floorf(tc) + 1.f;
+      cd1[d] = cube_fsub(ci, tc);
+      cd2[d] = cube_fsub(1.f, cd1[d]);
+      c1[d] = (cu[d] - (d == 0 ? x0 : d == 1 ? y0 : z0)) + ((int)ci - 1 - l) + 1;  // +1: region starts at -1
+    }
+#pragma unroll
+    for (int c8 = 0; c8 < 8; ++c8) {
+      const int sx = c8 & 1, sy = (c8 >> 1) & 1, sz = c8 >> 2;
+      const int nx = o1[0] + sx, ny = o1[1] + sy, nz = o1[2] + sz;
+      if (nx >= 0 && nx < FX && ny >= 0 && ny < FY && nz >= 0 && nz < FZ) {
+        const float w = cube_fmul(cube_fmul(cube_fmul(sx ? dx2[0] : dx1[0], sy ? dx2[1] : dx1[1]),
+                                            sz ? dx2[2] : dx1[2]), mass);
+        const unsigned long long qv = (unsigned long long)__double2ll_rn((double)w * FIX_SCALE);
+        atomicAdd(&facc[(nz * FY + ny) * FX + nx], qv);
+      }
+      if (own) {
+        const float w = cube_fmul(cube_fmul(cube_fmul(sx ? cd2[0] : cd1[0], sy ? cd2[1] : cd1[1]),
+                                            sz ? cd2[2] : cd1[2]), mass);
+        const unsigned long long qv = (unsigned long long)__double2ll_rn((double)w * FIX_SCALE);
+        atomicAdd(&cacc[((c1[2] + sz) * CY + (c1[1] + sy)) * CX + (c1[0] + sx)], qv);
+      }
+    }
+  }
+  __syncthreads();
+  unsigned long long msum = 0ull;
+  for (int i = threadIdx.x; i < FX * FY * FZ; i += blockDim.x) {
+    const int nx = i % FX, ny = (i / FX) % FY, nz = i / (FX * FY);
+    const unsigned long long a = facc[i];
+    msum += a;
+    rho[(size_t)(4 * z0 + nz) * plane + (size_t)(4 * y0 + ny) * rp + (4 * x0 + nx)] =
+        (float)((double)a * (1.0 / FIX_SCALE));
+  }
+  for (int i = threadIdx.x; i < CX * CY * CZ; i += blockDim.x) {
+    const unsigned long long a = cacc[i];
+    if (a) {
+      const int nx = i % CX - 1, ny = (i / CX) % CY - 1, nz = i / (CX * CY) - 1;
+      const int gx = (x0 + nx + nc) % nc, gy = (y0 + ny + nc) % nc, gz = (z0 + nz + nc) % nc;
+      atomicAdd(&rho_c_acc[((size_t)gz * nc + gy) * nc + gx], a);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) msum += __shfl_xor_sync(0xffffffffu, msum, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(mass_total, msum);
+}
+
+// coarse accumulator -> FP32 density (pitch rp), accumulator cleared for the next step
+__global__ void k_coarse_finalize(unsigned long long* __restrict__ acc, float* __restrict__ r3, int nc, int rp,
+                                  unsigned long long* __restrict__ mass_total) {
+  const int64_t n = (int64_t)nc * nc * nc;
+  unsigned long long msum = 0ull;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long a = acc[i];
+    acc[i] = 0ull;
+    msum += a;
+    const int64_t x = i % nc, yz = i / nc;
+    r3[yz * rp + x] = (float)((double)a * (1.0 / FIX_SCALE));
+  }
+  for (int o = 16; o > 0; o >>= 1) msum += __shfl_xor_sync(0xffffffffu, msum, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(mass_total, msum);
+}
+
+}  // namespace
+
+int cube_deposit(cube_ctx* ctx, cube_scalars* io) {
+  const int nc = ctx->nc;
+  if (nc % BX || nc % BY || nc % BZ) {
+    ctx->err = "nc must be a multiple of 8";
+    return CUBE_ERR_PARAM;
+  }
+  unsigned long long* mtot = reinterpret_cast<unsigned long long*>(ctx->red_tmp);
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(mtot, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  const int blocks = (nc / BX) * (nc / BY) * (nc / BZ);
+  const size_t smem = sizeof(unsigned long long) * (FX * FY * FZ + CX * CY * CZ);
+  if (ctx->izipx == 1) {
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_deposit<1><<<blocks, 256, smem, ctx->stream>>>(ctx->xp, ctx->cell_start, ctx->cap, nc, ctx->nt, ctx->nnt,
+                                                     io->mass_p_cdm, ctx->fine.rho, ctx->fine.rp, ctx->fine.plane,
+                                                     ctx->rho_c_acc, mtot);
+  } else {
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_deposit<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_deposit<2><<<blocks, 256, smem, ctx->stream>>>(ctx->xp, ctx->cell_start, ctx->cap, nc, ctx->nt, ctx->nnt,
+                                                     io->mass_p_cdm, ctx->fine.rho, ctx->fine.rp, ctx->fine.plane,
+                                                     ctx->rho_c_acc, mtot);
+  }
+  CUBE_LAUNCH_CHECK(ctx);
+  k_coarse_finalize<<<592, 256, 0, ctx->stream>>>(ctx->rho_c_acc, ctx->coarse.rho, nc, ctx->coarse.rp, mtot + 1);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}

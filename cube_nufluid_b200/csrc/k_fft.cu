@@ -1,0 +1,383 @@
+/*
+ * k_fft.cu -- 3-D real FFT Poisson solve of one mesh level (fine or coarse).
+ *
+ * Replaces the reference's FFTW calls of the PM step: the fine r2c + 3x
+ * (x i*kern_f, c2r) of pm.f90:112-125 and the coarse pencil_fft_forward +
+ * 3x (x i*kern_c, pencil_fft_backward) of pm.f90:288-300.  On one GPU the
+ * fine level is one periodic nf^3 transform: the fine kernel has a support of
+ * +-(nf_cutoff-1) fine cells, smaller than the nfb=24 buffer of the
+ * reference's per-tile meshes, so the per-tile circular convolutions and the
+ * periodic one agree cell for cell in exact arithmetic (checked against the
+ * per-tile oracle in the tests).
+ *
+ * Passes over HBM (each a Stockham mixed-radix FFT in shared memory):
+ *   X  : r2c along x, two real rows packed into one complex transform
+ *   Y  : complex along y, TK consecutive kx columns per CTA
+ *   Z  : complex along z, then per force component d: x i*K_d(k), inverse
+ *        along z, store  (one read, three writes)
+ *   Y^-1 x3, X^-1 (c2r) x3 with the max of f^2 fused (pm.f90:126,328)
+ * The half spectrum lives in place in the real arrays (row pitch rp floats,
+ * complex pitch cp = rp/2).  Normalisation 1/n^3 is folded into K.
+ */
+#include "cube_internal.cuh"
+
+#include <cmath>
+
+namespace {
+
+__device__ __forceinline__ float2 cmulf(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 caddf(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csubf(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+// multiply by sign*i
+__device__ __forceinline__ float2 mul_si(float2 a, float s) { return make_float2(-s * a.y, s * a.x); }
+
+template <int P>
+__device__ __forceinline__ void dft(float2* v, float s) {
+  if (P == 2) {
+    const float2 a = v[0], b = v[1];
+    v[0] = caddf(a, b);
+    v[1] = csubf(a, b);
+  } else if (P == 4) {
+    const float2 t0 = caddf(v[0], v[2]), t1 = csubf(v[0], v[2]);
+    const float2 t2 = caddf(v[1], v[3]), t3 = mul_si(csubf(v[1], v[3]), s);
+    v[0] = caddf(t0, t2);
+    v[2] = csubf(t0, t2);
+    v[1] = caddf(t1, t3);
+    v[3] = csubf(t1, t3);
+  } else if (P == 3) {
+    const float c = -0.5f, sn = 0.86602540378443865f;
+    const float2 sm = caddf(v[1], v[2]), df = csubf(v[1], v[2]);
+    const float2 m = make_float2(v[0].x + c * sm.x, v[0].y + c * sm.y);
+    const float2 r = mul_si(make_float2(sn * df.x, sn * df.y), s);
+    v[0] = caddf(v[0], sm);
+    v[1] = caddf(m, r);
+    v[2] = csubf(m, r);
+  } else if (P == 5) {
+    // X_k = sum_r v_r w^{rk}, w = exp(s 2 pi i/5)
+    const float c1 = 0.30901699437494742f, c2 = -0.80901699437494742f;
+    const float s1 = 0.95105651629515357f, s2 = 0.58778525229247313f;
+    const float2 a1 = caddf(v[1], v[4]), b1 = csubf(v[1], v[4]);
+    const float2 a2 = caddf(v[2], v[3]), b2 = csubf(v[2], v[3]);
+    const float2 m1 = make_float2(v[0].x + c1 * a1.x + c2 * a2.x, v[0].y + c1 * a1.y + c2 * a2.y);
+    const float2 m2 = make_float2(v[0].x + c2 * a1.x + c1 * a2.x, v[0].y + c2 * a1.y + c1 * a2.y);
+    const float2 n1 = mul_si(make_float2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), s);
+    const float2 n2 = mul_si(make_float2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), s);
+    v[0] = caddf(v[0], caddf(a1, a2));
+    v[1] = caddf(m1, n1);
+    v[4] = csubf(m1, n1);
+    v[2] = caddf(m2, n2);
+    v[3] = csubf(m2, n2);
+  }
+}
+
+// One Stockham stage on nseq sequences of length n stored at buf[s*ss + j*js].
+// Reads are staged in registers so the stage runs in place.
+template <int P, int MAXIT>
+__device__ __forceinline__ void fft_stage(float2* buf, int n, int nseq, int ss, int js, int T,
+                                          const float2* __restrict__ tw, float sgn, bool seq_fast) {
+  const int nb = n / P;
+  const int total = nb * nseq;
+  const int nthr = blockDim.x;
+  float2 v[MAXIT][P];
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int t = threadIdx.x + it * nthr;
+    if (t < total) {
+      int s, i;
+      if (seq_fast) { s = t % nseq; i = t / nseq; } else { i = t % nb; s = t / nb; }
+#pragma unroll
+      for (int r = 0; r < P; ++r) v[it][r] = buf[s * ss + (i + r * nb) * js];
+    }
+  }
+  __syncthreads();
+  const int tstep = n / (P * T);
+#pragma unroll
+  for (int it = 0; it < MAXIT; ++it) {
+    const int t = threadIdx.x + it * nthr;
+    if (t < total) {
+      int s, i;
+      if (seq_fast) { s = t % nseq; i = t / nseq; } else { i = t % nb; s = t / nb; }
+      const int k = i % T;
+#pragma unroll
+      for (int r = 1; r < P; ++r) {
+        float2 w = __ldg(&tw[r * k * tstep]);
+        w.y *= -sgn;  // table holds exp(-2 pi i j/n); sgn=-1 forward, +1 inverse
+        v[it][r] = cmulf(v[it][r], w);
+      }
+      dft<P>(v[it], sgn);
+      const int j0 = (i - k) * P + k;
+#pragma unroll
+      for (int r = 0; r < P; ++r) buf[s * ss + (j0 + r * T) * js] = v[it][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <int MAXIT>
+__device__ void fft_smem(float2* buf, int n, int nseq, int ss, int js, const FftPlan& pl, float sgn,
+                         bool seq_fast) {
+  int T = 1;
+  for (int st = 0; st < pl.nst; ++st) {
+    const int p = pl.radix[st];
+    if (p == 4) fft_stage<4, MAXIT>(buf, n, nseq, ss, js, T, pl.tw, sgn, seq_fast);
+    else if (p == 2) fft_stage<2, MAXIT * 2>(buf, n, nseq, ss, js, T, pl.tw, sgn, seq_fast);
+    else if (p == 3) fft_stage<3, MAXIT * 2>(buf, n, nseq, ss, js, T, pl.tw, sgn, seq_fast);
+    else if (p == 5) fft_stage<5, MAXIT>(buf, n, nseq, ss, js, T, pl.tw, sgn, seq_fast);
+    T *= p;
+  }
+}
+
+__device__ __forceinline__ void atomic_max_pos(unsigned int* addr, float v) {
+  atomicMax(addr, __float_as_uint(v));  // v >= 0: IEEE order equals unsigned order
+}
+
+// ---------------------------------------------------------------------------
+// X pass: r2c (inverse=0) or c2r (inverse=1) along contiguous rows.
+// Rows r = z*n + y at data + r*rp.  A CTA takes RPB row pairs; for the c2r of
+// the force (ncomp=3) it takes the same rows of the three components and
+// reduces max(fx^2+fy^2+fz^2).
+template <int MAXIT>
+__global__ void k_fft_x(float* __restrict__ data, size_t comp_stride, int ncomp, int n, int rp,
+                        int npairs, int rpb, FftPlan pl, int inverse, unsigned int* f2_bits) {
+  extern __shared__ float2 sm[];
+  const int ss = n + 1;  // odd pitch spreads rows over banks
+  const int pair0 = blockIdx.x * rpb;
+  const int np_blk = min(rpb, npairs - pair0);
+  const int cp = rp / 2;
+  for (int c = 0; c < ncomp; ++c) {
+    float* base = data + c * comp_stride;
+    float2* buf = sm + (size_t)c * rpb * ss;
+    if (!inverse) {
+      for (int t = threadIdx.x; t < np_blk * n; t += blockDim.x) {
+        const int q = t / n, j = t - q * n;
+        const size_t ra = (size_t)(2 * (pair0 + q)) * rp;
+        buf[q * ss + j] = make_float2(base[ra + j], base[ra + rp + j]);
+      }
+    } else {
+      const float2* cb = reinterpret_cast<const float2*>(base);
+      const int nh = n / 2;
+      for (int t = threadIdx.x; t < np_blk * n; t += blockDim.x) {
+        const int q = t / n, k = t - q * n;
+        const size_t ra = (size_t)(2 * (pair0 + q)) * cp;
+        float2 z;
+        if (k == 0 || k == nh) {
+          const float2 A = cb[ra + k], B = cb[ra + cp + k];
+          z = make_float2(A.x, B.x);
+        } else if (k < nh) {
+          const float2 A = cb[ra + k], B = cb[ra + cp + k];
+          z = make_float2(A.x - B.y, A.y + B.x);
+        } else {
+          const float2 A = cb[ra + (n - k)], B = cb[ra + cp + (n - k)];
+          z = make_float2(A.x + B.y, B.x - A.y);
+        }
+        buf[q * ss + k] = z;
+      }
+    }
+  }
+  __syncthreads();
+  for (int c = 0; c < ncomp; ++c)
+    fft_smem<MAXIT>(sm + (size_t)c * rpb * ss, n, np_blk, ss, 1, pl, inverse ? 1.f : -1.f, false);
+  if (!inverse) {
+    float* base = data;
+    float2* cb = reinterpret_cast<float2*>(base);
+    const int nh = n / 2;
+    for (int t = threadIdx.x; t < np_blk * (nh + 1); t += blockDim.x) {
+      const int q = t / (nh + 1), k = t - q * (nh + 1);
+      const float2 Zk = sm[q * ss + k];
+      const float2 Zm = sm[q * ss + ((n - k) % n)];
+      const float2 Zc = make_float2(Zm.x, -Zm.y);
+      const float2 A = make_float2(0.5f * (Zk.x + Zc.x), 0.5f * (Zk.y + Zc.y));
+      const float2 D = csubf(Zk, Zc);
+      const float2 B = make_float2(0.5f * D.y, -0.5f * D.x);
+      const size_t ra = (size_t)(2 * (pair0 + q)) * cp;
+      cb[ra + k] = A;
+      cb[ra + cp + k] = B;
+    }
+  } else {
+    float f2max = 0.f;
+    for (int t = threadIdx.x; t < np_blk * n; t += blockDim.x) {
+      const int q = t / n, j = t - q * n;
+      const size_t ra = (size_t)(2 * (pair0 + q)) * rp;
+      float fa[3], fb[3];
+      for (int c = 0; c < ncomp; ++c) {
+        const float2 z = sm[(size_t)c * rpb * ss + q * ss + j];
+        float* base = data + c * comp_stride;
+        base[ra + j] = z.x;
+        base[ra + rp + j] = z.y;
+        fa[c] = z.x;
+        fb[c] = z.y;
+      }
+      if (ncomp == 3 && f2_bits) {
+        const float a2 = __fadd_rn(__fadd_rn(__fmul_rn(fa[0], fa[0]), __fmul_rn(fa[1], fa[1])), __fmul_rn(fa[2], fa[2]));
+        const float b2 = __fadd_rn(__fadd_rn(__fmul_rn(fb[0], fb[0]), __fmul_rn(fb[1], fb[1])), __fmul_rn(fb[2], fb[2]));
+        f2max = fmaxf(f2max, fmaxf(a2, b2));
+      }
+    }
+    if (ncomp == 3 && f2_bits) {
+      for (int o = 16; o > 0; o >>= 1) f2max = fmaxf(f2max, __shfl_xor_sync(0xffffffffu, f2max, o));
+      if ((threadIdx.x & 31) == 0) atomic_max_pos(f2_bits, f2max);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column pass along y (other = z) or z (other = y): TK consecutive kx columns.
+template <int MAXIT>
+__global__ void k_fft_col(float2* __restrict__ base, size_t comp_stride, int n, int ncol, int tk,
+                          long long jstride, long long ostride, FftPlan pl, float sgn) {
+  extern __shared__ float2 sm[];
+  const int kx0 = blockIdx.x * tk;
+  const int nk = min(tk, ncol - kx0);
+  float2* b = base + blockIdx.z * comp_stride + (size_t)blockIdx.y * ostride + kx0;
+  for (int t = threadIdx.x; t < n * tk; t += blockDim.x) {
+    const int j = t / tk, c = t - j * tk;
+    sm[j * tk + c] = (c < nk) ? b[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_smem<MAXIT>(sm, n, tk, 1, tk, pl, sgn, true);
+  for (int t = threadIdx.x; t < n * tk; t += blockDim.x) {
+    const int j = t / tk, c = t - j * tk;
+    if (c < nk) b[(size_t)j * jstride + c] = sm[j * tk + c];
+  }
+}
+
+// Fused z pass: forward along z, then for each component d multiply by i*K_d
+// (octant table, odd in k_d, even in the others) and transform back.
+template <int MAXIT>
+__global__ void k_fft_z_green(const float2* __restrict__ in, float2* __restrict__ out0, size_t comp_stride,
+                              int n, int ncol, int tk, long long jstride, long long ostride, FftPlan pl,
+                              const float* __restrict__ kern, int kp) {
+  extern __shared__ float2 sm[];
+  float2* A = sm;
+  float2* B = sm + (size_t)n * tk;
+  const int kx0 = blockIdx.x * tk;
+  const int nk = min(tk, ncol - kx0);
+  const int ky = blockIdx.y;
+  const float2* bi = in + (size_t)ky * ostride + kx0;
+  for (int t = threadIdx.x; t < n * tk; t += blockDim.x) {
+    const int j = t / tk, c = t - j * tk;
+    A[j * tk + c] = (c < nk) ? bi[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  fft_smem<MAXIT>(A, n, tk, 1, tk, pl, -1.f, true);
+  const int nh = n / 2;
+  const int fy = ky <= nh ? ky : n - ky;
+  const float sy = ky <= nh ? 1.f : -1.f;
+  const size_t ksz = (size_t)kp * kp * kp;
+  for (int d = 0; d < 3; ++d) {
+    const float* K = kern + d * ksz;
+    for (int t = threadIdx.x; t < n * tk; t += blockDim.x) {
+      const int kz = t / tk, c = t - kz * tk;
+      const int kx = kx0 + c;
+      float kv = 0.f;
+      if (c < nk) {
+        const int fz = kz <= nh ? kz : n - kz;
+        kv = __ldg(&K[((size_t)fz * kp + fy) * kp + kx]);
+        if (d == 1) kv *= sy;
+        if (d == 2 && kz > nh) kv = -kv;
+      }
+      const float2 a = A[kz * tk + c];
+      B[kz * tk + c] = make_float2(-a.y * kv, a.x * kv);
+    }
+    __syncthreads();
+    fft_smem<MAXIT>(B, n, tk, 1, tk, pl, 1.f, true);
+    float2* bo = out0 + d * comp_stride + (size_t)ky * ostride + kx0;
+    for (int t = threadIdx.x; t < n * tk; t += blockDim.x) {
+      const int j = t / tk, c = t - j * tk;
+      if (c < nk) bo[(size_t)j * jstride + c] = B[j * tk + c];
+    }
+    __syncthreads();
+  }
+}
+
+int pick_threads(int butterflies4, int maxit) {
+  int t = (butterflies4 + maxit - 1) / maxit;
+  t = ((t + 31) / 32) * 32;
+  return t < 64 ? 64 : (t > 1024 ? 1024 : t);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n) {
+  p.n = n;
+  p.nst = 0;
+  int m = n;
+  while (m % 4 == 0) { p.radix[p.nst++] = 4; m /= 4; }
+  while (m % 2 == 0) { p.radix[p.nst++] = 2; m /= 2; }
+  while (m % 3 == 0) { p.radix[p.nst++] = 3; m /= 3; }
+  while (m % 5 == 0) { p.radix[p.nst++] = 5; m /= 5; }
+  if (m != 1 || p.nst > CUBE_MAX_RADIX_STAGES) {
+    ctx->err = "mesh size must factor into 2, 3 and 5";
+    return CUBE_ERR_PARAM;
+  }
+  std::vector<float2> tw(n);
+  for (int j = 0; j < n; ++j) {
+    const long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)j / (long double)n;
+    tw[j] = make_float2((float)cosl(ang), (float)sinl(ang));
+  }
+  CUBE_CUDA_TRY(ctx, cudaMalloc(&p.tw, sizeof(float2) * n));
+  CUBE_CUDA_TRY(ctx, cudaMemcpy(p.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  return CUBE_OK;
+}
+
+#define MAXIT_X 8
+#define MAXIT_C 8
+
+int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int ncomp, unsigned int* f2_bits) {
+  const int n = L.n;
+  const int npairs = n * n / 2;
+  const int rpb = ncomp == 3 ? 1 : 2;
+  const int ss = n + 1;
+  const size_t smem = sizeof(float2) * (size_t)ncomp * rpb * ss;
+  const int thr = pick_threads(rpb * n / 2, MAXIT_X);
+  const int blocks = (npairs + rpb - 1) / rpb;
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fft_x<MAXIT_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_fft_x<MAXIT_X><<<blocks, thr, smem, ctx->stream>>>(data, (size_t)n * L.plane, ncomp, n, L.rp, npairs, rpb,
+                                                       L.plan, inverse, f2_bits);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
+static int col_pass(cube_ctx* ctx, MeshLevel& L, float* data, int ncomp, int along_z, float sgn) {
+  const int n = L.n;
+  const int ncol = n / 2 + 1;
+  const int tk = n >= 512 ? 8 : 16;
+  const size_t smem = sizeof(float2) * (size_t)n * tk;
+  const int thr = pick_threads(tk * n / 4, MAXIT_C);
+  dim3 grid((ncol + tk - 1) / tk, n, ncomp);
+  const long long cp = L.cp;
+  const long long jstride = along_z ? (long long)n * cp : cp;
+  const long long ostride = along_z ? cp : (long long)n * cp;
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fft_col<MAXIT_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_fft_col<MAXIT_C><<<grid, thr, smem, ctx->stream>>>(reinterpret_cast<float2*>(data), (size_t)n * L.plane / 2,
+                                                       n, ncol, tk, jstride, ostride, L.plan, sgn);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
+int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
+  const int n = L.n;
+  int rc;
+  // forward r2c of the density, in place
+  if ((rc = cube_fft_r2c_x(ctx, L, L.rho, 0, 1, nullptr))) return rc;
+  if ((rc = col_pass(ctx, L, L.rho, 1, 0, -1.f))) return rc;
+  {
+    const int ncol = n / 2 + 1;
+    const int tk = n >= 512 ? 8 : 16;
+    const size_t smem = 2 * sizeof(float2) * (size_t)n * tk;
+    const int thr = pick_threads(tk * n / 4, MAXIT_C);
+    dim3 grid((ncol + tk - 1) / tk, n, 1);
+    const long long cp = L.cp;
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fft_z_green<MAXIT_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_fft_z_green<MAXIT_C><<<grid, thr, smem, ctx->stream>>>(
+        reinterpret_cast<const float2*>(L.rho), reinterpret_cast<float2*>(L.force), (size_t)n * L.plane / 2, n,
+        ncol, tk, (long long)n * cp, cp, L.plan, L.kern, L.kern_pitch);
+    CUBE_LAUNCH_CHECK(ctx);
+  }
+  if ((rc = col_pass(ctx, L, L.force, 3, 0, 1.f))) return rc;
+  if ((rc = cube_fft_r2c_x(ctx, L, L.force, 1, 3, f2_bits))) return rc;
+  return CUBE_OK;
+}

@@ -1,0 +1,154 @@
+/*
+ * k_kick.cu -- force interpolation and kick of particle_mesh, fine then
+ * coarse, fused into one pass over the particles (pm.f90:131-155, :335-372).
+ *
+ * Per particle and component the arithmetic is the reference's, in its
+ * order: decode with sigma_vi, add the eight fine CIC terms
+ * force*a_mid*dt/6/pi*dx*dy*dz (FP32 products, FP64 accumulation), encode
+ * with sigma_vi_new; decode that code again with sigma_vi_new, add the
+ * eight coarse terms, record |v+vfield| for vmax, encode.  The intermediate
+ * quantisation between the two kicks is kept, so the result is bit-identical
+ * to running the reference's two loops one after the other; the codes are
+ * read and written once.
+ *
+ * A CTA takes a contiguous range of cells (tile-major order), so the
+ * particles it touches are contiguous and the force nodes they read are
+ * neighbours in the mesh (served from L1/L2).
+ */
+#include "cube_internal.cuh"
+
+namespace {
+
+constexpr int KCELLS = 64;  // cells per CTA
+
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
+                                              const int64_t* __restrict__ cell_start, const float* __restrict__ vfield,
+                                              int64_t cap, int64_t ncells, int nc, int nt, int nnt,
+                                              const float* __restrict__ ff, size_t fcomp, int frp, size_t fplane,
+                                              const float* __restrict__ fc, size_t ccomp, int crp, size_t cplane,
+                                              const float* __restrict__ tan_table, int half_nvbin, cube_codec codec,
+                                              double coef_old, double coef_new, float a_mid, float dt,
+                                              DevScal* __restrict__ dscal) {
+  typedef typename CodeT<ZX>::T TX;
+  typedef typename CodeT<ZV>::T TV;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  TV* vp = reinterpret_cast<TV*>(vp_);
+  __shared__ int64_t cs[KCELLS + 1];
+  const int64_t c0 = (int64_t)blockIdx.x * KCELLS;
+  const int ncl = (int)min((int64_t)KCELLS, ncells - c0);
+  for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = cell_start[c0 + i];
+  __syncthreads();
+  const int nf = 4 * nc;
+  const float pi_f = codec.pi_f;
+  float vmx[3] = {0.f, 0.f, 0.f};
+  for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
+    int lo = 0, hi = ncl - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
+    }
+    const int64_t c = c0 + lo;
+    const int nt3 = nt * nt * nt;
+    const int64_t tile = c / nt3;
+    const int rem = (int)(c - tile * nt3);
+    const int l[3] = {rem % nt, (rem / nt) % nt, rem / (nt * nt)};
+    const int t[3] = {(int)(tile % nnt), (int)((tile / nnt) % nnt), (int)(tile / ((int64_t)nnt * nnt))};
+    double fr[3];
+    int n1[3], m1[3];
+    float dx1[3], dx2[3], cx1[3], cx2[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      fr[d] = cube_xfrac((int32_t)xp[(size_t)d * cap + ip], ZX);
+      const float tf = (float)cube_dadd(4.0 * (double)l[d], cube_dmul(4.0, fr[d]));
+      const float f = floorf(tf) + 1.f;
+      dx1[d] = cube_fsub(f, tf);
+      dx2[d] = cube_fsub(1.f, dx1[d]);
+      n1[d] = 4 * t[d] * nt + (int)f - 1;  // global fine node of idx1 (0-based), < nf
+      const double g = cube_dadd((double)(t[d] * nt + l[d]), fr[d]);
+      const float tc = (float)cube_dsub(g, 0.5);
+      const float ci = floorf(tc) + 1.f;
+      cx1[d] = cube_fsub(ci, tc);
+      cx2[d] = cube_fsub(1.f, cx1[d]);
+      m1[d] = (int)ci - 1;  // global coarse node of idx1, may be -1
+    }
+    size_t fo[2][2][2], co[2][2][2];
+#pragma unroll
+    for (int sz = 0; sz < 2; ++sz)
+#pragma unroll
+      for (int sy = 0; sy < 2; ++sy)
+#pragma unroll
+        for (int sx = 0; sx < 2; ++sx) {
+          const int fx = (n1[0] + sx) % nf, fy = (n1[1] + sy) % nf, fz = (n1[2] + sz) % nf;
+          fo[sz][sy][sx] = (size_t)fz * fplane + (size_t)fy * frp + fx;
+          const int gx = (m1[0] + sx + nc) % nc, gy = (m1[1] + sy + nc) % nc, gz = (m1[2] + sz + nc) % nc;
+          co[sz][sy][sx] = (size_t)gz * cplane + (size_t)gy * crp + gx;
+        }
+    // reference corner order: 111,211,121,112,122,212,221,222
+    const int ox[8] = {0, 1, 0, 0, 0, 1, 1, 1}, oy[8] = {0, 0, 1, 0, 1, 0, 1, 1}, oz[8] = {0, 0, 0, 1, 1, 1, 0, 1};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int code = (int)vp[(size_t)d * cap + ip];
+      double v = cube_vdecode(__ldg(&tan_table[code + half_nvbin]), coef_old);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float fv = __ldg(&ff[d * fcomp + fo[oz[k]][oy[k]][ox[k]]]);
+        float q = cube_fmul(fv, a_mid);
+        q = cube_fmul(q, dt);
+        q = cube_fdiv(q, 6.f);
+        q = cube_fdiv(q, pi_f);
+        q = cube_fmul(q, ox[k] ? dx2[0] : dx1[0]);
+        q = cube_fmul(q, oy[k] ? dx2[1] : dx1[1]);
+        q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
+        v = cube_dadd(v, (double)q);
+      }
+      const int code1 = cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
+      v = cube_vdecode(__ldg(&tan_table[code1 + half_nvbin]), coef_new);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const float fv = __ldg(&fc[d * ccomp + co[oz[k]][oy[k]][ox[k]]]);
+        float q = cube_fmul(fv, a_mid);
+        q = cube_fmul(q, dt);
+        q = cube_fdiv(q, 6.f);
+        q = cube_fdiv(q, pi_f);
+        q = cube_fmul(q, ox[k] ? cx2[0] : cx1[0]);
+        q = cube_fmul(q, oy[k] ? cx2[1] : cx1[1]);
+        q = cube_fmul(q, oz[k] ? cx2[2] : cx1[2]);
+        v = cube_dadd(v, (double)q);
+      }
+      const float am = (float)fabs(cube_dadd(v, (double)__ldg(&vfield[(size_t)d * ncells + c])));
+      vmx[d] = fmaxf(vmx[d], am);
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
+    }
+  }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    float m = vmx[d];
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(&dscal->vmax_bits[d], __float_as_uint(m));
+  }
+}
+
+template <int ZX, int ZV>
+int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
+  const int64_t blocks = (ctx->ncells + KCELLS - 1) / KCELLS;
+  const double coef_old = cube_vcoef(&ctx->codec, io->sigma_vi);
+  const double coef_new = cube_vcoef(&ctx->codec, io->sigma_vi_new);
+  MeshLevel& F = ctx->fine;
+  MeshLevel& Cc = ctx->coarse;
+  k_kick<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+      ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, F.force,
+      (size_t)F.n * F.plane, F.rp, F.plane, Cc.force, (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, ctx->tan_table,
+      ctx->nvbin / 2, ctx->codec, coef_old, coef_new, io->a_mid, io->dt, ctx->dscal);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
+}  // namespace
+
+int cube_kick(cube_ctx* ctx, cube_scalars* io) {
+  if (ctx->izipx == 1 && ctx->izipv == 1) return launch_kick<1, 1>(ctx, io);
+  if (ctx->izipx == 1 && ctx->izipv == 2) return launch_kick<1, 2>(ctx, io);
+  if (ctx->izipx == 2 && ctx->izipv == 1) return launch_kick<2, 1>(ctx, io);
+  return launch_kick<2, 2>(ctx, io);
+}

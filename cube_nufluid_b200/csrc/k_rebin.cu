@@ -1,0 +1,356 @@
+/*
+ * k_rebin.cu -- update_x: drift, re-bin by counting sort, re-encode
+ * (update_particle.f90:13-259).
+ *
+ * The reference drifts every particle of a tile plus its ncb-cell buffer,
+ * counts the new cells, builds the spine, scatters in its loop order
+ * (layer, k, j, i, l) with nlayer = 2*ceiling(dt_mid*vz_max/ncell)+1, and
+ * keeps the particles that land in the tile.  Inside a new cell the particles
+ * therefore sit in that loop order, and the cell's new mean velocity is an
+ * FP32 running sum in the same order.  The GPU reproduces both exactly:
+ *
+ *   count   : per particle, target cell (computed in the coordinates of the
+ *             target tile, as the reference does) and a 32-bit order key
+ *             ((layer*nte + k)*nte + j)*nte + i of the source cell in those
+ *             coordinates; count per target cell
+ *   scan    : cell starts
+ *   place   : slot = start + atomic cursor (arbitrary order inside the cell)
+ *   finalize: per target cell, sort its entries by (key, source index) --
+ *             the reference order -- then run the FP32 velocity sum in that
+ *             order, the division by (n + weight_v), and write x, v, pid in
+ *             order; per-cell velocity statistics for the fixed-tree sums.
+ *             Cells with more than 32 particles go to a block-wide sorter.
+ * Positions move by nint(dt_mid*v/(x_resolution*ncell)) with the integer
+ * wrap of the 1- or 2-byte store (update_particle.f90:117).
+ */
+#include "cube_internal.cuh"
+
+namespace {
+
+constexpr int RCELLS = 64;
+constexpr int SMALL = 32;
+constexpr int BIG_MAX = 4096;
+
+struct RebinArgs {
+  const void* xp; const void* vp; const int32_t* pid;
+  const int64_t* cell_start; const float* vfield;
+  void* xp2; void* vp2; int32_t* pid2;
+  int32_t* cnt2; int64_t* start2; float* vfield2;
+  int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
+  int32_t* big_list; double* stats;
+  const float* tan_table; int half_nvbin;
+  cube_codec codec; double coef;
+  int64_t cap, ncells;
+  int nc, nt, nnt, ncb, nte, ncell, nlayer, use_pid;
+  float dt_mid;
+  DevScal* dscal;
+};
+
+__device__ __forceinline__ int floordiv(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
+
+template <int ZX, int ZV>
+__device__ __forceinline__ double decode_v(const RebinArgs& A, int64_t ip, int d) {
+  typedef typename CodeT<ZV>::T TV;
+  const TV* vp = reinterpret_cast<const TV*>(A.vp);
+  const int code = (int)vp[(size_t)d * A.cap + ip];
+  return cube_vdecode(__ldg(&A.tan_table[code + A.half_nvbin]), A.coef);
+}
+
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256) k_rebin_count(RebinArgs A) {
+  typedef typename CodeT<ZX>::T TX;
+  const TX* xp = reinterpret_cast<const TX*>(A.xp);
+  __shared__ int64_t cs[RCELLS + 1];
+  const int64_t c0 = (int64_t)blockIdx.x * RCELLS;
+  const int ncl = (int)min((int64_t)RCELLS, A.ncells - c0);
+  for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = A.cell_start[c0 + i];
+  __syncthreads();
+  const int nt = A.nt, nnt = A.nnt, ncb = A.ncb, nte = A.nte;
+  const int nt3 = nt * nt * nt;
+  for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
+    int lo = 0, hi = ncl - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
+    }
+    const int64_t c = c0 + lo;
+    const int64_t tile = c / nt3;
+    const int rem = (int)(c - tile * nt3);
+    const int l[3] = {rem % nt, (rem / nt) % nt, rem / (nt * nt)};
+    const int t[3] = {(int)(tile % nnt), (int)((tile / nnt) % nnt), (int)(tile / ((int64_t)nnt * nnt))};
+    int tg[3], src[3];
+    bool bad = false;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double fr = cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip], ZX);
+      const double v = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + c]));
+      const double dx = cube_ddiv(cube_dmul((double)A.dt_mid, v), (double)A.ncell);
+      // ig = ceiling(xq + deltax), xq = (i-1) + frac in the coordinates of the tile that keeps it
+      int ig = (int)ceil(cube_dadd(cube_dadd((double)l[d], fr), dx));
+      int ls = l[d], tt = t[d];
+      if (ig < 1 || ig > nt) {
+        const int sh = floordiv(ig - 1, nt);
+        ls = l[d] - sh * nt;
+        tt = ((t[d] + sh) % nnt + nnt) % nnt;
+        const int ig2 = (int)ceil(cube_dadd(cube_dadd((double)ls, fr), dx));
+        if (ig2 >= 1 && ig2 <= nt) ig = ig2;
+        else { ig = ig - sh * nt; atomicAdd(&A.dscal->moved_far, 1ull); }
+      }
+      if (ls + 1 < 1 - ncb || ls + 1 > nt + ncb) bad = true;
+      tg[d] = tt * nt + ig - 1;
+      src[d] = ls + ncb;  // 0-based index in the target tile's extended range
+    }
+    if (bad) {
+      cube_dev_error(A.dscal, CUBE_ERR_MOVE, (int)(ip & 0x7fffffff));
+      src[0] = min(max(src[0], 0), nte - 1);
+      src[1] = min(max(src[1], 0), nte - 1);
+      src[2] = min(max(src[2], 0), nte - 1);
+    }
+    const int64_t tc = cube_cell_of(tg[0], tg[1], tg[2], nt, nnt);
+    const uint32_t layer = (uint32_t)(src[2] % A.nlayer);
+    const uint32_t key = ((layer * nte + src[2]) * nte + src[1]) * nte + src[0];
+    A.tcell[ip] = (int32_t)tc;
+    A.tkey[ip] = key;
+    atomicAdd(&A.cnt2[tc], 1);
+  }
+}
+
+__global__ void k_rebin_place(RebinArgs A, int64_t np) {
+  for (int64_t ip = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; ip < np; ip += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t tc = A.tcell[ip];
+    const int64_t slot = A.start2[tc] + atomicAdd(&A.cursor[tc], 1);
+    A.perm[slot] = (int32_t)ip;
+    A.pkey[slot] = A.tkey[ip];
+  }
+}
+
+// source cell of an entry from its key and the target cell's tile
+__device__ __forceinline__ int64_t src_cell(const RebinArgs& A, uint32_t key, const int tt[3]) {
+  const int nte = A.nte, nt = A.nt, nc = A.nc, ncb = A.ncb;
+  const int i = key % nte, j = (key / nte) % nte, k = (key / (nte * nte)) % nte;
+  const int gx = ((tt[0] * nt + i - ncb) % nc + nc) % nc;
+  const int gy = ((tt[1] * nt + j - ncb) % nc + nc) % nc;
+  const int gz = ((tt[2] * nt + k - ncb) % nc + nc) % nc;
+  return cube_cell_of(gx, gy, gz, nt, A.nnt);
+}
+
+template <int ZX, int ZV>
+__device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t ip, const double v[3], const float vfn[3],
+                                     double& sr, double& ss) {
+  typedef typename CodeT<ZX>::T TX;
+  typedef typename CodeT<ZV>::T TV;
+  const TX* xp = reinterpret_cast<const TX*>(A.xp);
+  TX* xp2 = reinterpret_cast<TX*>(A.xp2);
+  TV* vp2 = reinterpret_cast<TV*>(A.vp2);
+  const double xstep = cube_dmul(A.codec.x_resolution, (double)A.ncell);
+  double r2 = 0.0, s2 = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int64_t mv = cube_nint(cube_ddiv(cube_dmul((double)A.dt_mid, v[d]), xstep));
+    xp2[(size_t)d * A.cap + slot] = (TX)cube_wrap_code((int64_t)xp[(size_t)d * A.cap + ip] + (int32_t)mv, ZX);
+    const int code = cube_wrap_code(cube_vencode(&A.codec, cube_dsub(v[d], (double)vfn[d]), A.coef), ZV);
+    vp2[(size_t)d * A.cap + slot] = (TV)code;
+    const double vr = cube_vdecode(__ldg(&A.tan_table[code + A.half_nvbin]), A.coef);
+    const double vs = cube_dadd(vr, (double)vfn[d]);
+    r2 = cube_dadd(r2, cube_dmul(vr, vr));
+    s2 = cube_dadd(s2, cube_dmul(vs, vs));
+  }
+  if (A.use_pid) A.pid2[slot] = A.pid[ip];
+  sr = cube_dadd(sr, r2);
+  ss = cube_dadd(ss, s2);
+}
+
+__device__ __forceinline__ void cell_tile(const RebinArgs& A, int64_t c, int tt[3]) {
+  const int nt3 = A.nt * A.nt * A.nt;
+  const int64_t tile = c / nt3;
+  tt[0] = (int)(tile % A.nnt);
+  tt[1] = (int)((tile / A.nnt) % A.nnt);
+  tt[2] = (int)(tile / ((int64_t)A.nnt * A.nnt));
+}
+
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256) k_rebin_finalize(RebinArgs A) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= A.ncells) return;
+  const int n = A.cnt2[c];
+  const int64_t s = A.start2[c];
+  if (n > SMALL) {
+    const unsigned long long q = atomicAdd(&A.dscal->n_big, 1ull);
+    A.big_list[q] = (int32_t)c;
+    return;
+  }
+  // insertion sort of the cell's (key, source) entries, ascending
+  for (int i = 1; i < n; ++i) {
+    const uint32_t kk = A.pkey[s + i];
+    const int32_t pp = A.perm[s + i];
+    int j = i - 1;
+    while (j >= 0) {
+      const uint32_t kj = A.pkey[s + j];
+      const int32_t pj = A.perm[s + j];
+      if (kj > kk || (kj == kk && pj > pp)) {
+        A.pkey[s + j + 1] = kj;
+        A.perm[s + j + 1] = pj;
+        --j;
+      } else break;
+    }
+    A.pkey[s + j + 1] = kk;
+    A.perm[s + j + 1] = pp;
+  }
+  int tt[3];
+  cell_tile(A, c, tt);
+  float acc[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) acc[d] = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
+  for (int r = 0; r < n; ++r) {
+    const int64_t ip = A.perm[s + r];
+    const int64_t sc = src_cell(A, A.pkey[s + r], tt);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double v = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
+      acc[d] = (float)cube_dadd((double)acc[d], v);
+    }
+  }
+  float vfn[3];
+  const double den = cube_dadd((double)n, 0.1);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    vfn[d] = (float)cube_ddiv((double)acc[d], den);
+    A.vfield2[(size_t)d * A.ncells + c] = vfn[d];
+  }
+  double sr = 0.0, ss = 0.0;
+  for (int r = 0; r < n; ++r) {
+    const int64_t ip = A.perm[s + r];
+    const int64_t sc = src_cell(A, A.pkey[s + r], tt);
+    double v[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      v[d] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
+    emit<ZX, ZV>(A, s + r, ip, v, vfn, sr, ss);
+  }
+  const float f2 = cube_fadd(cube_fadd(cube_fmul(vfn[0], vfn[0]), cube_fmul(vfn[1], vfn[1])), cube_fmul(vfn[2], vfn[2]));
+  A.stats[c] = (double)f2;
+  A.stats[A.ncells + c] = sr;
+  A.stats[2 * A.ncells + c] = ss;
+}
+
+// one CTA per crowded cell: bitonic sort of (key<<32|source) in shared memory
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
+  extern __shared__ unsigned long long sk[];
+  double* sv = reinterpret_cast<double*>(sk + BIG_MAX);  // [3][BIG_MAX] velocities, later stats
+  __shared__ float vfn_s[3];
+  const unsigned long long nbig = A.dscal->n_big;
+  for (unsigned long long b = blockIdx.x; b < nbig; b += gridDim.x) {
+    const int64_t c = A.big_list[b];
+    const int n = A.cnt2[c];
+    const int64_t s = A.start2[c];
+    if (n > BIG_MAX) {
+      if (threadIdx.x == 0) cube_dev_error(A.dscal, CUBE_ERR_CELL, n);
+      continue;
+    }
+    int m = 1;
+    while (m < n) m <<= 1;
+    for (int i = threadIdx.x; i < m; i += blockDim.x)
+      sk[i] = i < n ? (((unsigned long long)A.pkey[s + i] << 32) | (uint32_t)A.perm[s + i]) : ~0ull;
+    __syncthreads();
+    for (int k = 2; k <= m; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int i = threadIdx.x; i < m; i += blockDim.x) {
+          const int ixj = i ^ j;
+          if (ixj > i) {
+            const unsigned long long a = sk[i], bb = sk[ixj];
+            const bool up = (i & k) == 0;
+            if ((a > bb) == up) { sk[i] = bb; sk[ixj] = a; }
+          }
+        }
+        __syncthreads();
+      }
+    int tt[3];
+    cell_tile(A, c, tt);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int64_t ip = (int64_t)(uint32_t)(sk[i] & 0xffffffffu);
+      const int64_t sc = src_cell(A, (uint32_t)(sk[i] >> 32), tt);
+      for (int d = 0; d < 3; ++d)
+        sv[d * BIG_MAX + i] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+      const int d = threadIdx.x;
+      float acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
+      for (int i = 0; i < n; ++i) acc = (float)cube_dadd((double)acc, sv[d * BIG_MAX + i]);
+      const float v = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
+      vfn_s[d] = v;
+      A.vfield2[(size_t)d * A.ncells + c] = v;
+    }
+    __syncthreads();
+    const float vfn[3] = {vfn_s[0], vfn_s[1], vfn_s[2]};
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int64_t ip = (int64_t)(uint32_t)(sk[i] & 0xffffffffu);
+      const double v[3] = {sv[i], sv[BIG_MAX + i], sv[2 * BIG_MAX + i]};
+      double sr = 0.0, ss = 0.0;
+      emit<ZX, ZV>(A, s + i, ip, v, vfn, sr, ss);
+      sv[i] = sr;  // per-particle terms, summed in order below
+      sv[BIG_MAX + i] = ss;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double sr = 0.0, ss = 0.0;
+      for (int i = 0; i < n; ++i) {
+        sr = cube_dadd(sr, sv[i]);
+        ss = cube_dadd(ss, sv[BIG_MAX + i]);
+      }
+      const float f2 = cube_fadd(cube_fadd(cube_fmul(vfn[0], vfn[0]), cube_fmul(vfn[1], vfn[1])), cube_fmul(vfn[2], vfn[2]));
+      A.stats[c] = (double)f2;
+      A.stats[A.ncells + c] = sr;
+      A.stats[2 * A.ncells + c] = ss;
+    }
+    __syncthreads();
+  }
+}
+
+template <int ZX, int ZV>
+int run_rebin(cube_ctx* ctx, RebinArgs& A) {
+  const int64_t nb = (ctx->ncells + RCELLS - 1) / RCELLS;
+  k_rebin_count<ZX, ZV><<<(unsigned)nb, 256, 0, ctx->stream>>>(A);
+  CUBE_LAUNCH_CHECK(ctx);
+  int rc = cube_exclusive_scan(ctx, A.cnt2, ctx->ncells, A.start2);
+  if (rc) return rc;
+  k_rebin_place<<<1184, 256, 0, ctx->stream>>>(A, ctx->np);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_rebin_finalize<ZX, ZV><<<(unsigned)((ctx->ncells + 255) / 256), 256, 0, ctx->stream>>>(A);
+  CUBE_LAUNCH_CHECK(ctx);
+  const size_t smem = sizeof(unsigned long long) * BIG_MAX + sizeof(double) * 3 * BIG_MAX;
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rebin_big<ZX, ZV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_rebin_big<ZX, ZV><<<296, 512, smem, ctx->stream>>>(A);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
+}  // namespace
+
+int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
+  io->dt_mid = (io->dt_old + io->dt) / 2;
+  const float q = cube_fdiv(cube_fmul(io->dt_mid, io->vz_max), (float)ctx->ncell);
+  const int nlayer = 2 * (int)ceilf(q) + 1;
+  io->nlayer = nlayer;
+  RebinArgs A;
+  A.xp = ctx->xp; A.vp = ctx->vp; A.pid = ctx->pid;
+  A.cell_start = ctx->cell_start; A.vfield = ctx->vfield;
+  A.xp2 = ctx->xp2; A.vp2 = ctx->vp2; A.pid2 = ctx->pid2;
+  A.cnt2 = ctx->rhoc2; A.start2 = ctx->cell_start2; A.vfield2 = ctx->vfield2;
+  A.tcell = ctx->tcell; A.tkey = ctx->tkey; A.perm = ctx->perm; A.pkey = ctx->pkey; A.cursor = ctx->cursor;
+  A.big_list = ctx->big_list; A.stats = ctx->cell_stats;
+  A.tan_table = ctx->tan_table; A.half_nvbin = ctx->nvbin / 2;
+  A.codec = ctx->codec; A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
+  A.cap = ctx->cap; A.ncells = ctx->ncells;
+  A.nc = ctx->nc; A.nt = ctx->nt; A.nnt = ctx->nnt; A.ncb = ctx->ncb; A.nte = ctx->nte; A.ncell = ctx->ncell;
+  A.nlayer = nlayer; A.use_pid = ctx->P.use_pid; A.dt_mid = io->dt_mid; A.dscal = ctx->dscal;
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->rhoc2, 0, sizeof(int32_t) * ctx->ncells, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->cursor, 0, sizeof(int32_t) * ctx->ncells, ctx->stream));
+  int rc;
+  if (ctx->izipx == 1 && ctx->izipv == 1) rc = run_rebin<1, 1>(ctx, A);
+  else if (ctx->izipx == 1) rc = run_rebin<1, 2>(ctx, A);
+  else if (ctx->izipv == 1) rc = run_rebin<2, 1>(ctx, A);
+  else rc = run_rebin<2, 2>(ctx, A);
+  return rc;
+}

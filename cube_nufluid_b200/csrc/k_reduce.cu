@@ -1,0 +1,165 @@
+/*
+ * k_reduce.cu -- deterministic reductions and the cell-count prefix scan.
+ *
+ * cube_tree_sum_dev: the sum of n doubles as a fixed pairwise tree over
+ * blocks of 1024 (pad with zeros; loc[i] += loc[i+s] for s = 512..1), then
+ * the same tree over the block sums, until one value is left.  The CPU
+ * oracle uses the identical tree, so sums such as the velocity statistics of
+ * update_x (update_particle.f90:174-226) agree to the last bit.
+ *
+ * cube_exclusive_scan: int32 cell counts -> int64 cell starts (n+1 entries),
+ * the role of spine_tile / spine_image (variables.f90:103-218).
+ */
+#include "cube_internal.cuh"
+
+namespace {
+
+__global__ void k_tree_block(const double* __restrict__ in, int64_t n, double* __restrict__ out) {
+  __shared__ double loc[1024];
+  const int i = threadIdx.x;  // 512 threads
+  const int64_t b = blockIdx.x;
+  const int64_t q0 = b * 1024 + i, q1 = q0 + 512;
+  const double a0 = q0 < n ? in[q0] : 0.0;
+  const double a1 = q1 < n ? in[q1] : 0.0;
+  loc[i] = __dadd_rn(a0, a1);  // s = 512
+  __syncthreads();
+  for (int s = 256; s >= 32; s >>= 1) {
+    if (i < s) loc[i] = __dadd_rn(loc[i], loc[i + s]);
+    __syncthreads();
+  }
+  if (i < 32) {
+    double v = loc[i];
+    for (int s = 16; s >= 1; s >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, v, s);
+      if (i < s) v = __dadd_rn(v, o);
+    }
+    if (i == 0) out[b] = v;
+  }
+}
+
+constexpr int SCAN_PER_THREAD = 8;
+constexpr int SCAN_THREADS = 256;
+constexpr int SCAN_BLOCK = SCAN_PER_THREAD * SCAN_THREADS;
+
+__global__ void k_scan_sums(const int32_t* __restrict__ in, int64_t n, int64_t* __restrict__ bsum) {
+  __shared__ int64_t ws[32];
+  const int64_t base = (int64_t)blockIdx.x * SCAN_BLOCK + threadIdx.x * SCAN_PER_THREAD;
+  int64_t s = 0;
+  for (int k = 0; k < SCAN_PER_THREAD; ++k)
+    if (base + k < n) s += in[base + k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int64_t t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += ws[w];
+    bsum[blockIdx.x] = t;
+  }
+}
+
+// exclusive scan of nb values in place by one block
+__global__ void k_scan_top(int64_t* __restrict__ v, int64_t nb) {
+  __shared__ int64_t carry;
+  __shared__ int64_t ws[32];
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int64_t base = 0; base < nb; base += blockDim.x) {
+    const int64_t q = base + threadIdx.x;
+    const int64_t x = q < nb ? v[q] : 0;
+    int64_t inc = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if ((threadIdx.x & 31) >= o) inc += y;
+    }
+    if ((threadIdx.x & 31) == 31) ws[threadIdx.x >> 5] = inc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      const int nw = blockDim.x >> 5;
+      int64_t w = threadIdx.x < nw ? ws[threadIdx.x] : 0;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+        if ((int)threadIdx.x >= o) w += y;
+      }
+      ws[threadIdx.x] = w;  // inclusive warp totals
+    }
+    __syncthreads();
+    const int wi = threadIdx.x >> 5;
+    const int64_t before = (wi ? ws[wi - 1] : 0) + carry;
+    if (q < nb) v[q] = before + inc - x;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = before + inc;
+    __syncthreads();
+  }
+}
+
+__global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const int64_t* __restrict__ boff,
+                             int64_t* __restrict__ out) {
+  __shared__ int64_t ws[32];
+  const int64_t base = (int64_t)blockIdx.x * SCAN_BLOCK + threadIdx.x * SCAN_PER_THREAD;
+  int64_t vals[SCAN_PER_THREAD];
+  int64_t s = 0;
+  for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+    vals[k] = (base + k < n) ? in[base + k] : 0;
+    s += vals[k];
+  }
+  int64_t inc = s;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if ((threadIdx.x & 31) >= o) inc += y;
+  }
+  if ((threadIdx.x & 31) == 31) ws[threadIdx.x >> 5] = inc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    const int nw = blockDim.x >> 5;
+    int64_t w = threadIdx.x < nw ? ws[threadIdx.x] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if ((int)threadIdx.x >= o) w += y;
+    }
+    ws[threadIdx.x] = w;
+  }
+  __syncthreads();
+  const int wi = threadIdx.x >> 5;
+  int64_t run = boff[blockIdx.x] + (wi ? ws[wi - 1] : 0) + inc - s;
+  for (int k = 0; k < SCAN_PER_THREAD; ++k) {
+    if (base + k < n) out[base + k] = run;
+    run += vals[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) out[n] = boff[blockIdx.x] + ws[(blockDim.x >> 5) - 1];
+}
+
+}  // namespace
+
+int cube_tree_sum_dev(cube_ctx* ctx, const double* in, int64_t n, double* out_host) {
+  double* a = ctx->red_tmp + 4;  // first slots hold the deposit mass totals
+  const double* src = in;
+  int64_t m = n;
+  int flip = 0;
+  double* bufs[2] = {a, a + (n + 1023) / 1024 + 8};
+  if (m == 0) { *out_host = 0.0; return CUBE_OK; }
+  while (true) {
+    const int64_t nb = (m + 1023) / 1024;
+    double* dst = bufs[flip];
+    k_tree_block<<<(unsigned)nb, 512, 0, ctx->stream>>>(src, m, dst);
+    CUBE_LAUNCH_CHECK(ctx);
+    src = dst;
+    m = nb;
+    flip ^= 1;
+    if (m == 1) break;
+  }
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(out_host, src, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return CUBE_OK;
+}
+
+int cube_exclusive_scan(cube_ctx* ctx, const int32_t* in, int64_t n, int64_t* out) {
+  const int64_t nb = (n + SCAN_BLOCK - 1) / SCAN_BLOCK;
+  int64_t* bs = ctx->scan_tmp;
+  k_scan_sums<<<(unsigned)nb, SCAN_THREADS, 0, ctx->stream>>>(in, n, bs);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_scan_top<<<1, 1024, 0, ctx->stream>>>(bs, nb);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_scan_apply<<<(unsigned)nb, SCAN_THREADS, 0, ctx->stream>>>(in, n, bs, out);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}

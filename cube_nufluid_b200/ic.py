@@ -1,0 +1,259 @@
+"""Seeded Zel'dovich initial conditions in CUBE's compressed checkpoint layout.
+
+This is the input harness of the particle-mesh step, restating the particle
+creation of the reference IC program (CUBE_v2.0/work/utilities/initial_conditions.f90)
+on a host with numpy:
+
+* linear power: Eisenstein & Hu (1998, ApJ 496, 605) no-wiggle transfer function
+  (their eqs. 26-31), n_s tilt, normalised to sigma_8 with the reference's top-hat
+  integral (initial_conditions.f90:235-242, tophat :1017-1026);
+* growth to z_i with the reference's Dgrow (initial_conditions.f90:1028-1041);
+* unit Gaussian white noise from a counter-based generator (numpy's Philox4x32-10,
+  Salmon et al. 2011) seeded explicitly, scaled as at initial_conditions.f90:373;
+* Zel'dovich displacement psi_k = i k delta_k / k^2 on the particle lattice and
+  velocity v = psi * vfactor(a) (initial_conditions.f90:705,799, vfactor :1068-1079);
+* zip packing as at initial_conditions.f90:797-838: cell g = ceiling(x),
+  xp = floor(x/x_resolution) wrapped to the code width, vfield = mean particle
+  velocity of the cell, vp = arctan code of v - vfield, pid = lattice index + 1.
+
+The reference computes the potential on the fine mesh with a discrete
+Laplacian and central differences; this harness uses the continuous-k
+displacement on the particle lattice (np_nc particles per coarse cell per
+dimension).  Particles are ordered tile-major by coarse cell, lattice order
+inside a cell.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+
+@dataclass
+class Cosmology:
+    omega_m: float = 0.3
+    omega_l: float = 0.7
+    h: float = 0.7
+    omega_b: float = 0.045
+    n_s: float = 0.96
+    sigma8: float = 0.8
+    t_cmb: float = 2.7255
+
+
+def eh_nowiggle(k_hmpc: np.ndarray, c: Cosmology) -> np.ndarray:
+    """Eisenstein & Hu (1998) zero-baryon-oscillation transfer function, k in h/Mpc."""
+    om = c.omega_m * c.h * c.h
+    ob = c.omega_b * c.h * c.h
+    fb = c.omega_b / c.omega_m
+    theta = c.t_cmb / 2.7
+    s = 44.5 * math.log(9.83 / om) / math.sqrt(1.0 + 10.0 * ob ** 0.75)  # Mpc
+    alpha = 1.0 - 0.328 * math.log(431.0 * om) * fb + 0.38 * math.log(22.3 * om) * fb * fb
+    k_mpc = k_hmpc * c.h
+    gamma = c.omega_m * c.h * (alpha + (1.0 - alpha) / (1.0 + (0.43 * k_mpc * s) ** 4))
+    q = k_hmpc * theta * theta / gamma
+    l0 = np.log(2.0 * math.e + 1.8 * q)
+    c0 = 14.2 + 731.0 / (1.0 + 62.5 * q)
+    return l0 / (l0 + c0 * q * q)
+
+
+def gaussian_noise(n: int, seed: int) -> np.ndarray:
+    """Unit Gaussian noise [z][y][x] (float32): Philox4x32-10 uniforms through the
+    reference's Box-Muller pairing along x (initial_conditions.f90:320-336)."""
+    if n % 2:
+        raise ValueError("noise grid must be even along x")
+    rng = np.random.Generator(np.random.Philox(seed))
+    u = rng.random((n, n, n), dtype=np.float32)
+    pif = pi_f32()
+    theta = np.float32(2.0) * pif * u[..., 0::2]
+    r = np.sqrt(np.float32(-2.0) * np.log(np.float32(1.0) - u[..., 1::2]))
+    out = np.empty_like(u)
+    out[..., 0::2] = r * np.cos(theta)
+    out[..., 1::2] = r * np.sin(theta)
+    return out
+
+
+def _tophat(x):
+    x = np.asarray(x, dtype=np.float64)
+    out = np.ones_like(x)
+    nz = x != 0
+    xx = x[nz]
+    out[nz] = 3.0 * (np.sin(xx) - np.cos(xx) * xx) / xx ** 3
+    return out
+
+
+def dgrow(a: float, om: float, ol: float) -> float:
+    """Carroll-Press-Turner growth as in initial_conditions.f90:1028-1041."""
+    def g(aa):
+        hsq = om / aa ** 3 + (1 - om - ol) / aa ** 2 + ol
+        oma = om / (aa ** 3 * hsq)
+        ola = ol / hsq
+        return 2.5 * oma / (oma ** (4.0 / 7) - ola + (1 + oma / 2) * (1 + ola / 70))
+    return a * g(a) / g(1.0)
+
+
+def vfactor(a: float, om: float, ol: float, f_neu: float = 0.0) -> float:
+    """a^2 H(a) times the growth exponent, simulation units (initial_conditions.f90:1068-1079)."""
+    npow = -(1.0 / 4.0) + (5.0 / 4.0) * math.sqrt(1 - 24.0 * f_neu / 25.0)
+    lm = ol / om
+    km = (1 - om - ol) / om
+    hub = 2 / (3 * math.sqrt(a ** 3)) * math.sqrt(1 + a * km + a ** 3 * lm)
+    return a * a * hub * npow
+
+
+def delta2(k_hmpc, c: Cosmology, a: float):
+    """Dimensionless linear power Delta^2(k) = k^3 P(k)/(2 pi^2) at scale factor a."""
+    kk = np.logspace(-4, 2, 4000)
+    t = eh_nowiggle(kk, c)
+    d2 = t * t * kk ** (3 + c.n_s)
+    w = _tophat(kk * 8.0)
+    v8 = np.trapezoid(d2 * w * w / kk, kk)
+    norm = c.sigma8 ** 2 / v8
+    tk = eh_nowiggle(np.asarray(k_hmpc, dtype=np.float64), c)
+    d = dgrow(a, c.omega_m, c.omega_l)
+    return norm * tk * tk * np.asarray(k_hmpc, dtype=np.float64) ** (3 + c.n_s) * d * d
+
+
+def pi_f32() -> np.float32:
+    return np.float32(4.0) * np.arctan(np.float32(1.0))
+
+
+def encode_velocity(v: np.ndarray, sigma: float, izipv: int, vrel_boost: float = 2.5) -> np.ndarray:
+    """Host encode used only to pack ICs (the step's encode is cube_vencode on the device)."""
+    pif = pi_f32()
+    nvbin_m1 = np.float32((1 << (8 * izipv)) - 1)
+    coef = float(np.sqrt(pif / np.float32(2.0))) / (float(np.float32(sigma)) * vrel_boost)
+    q = (float(nvbin_m1) * np.arctan(coef * v)) / float(pif)
+    code = np.sign(q) * np.floor(np.abs(q) + 0.5)
+    dt = np.int8 if izipv == 1 else np.int16
+    return code.astype(np.int64).astype(dt)
+
+
+@dataclass
+class ICState:
+    nc: int
+    nnt: int
+    izipx: int
+    izipv: int
+    xp: np.ndarray       # [np,3] int8/int16
+    vp: np.ndarray       # [np,3]
+    pid: np.ndarray      # [np] int32
+    rhoc: np.ndarray     # [ncells] int32, tile-major cell order
+    vfield: np.ndarray   # [ncells,3] float32
+    a: float
+    sigma_vi: float
+    mass_p_cdm: float
+    vmax: np.ndarray     # [3]
+    vsim2phys: float
+
+    @property
+    def np(self) -> int:
+        return int(self.pid.shape[0])
+
+
+def tile_major_cell_id(g: np.ndarray, nc: int, nnt: int) -> np.ndarray:
+    """g: [...,3] zero-based global coarse cell -> tile-major cell id (Fortran rhoc order)."""
+    nt = nc // nnt
+    t = g // nt
+    l = g % nt
+    tile = (t[..., 2] * nnt + t[..., 1]) * nnt + t[..., 0]
+    return ((tile * nt + l[..., 2]) * nt + l[..., 1]) * nt + l[..., 0]
+
+
+def zeldovich(nc: int, nnt: int, box: float, z_i: float, seed: int, *, np_nc: int = 2,
+              ncell: int = 4, izipx: int = 2, izipv: int = 2, cosmo: Cosmology | None = None,
+              f_cdm: float = 1.0, amplitude: float = 1.0) -> ICState:
+    """Build a seeded Zel'dovich state at z_i in checkpoint layout."""
+    c = cosmo or Cosmology()
+    npd = nc * np_nc
+    a = 1.0 / (1.0 + z_i)
+    noise = gaussian_noise(npd, seed)  # [z][y][x]
+    import scipy.fft as sfft
+    wk = sfft.rfftn(noise, workers=-1)
+    del noise
+    kx = np.fft.rfftfreq(npd, d=1.0 / npd).astype(np.float32)
+    ky = np.fft.fftfreq(npd, d=1.0 / npd).astype(np.float32)
+    kz = ky
+    kr2 = kz[:, None, None] ** 2 + ky[None, :, None] ** 2 + kx[None, None, :] ** 2
+    kr = np.sqrt(np.maximum(kr2, 1.0))
+    d2 = delta2(2 * math.pi * kr / box, c, a).astype(np.float32)
+    amp = np.sqrt(d2 / (4 * math.pi) * (npd / kr)) * (npd / kr) * amplitude
+    dk = wk * amp
+    dk[0, 0, 0] = 0
+    del wk, amp, d2
+    kgrid = 2 * math.pi / npd
+    inv = np.where(kr2 > 0, 1.0 / (kgrid * kgrid * np.maximum(kr2, 1e-30)), 0.0).astype(np.float32)
+    disp = np.empty((3, npd, npd, npd), dtype=np.float32)
+    for d, kk in enumerate((kx[None, None, :], ky[None, :, None], kz[:, None, None])):
+        psi_k = 1j * (kgrid * kk) * inv * dk
+        disp[d] = sfft.irfftn(psi_k, s=(npd, npd, npd), workers=-1)
+        del psi_k
+    del dk, inv
+    # lattice positions in coarse units: q = i/np_nc + 0.5/ncell (initial_conditions.f90:793)
+    ii = np.arange(npd, dtype=np.float64) / np_nc + 0.5 / ncell
+    zz, yy, xx = np.meshgrid(ii, ii, ii, indexing="ij")
+    pos = np.stack([xx, yy, zz], axis=-1).reshape(-1, 3)
+    del xx, yy, zz
+    dsp = np.stack([disp[0], disp[1], disp[2]], axis=-1).reshape(-1, 3).astype(np.float64) / np_nc
+    del disp
+    x = np.mod(pos + dsp, float(nc))
+    vf = vfactor(a, c.omega_m, c.omega_l)
+    vel = dsp * (ncell * vf)  # fine cells per unit time
+    del pos, dsp
+    return pack(x, vel, nc, nnt, ncell=ncell, izipx=izipx, izipv=izipv, a=a, box=box, omega_m=c.omega_m,
+                f_cdm=f_cdm)
+
+
+
+def clustered(nc: int, nnt: int, npart: int, seed: int, *, ncell: int = 4, izipx: int = 2, izipv: int = 2,
+              clumps: int = 8, clump_frac: float = 0.5, clump_size: float = 0.6, vel: float = 0.02,
+              box: float = 100.0) -> ICState:
+    """A test state with uniform background plus dense clumps (crowded cells, PP pairs).
+
+    Positions and velocities are drawn from Philox4x32-10 with the given seed
+    and packed exactly as zeldovich() packs them.  Not a cosmological IC: it
+    exercises the step on the clustering a late-time box has.
+    """
+    rng = np.random.Generator(np.random.Philox(seed))
+    nclump = int(npart * clump_frac)
+    nbg = npart - nclump
+    xb = rng.uniform(0, nc, (nbg, 3))
+    centers = rng.uniform(0, nc, (clumps, 3))
+    which = rng.integers(0, clumps, nclump)
+    xc = centers[which] + rng.normal(0, clump_size, (nclump, 3))
+    x = np.mod(np.concatenate([xb, xc]), float(nc))
+    v = rng.normal(0, vel, (npart, 3))
+    v[nbg:] += rng.normal(0, 2 * vel, (clumps, 3))[which]
+    return pack(x, v, nc, nnt, ncell=ncell, izipx=izipx, izipv=izipv, a=0.5, box=box)
+
+
+def pack(x: np.ndarray, vel: np.ndarray, nc: int, nnt: int, *, ncell: int = 4, izipx: int = 2, izipv: int = 2,
+         a: float = 0.02, box: float = 100.0, omega_m: float = 0.3, f_cdm: float = 1.0) -> ICState:
+    """Zip packing of initial_conditions.f90:797-838 for positions x (coarse units) and velocities."""
+    g = np.ceil(x).astype(np.int64) - 1
+    g %= nc
+    cid = tile_major_cell_id(g, nc, nnt)
+    order = np.argsort(cid, kind="stable")
+    cid = cid[order]
+    x = x[order]
+    vel = vel[order]
+    pid = (order + 1).astype(np.int32)
+    ncells = nc ** 3
+    rhoc = np.bincount(cid, minlength=ncells).astype(np.int32)
+    vsum = np.stack([np.bincount(cid, weights=vel[:, d], minlength=ncells) for d in range(3)], axis=-1)
+    vfield = (vsum / np.maximum(rhoc, 1)[:, None]).astype(np.float32)
+    res = vel - vfield[cid].astype(np.float64)
+    sigma_vi = float(np.float32(math.sqrt(float(np.mean(np.sum(res * res, axis=1)))) / math.sqrt(3.0)))
+    xres = 2.0 ** (-8 * izipx)
+    xcode = np.floor(x / xres).astype(np.int64)
+    xdt = np.int8 if izipx == 1 else np.int16
+    xp = (xcode & ((1 << (8 * izipx)) - 1)).astype(np.uint16 if izipx == 2 else np.uint8).view(xdt)
+    vp = encode_velocity(res, sigma_vi, izipv)
+    npart = x.shape[0]
+    nf = nc * ncell
+    mass_p = float(np.float32(f_cdm * float(nf) ** 3 / npart))
+    vmax = np.max(np.abs(vel), axis=0)
+    vsim2phys = (150.0 / a) * box * math.sqrt(omega_m) / nf
+    return ICState(nc=nc, nnt=nnt, izipx=izipx, izipv=izipv, xp=np.ascontiguousarray(xp),
+                   vp=np.ascontiguousarray(vp), pid=pid, rhoc=rhoc, vfield=vfield, a=a,
+                   sigma_vi=sigma_vi, mass_p_cdm=mass_p, vmax=vmax.astype(np.float32), vsim2phys=vsim2phys)

@@ -1,0 +1,201 @@
+/*
+ * cube_gpu.h -- C-ABI of the B200 particle-mesh step of CUBE.
+ *
+ * The reference step routines take no arguments and act on Fortran module
+ * globals (CUBE_v2.0/work/main/variables.f90:28-81):
+ *   particle_mesh  (pm.f90:2)            -> cube_particle_mesh
+ *   update_x       (update_particle.f90:5) -> cube_update_x
+ *   ext_pp_force   (ext_pp_force.f90:9)  -> cube_ext_pp_force
+ *   buffer_grid / buffer_x / buffer_v (buffer_grid.f90:5, buffer_particle.f90:5,13)
+ *                                       -> no device work: one image on one GPU
+ *                                          keeps every particle once and reads
+ *                                          neighbour cells by periodic index
+ *   neu(nu)%evolve (hydrodf.f90:86)     -> cube_nu_evolve
+ *   timestep       (timestep.f90:1)     -> cube_timestep (host arithmetic)
+ *   kernel_f / kernel_c (kernel_f.f90:2, kernel_c.f90:2) -> inside cube_create
+ *
+ * A Fortran host keeps its no-argument wrappers (see include/cube_gpu.f90) and
+ * passes the module arrays through these entry points.  The library owns the
+ * device-resident particle and mesh state between calls; the host keeps the
+ * scalar globals in a cube_scalars block that each call reads and updates.
+ *
+ * Array layouts are the reference's checkpoint layouts (checkpoint.f90:24-75):
+ *   xp, vp   int8|int16 [nplocal][3]   (Fortran xp(3,nplocal)), izipx/izipv bytes
+ *   pid      int32 [nplocal]
+ *   rhoc     int32 [nnt][nnt][nnt][nt][nt][nt]  (Fortran rhoc(1:nt,1:nt,1:nt,nnt,nnt,nnt))
+ *   vfield   float [nnt^3*nt^3][3]            (Fortran vfield(3,1:nt,1:nt,1:nt,...))
+ * Particles are sorted by tile (x fastest), then by coarse cell (x fastest)
+ * inside the tile, exactly as update_xp leaves them (update_particle.f90:134-149).
+ *
+ * Every entry point returns a cube_status; non-zero codes replace the
+ * reference's print + stop (update_particle.f90:90-96, buffer_grid.f90:131-137,
+ * ext_pp_force.f90:154-158).  Calls on one context come from one host thread;
+ * a context is bound to one CUDA stream.
+ */
+#ifndef CUBE_GPU_H
+#define CUBE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cube_status {
+  CUBE_OK = 0,
+  CUBE_ERR_PARAM = 1,      /* inconsistent sizes or parameters */
+  CUBE_ERR_CAPACITY = 2,   /* particle count beyond the allocated capacity */
+  CUBE_ERR_CUDA = 3,       /* a CUDA runtime call failed (see cube_last_error) */
+  CUBE_ERR_MOVE = 4,       /* a particle moved farther than ncb coarse cells in one drift */
+  CUBE_ERR_TIMEOUT = 5,    /* a bounded device wait gave up */
+  CUBE_ERR_STATE = 6,      /* call made before the state it needs was loaded */
+  CUBE_ERR_CELL = 7        /* one coarse cell holds more particles than a re-bin block can sort */
+} cube_status;
+
+/* Compile-time parameters of parameters.f90:8-116, as runtime fields. */
+typedef struct cube_params {
+  int32_t nc;            /* coarse cells per dimension of the (single) image, nc */
+  int32_t nnt;           /* tiles per dimension, nnt; nt = nc/nnt */
+  int32_t ncell;         /* fine cells per coarse cell per dimension (4) */
+  int32_t ncb;           /* coarse buffer depth (6) */
+  int32_t np_nc;         /* particles per coarse cell per dimension in the IC lattice */
+  int32_t izipx;         /* bytes per position component (1 or 2) */
+  int32_t izipv;         /* bytes per velocity component (1 or 2) */
+  int32_t nf_cutoff;     /* fine-force cutoff in fine cells (16) */
+  int32_t pp_range;      /* PP neighbour range in fine cells (1) */
+  int32_t ext_pp_force;  /* 1: PP on (Extended_pp_force), zeroes the fine-kernel core */
+  int32_t use_pid;       /* 1: particle IDs are carried (-DPID) */
+  int32_t neutrino;      /* 1: fluid neutrinos are coupled (neutrino_flag) */
+  float rsoft;           /* PP softening (0.3) */
+  float tile_buffer;     /* 1.5 */
+  float image_buffer;    /* 1.2 */
+  float vbuf;            /* 0.9 */
+  double vrel_boost;     /* 2.5 */
+  /* cosmology (parameters.f90:69-100) */
+  float box;             /* Mpc/h */
+  float h0;
+  float omega_m;
+  float omega_l;
+  float wde;
+  float ra_max;          /* 0.2 */
+  float dt_max;          /* 1 (variables.f90:20) */
+  /* neutrino fluid (hydrodf.f90:22-49, parameters.f90:73-93) */
+  float z_i_nu;          /* neutrino turn-on redshift */
+  float f_neu;           /* sum(f_neu) = omega_neu/omega_m */
+  float m_nu_ev;         /* neutrino mass per species, eV */
+  float deg_nu;          /* degeneracy */
+  int32_t nu_nc[3];      /* fluid mesh sizes per Gauss-Laguerre fluid (0 = nf/2,nf/4,nf/8) */
+  int32_t reserved[8];
+} cube_params;
+
+/* Scalar globals the step reads and writes (variables.f90:28-48 and sim_header,
+ * parameters.f90:129-153). */
+typedef struct cube_scalars {
+  float a, a_mid, da;
+  float dt, dt_old, dt_mid;
+  float t, tau;
+  float sigma_vi, sigma_vi_new;
+  float mass_p_cdm;
+  float vz_max;            /* sim%vz_max */
+  float dt_fine, dt_coarse, dt_pp, dt_vmax, dt_vmax_nu, dt_e, dt_neu;
+  float vmax[3];
+  float f2_max_fine, f2_max_coarse, f2_max_pp;
+  float vsim2phys;
+  int32_t nlayer;          /* update_xp ordering layers, 2*ceiling(dt_mid*vz_max/ncell)+1 */
+  int32_t timestep;
+  double std_vsim, std_vsim_c, std_vsim_res;
+  double testrhof, testrhoc;   /* mass sums (pm.f90:108,280) */
+  int64_t nplocal, npglobal;
+  int64_t npairs, itest1;      /* PP diagnostics (ext_pp_force.f90:98,87) */
+  int32_t reserved[16];
+} cube_scalars;
+
+typedef struct cube_ctx cube_ctx;
+
+/* Version of this ABI; bump on layout changes of the structs above. */
+int32_t cube_abi_version(void);
+
+/* Creates a context on the current CUDA device: allocates the device state
+ * for up to `np_capacity` particles and builds the fine and coarse Green's
+ * functions (kernel_f.f90:14-37, kernel_c.f90:1-134) in FP64.
+ *   fk_table: fine force table fk_table(16,16,16,3), Fortran order (kernel_f.f90:10-22)
+ *   ck_table: coarse matching table ck_table(3,4,4,4), Fortran order (kernel_c.f90:31-39) */
+int32_t cube_create(const cube_params* params, int64_t np_capacity,
+                    const float* fk_table, const float* ck_table, cube_ctx** out);
+
+/* Copies a checkpoint-layout state to the device (particle_initialization.f90:34-82). */
+int32_t cube_load_state(cube_ctx* ctx, int64_t nplocal, const void* xp, const void* vp,
+                        const int32_t* pid, const int32_t* rhoc, const float* vfield);
+
+/* Copies the device state back in checkpoint layout (checkpoint.f90:24-75).
+ * Any pointer may be NULL to skip that array. */
+int32_t cube_store_state(cube_ctx* ctx, int64_t* nplocal, void* xp, void* vp, int32_t* pid,
+                         int32_t* rhoc, float* vfield);
+
+/* update_x: drift by dt_mid, re-bin by counting sort, re-encode velocities
+ * against the new coarse velocity field, velocity statistics -> sigma_vi_new
+ * (update_particle.f90:13-259).  Reads dt, dt_old, sigma_vi, vz_max;
+ * writes dt_mid, nlayer, sigma_vi_new, std_vsim*, nplocal. */
+int32_t cube_update_x(cube_ctx* ctx, cube_scalars* io);
+
+/* ext_pp_force: particle-particle correction over +-pp_range fine cells
+ * (ext_pp_force.f90:34-143).  Reads a_mid, dt, sigma_vi, mass_p_cdm; writes
+ * dt_pp, f2_max_pp, npairs, itest1. */
+int32_t cube_ext_pp_force(cube_ctx* ctx, cube_scalars* io);
+
+/* particle_mesh: fine and coarse CIC deposit, Poisson solve by FFT, interpolate
+ * and kick (pm.f90:2-451).  Reads a, a_mid, dt, sigma_vi, sigma_vi_new,
+ * mass_p_cdm; writes sigma_vi (= sigma_vi_new), vmax, vz_max, dt_fine,
+ * dt_coarse, dt_vmax, f2_max_*, testrhof, testrhoc, vsim2phys. */
+int32_t cube_particle_mesh(cube_ctx* ctx, cube_scalars* io);
+
+/* timestep (timestep.f90:1-95) in its adaptive form, host arithmetic with the
+ * FP64 Friedmann expansion of timestep.f90:136-180.  If a_next > 0 the step is
+ * snapped to reach a_next exactly (the checkpoint logic of timestep.f90:46-61),
+ * which is also the prescribed-step mode.  Returns 1 in *hit if a_next was hit. */
+int32_t cube_timestep(const cube_params* params, cube_scalars* io, float a_next, int32_t* hit);
+
+/* Friedmann expansion of timestep.f90:136-180 (real(4) interface, FP64 inside). */
+void cube_expansion(const cube_params* params, float a0, float dt0, float* da1, float* da2);
+
+/* Fluid-neutrino half step (hydrodf.f90:86-109). dir=+1 sweeps x,y,z; -1 z,y,x. */
+int32_t cube_nu_evolve(cube_ctx* ctx, float dt, float* dtg, int32_t dir, float a);
+
+/* Device time of the phases of the last step call, milliseconds:
+ * [0] update_x, [1] ext_pp_force, [2] deposit, [3] fine FFT+Green, [4] coarse
+ * FFT+Green, [5] kick, [6] neutrino fluid, [7] total. */
+int32_t cube_phase_times(cube_ctx* ctx, float* ms8);
+
+/* Number of kernels the library launched on this context so far. */
+int64_t cube_launch_count(cube_ctx* ctx);
+
+/* Sets the CUDA stream (cudaStream_t passed as void*) the context launches on. */
+int32_t cube_set_stream(cube_ctx* ctx, void* stream);
+
+/* Text of the last error on this context (or the last create error if ctx is NULL). */
+const char* cube_last_error(cube_ctx* ctx);
+
+void cube_destroy(cube_ctx* ctx);
+
+/* ---- inspection entry points used by the parity tests -----------------------
+ * Copies device meshes to host buffers:
+ *   which=0 fine density rho_f   [nf^3]   (x fastest, global periodic fine mesh)
+ *   which=1 coarse density r3    [nc^3]
+ *   which=2 fine force           [3][nf^3]
+ *   which=3 coarse force         [3][nc^3]
+ *   which=4 fine Green multiplier octant [3][(nf/2+1)^3]
+ *   which=5 coarse Green multiplier      [3][nc][nc][nc/2+1]
+ * Returns the element count written, or -1. */
+int64_t cube_debug_fetch(cube_ctx* ctx, int32_t which, void* host, int64_t capacity);
+
+/* Uploads a fine (which=2) or coarse (which=3) force mesh and runs only the
+ * interpolate+kick of particle_mesh on it (parity of the kick against the oracle
+ * on identical forces). */
+int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float* fine_force,
+                                   const float* coarse_force);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUBE_GPU_H */

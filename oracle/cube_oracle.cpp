@@ -1,0 +1,965 @@
+/*
+ * cube_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatement of CUBE's particle-mesh step, used as the checker of the
+ * CUDA library's parity tests and as the timed CPU baseline.  Nothing in the
+ * product links or calls this file.  It follows the reference Fortran
+ * (CUBE_v2.0/work/main/) routine by routine, in the reference's own data layout:
+ * per-tile extended arrays with ncb buffer cells, particles duplicated into the
+ * buffers, the nlayer interleaved loop orders, per-tile fine meshes of nfe^3
+ * with an nfb buffer and one FFT per tile.
+ *
+ *   spine_image        variables.f90:148-218
+ *   buffer_grid/x/v    buffer_grid.f90:16-192, buffer_particle.f90:21-343
+ *                      (one image, periodic: every halo cell holds a copy of the
+ *                      periodic physical cell, in the same particle order)
+ *   update_xp          update_particle.f90:13-259
+ *   particle_mesh      pm.f90:2-451 (fine per tile, then coarse)
+ *   ext_pp_force       ext_pp_force.f90:9-160
+ *   kernel_f/kernel_c  kernel_f.f90:2-43, kernel_c.f90:2-134 (FP64 here)
+ *
+ * Precision: FP32 where the reference is FP32 (rho_f, force_f, vfield, ...),
+ * FP64 where it is real(8).  The FFTs run in FP64 (FFTW single precision is
+ * not available; see oracle_fft.h), which makes this an FP64-FFT oracle.
+ *
+ * Two choices replace reference behaviour that is not deterministic:
+ *   - the velocity statistics of update_xp (update_particle.f90:174-226) are an
+ *     OpenMP reduction in the reference; here they are per-cell sequential sums
+ *     followed by a fixed pairwise tree over cells (cube_tree_sum below), the
+ *     same order the GPU uses;
+ *   - the fine deposit has two modes: the reference's FP32 accumulation in its
+ *     (layer,k,j,i,l) order, and a 64-bit fixed-point accumulation (weights
+ *     scaled by 2^32) whose result is order-independent.
+ */
+#include <stdint.h>
+#include <string.h>
+#include <math.h>
+#include <algorithm>
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "../include/cube_gpu.h"
+#include "../cube_nufluid_b200/csrc/cube_codec.h"
+#include "oracle_fft.h"
+
+namespace {
+
+typedef std::complex<double> cd;
+
+struct Orc {
+  cube_params P;
+  int nc, nnt, nt, ncell, ncb, nte, nf, nft, nfe, nfb, nfc;
+  int izipx, izipv;
+  cube_codec codec;
+  std::vector<float> tan_table;  // tanf of each velocity code, index code+nvbin/2
+  int nvbin;
+  // compact physical state (checkpoint layout)
+  int64_t np;
+  std::vector<int32_t> xp, vp;  // [np][3] as wrapped codes
+  std::vector<int32_t> pid;
+  std::vector<int32_t> rhoc;    // [tile][nt^3]
+  std::vector<float> vfield;    // [cell][3]
+  // Green's functions
+  std::vector<double> kern_f;   // [3][nfe][nfe][nfe/2+1] imaginary parts
+  std::vector<double> kern_c;   // [3][nc][nc][nc/2+1]
+  std::vector<float> fk_table, ck_table;
+  // diagnostics of the last particle_mesh
+  std::vector<float> rho_f_global;    // [nf^3] central regions of the tile meshes
+  std::vector<float> force_f_global;  // [3][nf^3]
+  std::vector<float> r3;              // [nc^3]
+  std::vector<float> force_c;         // [3][nc^3]
+  std::string err;
+};
+
+inline int64_t cell_id(const Orc& o, int tx, int ty, int tz, int lx, int ly, int lz) {
+  return ((((int64_t)tz * o.nnt + ty) * o.nnt + tx) * o.nt + lz) * (int64_t)o.nt * o.nt +
+         (int64_t)ly * o.nt + lx;
+}
+
+inline float tanf_code(const Orc& o, int code) { return o.tan_table[code + o.nvbin / 2]; }
+
+/* ------------------------------------------------------------------------- */
+/* Extended tile view: the reference's rhoc/vfield/xp after buffer_grid +    */
+/* buffer_x + buffer_v, built in closed form for one image (periodic copies). */
+struct ExtTile {
+  int tx, ty, tz;
+  std::vector<int32_t> rho;      // rhoc(1-ncb:nt+ncb)^3, x fastest
+  std::vector<float> vf;         // vfield(3, ...)
+  std::vector<int64_t> idx_b_r;  // idx_b_r(1-ncb:nt+ncb,1-ncb:nt+ncb) within this tile's array
+  std::vector<int64_t> src;      // compact index of each extended particle slot
+  std::vector<int64_t> cstart;   // start offset of each extended cell inside src
+};
+
+void build_ext(const Orc& o, const std::vector<int64_t>& cell_start, int tx, int ty, int tz,
+               ExtTile& e) {
+  const int nte = o.nte, lo = 1 - o.ncb;
+  e.tx = tx; e.ty = ty; e.tz = tz;
+  e.rho.assign((size_t)nte * nte * nte, 0);
+  e.vf.assign((size_t)3 * nte * nte * nte, 0.f);
+  e.idx_b_r.assign((size_t)nte * nte, 0);
+  e.cstart.assign((size_t)nte * nte * nte + 1, 0);
+  e.src.clear();
+  int64_t n = 0;
+  for (int k = lo; k <= o.nt + o.ncb; ++k)
+    for (int j = lo; j <= o.nt + o.ncb; ++j) {
+      for (int i = lo; i <= o.nt + o.ncb; ++i) {
+        const int gx = ((tx * o.nt + i - 1) % o.nc + o.nc) % o.nc;
+        const int gy = ((ty * o.nt + j - 1) % o.nc + o.nc) % o.nc;
+        const int gz = ((tz * o.nt + k - 1) % o.nc + o.nc) % o.nc;
+        const int64_t c = cell_id(o, gx / o.nt, gy / o.nt, gz / o.nt, gx % o.nt, gy % o.nt, gz % o.nt);
+        const size_t q = ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo);
+        const int32_t cnt = o.rhoc[c];
+        e.rho[q] = cnt;
+        for (int d = 0; d < 3; ++d) e.vf[3 * q + d] = o.vfield[3 * c + d];
+        e.cstart[q] = n;
+        for (int l = 0; l < cnt; ++l) e.src.push_back(cell_start[c] + l);
+        n += cnt;
+      }
+      e.idx_b_r[(size_t)(k - lo) * nte + (j - lo)] = n;
+    }
+  e.cstart[(size_t)nte * nte * nte] = n;
+}
+
+std::vector<int64_t> compact_cell_start(const Orc& o) {
+  const int64_t ncells = (int64_t)o.nc * o.nc * o.nc;
+  std::vector<int64_t> cs(ncells + 1, 0);
+  for (int64_t c = 0; c < ncells; ++c) cs[c + 1] = cs[c] + o.rhoc[c];
+  return cs;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Deterministic sum: fixed pairwise tree over blocks of 1024 (the GPU order). */
+double cube_tree_sum(std::vector<double> a) {
+  if (a.empty()) return 0.0;
+  while (a.size() > 1) {
+    const size_t nb = (a.size() + 1023) / 1024;
+    std::vector<double> out(nb);
+    for (size_t b = 0; b < nb; ++b) {
+      double loc[1024];
+      for (int i = 0; i < 1024; ++i) {
+        const size_t q = b * 1024 + i;
+        loc[i] = q < a.size() ? a[q] : 0.0;
+      }
+      for (int s = 512; s >= 1; s >>= 1)
+        for (int i = 0; i < s; ++i) loc[i] = cube_dadd(loc[i], loc[i + s]);
+      out[b] = loc[0];
+    }
+    a.swap(out);
+  }
+  return a[0];
+}
+
+/* ------------------------------------------------------------------------- */
+/* update_xp (update_particle.f90:13-259)                                     */
+int update_xp(Orc& o, cube_scalars* s) {
+  const int nt = o.nt, ncb = o.ncb;
+  const int lo2 = 1 - 2 * ncb, n2 = nt + 4 * ncb;  // rhoce(1-2ncb:nt+2ncb)
+  s->dt_mid = (s->dt_old + s->dt) / 2;
+  const float dt_mid = s->dt_mid;
+  // nlayer=2*ceiling(dt_mid*sim%vz_max/ncell)+1 : float product, int8 division -> real
+  const int nlayer = 2 * (int)ceilf(cube_fdiv(cube_fmul(dt_mid, s->vz_max), (float)o.ncell)) + 1;
+  s->nlayer = nlayer;
+  const double coef = cube_vcoef(&o.codec, s->sigma_vi);
+  const std::vector<int64_t> cs = compact_cell_start(o);
+  const int64_t ncells = (int64_t)o.nc * o.nc * o.nc;
+  std::vector<int32_t> nx, nv, npid;
+  std::vector<int32_t> nrho(ncells, 0);
+  std::vector<float> nvf((size_t)3 * ncells, 0.f);
+  nx.reserve(o.np * 3); nv.reserve(o.np * 3); npid.reserve(o.np);
+  int64_t np_prev = 0;
+  int rc = CUBE_OK;
+  ExtTile e;
+  for (int tz = 0; tz < o.nnt; ++tz)
+    for (int ty = 0; ty < o.nnt; ++ty)
+      for (int tx = 0; tx < o.nnt; ++tx) {
+        build_ext(o, cs, tx, ty, tz, e);
+        const int nte = o.nte, lo = 1 - ncb;
+        std::vector<int32_t> rhoce((size_t)n2 * n2 * n2, 0), rholocal((size_t)n2 * n2 * n2, 0);
+        std::vector<float> vfn((size_t)3 * n2 * n2 * n2, 0.f);
+        auto q2 = [&](int i, int j, int k) { return ((size_t)(k - lo2) * n2 + (j - lo2)) * n2 + (i - lo2); };
+        // vfield_new(:,1-ncb:nt+ncb,...)=vfield*weight_v
+        for (int k = lo; k <= nt + ncb; ++k)
+          for (int j = lo; j <= nt + ncb; ++j)
+            for (int i = lo; i <= nt + ncb; ++i) {
+              const size_t qe = ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo);
+              for (int d = 0; d < 3; ++d)
+                vfn[3 * q2(i, j, k) + d] = (float)cube_dmul((double)e.vf[3 * qe + d], 0.1);
+            }
+        struct Hit { int ig[3]; double v[3]; };
+        auto drift = [&](size_t qe, int i, int j, int k, int64_t ip, Hit& h) {
+          const int ijk[3] = {i, j, k};
+          for (int d = 0; d < 3; ++d) {
+            const double xq = cube_dadd((double)ijk[d] - 1.0, cube_xfrac(o.xp[3 * ip + d], o.izipx));
+            double v = cube_vdecode(tanf_code(o, o.vp[3 * ip + d]), coef);
+            v = cube_dadd(v, (double)e.vf[3 * qe + d]);
+            const double dx = cube_ddiv(cube_dmul((double)dt_mid, v), (double)o.ncell);
+            h.ig[d] = (int)ceil(cube_dadd(xq, dx));
+            h.v[d] = v;
+          }
+        };
+        // density loop (update_particle.f90:57-80)
+        for (int il = 0; il < nlayer; ++il)
+          for (int k = lo + il; k <= nt + ncb; k += nlayer)
+            for (int j = lo; j <= nt + ncb; ++j)
+              for (int i = lo; i <= nt + ncb; ++i) {
+                const size_t qe = ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo);
+                for (int64_t l = 0; l < e.rho[qe]; ++l) {
+                  const int64_t ip = e.src[e.cstart[qe] + l];
+                  Hit h;
+                  drift(qe, i, j, k, ip, h);
+                  for (int d = 0; d < 3; ++d)
+                    if (h.ig[d] < lo2 || h.ig[d] > nt + 2 * ncb) { o.err = "particle left the extended tile"; return CUBE_ERR_MOVE; }
+                  const size_t q = q2(h.ig[0], h.ig[1], h.ig[2]);
+                  rhoce[q] += 1;
+                  for (int d = 0; d < 3; ++d) vfn[3 * q + d] = (float)cube_dadd((double)vfn[3 * q + d], h.v[d]);
+                }
+              }
+        for (size_t q = 0; q < rhoce.size(); ++q)
+          for (int d = 0; d < 3; ++d)
+            vfn[3 * q + d] = (float)cube_ddiv((double)vfn[3 * q + d], cube_dadd((double)rhoce[q], 0.1));
+        // spine_tile (variables.f90:103-146): cumulative index over (y,z) rows
+        std::vector<int64_t> idx_ex_r((size_t)n2 * n2);
+        int64_t nsum = 0;
+        for (int k = lo2; k <= nt + 2 * ncb; ++k)
+          for (int j = lo2; j <= nt + 2 * ncb; ++j) {
+            for (int i = lo2; i <= nt + 2 * ncb; ++i) nsum += rhoce[q2(i, j, k)];
+            idx_ex_r[(size_t)(k - lo2) * n2 + (j - lo2)] = nsum;
+          }
+        const int64_t ntot = nsum;
+        std::vector<int32_t> xn((size_t)3 * ntot), vn((size_t)3 * ntot), pn(ntot);
+        // xvnew loop (update_particle.f90:99-128)
+        for (int il = 0; il < nlayer; ++il)
+          for (int k = lo + il; k <= nt + ncb; k += nlayer)
+            for (int j = lo; j <= nt + ncb; ++j)
+              for (int i = lo; i <= nt + ncb; ++i) {
+                const size_t qe = ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo);
+                for (int64_t l = 0; l < e.rho[qe]; ++l) {
+                  const int64_t ip = e.src[e.cstart[qe] + l];
+                  Hit h;
+                  drift(qe, i, j, k, ip, h);
+                  const size_t q = q2(h.ig[0], h.ig[1], h.ig[2]);
+                  rholocal[q] += 1;
+                  int64_t right = 0;
+                  for (int ii = h.ig[0]; ii <= nt + 2 * ncb; ++ii) right += rhoce[q2(ii, h.ig[1], h.ig[2])];
+                  const int64_t idx = idx_ex_r[(size_t)(h.ig[2] - lo2) * n2 + (h.ig[1] - lo2)] - right + rholocal[q];
+                  for (int d = 0; d < 3; ++d) {
+                    const double step = cube_ddiv(cube_dmul((double)dt_mid, h.v[d]),
+                                                  cube_dmul(o.codec.x_resolution, (double)o.ncell));
+                    const int64_t nv_ = cube_nint(step);
+                    xn[3 * (idx - 1) + d] = cube_wrap_code((int64_t)o.xp[3 * ip + d] + (int32_t)nv_, o.izipx);
+                    const double vr = cube_dsub(h.v[d], (double)vfn[3 * q + d]);
+                    vn[3 * (idx - 1) + d] = cube_wrap_code(cube_vencode(&o.codec, vr, coef), o.izipv);
+                  }
+                  pn[idx - 1] = o.pid.empty() ? 0 : o.pid[ip];
+                }
+              }
+        // keep physical particles, tile-major compact order (update_particle.f90:134-149)
+        for (int k = 1; k <= nt; ++k)
+          for (int j = 1; j <= nt; ++j)
+            for (int i = 1; i <= nt; ++i) {
+              const size_t q = q2(i, j, k);
+              int64_t right = 0;
+              for (int ii = i; ii <= nt + 2 * ncb; ++ii) right += rhoce[q2(ii, j, k)];
+              const int64_t first = idx_ex_r[(size_t)(k - lo2) * n2 + (j - lo2)] - right;  // zero-based start
+              const int64_t c = cell_id(o, tx, ty, tz, i - 1, j - 1, k - 1);
+              nrho[c] = rhoce[q];
+              for (int d = 0; d < 3; ++d) nvf[3 * c + d] = vfn[3 * q + d];
+              for (int64_t l = 0; l < rhoce[q]; ++l) {
+                for (int d = 0; d < 3; ++d) {
+                  nx.push_back(xn[3 * (first + l) + d]);
+                  nv.push_back(vn[3 * (first + l) + d]);
+                }
+                npid.push_back(pn[first + l]);
+              }
+              np_prev += rhoce[q];
+            }
+      }
+  o.xp.swap(nx); o.vp.swap(nv);
+  if (!o.pid.empty()) o.pid.swap(npid);
+  o.rhoc.swap(nrho); o.vfield.swap(nvf);
+  o.np = np_prev;
+  s->nplocal = np_prev;
+  // velocity statistics (update_particle.f90:171-226) in the fixed order
+  std::vector<int64_t> cs2 = compact_cell_start(o);
+  std::vector<double> sc(ncells), sr(ncells), ss(ncells);
+  for (int64_t c = 0; c < ncells; ++c) {
+    const float* vf = &o.vfield[3 * c];
+    float f2 = cube_fadd(cube_fadd(cube_fmul(vf[0], vf[0]), cube_fmul(vf[1], vf[1])), cube_fmul(vf[2], vf[2]));
+    sc[c] = (double)f2;
+    double r = 0, q = 0;
+    for (int64_t ip = cs2[c]; ip < cs2[c + 1]; ++ip) {
+      double v[3], w[3];
+      for (int d = 0; d < 3; ++d) {
+        v[d] = cube_vdecode(tanf_code(o, o.vp[3 * ip + d]), coef);
+        w[d] = cube_dadd(v[d], (double)vf[d]);
+      }
+      r = cube_dadd(r, cube_dadd(cube_dadd(cube_dmul(v[0], v[0]), cube_dmul(v[1], v[1])), cube_dmul(v[2], v[2])));
+      q = cube_dadd(q, cube_dadd(cube_dadd(cube_dmul(w[0], w[0]), cube_dmul(w[1], w[1])), cube_dmul(w[2], w[2])));
+    }
+    sr[c] = r; ss[c] = q;
+  }
+  const double sum_c = cube_tree_sum(sc), sum_r = cube_tree_sum(sr), sum_s = cube_tree_sum(ss);
+  const double npg = (double)(s->npglobal > 0 ? s->npglobal : o.np);
+  s->std_vsim = sqrt(sum_s / npg);
+  s->std_vsim_c = sqrt(sum_c / (double)ncells);
+  s->std_vsim_res = sqrt(sum_r / npg);
+  s->sigma_vi_new = (float)(s->std_vsim_res / (double)sqrtf(3.f));
+  return rc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* kernel_f (kernel_f.f90:14-37) on the nfe grid, FP64                        */
+void kernel_f(Orc& o) {
+  const int nfe = o.nfe, nfc = o.nfc, nh = nfe / 2 + 1;
+  o.kern_f.assign((size_t)3 * nfe * nfe * nh, 0.0);
+  std::vector<double> r((size_t)nfe * nfe * nfe);
+  std::vector<cd> h;
+  for (int d = 0; d < 3; ++d) {
+    std::fill(r.begin(), r.end(), 0.0);
+    auto at = [&](int i, int j, int k) -> double& { return r[((size_t)(k - 1) * nfe + (j - 1)) * nfe + (i - 1)]; };
+    for (int k = 1; k <= nfc; ++k)
+      for (int j = 1; j <= nfc; ++j)
+        for (int i = 1; i <= nfc; ++i)
+          at(i, j, k) = (double)o.fk_table[(((size_t)d * nfc + (k - 1)) * nfc + (j - 1)) * nfc + (i - 1)];
+    if (o.P.ext_pp_force)
+      for (int k = 1; k <= o.P.pp_range + 1; ++k)
+        for (int j = 1; j <= o.P.pp_range + 1; ++j)
+          for (int i = 1; i <= o.P.pp_range + 1; ++i) at(i, j, k) = 0;
+    const double mf[3] = {d == 0 ? -1.0 : 1.0, d == 1 ? -1.0 : 1.0, d == 2 ? -1.0 : 1.0};
+    for (int k = 1; k <= nfe; ++k)
+      for (int j = 1; j <= nfe; ++j)
+        for (int m = 0; m < nfc - 1; ++m) at(nfe - nfc + 2 + m, j, k) = mf[0] * at(nfc - m, j, k);
+    for (int k = 1; k <= nfe; ++k)
+      for (int m = 0; m < nfc - 1; ++m)
+        for (int i = 1; i <= nfe; ++i) at(i, nfe - nfc + 2 + m, k) = mf[1] * at(i, nfc - m, k);
+    for (int m = 0; m < nfc - 1; ++m)
+      for (int j = 1; j <= nfe; ++j)
+        for (int i = 1; i <= nfe; ++i) at(i, j, nfe - nfc + 2 + m) = mf[2] * at(i, j, nfc - m);
+    orc::rfft3_forward(r.data(), h, nfe);
+    for (size_t q = 0; q < h.size(); ++q) o.kern_f[(size_t)d * h.size() + q] = h[q].imag();
+  }
+}
+
+/* kernel_c (kernel_c.f90:1-134) with LRCKCORR, one image, FP64 */
+void kernel_c(Orc& o) {
+  const int nc = o.nc, nh = nc / 2 + 1, ncell = o.ncell;
+  const double pi = 3.14159265358979323846;
+  std::vector<double> ck((size_t)3 * nc * nc * nc), direct((size_t)3 * nc * nc * nc);
+  auto ckat = [&](std::vector<double>& a, int d, int i, int j, int k) -> double& {
+    return a[(((size_t)d * nc + (k - 1)) * nc + (j - 1)) * nc + (i - 1)];
+  };
+  for (int k = 1; k <= nc; ++k)
+    for (int j = 1; j <= nc; ++j)
+      for (int i = 1; i <= nc; ++i) {
+        const int g[3] = {i, j, k};
+        double rx[3];
+        for (int d = 0; d < 3; ++d) rx[d] = (double)ncell * (double)(((g[d] + nc / 2 - 1) % nc) - nc / 2);
+        const double r = sqrt(rx[0] * rx[0] + rx[1] * rx[1] + rx[2] * rx[2]);
+        for (int d = 0; d < 3; ++d) {
+          const double v = (r == 0) ? 0.0 : -rx[d] / (r * r * r);
+          ckat(ck, d, i, j, k) = v;
+          ckat(direct, d, i, j, k) = v;
+        }
+      }
+  // ck_table(3,4,4,4): component fastest
+  auto tab = [&](int d, int i, int j, int k) -> double {
+    return (double)o.ck_table[(((size_t)(k - 1) * 4 + (j - 1)) * 4 + (i - 1)) * 3 + d];
+  };
+  // octants (kernel_c.f90:43-72): each dimension is either offsets 0..3 (index 1..4)
+  // or offsets -3..-1 (index nc-2..nc, from table index 4..2), odd in the component's own dimension
+  for (int oct = 0; oct < 8; ++oct) {
+    const bool fx = oct & 1, fy = oct & 2, fz = oct & 4;
+    for (int k = 1; k <= (fz ? 3 : 4); ++k)
+      for (int j = 1; j <= (fy ? 3 : 4); ++j)
+        for (int i = 1; i <= (fx ? 3 : 4); ++i) {
+          const int ti = fx ? 5 - i : i, tj = fy ? 5 - j : j, tk = fz ? 5 - k : k;  // 4:2:-1 -> 4,3,2
+          const int ci = fx ? nc - 3 + i : i, cj = fy ? nc - 3 + j : j, ck_ = fz ? nc - 3 + k : k;
+          for (int d = 0; d < 3; ++d) {
+            double sgn = 1.0;
+            if ((d == 0 && fx) || (d == 1 && fy) || (d == 2 && fz)) sgn = -1.0;
+            ckat(ck, d, ci, cj, ck_) = sgn * tab(d, ti, tj, tk);
+          }
+        }
+  }
+  o.kern_c.assign((size_t)3 * nc * nc * nh, 0.0);
+  std::vector<cd> hc, hd;
+  for (int d = 0; d < 3; ++d) {
+    orc::rfft3_forward(&ck[(size_t)d * nc * nc * nc], hc, nc);
+    orc::rfft3_forward(&direct[(size_t)d * nc * nc * nc], hd, nc);
+    for (int k = 0; k < nc; ++k)
+      for (int j = 0; j < nc; ++j)
+        for (int i = 0; i < nh; ++i) {
+          const size_t q = ((size_t)k * nc + j) * nh + i;
+          const int kg = k + 1, jg = j + 1, ig = i + 1;
+          const int kx[3] = {((ig + nc / 2 - 1) % nc) - nc / 2, ((jg + nc / 2 - 1) % nc) - nc / 2,
+                             ((kg + nc / 2 - 1) % nc) - nc / 2};
+          const double kr = sqrt((double)kx[0] * kx[0] + (double)kx[1] * kx[1] + (double)kx[2] * kx[2]);
+          double ks[3], ks2 = 0;
+          for (int e = 0; e < 3; ++e) { ks[e] = 2 * sin(pi * kx[e] / (double)nc); ks2 += ks[e] * ks[e]; }
+          double v = hc[q].imag();
+          // the component is odd in its own dimension: zero on the Nyquist plane
+          // (FP64 round-off there would otherwise enter the |k|<=8 rescaling when nc=16)
+          if (kx[d] == -nc / 2) v = 0.0;
+          else if (!(kr > 8.0 || kx[d] == 0))
+            v = v * 0.25 * pi * ks[d] / ks2 / hd[q].imag();
+          o.kern_c[(size_t)d * nc * nc * nh + q] = v;
+        }
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* particle_mesh (pm.f90:2-451); neutrino terms enter through the fluid module */
+/* dt constraints (pm.f90:427-443), FP32 like the reference */
+void dt_constraints(const Orc& o, cube_scalars* s) {
+  const float pi_f = o.codec.pi_f;
+  const float GG = cube_fdiv(cube_fdiv(1.0f, 6.0f), pi_f);  /* variables.f90:22 */
+  float v = cube_fdiv(1.5f, s->a);
+  v = cube_fmul(v, o.P.box);
+  v = cube_fmul(v, o.P.h0);
+  v = cube_fmul(v, 100.f);
+  v = cube_fmul(v, sqrtf(o.P.omega_m));
+  s->vsim2phys = cube_fdiv(v, (float)o.nf);
+  s->dt_fine = sqrtf(cube_fdiv(1.0f, cube_fmul(cube_fmul(sqrtf(s->f2_max_fine), s->a_mid), GG)));
+  s->dt_coarse = sqrtf(cube_fdiv((float)o.ncell, cube_fmul(cube_fmul(sqrtf(s->f2_max_coarse), s->a_mid), GG)));
+  const float vm = std::max(s->vmax[0], std::max(s->vmax[1], s->vmax[2]));
+  s->dt_vmax = cube_fdiv(cube_fmul(o.P.vbuf, 20.f), vm);
+  s->vz_max = s->vmax[2];
+}
+
+struct KickIn {
+  const std::vector<float>* fine_force;    // optional external [3][nf^3]
+  const std::vector<float>* coarse_force;  // optional external [3][nc^3]
+};
+
+int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) {
+  const int nt = o.nt, ncb = o.ncb, ncell = o.ncell, nfe = o.nfe, nfb = o.nfb, nft = o.nft;
+  const int nh = nfe / 2 + 1, nf = o.nf, nc = o.nc;
+  const float mass = s->mass_p_cdm;
+  const float a_mid = s->a_mid, dt = s->dt;
+  const float pi_f = o.codec.pi_f;
+  double vmax[3] = {0, 0, 0};
+  float f2_max_fine = 0.f;
+  double testrhof = 0, testrhoc = 0;
+  const std::vector<int64_t> cs = compact_cell_start(o);
+  o.rho_f_global.assign((size_t)nf * nf * nf, 0.f);
+  o.force_f_global.assign((size_t)3 * nf * nf * nf, 0.f);
+  const double coef_old = cube_vcoef(&o.codec, s->sigma_vi);
+  const double coef_new = cube_vcoef(&o.codec, s->sigma_vi_new);
+  std::vector<float> rho_f((size_t)nfe * nfe * nfe);
+  std::vector<int64_t> rho_q;
+  std::vector<float> force_f((size_t)3 * (nft + 2) * (nft + 2) * (nft + 2));
+  std::vector<cd> spec, prod;
+  std::vector<double> rr((size_t)nfe * nfe * nfe);
+  ExtTile e;
+  const int lo = 1 - ncb, nte = o.nte;
+  auto ptempx = [&](int ijk, int32_t code) -> float {  // ncell*(i-1)+ncell*frac, FP64 -> real
+    return (float)cube_dadd((double)ncell * (double)(ijk - 1), cube_dmul((double)ncell, cube_xfrac(code, o.izipx)));
+  };
+  for (int tz = 0; tz < o.nnt; ++tz)
+    for (int ty = 0; ty < o.nnt; ++ty)
+      for (int tx = 0; tx < o.nnt; ++tx) {
+        build_ext(o, cs, tx, ty, tz, e);
+        auto eq = [&](int i, int j, int k) { return ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo); };
+        std::fill(rho_f.begin(), rho_f.end(), 0.f);
+        if (deposit_mode == 1) rho_q.assign(rho_f.size(), 0);
+        auto fat = [&](int i, int j, int k) -> size_t { return ((size_t)(k - 1) * nfe + (j - 1)) * nfe + (i - 1); };
+        // fine_cic_mass (pm.f90:76-107)
+        for (int il = 0; il < 3; ++il)
+          for (int k = 2 - ncb + il; k <= nt + ncb - 1; k += 3)
+            for (int j = 2 - ncb; j <= nt + ncb - 1; ++j)
+              for (int i = 2 - ncb; i <= nt + ncb - 1; ++i) {
+                const size_t qe = eq(i, j, k);
+                for (int64_t l = 0; l < e.rho[qe]; ++l) {
+                  const int64_t ip = e.src[e.cstart[qe] + l];
+                  const int ijk[3] = {i, j, k};
+                  int i1[3], i2[3];
+                  float dx1[3], dx2[3];
+                  for (int d = 0; d < 3; ++d) {
+                    const float tx_ = ptempx(ijk[d], o.xp[3 * ip + d]);
+                    const int f = (int)floorf(tx_) + 1;
+                    dx1[d] = cube_fsub((float)f, tx_);
+                    dx2[d] = cube_fsub(1.f, dx1[d]);
+                    i1[d] = f + nfb; i2[d] = f + 1 + nfb;
+                  }
+                  const int cx[8][3] = {{0,0,0},{1,0,0},{0,1,0},{0,0,1},{0,1,1},{1,0,1},{1,1,0},{1,1,1}};
+                  for (int c8 = 0; c8 < 8; ++c8) {
+                    const float wx = cx[c8][0] ? dx2[0] : dx1[0];
+                    const float wy = cx[c8][1] ? dx2[1] : dx1[1];
+                    const float wz = cx[c8][2] ? dx2[2] : dx1[2];
+                    const float w = cube_fmul(cube_fmul(cube_fmul(wx, wy), wz), mass);
+                    const size_t q = fat(cx[c8][0] ? i2[0] : i1[0], cx[c8][1] ? i2[1] : i1[1], cx[c8][2] ? i2[2] : i1[2]);
+                    if (deposit_mode == 1) rho_q[q] += (int64_t)llrint((double)w * 4294967296.0);
+                    else rho_f[q] = cube_fadd(rho_f[q], w);
+                  }
+                }
+              }
+        if (deposit_mode == 1)
+          for (size_t q = 0; q < rho_f.size(); ++q) rho_f[q] = (float)((double)rho_q[q] * (1.0 / 4294967296.0));
+        for (int k = nfb + 1; k <= nft + nfb; ++k)
+          for (int j = nfb + 1; j <= nft + nfb; ++j)
+            for (int i = nfb + 1; i <= nft + nfb; ++i) {
+              testrhof += (double)rho_f[fat(i, j, k)];
+              const size_t g = ((size_t)(tz * nft + k - nfb - 1) * nf + (ty * nft + j - nfb - 1)) * nf + (tx * nft + i - nfb - 1);
+              o.rho_f_global[g] = rho_f[fat(i, j, k)];
+            }
+        // fine force (pm.f90:112-126)
+        const int nfo = nft + 2;  // force_f(3, nfb:nfe-nfb+1)
+        if (ext && ext->fine_force) {
+          for (int k = 0; k < nfo; ++k)
+            for (int j = 0; j < nfo; ++j)
+              for (int i = 0; i < nfo; ++i) {
+                const int gx = ((tx * nft + i - 1) % nf + nf) % nf, gy = ((ty * nft + j - 1) % nf + nf) % nf,
+                          gz = ((tz * nft + k - 1) % nf + nf) % nf;
+                for (int d = 0; d < 3; ++d)
+                  force_f[(((size_t)k * nfo + j) * nfo + i) * 3 + d] =
+                      (*ext->fine_force)[(size_t)d * nf * nf * nf + ((size_t)gz * nf + gy) * nf + gx];
+              }
+        } else {
+          for (size_t q = 0; q < rr.size(); ++q) rr[q] = (double)rho_f[q];
+          orc::rfft3_forward(rr.data(), spec, nfe);
+          prod.resize(spec.size());
+          for (int d = 0; d < 3; ++d) {
+            for (size_t q = 0; q < spec.size(); ++q) {
+              const double kv = o.kern_f[(size_t)d * spec.size() + q];
+              prod[q] = cd(-spec[q].imag() * kv, spec[q].real() * kv);
+            }
+            orc::rfft3_backward(prod, rr.data(), nfe);
+            const double norm = (double)nfe * nfe * nfe;
+            for (int k = 0; k < nfo; ++k)
+              for (int j = 0; j < nfo; ++j)
+                for (int i = 0; i < nfo; ++i)
+                  force_f[(((size_t)k * nfo + j) * nfo + i) * 3 + d] =
+                      (float)(rr[fat(nfb + i, nfb + j, nfb + k)] / norm);
+          }
+          (void)nh;
+        }
+        for (int k = 0; k < nfo; ++k)
+          for (int j = 0; j < nfo; ++j)
+            for (int i = 0; i < nfo; ++i) {
+              const float* f = &force_f[(((size_t)k * nfo + j) * nfo + i) * 3];
+              const float f2 = cube_fadd(cube_fadd(cube_fmul(f[0], f[0]), cube_fmul(f[1], f[1])), cube_fmul(f[2], f[2]));
+              f2_max_fine = std::max(f2_max_fine, f2);
+              if (i >= 1 && i <= nft && j >= 1 && j <= nft && k >= 1 && k <= nft) {
+                const size_t g = ((size_t)(tz * nft + k - 1) * nf + (ty * nft + j - 1)) * nf + (tx * nft + i - 1);
+                for (int d = 0; d < 3; ++d) o.force_f_global[(size_t)d * nf * nf * nf + g] = f[d];
+              }
+            }
+        // fine velocity (pm.f90:131-155)
+        const float kfac_a = a_mid, kfac_dt = dt;
+        for (int k = 1; k <= nt; ++k)
+          for (int j = 1; j <= nt; ++j)
+            for (int i = 1; i <= nt; ++i) {
+              const size_t qe = eq(i, j, k);
+              for (int64_t l = 0; l < e.rho[qe]; ++l) {
+                const int64_t ip = e.src[e.cstart[qe] + l];
+                const int ijk[3] = {i, j, k};
+                int i1[3];
+                float dx1[3], dx2[3];
+                for (int d = 0; d < 3; ++d) {
+                  const float tx_ = ptempx(ijk[d], o.xp[3 * ip + d]);
+                  const int f = (int)floorf(tx_) + 1;
+                  dx1[d] = cube_fsub((float)f, tx_);
+                  dx2[d] = cube_fsub(1.f, dx1[d]);
+                  i1[d] = f + nfb;  // index into force_f(nfb:...) -> offset i1-nfb
+                }
+                const int cx[8][3] = {{0,0,0},{1,0,0},{0,1,0},{0,0,1},{0,1,1},{1,0,1},{1,1,0},{1,1,1}};
+                for (int d = 0; d < 3; ++d) {
+                  double v = cube_vdecode(tanf_code(o, o.vp[3 * ip + d]), coef_old);
+                  for (int c8 = 0; c8 < 8; ++c8) {
+                    const int fi = i1[0] + cx[c8][0] - nfb, fj = i1[1] + cx[c8][1] - nfb, fk = i1[2] + cx[c8][2] - nfb;
+                    const float fv = force_f[(((size_t)fk * nfo + fj) * nfo + fi) * 3 + d];
+                    float t = cube_fmul(fv, kfac_a);
+                    t = cube_fmul(t, kfac_dt);
+                    t = cube_fdiv(t, 6.f);
+                    t = cube_fdiv(t, pi_f);
+                    t = cube_fmul(t, cx[c8][0] ? dx2[0] : dx1[0]);
+                    t = cube_fmul(t, cx[c8][1] ? dx2[1] : dx1[1]);
+                    t = cube_fmul(t, cx[c8][2] ? dx2[2] : dx1[2]);
+                    v = cube_dadd(v, (double)t);
+                  }
+                  o.vp[3 * ip + d] = cube_wrap_code(cube_vencode(&o.codec, v, coef_new), o.izipv);
+                }
+              }
+            }
+      }
+  s->f2_max_fine = f2_max_fine;
+  s->sigma_vi = s->sigma_vi_new;
+  // coarse_cic_mass (pm.f90:192-278)
+  o.r3.assign((size_t)nc * nc * nc, 0.f);
+  for (int tz = 0; tz < o.nnt; ++tz)
+    for (int ty = 0; ty < o.nnt; ++ty)
+      for (int tx = 0; tx < o.nnt; ++tx) {
+        build_ext(o, cs, tx, ty, tz, e);
+        auto eq = [&](int i, int j, int k) { return ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo); };
+        const int n3 = nt + 4;  // r3t(-1:nt+2)
+        std::vector<float> r3t((size_t)n3 * n3 * n3, 0.f);
+        std::vector<int64_t> r3q;
+        if (deposit_mode == 1) r3q.assign(r3t.size(), 0);
+        auto tat = [&](int i, int j, int k) { return ((size_t)(k + 1) * n3 + (j + 1)) * n3 + (i + 1); };
+        for (int il = 0; il < 3; ++il)
+          for (int k = 0 + il; k <= nt + 1; k += 3)
+            for (int j = 0; j <= nt + 1; ++j)
+              for (int i = 0; i <= nt + 1; ++i) {
+                const size_t qe = eq(i, j, k);
+                for (int64_t l = 0; l < e.rho[qe]; ++l) {
+                  const int64_t ip = e.src[e.cstart[qe] + l];
+                  const int ijk[3] = {i, j, k};
+                  int i1[3];
+                  float dx1[3], dx2[3];
+                  for (int d = 0; d < 3; ++d) {
+                    const float t_ = (float)cube_dsub(cube_dadd((double)(ijk[d] - 1), cube_xfrac(o.xp[3 * ip + d], o.izipx)), 0.5);
+                    i1[d] = (int)floorf(t_) + 1;
+                    dx1[d] = cube_fsub((float)i1[d], t_);
+                    dx2[d] = cube_fsub(1.f, dx1[d]);
+                  }
+                  const int cx[8][3] = {{0,0,0},{1,0,0},{0,1,0},{0,0,1},{0,1,1},{1,0,1},{1,1,0},{1,1,1}};
+                  for (int c8 = 0; c8 < 8; ++c8) {
+                    const float wx = cx[c8][0] ? dx2[0] : dx1[0];
+                    const float wy = cx[c8][1] ? dx2[1] : dx1[1];
+                    const float wz = cx[c8][2] ? dx2[2] : dx1[2];
+                    const float w = cube_fmul(cube_fmul(cube_fmul(wx, wy), wz), mass);
+                    const size_t q = tat(i1[0] + cx[c8][0], i1[1] + cx[c8][1], i1[2] + cx[c8][2]);
+                    if (deposit_mode == 1) r3q[q] += (int64_t)llrint((double)w * 4294967296.0);
+                    else r3t[q] = cube_fadd(r3t[q], w);
+                  }
+                }
+              }
+        if (deposit_mode == 1)
+          for (size_t q = 0; q < r3t.size(); ++q) r3t[q] = (float)((double)r3q[q] * (1.0 / 4294967296.0));
+        for (int k = 1; k <= nt; ++k)
+          for (int j = 1; j <= nt; ++j)
+            for (int i = 1; i <= nt; ++i)
+              o.r3[((size_t)(tz * nt + k - 1) * nc + (ty * nt + j - 1)) * nc + (tx * nt + i - 1)] = r3t[tat(i, j, k)];
+      }
+  for (size_t q = 0; q < o.r3.size(); ++q) testrhoc += (double)o.r3[q];
+  // coarse force (pm.f90:288-300), pencil_fft on one image = 3-D r2c/c2r
+  o.force_c.assign((size_t)3 * nc * nc * nc, 0.f);
+  if (ext && ext->coarse_force) {
+    o.force_c = *ext->coarse_force;
+  } else {
+    std::vector<double> r((size_t)nc * nc * nc);
+    for (size_t q = 0; q < r.size(); ++q) r[q] = (double)o.r3[q];
+    std::vector<cd> sp, pr;
+    orc::rfft3_forward(r.data(), sp, nc);
+    pr.resize(sp.size());
+    for (int d = 0; d < 3; ++d) {
+      for (size_t q = 0; q < sp.size(); ++q) {
+        const double kv = o.kern_c[(size_t)d * sp.size() + q];
+        pr[q] = cd(-sp[q].imag() * kv, sp[q].real() * kv);
+      }
+      orc::rfft3_backward(pr, r.data(), nc);
+      const double norm = (double)nc * nc * nc;
+      for (size_t q = 0; q < r.size(); ++q) o.force_c[(size_t)d * r.size() + q] = (float)(r[q] / norm);
+    }
+  }
+  float f2c = 0.f;
+  for (size_t q = 0; q < (size_t)nc * nc * nc; ++q) {
+    const float a = o.force_c[q], b = o.force_c[(size_t)nc * nc * nc + q], c = o.force_c[(size_t)2 * nc * nc * nc + q];
+    f2c = std::max(f2c, cube_fadd(cube_fadd(cube_fmul(a, a), cube_fmul(b, b)), cube_fmul(c, c)));
+  }
+  s->f2_max_coarse = f2c;
+  // coarse velocity (pm.f90:335-372)
+  const double coef = cube_vcoef(&o.codec, s->sigma_vi);
+  for (int tz = 0; tz < o.nnt; ++tz)
+    for (int ty = 0; ty < o.nnt; ++ty)
+      for (int tx = 0; tx < o.nnt; ++tx)
+        for (int k = 1; k <= nt; ++k)
+          for (int j = 1; j <= nt; ++j)
+            for (int i = 1; i <= nt; ++i) {
+              const int64_t c = cell_id(o, tx, ty, tz, i - 1, j - 1, k - 1);
+              const int tt[3] = {tx, ty, tz}, ijk[3] = {i, j, k};
+              for (int64_t ip = cs[c]; ip < cs[c + 1]; ++ip) {
+                int i1[3];
+                float dx1[3], dx2[3];
+                for (int d = 0; d < 3; ++d) {
+                  const double g = cube_dadd((double)(tt[d] * nt) + (double)(ijk[d] - 1), cube_xfrac(o.xp[3 * ip + d], o.izipx));
+                  const float t_ = (float)cube_dsub(g, 0.5);
+                  i1[d] = (int)floorf(t_) + 1;
+                  dx1[d] = cube_fsub((float)i1[d], t_);
+                  dx2[d] = cube_fsub(1.f, dx1[d]);
+                }
+                const int cx[8][3] = {{0,0,0},{1,0,0},{0,1,0},{0,0,1},{0,1,1},{1,0,1},{1,1,0},{1,1,1}};
+                for (int d = 0; d < 3; ++d) {
+                  double v = cube_vdecode(tanf_code(o, o.vp[3 * ip + d]), coef);
+                  for (int c8 = 0; c8 < 8; ++c8) {
+                    // force_c(:,0:nc+1) with periodic halo: node index idx in 0..nc+1
+                    const int fi = ((i1[0] + cx[c8][0] - 1) % nc + nc) % nc;
+                    const int fj = ((i1[1] + cx[c8][1] - 1) % nc + nc) % nc;
+                    const int fk = ((i1[2] + cx[c8][2] - 1) % nc + nc) % nc;
+                    const float fv = o.force_c[(size_t)d * nc * nc * nc + ((size_t)fk * nc + fj) * nc + fi];
+                    float t = cube_fmul(fv, a_mid);
+                    t = cube_fmul(t, dt);
+                    t = cube_fdiv(t, 6.f);
+                    t = cube_fdiv(t, pi_f);
+                    t = cube_fmul(t, cx[c8][0] ? dx2[0] : dx1[0]);
+                    t = cube_fmul(t, cx[c8][1] ? dx2[1] : dx1[1]);
+                    t = cube_fmul(t, cx[c8][2] ? dx2[2] : dx1[2]);
+                    v = cube_dadd(v, (double)t);
+                  }
+                  vmax[d] = std::max(vmax[d], fabs(cube_dadd(v, (double)o.vfield[3 * c + d])));
+                  o.vp[3 * ip + d] = cube_wrap_code(cube_vencode(&o.codec, v, coef), o.izipv);
+                }
+              }
+            }
+  for (int d = 0; d < 3; ++d) s->vmax[d] = (float)vmax[d];
+  s->testrhof = testrhof;
+  s->testrhoc = testrhoc;
+  dt_constraints(o, s);
+  return CUBE_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* ext_pp_force (ext_pp_force.f90:34-143)                                     */
+int ext_pp_force(Orc& o, cube_scalars* s) {
+  const int nt = o.nt, ncb = o.ncb, ncell = o.ncell, nft = o.nft, pr = o.P.pp_range;
+  const int lo = 1 - ncb, nte = o.nte;
+  const double coef = cube_vcoef(&o.codec, s->sigma_vi);
+  const std::vector<int64_t> cs = compact_cell_start(o);
+  const double rsoft = (double)o.P.rsoft;
+  const double mass = (double)s->mass_p_cdm;
+  double ftemp = (double)s->f2_max_pp;  // saved local in the reference: never reset between calls
+  int64_t itest1 = 0, npairs = 0;
+  ExtTile e;
+  const int nfl = nft + 2 * ncell;  // hoc(1-ncell:nft+ncell)
+  std::vector<int64_t> hoc((size_t)nfl * nfl * nfl);
+  std::vector<int64_t> ll;
+  for (int tz = 0; tz < o.nnt; ++tz)
+    for (int ty = 0; ty < o.nnt; ++ty)
+      for (int tx = 0; tx < o.nnt; ++tx) {
+        build_ext(o, cs, tx, ty, tz, e);
+        auto eq = [&](int i, int j, int k) { return ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo); };
+        auto hq = [&](int i, int j, int k) { return ((size_t)(k + ncell - 1) * nfl + (j + ncell - 1)) * nfl + (i + ncell - 1); };
+        std::fill(hoc.begin(), hoc.end(), -1);
+        ll.assign(e.src.size(), -1);
+        // linked list (ext_pp_force.f90:51-73): LIFO per fine cell
+        for (int igz = 0; igz <= nt + 1; ++igz)
+          for (int igy = 0; igy <= nt + 1; ++igy)
+            for (int igx = 0; igx <= nt + 1; ++igx) {
+              const size_t qe = eq(igx, igy, igz);
+              const int g[3] = {igx, igy, igz};
+              for (int64_t l = 0; l < e.rho[qe]; ++l) {
+                const int64_t slot = e.cstart[qe] + l;
+                const int64_t ip = e.src[slot];
+                int iv[3];
+                for (int d = 0; d < 3; ++d) {
+                  const double xv = cube_dadd((double)ncell * (double)(g[d] - 1), cube_dmul((double)ncell, cube_xfrac(o.xp[3 * ip + d], o.izipx)));
+                  iv[d] = (int)floor(xv) + 1;
+                }
+                const size_t h = hq(iv[0], iv[1], iv[2]);
+                ll[slot] = hoc[h];
+                hoc[h] = slot;
+              }
+            }
+        auto xvec = [&](int fi, int32_t code) -> double {
+          const int cidx = (int)floorf(cube_fdiv((float)(fi - 1), 4.f));
+          return cube_dadd((double)ncell * (double)cidx, cube_dmul((double)ncell, cube_xfrac(code, o.izipx)));
+        };
+        for (int igz = 1; igz <= nft; ++igz)
+          for (int igy = 1; igy <= nft; ++igy)
+            for (int igx = 1; igx <= nft; ++igx) {
+              int64_t s1 = hoc[hq(igx, igy, igz)];
+              while (s1 >= 0) {
+                ++itest1;
+                const int64_t ip1 = e.src[s1];
+                double x1[3], v[3], ft[3] = {0, 0, 0};
+                const int g1[3] = {igx, igy, igz};
+                for (int d = 0; d < 3; ++d) {
+                  x1[d] = xvec(g1[d], o.xp[3 * ip1 + d]);
+                  v[d] = cube_vdecode(tanf_code(o, o.vp[3 * ip1 + d]), coef);
+                }
+                for (int kk = igz - pr; kk <= igz + pr; ++kk)
+                  for (int jj = igy - pr; jj <= igy + pr; ++jj)
+                    for (int ii = igx - pr; ii <= igx + pr; ++ii) {
+                      int64_t s2 = hoc[hq(ii, jj, kk)];
+                      const int g2[3] = {ii, jj, kk};
+                      while (s2 >= 0) {
+                        ++npairs;
+                        const int64_t ip2 = e.src[s2];
+                        double x21[3];
+                        for (int d = 0; d < 3; ++d) x21[d] = cube_dsub(xvec(g2[d], o.xp[3 * ip2 + d]), x1[d]);
+                        double rmag = sqrt(cube_dadd(cube_dadd(cube_dmul(x21[0], x21[0]), cube_dmul(x21[1], x21[1])), cube_dmul(x21[2], x21[2])));
+                        if (rmag == 0) rmag = 1.0;
+                        const double rc = cube_ddiv(rmag, (double)o.P.nf_cutoff);
+                        const double rc2 = cube_dmul(rc, rc);
+                        const double rc3 = cube_dmul(rc2, rc);
+                        const double rc5 = cube_dmul(cube_dmul(rc2, rc2), rc);
+                        const double pcut = cube_dadd(cube_dsub(1.0, cube_dmul(1.75, rc3)), cube_dmul(0.75, rc5));
+                        const double r3 = cube_dmul(cube_dmul(rmag, rmag), rmag);
+                        for (int d = 0; d < 3; ++d) {
+                          double fp = cube_dmul(cube_dmul(mass, cube_ddiv(x21[d], r3)), pcut);
+                          if (!(rmag > rsoft)) fp = cube_dmul(fp, 0.0);
+                          ft[d] = cube_dadd(ft[d], fp);
+                        }
+                        s2 = ll[s2];
+                      }
+                    }
+                for (int d = 0; d < 3; ++d) {
+                  double k = cube_dmul(ft[d], (double)s->a_mid);
+                  k = cube_dmul(k, (double)s->dt);
+                  k = cube_ddiv(k, 6.0);
+                  k = cube_ddiv(k, (double)o.codec.pi_f);
+                  v[d] = cube_dadd(v[d], k);
+                }
+                // vp(:,ip1) is written at the physical slot; buffer copies are refreshed by buffer_v
+                for (int d = 0; d < 3; ++d)
+                  o.vp[3 * ip1 + d] = cube_wrap_code(cube_vencode(&o.codec, v[d], coef), o.izipv);
+                const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
+                ftemp = std::max(ftemp, (double)(float)f2);
+                s1 = ll[s1];
+              }
+            }
+      }
+  s->f2_max_pp = (float)ftemp;
+  const float pi_f = o.codec.pi_f;
+  const float GG = cube_fdiv(cube_fdiv(1.0f, 6.0f), pi_f);
+  s->dt_pp = cube_fdiv(cube_fmul(1.0f, sqrtf(1.0f)), cube_fmul(cube_fmul(sqrtf(s->f2_max_pp), s->a_mid), GG));
+  s->itest1 = itest1;
+  s->npairs = npairs;
+  if (itest1 != o.np) { o.err = "PP did not touch every particle once"; return CUBE_ERR_STATE; }
+  return CUBE_OK;
+}
+
+void setup_sizes(Orc& o, const cube_params* p) {
+  o.P = *p;
+  o.nc = p->nc; o.nnt = p->nnt; o.nt = p->nc / p->nnt; o.ncell = p->ncell; o.ncb = p->ncb;
+  o.nte = o.nt + 2 * o.ncb; o.nf = o.nc * o.ncell; o.nft = o.nt * o.ncell;
+  o.nfb = o.ncb * o.ncell; o.nfe = o.nft + 2 * o.nfb; o.nfc = p->nf_cutoff;
+  o.izipx = p->izipx; o.izipv = p->izipv;
+  o.codec.pi_f = 4.0f * atanf(1.0f);
+  o.codec.sqrt_pio2_f = sqrtf(o.codec.pi_f / 2.0f);
+  o.nvbin = 1 << (8 * p->izipv);
+  o.codec.nvbin_m1_f = (float)(o.nvbin - 1);
+  o.codec.izipx = p->izipx; o.codec.izipv = p->izipv;
+  o.codec.vrel_boost = p->vrel_boost;
+  o.codec.x_resolution = (p->izipx == 1) ? 1.0 / 256.0 : 1.0 / 65536.0;
+  o.tan_table.resize(o.nvbin);
+  for (int c = -o.nvbin / 2; c < o.nvbin / 2; ++c) o.tan_table[c + o.nvbin / 2] = tanf(cube_varg(&o.codec, c));
+}
+
+}  // namespace
+
+/* ========================================================================= */
+/* C interface for the tests (ctypes)                                         */
+extern "C" {
+
+void* orc_create(const cube_params* p, const float* fk_table, const float* ck_table, int build_kernels) {
+  Orc* o = new Orc();
+  setup_sizes(*o, p);
+  o->fk_table.assign(fk_table, fk_table + (size_t)3 * p->nf_cutoff * p->nf_cutoff * p->nf_cutoff);
+  o->ck_table.assign(ck_table, ck_table + 3 * 64);
+  o->np = 0;
+  if (build_kernels) { kernel_f(*o); kernel_c(*o); }
+  return o;
+}
+
+void orc_destroy(void* h) { delete (Orc*)h; }
+
+const char* orc_error(void* h) { return ((Orc*)h)->err.c_str(); }
+
+int orc_load_state(void* h, int64_t np, const void* xp, const void* vp, const int32_t* pid,
+                   const int32_t* rhoc, const float* vfield) {
+  Orc& o = *(Orc*)h;
+  const int64_t ncells = (int64_t)o.nc * o.nc * o.nc;
+  o.np = np;
+  o.xp.resize(3 * np); o.vp.resize(3 * np);
+  for (int64_t q = 0; q < 3 * np; ++q) {
+    o.xp[q] = o.izipx == 1 ? ((const int8_t*)xp)[q] : ((const int16_t*)xp)[q];
+    o.vp[q] = o.izipv == 1 ? ((const int8_t*)vp)[q] : ((const int16_t*)vp)[q];
+  }
+  if (pid) o.pid.assign(pid, pid + np); else o.pid.clear();
+  o.rhoc.assign(rhoc, rhoc + ncells);
+  o.vfield.assign(vfield, vfield + 3 * ncells);
+  int64_t tot = 0;
+  for (int64_t c = 0; c < ncells; ++c) tot += o.rhoc[c];
+  if (tot != np) { o.err = "sum(rhoc) != nplocal"; return CUBE_ERR_PARAM; }
+  return CUBE_OK;
+}
+
+int orc_store_state(void* h, int64_t* np, void* xp, void* vp, int32_t* pid, int32_t* rhoc, float* vfield) {
+  Orc& o = *(Orc*)h;
+  const int64_t ncells = (int64_t)o.nc * o.nc * o.nc;
+  if (np) *np = o.np;
+  for (int64_t q = 0; q < 3 * o.np; ++q) {
+    if (xp) { if (o.izipx == 1) ((int8_t*)xp)[q] = (int8_t)o.xp[q]; else ((int16_t*)xp)[q] = (int16_t)o.xp[q]; }
+    if (vp) { if (o.izipv == 1) ((int8_t*)vp)[q] = (int8_t)o.vp[q]; else ((int16_t*)vp)[q] = (int16_t)o.vp[q]; }
+  }
+  if (pid && !o.pid.empty()) memcpy(pid, o.pid.data(), sizeof(int32_t) * o.np);
+  if (rhoc) memcpy(rhoc, o.rhoc.data(), sizeof(int32_t) * ncells);
+  if (vfield) memcpy(vfield, o.vfield.data(), sizeof(float) * 3 * ncells);
+  return CUBE_OK;
+}
+
+int orc_update_x(void* h, cube_scalars* s) { return update_xp(*(Orc*)h, s); }
+
+int orc_ext_pp_force(void* h, cube_scalars* s) { return ext_pp_force(*(Orc*)h, s); }
+
+/* deposit_mode 0: reference FP32 order; 1: 64-bit fixed point */
+int orc_particle_mesh(void* h, cube_scalars* s, int deposit_mode) {
+  return particle_mesh(*(Orc*)h, s, deposit_mode, nullptr);
+}
+
+/* particle_mesh with externally supplied force meshes ([3][nf^3] and [3][nc^3]) */
+int orc_particle_mesh_with_force(void* h, cube_scalars* s, int deposit_mode, const float* fine,
+                                 const float* coarse) {
+  Orc& o = *(Orc*)h;
+  std::vector<float> f(fine, fine + (size_t)3 * o.nf * o.nf * o.nf);
+  std::vector<float> c(coarse, coarse + (size_t)3 * o.nc * o.nc * o.nc);
+  KickIn k{&f, &c};
+  return particle_mesh(o, s, deposit_mode, &k);
+}
+
+/* which: 0 rho_f (nf^3), 1 r3 (nc^3), 2 force_f (3 nf^3), 3 force_c (3 nc^3),
+ *        4 kern_f (3 nfe nfe (nfe/2+1), double), 5 kern_c (3 nc nc (nc/2+1), double) */
+int64_t orc_fetch(void* h, int which, void* out, int64_t cap) {
+  Orc& o = *(Orc*)h;
+  const void* src = nullptr;
+  int64_t n = 0;
+  size_t es = 4;
+  switch (which) {
+    case 0: src = o.rho_f_global.data(); n = o.rho_f_global.size(); break;
+    case 1: src = o.r3.data(); n = o.r3.size(); break;
+    case 2: src = o.force_f_global.data(); n = o.force_f_global.size(); break;
+    case 3: src = o.force_c.data(); n = o.force_c.size(); break;
+    case 4: src = o.kern_f.data(); n = o.kern_f.size(); es = 8; break;
+    case 5: src = o.kern_c.data(); n = o.kern_c.size(); es = 8; break;
+    default: return -1;
+  }
+  if (n > cap) return -1;
+  memcpy(out, src, es * n);
+  return n;
+}
+
+/* dt constraints only (pm.f90:427-443) */
+void orc_dt_constraints(void* h, cube_scalars* s) { dt_constraints(*(Orc*)h, s); }
+
+/* codec helpers for the tests */
+float orc_tanf_code(void* h, int code) { return tanf_code(*(Orc*)h, code); }
+double orc_atan(double x) { return cube_atan(x); }
+int orc_vencode(void* h, double v, float sigma) {
+  Orc& o = *(Orc*)h;
+  return cube_wrap_code(cube_vencode(&o.codec, v, cube_vcoef(&o.codec, sigma)), o.izipv);
+}
+double orc_vdecode(void* h, int code, float sigma) {
+  Orc& o = *(Orc*)h;
+  return cube_vdecode(tanf_code(o, code), cube_vcoef(&o.codec, sigma));
+}
+/* same encode with the C library's atan instead of the project arctangent */
+int orc_vencode_libm(void* h, double v, float sigma) {
+  Orc& o = *(Orc*)h;
+  const double coef = cube_vcoef(&o.codec, sigma);
+  const double q = ((double)o.codec.nvbin_m1_f * atan(coef * v)) / (double)o.codec.pi_f;
+  return cube_wrap_code((int64_t)round(q), o.izipv);
+}
+double orc_tree_sum(const double* a, int64_t n) { return cube_tree_sum(std::vector<double>(a, a + n)); }
+
+}  // extern "C"
+
+extern "C" {
+/* forward r2c of an n^3 real array (x fastest) into (n/2+1) x n x n complex (interleaved re,im) */
+void orc_rfft3(const double* in, int n, double* out) {
+  std::vector<cd> h;
+  orc::rfft3_forward(in, h, n);
+  memcpy(out, h.data(), sizeof(cd) * h.size());
+}
+}

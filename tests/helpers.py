@@ -1,0 +1,42 @@
+"""Shared set-up of the parity tests: seeded states and scalar blocks."""
+from __future__ import annotations
+
+import numpy as np
+
+from cube_nufluid_b200 import ic
+from cube_nufluid_b200.abi import CubeScalars, make_params
+from cube_nufluid_b200.cube import scalars_from_ic
+
+
+def small_state(nc=16, nnt=2, box=100.0, z_i=49.0, seed=1, izipx=2, izipv=2, amplitude=1.0):
+    st = ic.zeldovich(nc, nnt, box=box, z_i=z_i, seed=seed, izipx=izipx, izipv=izipv, amplitude=amplitude)
+    p = make_params(nc, nnt, box=box, izipx=izipx, izipv=izipv)
+    s = scalars_from_ic(st)
+    return st, p, s
+
+
+def clustered_state(nc=16, nnt=2, npart=40000, seed=3, izipx=2, izipv=2, box=100.0):
+    st = ic.clustered(nc, nnt, npart, seed, izipx=izipx, izipv=izipv, box=box)
+    p = make_params(nc, nnt, box=box, izipx=izipx, izipv=izipv)
+    s = scalars_from_ic(st)
+    return st, p, s
+
+
+def copy_scalars(s: CubeScalars) -> CubeScalars:
+    return s.copy()
+
+
+def first_step_scalars(p, s, a_next):
+    """timestep() of the library for both arms, so oracle and GPU see the same dt."""
+    from cube_nufluid_b200.cube import load_library
+    import ctypes as C
+    L = load_library()
+    hit = C.c_int32(0)
+    L.cube_timestep(C.byref(p), C.byref(s), a_next, C.byref(hit))
+    return s
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b ** 2)), 1e-300))

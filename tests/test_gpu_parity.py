@@ -1,0 +1,180 @@
+"""GPU parity tests: the CUDA library through its C-ABI against the CPU oracle.
+
+Bars: integer deposit, positions and velocity
+re-quantisation bit-exact; forces within FP32 tolerance of the FP64-FFT oracle
+(relative RMS <= 1e-5).  Sizes are small enough for the oracle to finish in
+seconds; crowded cells come from the clustered test state.
+"""
+import numpy as np
+import pytest
+
+from helpers import clustered_state, first_step_scalars, rel_rms, small_state
+from oracle_ref import Oracle
+from cube_nufluid_b200 import Cube
+from cube_nufluid_b200.abi import make_params
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5   # relative RMS, FP32 FFT vs FP64 oracle
+
+
+def pair(st, p, tables, build=True):
+    fk, ck = tables
+    o = Oracle(p, fk, ck, build_kernels=build)
+    o.load(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    g = Cube(p, np_capacity=st.np + 1024, fk_table=fk, ck_table=ck)
+    g.load_state(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    return o, g
+
+
+def assert_same_state(o, g):
+    a = o.store()
+    b = g.store_state()
+    for name, x, y in zip(("xp", "vp", "pid", "rhoc", "vfield"), a, b):
+        assert x.shape == y.shape, name
+        if x.dtype.kind == "f":
+            assert np.array_equal(x.view(np.int32), y.view(np.int32)), name
+        else:
+            nbad = int(np.count_nonzero(x != y))
+            assert nbad == 0, f"{name}: {nbad} entries differ"
+
+
+@pytest.mark.parametrize("kind,izip", [("smooth", 2), ("clustered", 2), ("clustered", 1)])
+def test_update_x_bit_exact(tables, kind, izip):
+    if kind == "smooth":
+        st, p, s = small_state(nc=16, nnt=2, seed=21, izipx=izip, izipv=izip, amplitude=8.0)
+        s.dt_old, s.dt = 2.0, 2.0
+    else:
+        st, p, s = clustered_state(nc=16, nnt=2, seed=22, izipx=izip, izipv=izip)
+        s.dt_old, s.dt = 60.0, 60.0
+    o, g = pair(st, p, tables, build=False)
+    so, sg = s.copy(), s.copy()
+    o.update_x(so)
+    g.update_x(sg)
+    assert so.nlayer == sg.nlayer and so.nlayer >= 3
+    assert_same_state(o, g)
+    assert so.sigma_vi_new == sg.sigma_vi_new
+    assert so.std_vsim == sg.std_vsim and so.std_vsim_c == sg.std_vsim_c and so.std_vsim_res == sg.std_vsim_res
+    # particles did move between cells
+    assert not np.array_equal(g.store_state()[3], st.rhoc)
+
+
+@pytest.fixture(scope="module")
+def pm_pair(tables):
+    st, p, s = clustered_state(nc=16, nnt=2, seed=31)
+    o, g = pair(st, p, tables)
+    s.a, s.a_mid, s.dt = 0.5, 0.5, 20.0
+    so, sg = s.copy(), s.copy()
+    o.particle_mesh(so, 1)
+    g.particle_mesh(sg)
+    return st, p, s, o, g, so, sg
+
+
+def test_deposit_bit_exact(pm_pair):
+    st, p, s, o, g, so, sg = pm_pair
+    assert np.array_equal(o.fetch(0).view(np.int32), g.fetch(0).view(np.int32))
+    assert np.array_equal(o.fetch(1).view(np.int32), g.fetch(1).view(np.int32))
+    assert so.testrhoc == pytest.approx(sg.testrhoc, rel=1e-12)
+    assert sg.testrhof == pytest.approx(st.np * st.mass_p_cdm, rel=1e-9)
+
+
+def test_forces_match_fp64_oracle(pm_pair):
+    st, p, s, o, g, so, sg = pm_pair
+    assert rel_rms(g.fetch(2), o.fetch(2)) <= FORCE_TOL
+    assert rel_rms(g.fetch(3), o.fetch(3)) <= FORCE_TOL
+    assert sg.f2_max_fine == pytest.approx(so.f2_max_fine, rel=1e-4)
+    assert sg.f2_max_coarse == pytest.approx(so.f2_max_coarse, rel=1e-4)
+
+
+def test_kicked_velocities_close(pm_pair):
+    st, p, s, o, g, so, sg = pm_pair
+    vo = o.store()[1].astype(np.int32)
+    vg = g.store_state()[1].astype(np.int32)
+    assert np.max(np.abs(vo - vg)) <= 1
+    assert np.mean(vo != vg) < 1e-3
+    assert sg.dt_fine == pytest.approx(so.dt_fine, rel=1e-4)
+    assert sg.dt_coarse == pytest.approx(so.dt_coarse, rel=1e-4)
+    assert sg.sigma_vi == so.sigma_vi
+
+
+@pytest.mark.parametrize("izip", [2, 1])
+def test_kick_bit_exact_on_identical_forces(tables, izip):
+    st, p, s = clustered_state(nc=16, nnt=2, seed=41, izipx=izip, izipv=izip)
+    o, g = pair(st, p, tables, build=False)
+    s.a, s.a_mid, s.dt = 0.5, 0.5, 20.0
+    s.sigma_vi_new = np.float32(s.sigma_vi * 1.01)
+    rng = np.random.default_rng(9)
+    nf, nc = 64, 16
+    fine = rng.normal(0, 2.0, 3 * nf ** 3).astype(np.float32)
+    coarse = rng.normal(0, 0.5, 3 * nc ** 3).astype(np.float32)
+    so, sg = s.copy(), s.copy()
+    o.particle_mesh_with_force(so, fine, coarse, 1)
+    g.kick_with_force(sg, fine, coarse)
+    assert_same_state(o, g)
+    assert list(so.vmax) == list(sg.vmax)
+
+
+@pytest.mark.parametrize("izip", [2, 1])
+def test_pp_bit_exact(tables, izip):
+    st, p, s = clustered_state(nc=16, nnt=2, seed=51, izipx=izip, izipv=izip)
+    p.ext_pp_force = 1
+    o, g = pair(st, p, tables, build=False)
+    s.a_mid, s.dt = 0.5, 5.0
+    so, sg = s.copy(), s.copy()
+    o.ext_pp_force(so)
+    g.ext_pp_force(sg)
+    assert so.itest1 == sg.itest1 == st.np
+    assert so.npairs == sg.npairs
+    assert so.f2_max_pp == sg.f2_max_pp
+    assert so.dt_pp == sg.dt_pp
+    assert_same_state(o, g)
+
+
+def test_fine_green_octant_matches_closed_form(tables):
+    from test_oracle import separable_green
+    fk, ck = tables
+    st, p, s = small_state(nc=16, nnt=2, seed=1)
+    g = Cube(p, np_capacity=st.np, fk_table=fk, ck_table=ck)
+    nf = 64
+    kp = nf // 2 + 1
+    got = g.fetch(4).reshape(3, kp, kp, kp).astype(np.float64)
+    ref = separable_green(fk, nf) / nf ** 3
+    assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
+
+
+def test_radix3_mesh_forces(tables):
+    # nc=24 -> nf=96 = 3*2^5 exercises the radix-3 stages of the FFT
+    st, p, s = clustered_state(nc=24, nnt=2, npart=60000, seed=61)
+    o, g = pair(st, p, tables)
+    s.a, s.a_mid, s.dt = 0.5, 0.5, 20.0
+    so, sg = s.copy(), s.copy()
+    o.particle_mesh(so, 1)
+    g.particle_mesh(sg)
+    assert np.array_equal(o.fetch(0).view(np.int32), g.fetch(0).view(np.int32))
+    assert rel_rms(g.fetch(2), o.fetch(2)) <= FORCE_TOL
+    assert rel_rms(g.fetch(3), o.fetch(3)) <= FORCE_TOL
+
+
+def test_multi_step_run_tracks_oracle(tables):
+    # three full steps (timestep, update_x, particle_mesh) on a Zel'dovich box
+    st, p, s = small_state(nc=16, nnt=2, seed=71, amplitude=4.0)
+    o, g = pair(st, p, tables)
+    so, sg = s.copy(), s.copy()
+    for _ in range(3):
+        first_step_scalars(p, so, 0.0)
+        first_step_scalars(p, sg, 0.0)
+        assert so.dt == sg.dt
+        o.update_x(so)
+        g.update_x(sg)
+        o.particle_mesh(so, 1)
+        g.particle_mesh(sg)
+    xo, vo, po, ro, _ = o.store()
+    xg, vg, pg, rg, _ = g.store_state()
+    # compare per particle by PID: positions to the last code, velocities to one code
+    io, ig = np.argsort(po), np.argsort(pg)
+    assert np.array_equal(po[io], pg[ig])
+    dx = np.abs(xo[io].astype(np.int32) - xg[ig].astype(np.int32))
+    dx = np.minimum(dx, 65536 - dx)
+    assert np.mean(dx == 0) > 0.99 and dx.max() <= 2
+    dv = np.abs(vo[io].astype(np.int32) - vg[ig].astype(np.int32))
+    assert np.mean(dv == 0) > 0.99
