@@ -100,9 +100,24 @@ class ClockSampler:
 
 
 def make_state(cfg, seed):
+    """Seeded Zel'dovich state; cached under $TMPDIR so repeated runs on one host skip the host-side IC."""
+    import pickle
+    import tempfile
     from cube_nufluid_b200 import ic
-    return ic.zeldovich(cfg["nc"], cfg["nnt"], box=cfg["box"], z_i=cfg["z_i"], seed=seed,
-                        izipx=cfg["izip"], izipv=cfg["izip"])
+    key = f"cube_ic_{cfg['nc']}_{cfg['nnt']}_{cfg['box']}_{cfg['z_i']}_{cfg['izip']}_{seed}.pkl"
+    path = os.path.join(tempfile.gettempdir(), key)
+    if os.path.exists(path):
+        with open(path, "rb") as f:
+            return pickle.load(f)
+    st = ic.zeldovich(cfg["nc"], cfg["nnt"], box=cfg["box"], z_i=cfg["z_i"], seed=seed,
+                      izipx=cfg["izip"], izipv=cfg["izip"])
+    try:
+        with open(path + ".tmp", "wb") as f:
+            pickle.dump(st, f, protocol=4)
+        os.replace(path + ".tmp", path)
+    except OSError:
+        pass
+    return st
 
 
 def algorithmic_bytes(cfg, npart):

@@ -504,6 +504,20 @@ int64_t cube_debug_fetch(cube_ctx* ctx, int32_t which, void* host, int64_t capac
   return e == cudaSuccess ? n : -1;
 }
 
+int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io) {
+  if (!ctx || !io) return CUBE_ERR_PARAM;
+  if (!ctx->state_loaded) return CUBE_ERR_STATE;
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dscal, 0, sizeof(DevScal), ctx->stream));
+  int rc = cube_deposit(ctx, io);
+  if (rc) return rc;
+  unsigned long long mt[2];
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(mt, ctx->red_tmp, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  if ((rc = check_device_error(ctx))) return rc;
+  io->testrhof = (double)mt[0] * (1.0 / 4294967296.0);
+  io->testrhoc = (double)mt[1] * (1.0 / 4294967296.0);
+  return CUBE_OK;
+}
+
 int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float* fine_force,
                                    const float* coarse_force) {
   if (!ctx || !io || !fine_force || !coarse_force) return CUBE_ERR_PARAM;

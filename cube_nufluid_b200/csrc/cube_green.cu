@@ -9,7 +9,8 @@
  *   Im K_d(k) = sum_a T_d(a) * S_d(k_d, a_d) * C(k_e, a_e) * C(k_f, a_f),
  *   S(k,a) = -2 sin(2 pi k a/nf) (a > 0),  C(k,0) = 1,  C(k,a) = 2 cos(2 pi k a/nf),
  * evaluated on the device in FP64 in three passes (x, y, z) over the octant
- * 0 <= kx,ky,kz <= nf/2 and stored as FP32 divided by nf^3.
+ * 0 <= kx,ky,kz <= nf/2 and stored as FP32 divided by nf^3, layout
+ * [d][ky][kx][kz] (kz fastest, the order in which the z pass reads it).
  *
  * Coarse level (kernel_c.f90:16-117, LRCKCORR on): ck = -r/r^3 on the periodic
  * coarse mesh (fine-cell units), the 4^3 corner replaced by the matching table
@@ -61,13 +62,14 @@ __global__ void k_green_y(const double* __restrict__ s1, int nfc, int n, int d, 
   }
 }
 
-// K[kz][ky][kx] = sum_az S2[kx][ky][az] F_z(kz,az) / n^3
+// K[ky][kx][kz] = sum_az S2[kx][ky][az] F_z(kz,az) / n^3
 __global__ void k_green_z(const double* __restrict__ s2, int nfc, int n, int d, float* __restrict__ kern) {
   const int kp = n / 2 + 1;
   const int64_t tot = (int64_t)kp * kp * kp;
   const double inv = 1.0 / ((double)n * n * n);
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < tot; q += (int64_t)gridDim.x * blockDim.x) {
-    const int kx = q % kp, ky = (q / kp) % kp, kz = (int)(q / ((int64_t)kp * kp));
+    // octant layout [ky][kx][kz], kz fastest (the z pass reads columns along kz)
+    const int kz = q % kp, kx = (q / kp) % kp, ky = (int)(q / ((int64_t)kp * kp));
     double acc = 0.0;
     for (int az = 0; az < nfc; ++az) acc += s2[((size_t)kx * kp + ky) * nfc + az] * fac(kz, az, n, d == 2);
     kern[(size_t)d * tot + q] = (float)(acc * inv);
@@ -218,7 +220,7 @@ int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table
             double v = C.imag();
             if (kk[d] == nc / 2) v = 0.0;  // odd in k_d: exactly zero on the Nyquist plane
             else if (!(kr > 8.0 || kk[d] == 0)) v = v * 0.25 * pi * ks[d] / ks2 / D.imag();
-            oct[(size_t)d * kp * kp * kp + ((size_t)kz * kp + ky) * kp + kx] = (float)(v / (double)n3);
+            oct[(size_t)d * kp * kp * kp + ((size_t)ky * kp + kx) * kp + kz] = (float)(v / (double)n3);
           }
     }
     CUBE_CUDA_TRY(ctx, cudaMemcpy(ctx->coarse.kern, oct.data(), sizeof(float) * oct.size(), cudaMemcpyHostToDevice));

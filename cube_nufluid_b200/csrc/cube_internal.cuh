@@ -136,6 +136,7 @@ __device__ __forceinline__ int64_t cube_cell_of(int gx, int gy, int gz, int nt, 
 int cube_rebin(cube_ctx* ctx, cube_scalars* io);
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits);
+int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, int* rc);
 int cube_kick(cube_ctx* ctx, cube_scalars* io);
 int cube_pp(cube_ctx* ctx, cube_scalars* io);
 int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table);

@@ -274,7 +274,7 @@ __global__ void k_fft_z_green(const float2* __restrict__ in, float2* __restrict_
       float kv = 0.f;
       if (c < nk) {
         const int fz = kz <= nh ? kz : n - kz;
-        kv = __ldg(&K[((size_t)fz * kp + fy) * kp + kx]);
+        kv = __ldg(&K[((size_t)fy * kp + kx) * kp + fz]);
         if (d == 1) kv *= sy;
         if (d == 2 && kz > nh) kv = -kv;
       }
@@ -361,6 +361,7 @@ static int col_pass(cube_ctx* ctx, MeshLevel& L, float* data, int ncomp, int alo
 int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
   const int n = L.n;
   int rc;
+  if (!ctx->P.reserved[0] && cube_fft_poisson_fast(ctx, L, f2_bits, &rc)) return rc;
   // forward r2c of the density, in place
   if ((rc = cube_fft_r2c_x(ctx, L, L.rho, 0, 1, nullptr))) return rc;
   if ((rc = col_pass(ctx, L, L.rho, 1, 0, -1.f))) return rc;

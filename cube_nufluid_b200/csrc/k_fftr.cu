@@ -1,0 +1,378 @@
+/*
+ * k_fftr.cu -- register-resident FFT passes for power-of-two meshes.
+ *
+ * A length N = R*T transform runs on a group of T threads (T <= 32, inside
+ * one warp): with n = t + T*q and k = k1 + R*k2,
+ *   X[k1 + R*k2] = sum_t W_N^{t k1} W_T^{t k2} sum_q x[t + T q] W_R^{q k1}
+ * so each thread does one R-point DFT in registers (over q), multiplies by
+ * W_N^{t k1}, the group exchanges once through shared memory (swizzled so
+ * neither side of the transpose has bank conflicts), and each thread does
+ * R/T T-point DFTs in registers (over t).  Only __syncwarp is needed inside a
+ * transform.  Sizes: 1024 = 32*32, 512 = 32*16, 256 = 16*16, 128 = 16*8,
+ * 64 = 8*8, 32 = 8*4; other sizes use the shared-memory Stockham passes of
+ * k_fft.cu.
+ *
+ * Passes (same roles as in k_fft.cu):
+ *   x r2c   : RB row pairs per CTA packed as complex rows
+ *   column  : TK consecutive kx columns per CTA (y or z direction)
+ *   z+Green : forward along z, the spectrum kept in registers, then for
+ *             each component d: x i*K_d on the way into the inverse FFT
+ *   x c2r   : the three force components of RB row pairs, max f^2 fused
+ */
+#include "cube_internal.cuh"
+
+#include <utility>
+
+namespace {
+
+// cos(pi*k/16), k = 0..8
+__device__ constexpr float kC16[9] = {1.0f,
+                                      0.98078528040323044913f,
+                                      0.92387953251128675613f,
+                                      0.83146961230254523708f,
+                                      0.70710678118654752440f,
+                                      0.55557023301960222474f,
+                                      0.38268343236508977173f,
+                                      0.19509032201612826785f,
+                                      0.0f};
+
+__device__ constexpr float cos16(int j) {  // cos(pi j / 16), any integer j
+  return (j & 31) <= 8    ? kC16[j & 31]
+         : (j & 31) <= 16 ? -kC16[16 - (j & 31)]
+         : (j & 31) <= 24 ? -kC16[(j & 31) - 16]
+                          : kC16[32 - (j & 31)];
+}
+__device__ constexpr float sin16(int j) { return cos16(8 - j); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__host__ __device__ constexpr int bitrev(int L, int i) {
+  int r = 0;
+  for (int b = 1; b < L; b <<= 1) {
+    r = (r << 1) | (i & 1);
+    i >>= 1;
+  }
+  return r;
+}
+
+template <int L, int I>
+struct BitRev {
+  static constexpr int value = bitrev(L, I);
+};
+
+// bit-reversal permutation with every index fixed at compile time (keeps v in registers)
+template <int L, int... I>
+__device__ __forceinline__ void bitrev_perm(float2* v, std::integer_sequence<int, I...>) {
+  const float2 t[L] = {v[BitRev<L, I>::value]...};
+  ((v[I] = t[I]), ...);
+}
+
+// one radix-2 butterfly stage of span LEN (twiddles are compile-time constants)
+template <int L, int SIGN, int LEN>
+__device__ __forceinline__ void dft_stage(float2* v) {
+#pragma unroll
+  for (int i = 0; i < L; i += LEN) {
+#pragma unroll
+    for (int j = 0; j < LEN / 2; ++j) {
+      const int e = j * (32 / LEN);  // exponent in units of 2 pi/32
+      float2 b = v[i + j + LEN / 2];
+      if (e == 0) {
+      } else if (e == 8) {  // w = SIGN * i
+        b = make_float2(-SIGN * b.y, SIGN * b.x);
+      } else {
+        const float2 w = make_float2(cos16(e), SIGN * sin16(e));
+        b = cmul(b, w);
+      }
+      const float2 a = v[i + j];
+      v[i + j] = make_float2(a.x + b.x, a.y + b.y);
+      v[i + j + LEN / 2] = make_float2(a.x - b.x, a.y - b.y);
+    }
+  }
+  if constexpr (LEN < L) dft_stage<L, SIGN, 2 * LEN>(v);
+}
+
+// in-register DFT of length L (power of two <= 32) on v[0..L-1], natural order out;
+// SIGN = -1 forward (exp(-2 pi i jk/L)), +1 inverse.  Decimation in time.
+template <int L, int SIGN>
+__device__ __forceinline__ void dft_reg(float2* v) {
+  bitrev_perm<L>(v, std::make_integer_sequence<int, L>{});
+  if constexpr (L > 1) dft_stage<L, SIGN, 2>(v);
+}
+
+// sequence element n at s[n*ES]; ROW layout has ES = 1 and a padded exchange,
+// COL layout has ES = pitch of the interleaved columns and a swizzled exchange
+template <int R, int T, bool ROW>
+__device__ __forceinline__ int xidx(int k1, int t, int es) {
+  if (ROW) return k1 * (T + 1) + t;
+  return (k1 * T + ((t + k1) & (T - 1))) * es;
+}
+
+// stage 1 (R-point DFT + twiddle) from registers v, exchange, stage 2; result
+// in natural order in s.  The T threads of the group call it together.
+template <int N, int R, int T, int SIGN, bool ROW>
+__device__ __forceinline__ void fft_from_regs(float2* v, float2* s, int es, int t, const float2* __restrict__ tw) {
+  dft_reg<R, SIGN>(v);
+#pragma unroll
+  for (int k1 = 1; k1 < R; ++k1) {
+    float2 w = __ldg(&tw[(t * k1) & (N - 1)]);
+    if (SIGN > 0) w.y = -w.y;
+    v[k1] = cmul(v[k1], w);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k1 = 0; k1 < R; ++k1) s[xidx<R, T, ROW>(k1, t, es)] = v[k1];
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < R / T; ++m)
+#pragma unroll
+    for (int tt = 0; tt < T; ++tt) v[m * T + tt] = s[xidx<R, T, ROW>(t + T * m, tt, es)];
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < R / T; ++m) dft_reg<T, SIGN>(v + m * T);
+#pragma unroll
+  for (int m = 0; m < R / T; ++m)
+#pragma unroll
+    for (int k2 = 0; k2 < T; ++k2) s[(t + T * m + R * k2) * (ROW ? 1 : es)] = v[m * T + k2];
+  __syncwarp();
+}
+
+template <int N, int R, int T, int SIGN, bool ROW>
+__device__ __forceinline__ void fft_seq(float2* s, int es, int t, const float2* __restrict__ tw) {
+  float2 v[R];
+  const int e = ROW ? 1 : es;
+#pragma unroll
+  for (int q = 0; q < R; ++q) v[q] = s[(t + T * q) * e];
+  fft_from_regs<N, R, T, SIGN, ROW>(v, s, es, t, tw);
+}
+
+// ---------------------------------------------------------------------------
+// column pass: TK columns (kx0..kx0+TK-1) of length N, element j at b + j*jstride
+template <int N, int R, int T, int TK, int SIGN>
+__global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_t comp_stride, int ncol,
+                                                long long jstride, long long ostride,
+                                                const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  constexpr int P = TK + 1;
+  const int kx0 = blockIdx.x * TK;
+  const int nk = min(TK, ncol - kx0);
+  float2* b = base + blockIdx.z * comp_stride + (size_t)blockIdx.y * ostride + kx0;
+  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+    const int j = i / TK, c = i - j * TK;
+    sm[j * P + c] = (c < nk) ? b[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  fft_seq<N, R, T, SIGN, false>(sm + g, P, t, tw);
+  __syncthreads();
+  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+    const int j = i / TK, c = i - j * TK;
+    if (c < nk) b[(size_t)j * jstride + c] = sm[j * P + c];
+  }
+}
+
+// fused z pass with the Green multiply (kernel octant [d][ky][kx][kz], kz fastest)
+template <int N, int R, int T, int TK>
+__global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in, float2* __restrict__ out0,
+                                                   size_t comp_stride, int ncol, long long jstride,
+                                                   long long ostride, const float2* __restrict__ tw,
+                                                   const float* __restrict__ kern, int kp) {
+  extern __shared__ float2 sm[];
+  constexpr int P = TK + 1;
+  const int kx0 = blockIdx.x * TK;
+  const int nk = min(TK, ncol - kx0);
+  const int ky = blockIdx.y;
+  const float2* bi = in + (size_t)ky * ostride + kx0;
+  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+    const int j = i / TK, c = i - j * TK;
+    sm[j * P + c] = (c < nk) ? bi[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  float2* s = sm + g;
+  fft_seq<N, R, T, -1, false>(s, P, t, tw);
+  float2 keep[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) keep[q] = s[(t + T * q) * P];
+  constexpr int nh = N / 2;
+  const int fy = ky <= nh ? ky : N - ky;
+  const float sy = ky <= nh ? 1.f : -1.f;
+  const int kx = min(kx0 + g, ncol - 1);
+  const size_t ksz = (size_t)kp * kp * kp;
+  for (int d = 0; d < 3; ++d) {
+    const float* K = kern + d * ksz + ((size_t)fy * kp + kx) * kp;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int kz = t + T * q;
+      const int fz = kz <= nh ? kz : N - kz;
+      float kv = __ldg(&K[fz]);
+      if (d == 1) kv *= sy;
+      if (d == 2 && kz > nh) kv = -kv;
+      v[q] = make_float2(-keep[q].y * kv, keep[q].x * kv);
+    }
+    __syncwarp();
+    fft_from_regs<N, R, T, 1, false>(v, s, P, t, tw);
+    __syncthreads();
+    float2* bo = out0 + d * comp_stride + (size_t)ky * ostride + kx0;
+    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+      const int j = i / TK, c = i - j * TK;
+      if (c < nk) bo[(size_t)j * jstride + c] = sm[j * P + c];
+    }
+    __syncthreads();
+  }
+}
+
+// x pass, r2c: RB row pairs per CTA, rows (z*N + y) at data + row*rp
+template <int N, int R, int T, int RB>
+__global__ void __launch_bounds__(T * RB) k_xr2c(float* __restrict__ data, int rp, int npairs,
+                                                 const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  constexpr int CS = N + R + 8;
+  const int pair0 = blockIdx.x * RB;
+  const int cp = rp / 2;
+  for (int i = threadIdx.x; i < RB * N; i += T * RB) {
+    const int q = i / N, j = i - q * N;
+    const int pr = min(pair0 + q, npairs - 1);
+    const size_t ra = (size_t)(2 * pr) * rp;
+    sm[q * CS + j] = make_float2(data[ra + j], data[ra + rp + j]);
+  }
+  __syncthreads();
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  fft_seq<N, R, T, -1, true>(sm + g * CS, 1, t, tw);
+  __syncthreads();
+  float2* cb = reinterpret_cast<float2*>(data);
+  constexpr int nh = N / 2;
+  for (int i = threadIdx.x; i < RB * (nh + 1); i += T * RB) {
+    const int q = i / (nh + 1), k = i - q * (nh + 1);
+    if (pair0 + q >= npairs) continue;
+    const float2 Zk = sm[q * CS + k];
+    const float2 Zm = sm[q * CS + ((N - k) & (N - 1))];
+    const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    const float2 B = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+    const size_t ra = (size_t)(2 * (pair0 + q)) * cp;
+    cb[ra + k] = A;
+    cb[ra + cp + k] = B;
+  }
+}
+
+// x pass, c2r of the three force components, max(fx^2+fy^2+fz^2) fused
+template <int N, int R, int T, int RB>
+__global__ void __launch_bounds__(T * RB) k_xc2r3(float* __restrict__ data, size_t comp_stride, int rp,
+                                                  int npairs, const float2* __restrict__ tw,
+                                                  unsigned int* __restrict__ f2_bits) {
+  extern __shared__ float2 sm[];
+  constexpr int CS = N + R + 8;
+  const int pair0 = blockIdx.x * RB;
+  const int cp = rp / 2;
+  constexpr int nh = N / 2;
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  for (int c = 0; c < 3; ++c) {
+    const float2* cb = reinterpret_cast<const float2*>(data + c * comp_stride);
+    float2* buf = sm + (size_t)c * RB * CS;
+    for (int i = threadIdx.x; i < RB * N; i += T * RB) {
+      const int q = i / N, k = i - q * N;
+      const int pr = min(pair0 + q, npairs - 1);
+      const size_t ra = (size_t)(2 * pr) * cp;
+      float2 z;
+      if (k == 0 || k == nh) {
+        const float2 A = cb[ra + k], B = cb[ra + cp + k];
+        z = make_float2(A.x, B.x);
+      } else if (k < nh) {
+        const float2 A = cb[ra + k], B = cb[ra + cp + k];
+        z = make_float2(A.x - B.y, A.y + B.x);
+      } else {
+        const float2 A = cb[ra + (N - k)], B = cb[ra + cp + (N - k)];
+        z = make_float2(A.x + B.y, B.x - A.y);
+      }
+      buf[q * CS + k] = z;
+    }
+    __syncthreads();
+    fft_seq<N, R, T, 1, true>(buf + g * CS, 1, t, tw);
+    __syncthreads();
+  }
+  float f2max = 0.f;
+  for (int i = threadIdx.x; i < RB * N; i += T * RB) {
+    const int q = i / N, j = i - q * N;
+    if (pair0 + q >= npairs) continue;
+    const size_t ra = (size_t)(2 * (pair0 + q)) * rp;
+    float fa[3], fb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float2 z = sm[(size_t)c * RB * CS + q * CS + j];
+      float* base = data + c * comp_stride;
+      base[ra + j] = z.x;
+      base[ra + rp + j] = z.y;
+      fa[c] = z.x;
+      fb[c] = z.y;
+    }
+    const float a2 = __fadd_rn(__fadd_rn(__fmul_rn(fa[0], fa[0]), __fmul_rn(fa[1], fa[1])), __fmul_rn(fa[2], fa[2]));
+    const float b2 = __fadd_rn(__fadd_rn(__fmul_rn(fb[0], fb[0]), __fmul_rn(fb[1], fb[1])), __fmul_rn(fb[2], fb[2]));
+    f2max = fmaxf(f2max, fmaxf(a2, b2));
+  }
+  for (int o = 16; o > 0; o >>= 1) f2max = fmaxf(f2max, __shfl_xor_sync(0xffffffffu, f2max, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(f2_bits, __float_as_uint(f2max));
+}
+
+template <int N, int R, int T>
+int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
+  constexpr int TK = (T >= 16) ? 8 : 16;
+  constexpr int RB = (T >= 32) ? 4 : (T >= 16 ? 8 : 16);
+  constexpr int RB3 = (T >= 32) ? 2 : (T >= 16 ? 4 : 8);
+  const int ncol = N / 2 + 1;
+  const long long cp = L.cp;
+  const size_t cstride = (size_t)N * L.plane / 2;
+  const float2* tw = L.plan.tw;
+  // x r2c
+  {
+    const int npairs = N * N / 2;
+    const size_t smem = sizeof(float2) * RB * (N + R + 8);
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, smem, ctx->stream>>>(L.rho, L.rp, npairs, tw);
+    CUBE_LAUNCH_CHECK(ctx);
+  }
+  const size_t csm = sizeof(float2) * (size_t)N * (TK + 1);
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen<N, R, T, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  const dim3 g1((ncol + TK - 1) / TK, N, 1), g3((ncol + TK - 1) / TK, N, 3);
+  // y forward
+  k_col<N, R, T, TK, -1><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.rho), cstride, ncol, cp,
+                                                             (long long)N * cp, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  // z forward, Green, z inverse
+  k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
+                                                            reinterpret_cast<float2*>(L.force), cstride, ncol,
+                                                            (long long)N * cp, cp, tw, L.kern, L.kern_pitch);
+  CUBE_LAUNCH_CHECK(ctx);
+  // y inverse, three components
+  k_col<N, R, T, TK, 1><<<g3, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.force), cstride, ncol, cp,
+                                                            (long long)N * cp, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  // x c2r, three components, max f^2
+  {
+    const int npairs = N * N / 2;
+    const size_t smem = sizeof(float2) * 3 * RB3 * (N + R + 8);
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, T * RB3, smem, ctx->stream>>>(L.force, (size_t)N * L.plane,
+                                                                                    L.rp, npairs, tw, f2_bits);
+    CUBE_LAUNCH_CHECK(ctx);
+  }
+  return CUBE_OK;
+}
+
+}  // namespace
+
+// returns 1 if handled by a register-resident path
+int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, int* rc) {
+  switch (L.n) {
+    case 1024: *rc = run_poisson<1024, 32, 32>(ctx, L, f2_bits); return 1;
+    case 512: *rc = run_poisson<512, 32, 16>(ctx, L, f2_bits); return 1;
+    case 256: *rc = run_poisson<256, 16, 16>(ctx, L, f2_bits); return 1;
+    case 128: *rc = run_poisson<128, 16, 8>(ctx, L, f2_bits); return 1;
+    case 64: *rc = run_poisson<64, 8, 8>(ctx, L, f2_bits); return 1;
+    case 32: *rc = run_poisson<32, 8, 4>(ctx, L, f2_bits); return 1;
+    default: return 0;
+  }
+}

@@ -77,6 +77,8 @@ def load_library():
     L.cube_destroy.restype = None
     L.cube_debug_fetch.argtypes = [vp, C.c_int32, vp, C.c_int64]
     L.cube_debug_fetch.restype = C.c_int64
+    L.cube_debug_deposit.argtypes = [vp, S]
+    L.cube_debug_deposit.restype = C.c_int32
     L.cube_debug_kick_with_force.argtypes = [vp, S, vp, vp]
     L.cube_debug_kick_with_force.restype = C.c_int32
     if L.cube_abi_version() != ABI_VERSION:
@@ -203,6 +205,10 @@ class Cube:
         if got < 0:
             raise CubeError(3, "debug fetch failed")
         return out
+
+    def debug_deposit(self, s: CubeScalars):
+        """Deposit only; fetch(0) / fetch(1) then return the fine / coarse density."""
+        self._check(self.L.cube_debug_deposit(self.h, C.byref(s)))
 
     def kick_with_force(self, s: CubeScalars, fine: np.ndarray, coarse: np.ndarray):
         f = np.ascontiguousarray(fine, dtype=np.float32)

@@ -188,6 +188,11 @@ void cube_destroy(cube_ctx* ctx);
  * Returns the element count written, or -1. */
 int64_t cube_debug_fetch(cube_ctx* ctx, int32_t which, void* host, int64_t capacity);
 
+/* Runs only the fine and coarse CIC deposit of particle_mesh (pm.f90:76-107,
+ * :192-278), so that cube_debug_fetch(0/1) returns the densities before the
+ * FFT reuses their storage.  Writes testrhof and testrhoc. */
+int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io);
+
 /* Uploads a fine (which=2) or coarse (which=3) force mesh and runs only the
  * interpolate+kick of particle_mesh on it (parity of the kick against the oracle
  * on identical forces). */

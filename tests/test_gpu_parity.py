@@ -70,12 +70,16 @@ def pm_pair(tables):
     return st, p, s, o, g, so, sg
 
 
-def test_deposit_bit_exact(pm_pair):
+def test_deposit_bit_exact(pm_pair, tables):
     st, p, s, o, g, so, sg = pm_pair
-    assert np.array_equal(o.fetch(0).view(np.int32), g.fetch(0).view(np.int32))
-    assert np.array_equal(o.fetch(1).view(np.int32), g.fetch(1).view(np.int32))
-    assert so.testrhoc == pytest.approx(sg.testrhoc, rel=1e-12)
-    assert sg.testrhof == pytest.approx(st.np * st.mass_p_cdm, rel=1e-9)
+    g2 = Cube(p, np_capacity=st.np, fk_table=tables[0], ck_table=tables[1])
+    g2.load_state(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    sd = s.copy()
+    g2.debug_deposit(sd)
+    assert np.array_equal(o.fetch(0).view(np.int32), g2.fetch(0).view(np.int32))
+    assert np.array_equal(o.fetch(1).view(np.int32), g2.fetch(1).view(np.int32))
+    assert so.testrhoc == pytest.approx(sd.testrhoc, rel=1e-12)
+    assert sd.testrhof == pytest.approx(st.np * st.mass_p_cdm, rel=1e-9)
 
 
 def test_forces_match_fp64_oracle(pm_pair):
@@ -90,8 +94,10 @@ def test_kicked_velocities_close(pm_pair):
     st, p, s, o, g, so, sg = pm_pair
     vo = o.store()[1].astype(np.int32)
     vg = g.store_state()[1].astype(np.int32)
-    assert np.max(np.abs(vo - vg)) <= 1
+    # FP32 vs FP64 forces: codes agree except near rounding boundaries; in the
+    # saturated arctan tail (|code| ~ 32700) one force ulp spans more than one code
     assert np.mean(vo != vg) < 1e-3
+    assert np.max(np.abs(vo - vg)[np.abs(vo) < 32000]) <= 1
     assert sg.dt_fine == pytest.approx(so.dt_fine, rel=1e-4)
     assert sg.dt_coarse == pytest.approx(so.dt_coarse, rel=1e-4)
     assert sg.sigma_vi == so.sigma_vi
@@ -137,8 +143,8 @@ def test_fine_green_octant_matches_closed_form(tables):
     g = Cube(p, np_capacity=st.np, fk_table=fk, ck_table=ck)
     nf = 64
     kp = nf // 2 + 1
-    got = g.fetch(4).reshape(3, kp, kp, kp).astype(np.float64)
-    ref = separable_green(fk, nf) / nf ** 3
+    got = g.fetch(4).reshape(3, kp, kp, kp).astype(np.float64)      # [d][ky][kx][kz]
+    ref = (separable_green(fk, nf) / nf ** 3).transpose(0, 2, 3, 1)  # [d][kz][ky][kx] -> [d][ky][kx][kz]
     assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
 
 
@@ -148,9 +154,11 @@ def test_radix3_mesh_forces(tables):
     o, g = pair(st, p, tables)
     s.a, s.a_mid, s.dt = 0.5, 0.5, 20.0
     so, sg = s.copy(), s.copy()
+    g.debug_deposit(sg.copy())
+    dens = g.fetch(0)
     o.particle_mesh(so, 1)
     g.particle_mesh(sg)
-    assert np.array_equal(o.fetch(0).view(np.int32), g.fetch(0).view(np.int32))
+    assert np.array_equal(o.fetch(0).view(np.int32), dens.view(np.int32))
     assert rel_rms(g.fetch(2), o.fetch(2)) <= FORCE_TOL
     assert rel_rms(g.fetch(3), o.fetch(3)) <= FORCE_TOL
 
