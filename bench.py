@@ -38,6 +38,8 @@ sys.path.insert(0, ROOT)
 CONFIGS = {
     "c2": dict(nc=256, nnt=8, box=1000.0, izip=2, pp=True, z_i=49.0,
                workload="512^3 particles, 1000 Mpc/h, fine 1024^3, coarse 256^3, int2 x/v, PP on (pp_range=1)"),
+    "c2s": dict(nc=128, nnt=4, box=500.0, izip=2, pp=True, z_i=49.0,
+                workload="256^3 particles, 500 Mpc/h, fine 512^3, coarse 128^3, int2 x/v, PP on (profiling size)"),
     "c1": dict(nc=32, nnt=2, box=200.0, izip=2, pp=False, z_i=49.0,
                workload="64^3 particles, 200 Mpc/h, fine 128^3, coarse 32^3, int2 x/v, PP off"),
 }

@@ -158,6 +158,7 @@ __global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_
   const int kx0 = blockIdx.x * TK;
   const int nk = min(TK, ncol - kx0);
   float2* b = base + blockIdx.z * comp_stride + (size_t)blockIdx.y * ostride + kx0;
+#pragma unroll 8
   for (int i = threadIdx.x; i < N * TK; i += T * TK) {
     const int j = i / TK, c = i - j * TK;
     sm[j * P + c] = (c < nk) ? b[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
@@ -184,6 +185,7 @@ __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in
   const int nk = min(TK, ncol - kx0);
   const int ky = blockIdx.y;
   const float2* bi = in + (size_t)ky * ostride + kx0;
+#pragma unroll 8
   for (int i = threadIdx.x; i < N * TK; i += T * TK) {
     const int j = i / TK, c = i - j * TK;
     sm[j * P + c] = (c < nk) ? bi[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
@@ -232,6 +234,7 @@ __global__ void __launch_bounds__(T * RB) k_xr2c(float* __restrict__ data, int r
   constexpr int CS = N + R + 8;
   const int pair0 = blockIdx.x * RB;
   const int cp = rp / 2;
+#pragma unroll 8
   for (int i = threadIdx.x; i < RB * N; i += T * RB) {
     const int q = i / N, j = i - q * N;
     const int pr = min(pair0 + q, npairs - 1);
@@ -257,50 +260,46 @@ __global__ void __launch_bounds__(T * RB) k_xr2c(float* __restrict__ data, int r
   }
 }
 
-// x pass, c2r of the three force components, max(fx^2+fy^2+fz^2) fused
+// x pass, c2r of the three force components, max f^2 fused; group g handles
+// component g / RB and row pair g % RB, so the three transforms run side by side
 template <int N, int R, int T, int RB>
-__global__ void __launch_bounds__(T * RB) k_xc2r3(float* __restrict__ data, size_t comp_stride, int rp,
-                                                  int npairs, const float2* __restrict__ tw,
-                                                  unsigned int* __restrict__ f2_bits) {
+__global__ void __launch_bounds__(3 * T * RB) k_xc2r3(float* __restrict__ data, size_t comp_stride, int rp,
+                                                      int npairs, const float2* __restrict__ tw,
+                                                      unsigned int* __restrict__ f2_bits) {
   extern __shared__ float2 sm[];
   constexpr int CS = N + R + 8;
+  constexpr int NT = 3 * T * RB;
   const int pair0 = blockIdx.x * RB;
   const int cp = rp / 2;
   constexpr int nh = N / 2;
   const int g = threadIdx.x / T, t = threadIdx.x % T;
-  for (int c = 0; c < 3; ++c) {
+#pragma unroll 4
+  for (int i = threadIdx.x; i < 3 * RB * N; i += NT) {
+    const int cq = i / N, k = i - cq * N;
+    const int c = cq / RB, q = cq - c * RB;
     const float2* cb = reinterpret_cast<const float2*>(data + c * comp_stride);
-    float2* buf = sm + (size_t)c * RB * CS;
-    for (int i = threadIdx.x; i < RB * N; i += T * RB) {
-      const int q = i / N, k = i - q * N;
-      const int pr = min(pair0 + q, npairs - 1);
-      const size_t ra = (size_t)(2 * pr) * cp;
-      float2 z;
-      if (k == 0 || k == nh) {
-        const float2 A = cb[ra + k], B = cb[ra + cp + k];
-        z = make_float2(A.x, B.x);
-      } else if (k < nh) {
-        const float2 A = cb[ra + k], B = cb[ra + cp + k];
-        z = make_float2(A.x - B.y, A.y + B.x);
-      } else {
-        const float2 A = cb[ra + (N - k)], B = cb[ra + cp + (N - k)];
-        z = make_float2(A.x + B.y, B.x - A.y);
-      }
-      buf[q * CS + k] = z;
-    }
-    __syncthreads();
-    fft_seq<N, R, T, 1, true>(buf + g * CS, 1, t, tw);
-    __syncthreads();
+    const int pr = min(pair0 + q, npairs - 1);
+    const size_t ra = (size_t)(2 * pr) * cp;
+    const int kk = k <= nh ? k : N - k;
+    const float2 A = cb[ra + kk], B = cb[ra + cp + kk];
+    float2 z;
+    if (k == 0 || k == nh) z = make_float2(A.x, B.x);
+    else if (k < nh) z = make_float2(A.x - B.y, A.y + B.x);
+    else z = make_float2(A.x + B.y, B.x - A.y);
+    sm[cq * CS + k] = z;
   }
+  __syncthreads();
+  fft_seq<N, R, T, 1, true>(sm + g * CS, 1, t, tw);
+  __syncthreads();
   float f2max = 0.f;
-  for (int i = threadIdx.x; i < RB * N; i += T * RB) {
+  for (int i = threadIdx.x; i < RB * N; i += NT) {
     const int q = i / N, j = i - q * N;
     if (pair0 + q >= npairs) continue;
     const size_t ra = (size_t)(2 * (pair0 + q)) * rp;
     float fa[3], fb[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float2 z = sm[(size_t)c * RB * CS + q * CS + j];
+      const float2 z = sm[(c * RB + q) * CS + j];
       float* base = data + c * comp_stride;
       base[ra + j] = z.x;
       base[ra + rp + j] = z.y;
@@ -355,7 +354,7 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
     const int npairs = N * N / 2;
     const size_t smem = sizeof(float2) * 3 * RB3 * (N + R + 8);
     CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, T * RB3, smem, ctx->stream>>>(L.force, (size_t)N * L.plane,
+    k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, smem, ctx->stream>>>(L.force, (size_t)N * L.plane,
                                                                                     L.rp, npairs, tw, f2_bits);
     CUBE_LAUNCH_CHECK(ctx);
   }

@@ -8,9 +8,13 @@
  * for r <= rsoft, over the neighbour cells in (k,j,i) order, each chain
  * newest-first.  A fine cell lies inside exactly one coarse cell, so its chain
  * is that coarse cell's particles in reverse storage order, filtered by fine
- * cell.  The GPU walks the coarse cells directly in that order, with the
- * pair arithmetic in FP64 as in the reference (xvec* are real(8)), so the
- * kicked codes are bit-identical to the oracle.  One thread per particle.
+ * cell.  Per particle the GPU scans the (at most 2^3) coarse cells under the
+ * +-pp_range fine window newest-first, keeps the members of the window (from
+ * a precomputed fine sub-cell byte per particle), and sorts them stably by
+ * window cell, which is exactly the reference's summation order; lists longer
+ * than MAXL fall back to walking the window cell by cell.  The pair
+ * arithmetic is FP64 as in the reference (xvec* are real(8)), so the kicked
+ * codes are bit-identical to the oracle.  One thread per particle.
  */
 #include "cube_internal.cuh"
 
@@ -18,13 +22,33 @@ namespace {
 
 constexpr int PCELLS = 64;
 
+// fine sub-cell of every particle inside its coarse cell: sx + 4 sy + 16 sz,
+// s = floor(ncell*frac) (exact: the FP64 position ncell*(i-1)+ncell*frac has no rounding)
+template <int ZX>
+__global__ void k_pp_subcell(const void* __restrict__ xp_, int64_t cap, int64_t np, uint8_t* __restrict__ sub) {
+  typedef typename CodeT<ZX>::T TX;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < np; i += (int64_t)gridDim.x * blockDim.x) {
+    int sc = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double fr = cube_xfrac((int32_t)xp[(size_t)d * cap + i], ZX);
+      sc |= ((int)floor(cube_dmul(4.0, fr))) << (2 * d);
+    }
+    sub[i] = (uint8_t)sc;
+  }
+}
+
+constexpr int MAXL = 40;  // candidate list of one particle; longer lists take the direct walk
+
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_pp(const void* __restrict__ xp_, void* __restrict__ vp_,
                                             const int64_t* __restrict__ cell_start, int64_t cap, int64_t ncells,
                                             int nc, int nt, int nnt, int pr, int nf_cutoff, double rsoft,
                                             double mass, double a_mid, double dt, double pi_d,
                                             const float* __restrict__ tan_table, int half_nvbin, cube_codec codec,
-                                            double coef, DevScal* __restrict__ dscal) {
+                                            double coef, const uint8_t* __restrict__ sub,
+                                            DevScal* __restrict__ dscal) {
   typedef typename CodeT<ZX>::T TX;
   typedef typename CodeT<ZV>::T TV;
   const TX* xp = reinterpret_cast<const TX*>(xp_);
@@ -59,50 +83,106 @@ __global__ void __launch_bounds__(256) k_pp(const void* __restrict__ xp_, void* 
       v[d] = cube_vdecode(__ldg(&tan_table[code + half_nvbin]), coef);
     }
     ++n1;
-    for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
-      for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj)
-        for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii) {
-          const int fc[3] = {ii, jj, kk};
-          int cf[3], gg[3];
+    auto pair_force = [&](int64_t jp, const int cf[3]) {
+      double x21[3];
 #pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            cf[d] = (fc[d] - 1 >= 0) ? (fc[d] - 1) / 4 : -((4 - fc[d]) / 4);  // floor((f-1)/4)
-            gg[d] = ((t[d] * nt + cf[d]) % nc + nc) % nc;
-          }
-          const int64_t c2 = cube_cell_of(gg[0], gg[1], gg[2], nt, nnt);
+      for (int d = 0; d < 3; ++d) {
+        const double fr = cube_xfrac((int32_t)xp[(size_t)d * cap + jp], ZX);
+        x21[d] = cube_dsub(cube_dadd(4.0 * (double)cf[d], cube_dmul(4.0, fr)), x1[d]);
+      }
+      double rmag = sqrt(cube_dadd(cube_dadd(cube_dmul(x21[0], x21[0]), cube_dmul(x21[1], x21[1])),
+                                   cube_dmul(x21[2], x21[2])));
+      if (rmag == 0.0) rmag = 1.0;
+      const double rc = cube_ddiv(rmag, (double)nf_cutoff);
+      const double rc2 = cube_dmul(rc, rc);
+      const double rc3 = cube_dmul(rc2, rc);
+      const double rc5 = cube_dmul(cube_dmul(rc2, rc2), rc);
+      const double pcut = cube_dadd(cube_dsub(1.0, cube_dmul(1.75, rc3)), cube_dmul(0.75, rc5));
+      const double r3 = cube_dmul(cube_dmul(rmag, rmag), rmag);
+      const bool keep = rmag > rsoft;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        double fp = cube_dmul(cube_dmul(mass, cube_ddiv(x21[d], r3)), pcut);
+        if (!keep) fp = cube_dmul(fp, 0.0);
+        ft[d] = cube_dadd(ft[d], fp);
+      }
+    };
+    // coarse cells (T coordinates, 0-based) covering the fine window g1 +- pr
+    int clo[3], chi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int a = g1[d] - pr - 1, b = g1[d] + pr - 1;
+      clo[d] = a >= 0 ? a / 4 : -((3 - a) / 4);
+      chi[d] = b >= 0 ? b / 4 : -((3 - b) / 4);
+    }
+    const int W = 2 * pr + 1;
+    uint8_t lw[MAXL];
+    int64_t li[MAXL];
+    int8_t lc[MAXL][3];
+    int nl = 0;
+    bool overflow = false;
+    for (int cz = clo[2]; cz <= chi[2] && !overflow; ++cz)
+      for (int cy = clo[1]; cy <= chi[1] && !overflow; ++cy)
+        for (int cx = clo[0]; cx <= chi[0] && !overflow; ++cx) {
+          const int gx = ((t[0] * nt + cx) % nc + nc) % nc, gy = ((t[1] * nt + cy) % nc + nc) % nc,
+                    gz = ((t[2] * nt + cz) % nc + nc) % nc;
+          const int64_t c2 = cube_cell_of(gx, gy, gz, nt, nnt);
           const int64_t b0 = cell_start[c2], b1 = cell_start[c2 + 1];
-          for (int64_t jp = b1 - 1; jp >= b0; --jp) {
-            double x2[3];
-            bool inside = true;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const double fr = cube_xfrac((int32_t)xp[(size_t)d * cap + jp], ZX);
-              x2[d] = cube_dadd(4.0 * (double)cf[d], cube_dmul(4.0, fr));
-              if ((int)floor(x2[d]) + 1 != fc[d]) inside = false;
-            }
-            if (!inside) continue;
-            ++npair;
-            double x21[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) x21[d] = cube_dsub(x2[d], x1[d]);
-            double rmag = sqrt(cube_dadd(cube_dadd(cube_dmul(x21[0], x21[0]), cube_dmul(x21[1], x21[1])),
-                                         cube_dmul(x21[2], x21[2])));
-            if (rmag == 0.0) rmag = 1.0;
-            const double rc = cube_ddiv(rmag, (double)nf_cutoff);
-            const double rc2 = cube_dmul(rc, rc);
-            const double rc3 = cube_dmul(rc2, rc);
-            const double rc5 = cube_dmul(cube_dmul(rc2, rc2), rc);
-            const double pcut = cube_dadd(cube_dsub(1.0, cube_dmul(1.75, rc3)), cube_dmul(0.75, rc5));
-            const double r3 = cube_dmul(cube_dmul(rmag, rmag), rmag);
-            const bool keep = rmag > rsoft;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              double fp = cube_dmul(cube_dmul(mass, cube_ddiv(x21[d], r3)), pcut);
-              if (!keep) fp = cube_dmul(fp, 0.0);
-              ft[d] = cube_dadd(ft[d], fp);
-            }
+          for (int64_t jp = b1 - 1; jp >= b0; --jp) {  // newest-first, as the linked list
+            const int sc = sub[jp];
+            const int wx = 4 * cx + (sc & 3) + 1 - g1[0] + pr;
+            const int wy = 4 * cy + ((sc >> 2) & 3) + 1 - g1[1] + pr;
+            const int wz = 4 * cz + (sc >> 4) + 1 - g1[2] + pr;
+            if ((unsigned)wx >= (unsigned)W || (unsigned)wy >= (unsigned)W || (unsigned)wz >= (unsigned)W) continue;
+            if (nl == MAXL) { overflow = true; break; }
+            lw[nl] = (uint8_t)((wz * W + wy) * W + wx);
+            li[nl] = jp;
+            lc[nl][0] = (int8_t)cx; lc[nl][1] = (int8_t)cy; lc[nl][2] = (int8_t)cz;
+            ++nl;
           }
         }
+    if (!overflow) {
+      // stable insertion sort by window cell: the reference's (k,j,i) cell order,
+      // chain order (newest first) kept inside a cell
+      for (int i = 1; i < nl; ++i) {
+        const uint8_t w = lw[i];
+        const int64_t ix = li[i];
+        const int8_t c0_ = lc[i][0], c1_ = lc[i][1], c2_ = lc[i][2];
+        int j = i - 1;
+        while (j >= 0 && lw[j] > w) {
+          lw[j + 1] = lw[j]; li[j + 1] = li[j];
+          lc[j + 1][0] = lc[j][0]; lc[j + 1][1] = lc[j][1]; lc[j + 1][2] = lc[j][2];
+          --j;
+        }
+        lw[j + 1] = w; li[j + 1] = ix;
+        lc[j + 1][0] = c0_; lc[j + 1][1] = c1_; lc[j + 1][2] = c2_;
+      }
+      npair += nl;
+      for (int i = 0; i < nl; ++i) {
+        const int cf[3] = {lc[i][0], lc[i][1], lc[i][2]};
+        pair_force(li[i], cf);
+      }
+    } else {
+      for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
+        for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj)
+          for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii) {
+            const int fc[3] = {ii, jj, kk};
+            int cf[3], gg[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              cf[d] = (fc[d] - 1 >= 0) ? (fc[d] - 1) / 4 : -((4 - fc[d]) / 4);  // floor((f-1)/4)
+              gg[d] = ((t[d] * nt + cf[d]) % nc + nc) % nc;
+            }
+            const int want = ((fc[0] - 1 - 4 * cf[0])) | ((fc[1] - 1 - 4 * cf[1]) << 2) | ((fc[2] - 1 - 4 * cf[2]) << 4);
+            const int64_t c2 = cube_cell_of(gg[0], gg[1], gg[2], nt, nnt);
+            const int64_t b0 = cell_start[c2], b1 = cell_start[c2 + 1];
+            for (int64_t jp = b1 - 1; jp >= b0; --jp) {
+              if (sub[jp] != want) continue;
+              ++npair;
+              pair_force(jp, cf);
+            }
+          }
+    }
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       double k = cube_dmul(ft[d], a_mid);
@@ -131,10 +211,13 @@ template <int ZX, int ZV>
 int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   const int64_t blocks = (ctx->ncells + PCELLS - 1) / PCELLS;
   const double coef = cube_vcoef(&ctx->codec, io->sigma_vi);
+  uint8_t* sub = reinterpret_cast<uint8_t*>(ctx->tkey);  // re-bin scratch, free outside update_x
+  k_pp_subcell<ZX><<<1184, 256, 0, ctx->stream>>>(ctx->xp, ctx->cap, ctx->np, sub);
+  CUBE_LAUNCH_CHECK(ctx);
   k_pp<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
       ctx->xp, ctx->vp, ctx->cell_start, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, ctx->P.pp_range,
       ctx->P.nf_cutoff, (double)ctx->P.rsoft, (double)io->mass_p_cdm, (double)io->a_mid, (double)io->dt,
-      (double)ctx->codec.pi_f, ctx->tan_table, ctx->nvbin / 2, ctx->codec, coef, ctx->dscal);
+      (double)ctx->codec.pi_f, ctx->tan_table, ctx->nvbin / 2, ctx->codec, coef, sub, ctx->dscal);
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }

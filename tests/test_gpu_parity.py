@@ -78,7 +78,8 @@ def test_deposit_bit_exact(pm_pair, tables):
     g2.debug_deposit(sd)
     assert np.array_equal(o.fetch(0).view(np.int32), g2.fetch(0).view(np.int32))
     assert np.array_equal(o.fetch(1).view(np.int32), g2.fetch(1).view(np.int32))
-    assert so.testrhoc == pytest.approx(sd.testrhoc, rel=1e-12)
+    # the oracle sums the FP32-rounded nodes, the GPU the exact fixed-point integers
+    assert so.testrhoc == pytest.approx(sd.testrhoc, rel=1e-7)
     assert sd.testrhof == pytest.approx(st.np * st.mass_p_cdm, rel=1e-9)
 
 
