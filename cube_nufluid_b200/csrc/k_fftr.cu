@@ -57,6 +57,19 @@ __host__ __device__ constexpr int bitrev(int L, int i) {
   return r;
 }
 
+// cp.async (LDGSTS) copies: the loads of a pass are all in flight before the
+// first use, instead of one register round trip per element
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int n = valid ? 8 : 0;  // 0 bytes read: the 8 destination bytes are zero-filled
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(n));
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 template <int L, int I>
 struct BitRev {
   static constexpr int value = bitrev(L, I);
@@ -158,11 +171,11 @@ __global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_
   const int kx0 = blockIdx.x * TK;
   const int nk = min(TK, ncol - kx0);
   float2* b = base + blockIdx.z * comp_stride + (size_t)blockIdx.y * ostride + kx0;
-#pragma unroll 8
   for (int i = threadIdx.x; i < N * TK; i += T * TK) {
     const int j = i / TK, c = i - j * TK;
-    sm[j * P + c] = (c < nk) ? b[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
+    cp_async8(&sm[j * P + c], c < nk ? &b[(size_t)j * jstride + c] : b, c < nk);
   }
+  cp_async_wait_all();
   __syncthreads();
   const int g = threadIdx.x / T, t = threadIdx.x % T;
   fft_seq<N, R, T, SIGN, false>(sm + g, P, t, tw);
@@ -185,11 +198,11 @@ __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in
   const int nk = min(TK, ncol - kx0);
   const int ky = blockIdx.y;
   const float2* bi = in + (size_t)ky * ostride + kx0;
-#pragma unroll 8
   for (int i = threadIdx.x; i < N * TK; i += T * TK) {
     const int j = i / TK, c = i - j * TK;
-    sm[j * P + c] = (c < nk) ? bi[(size_t)j * jstride + c] : make_float2(0.f, 0.f);
+    cp_async8(&sm[j * P + c], c < nk ? &bi[(size_t)j * jstride + c] : bi, c < nk);
   }
+  cp_async_wait_all();
   __syncthreads();
   const int g = threadIdx.x / T, t = threadIdx.x % T;
   float2* s = sm + g;
@@ -234,13 +247,15 @@ __global__ void __launch_bounds__(T * RB) k_xr2c(float* __restrict__ data, int r
   constexpr int CS = N + R + 8;
   const int pair0 = blockIdx.x * RB;
   const int cp = rp / 2;
-#pragma unroll 8
   for (int i = threadIdx.x; i < RB * N; i += T * RB) {
     const int q = i / N, j = i - q * N;
     const int pr = min(pair0 + q, npairs - 1);
     const size_t ra = (size_t)(2 * pr) * rp;
-    sm[q * CS + j] = make_float2(data[ra + j], data[ra + rp + j]);
+    float* dst = reinterpret_cast<float*>(&sm[q * CS + j]);
+    cp_async4(dst, &data[ra + j]);
+    cp_async4(dst + 1, &data[ra + rp + j]);
   }
+  cp_async_wait_all();
   __syncthreads();
   const int g = threadIdx.x / T, t = threadIdx.x % T;
   fft_seq<N, R, T, -1, true>(sm + g * CS, 1, t, tw);
@@ -273,15 +288,22 @@ __global__ void __launch_bounds__(3 * T * RB) k_xc2r3(float* __restrict__ data, 
   const int cp = rp / 2;
   constexpr int nh = N / 2;
   const int g = threadIdx.x / T, t = threadIdx.x % T;
-#pragma unroll 4
-  for (int i = threadIdx.x; i < 3 * RB * N; i += NT) {
-    const int cq = i / N, k = i - cq * N;
+  float2* stage = sm + 3 * RB * CS;  // raw half rows A,B of each (component, pair): 2*(nh+1)
+  constexpr int SS = 2 * (nh + 1);
+  for (int i = threadIdx.x; i < 3 * RB * SS; i += NT) {
+    const int cq = i / SS, k = i - cq * SS;
     const int c = cq / RB, q = cq - c * RB;
     const float2* cb = reinterpret_cast<const float2*>(data + c * comp_stride);
     const int pr = min(pair0 + q, npairs - 1);
-    const size_t ra = (size_t)(2 * pr) * cp;
+    const size_t ra = (size_t)(2 * pr) * cp + (k <= nh ? k : cp + (k - nh - 1));
+    cp_async8(&stage[i], &cb[ra], true);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * RB * N; i += NT) {
+    const int cq = i / N, k = i - cq * N;
     const int kk = k <= nh ? k : N - k;
-    const float2 A = cb[ra + kk], B = cb[ra + cp + kk];
+    const float2 A = stage[cq * SS + kk], B = stage[cq * SS + nh + 1 + kk];
     float2 z;
     if (k == 0 || k == nh) z = make_float2(A.x, B.x);
     else if (k < nh) z = make_float2(A.x - B.y, A.y + B.x);
@@ -352,7 +374,7 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
   // x c2r, three components, max f^2
   {
     const int npairs = N * N / 2;
-    const size_t smem = sizeof(float2) * 3 * RB3 * (N + R + 8);
+    const size_t smem = sizeof(float2) * 3 * RB3 * ((N + R + 8) + (N + 2));
     CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, smem, ctx->stream>>>(L.force, (size_t)N * L.plane,
                                                                                     L.rp, npairs, tw, f2_bits);

@@ -21,6 +21,12 @@ namespace {
 
 constexpr int KCELLS = 64;  // cells per CTA
 
+// One thread per (particle, component): the three components of a particle are
+// independent chains (decode, eight fine terms, encode, decode, eight coarse
+// terms, encode), so splitting them triples the threads in flight and keeps
+// each thread's 16 force gathers independent of its FP64 work.  Warps are
+// uniform in the component (d = i / n inside the CTA), so code and force
+// reads of a warp go to one array.
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                               const int64_t* __restrict__ cell_start, const float* __restrict__ vfield,
@@ -35,98 +41,93 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
   const TX* xp = reinterpret_cast<const TX*>(xp_);
   TV* vp = reinterpret_cast<TV*>(vp_);
   __shared__ int64_t cs[KCELLS + 1];
+  __shared__ unsigned int vmx_s[3];
   const int64_t c0 = (int64_t)blockIdx.x * KCELLS;
   const int ncl = (int)min((int64_t)KCELLS, ncells - c0);
   for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = cell_start[c0 + i];
+  if (threadIdx.x < 3) vmx_s[threadIdx.x] = 0u;
   __syncthreads();
   const int nf = 4 * nc;
   const float pi_f = codec.pi_f;
-  float vmx[3] = {0.f, 0.f, 0.f};
-  for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
+  const int64_t p0 = cs[0];
+  const int npb = (int)(cs[ncl] - p0);
+  const int nt3 = nt * nt * nt;
+  // reference corner order: 111,211,121,112,122,212,221,222
+  const int ox[8] = {0, 1, 0, 0, 0, 1, 1, 1}, oy[8] = {0, 0, 1, 0, 1, 0, 1, 1}, oz[8] = {0, 0, 0, 1, 1, 1, 0, 1};
+  for (int i = threadIdx.x; i < 3 * npb; i += blockDim.x) {
+    const int d = i / npb;
+    const int64_t ip = p0 + (i - d * npb);
     int lo = 0, hi = ncl - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
     }
     const int64_t c = c0 + lo;
-    const int nt3 = nt * nt * nt;
     const int64_t tile = c / nt3;
     const int rem = (int)(c - tile * nt3);
     const int l[3] = {rem % nt, (rem / nt) % nt, rem / (nt * nt)};
     const int t[3] = {(int)(tile % nnt), (int)((tile / nnt) % nnt), (int)(tile / ((int64_t)nnt * nnt))};
-    double fr[3];
+    const int code = (int)vp[(size_t)d * cap + ip];
+    const float tan0 = __ldg(&tan_table[code + half_nvbin]);
+    const float vf = __ldg(&vfield[(size_t)d * ncells + c]);
     int n1[3], m1[3];
     float dx1[3], dx2[3], cx1[3], cx2[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      fr[d] = cube_xfrac((int32_t)xp[(size_t)d * cap + ip], ZX);
-      const float tf = (float)cube_dadd(4.0 * (double)l[d], cube_dmul(4.0, fr[d]));
+    for (int e = 0; e < 3; ++e) {
+      const double fr = cube_xfrac((int32_t)xp[(size_t)e * cap + ip], ZX);
+      const float tf = (float)cube_dadd(4.0 * (double)l[e], cube_dmul(4.0, fr));
       const float f = floorf(tf) + 1.f;
-      dx1[d] = cube_fsub(f, tf);
-      dx2[d] = cube_fsub(1.f, dx1[d]);
-      n1[d] = 4 * t[d] * nt + (int)f - 1;  // global fine node of idx1 (0-based), < nf
-      const double g = cube_dadd((double)(t[d] * nt + l[d]), fr[d]);
+      dx1[e] = cube_fsub(f, tf);
+      dx2[e] = cube_fsub(1.f, dx1[e]);
+      n1[e] = 4 * t[e] * nt + (int)f - 1;  // global fine node of idx1 (0-based), < nf
+      const double g = cube_dadd((double)(t[e] * nt + l[e]), fr);
       const float tc = (float)cube_dsub(g, 0.5);
       const float ci = floorf(tc) + 1.f;
-      cx1[d] = cube_fsub(ci, tc);
-      cx2[d] = cube_fsub(1.f, cx1[d]);
-      m1[d] = (int)ci - 1;  // global coarse node of idx1, may be -1
+      cx1[e] = cube_fsub(ci, tc);
+      cx2[e] = cube_fsub(1.f, cx1[e]);
+      m1[e] = (int)ci - 1;  // global coarse node of idx1, may be -1
     }
-    size_t fo[2][2][2], co[2][2][2];
+    const float* F = ff + d * fcomp;
+    const float* G = fc + d * ccomp;
+    float fv[8], gv[8];
 #pragma unroll
-    for (int sz = 0; sz < 2; ++sz)
-#pragma unroll
-      for (int sy = 0; sy < 2; ++sy)
-#pragma unroll
-        for (int sx = 0; sx < 2; ++sx) {
-          const int fx = (n1[0] + sx) % nf, fy = (n1[1] + sy) % nf, fz = (n1[2] + sz) % nf;
-          fo[sz][sy][sx] = (size_t)fz * fplane + (size_t)fy * frp + fx;
-          const int gx = (m1[0] + sx + nc) % nc, gy = (m1[1] + sy + nc) % nc, gz = (m1[2] + sz + nc) % nc;
-          co[sz][sy][sx] = (size_t)gz * cplane + (size_t)gy * crp + gx;
-        }
-    // reference corner order: 111,211,121,112,122,212,221,222
-    const int ox[8] = {0, 1, 0, 0, 0, 1, 1, 1}, oy[8] = {0, 0, 1, 0, 1, 0, 1, 1}, oz[8] = {0, 0, 0, 1, 1, 1, 0, 1};
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const int code = (int)vp[(size_t)d * cap + ip];
-      double v = cube_vdecode(__ldg(&tan_table[code + half_nvbin]), coef_old);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const float fv = __ldg(&ff[d * fcomp + fo[oz[k]][oy[k]][ox[k]]]);
-        float q = cube_fmul(fv, a_mid);
-        q = cube_fmul(q, dt);
-        q = cube_fdiv(q, 6.f);
-        q = cube_fdiv(q, pi_f);
-        q = cube_fmul(q, ox[k] ? dx2[0] : dx1[0]);
-        q = cube_fmul(q, oy[k] ? dx2[1] : dx1[1]);
-        q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
-        v = cube_dadd(v, (double)q);
-      }
-      const int code1 = cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
-      v = cube_vdecode(__ldg(&tan_table[code1 + half_nvbin]), coef_new);
-#pragma unroll
-      for (int k = 0; k < 8; ++k) {
-        const float fv = __ldg(&fc[d * ccomp + co[oz[k]][oy[k]][ox[k]]]);
-        float q = cube_fmul(fv, a_mid);
-        q = cube_fmul(q, dt);
-        q = cube_fdiv(q, 6.f);
-        q = cube_fdiv(q, pi_f);
-        q = cube_fmul(q, ox[k] ? cx2[0] : cx1[0]);
-        q = cube_fmul(q, oy[k] ? cx2[1] : cx1[1]);
-        q = cube_fmul(q, oz[k] ? cx2[2] : cx1[2]);
-        v = cube_dadd(v, (double)q);
-      }
-      const float am = (float)fabs(cube_dadd(v, (double)__ldg(&vfield[(size_t)d * ncells + c])));
-      vmx[d] = fmaxf(vmx[d], am);
-      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
+    for (int k = 0; k < 8; ++k) {
+      const int fx = (n1[0] + ox[k]) % nf, fy = (n1[1] + oy[k]) % nf, fz = (n1[2] + oz[k]) % nf;
+      fv[k] = __ldg(&F[(size_t)fz * fplane + (size_t)fy * frp + fx]);
+      const int gx = (m1[0] + ox[k] + nc) % nc, gy = (m1[1] + oy[k] + nc) % nc, gz = (m1[2] + oz[k] + nc) % nc;
+      gv[k] = __ldg(&G[(size_t)gz * cplane + (size_t)gy * crp + gx]);
     }
-  }
+    double v = cube_vdecode(tan0, coef_old);
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    float m = vmx[d];
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0) atomicMax(&dscal->vmax_bits[d], __float_as_uint(m));
+    for (int k = 0; k < 8; ++k) {
+      float q = cube_fmul(fv[k], a_mid);
+      q = cube_fmul(q, dt);
+      q = cube_fdiv(q, 6.f);
+      q = cube_fdiv(q, pi_f);
+      q = cube_fmul(q, ox[k] ? dx2[0] : dx1[0]);
+      q = cube_fmul(q, oy[k] ? dx2[1] : dx1[1]);
+      q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
+      v = cube_dadd(v, (double)q);
+    }
+    const int code1 = cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
+    v = cube_vdecode(__ldg(&tan_table[code1 + half_nvbin]), coef_new);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      float q = cube_fmul(gv[k], a_mid);
+      q = cube_fmul(q, dt);
+      q = cube_fdiv(q, 6.f);
+      q = cube_fdiv(q, pi_f);
+      q = cube_fmul(q, ox[k] ? cx2[0] : cx1[0]);
+      q = cube_fmul(q, oy[k] ? cx2[1] : cx1[1]);
+      q = cube_fmul(q, oz[k] ? cx2[2] : cx1[2]);
+      v = cube_dadd(v, (double)q);
+    }
+    const float am = (float)fabs(cube_dadd(v, (double)vf));
+    atomicMax(&vmx_s[d], __float_as_uint(am));
+    vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
   }
+  __syncthreads();
+  if (threadIdx.x < 3) atomicMax(&dscal->vmax_bits[threadIdx.x], vmx_s[threadIdx.x]);
 }
 
 template <int ZX, int ZV>

@@ -91,14 +91,29 @@ def test_forces_match_fp64_oracle(pm_pair):
     assert sg.f2_max_coarse == pytest.approx(so.f2_max_coarse, rel=1e-4)
 
 
+def decode(codes, sigma, izipv=2):
+    """Velocity decode of pm.f90:145 in numpy (FP32 argument and tan, FP64 divide)."""
+    nvbin = 1 << (8 * izipv)
+    pif = np.float32(4.0) * np.arctan(np.float32(1.0))
+    arg = (pif * codes.astype(np.float32)) / np.float32(nvbin - 1)
+    coef = float(np.sqrt(pif / np.float32(2.0))) / (float(np.float32(sigma)) * 2.5)
+    return np.tan(arg).astype(np.float64) / coef
+
+
 def test_kicked_velocities_close(pm_pair):
     st, p, s, o, g, so, sg = pm_pair
     vo = o.store()[1].astype(np.int32)
     vg = g.store_state()[1].astype(np.int32)
-    # FP32 vs FP64 forces: codes agree except near rounding boundaries; in the
-    # saturated arctan tail (|code| ~ 32700) one force ulp spans more than one code
-    assert np.mean(vo != vg) < 1e-3
-    assert np.max(np.abs(vo - vg)[np.abs(vo) < 32000]) <= 1
+    # FP32 (GPU) vs FP64 (oracle) forces: the codes agree except where the force
+    # difference crosses a rounding boundary; in velocity the difference is bounded
+    # by the force tolerance times the kick, plus one code step either side
+    assert np.mean(vo != vg) < 5e-3
+    v_o, v_g = decode(vo, so.sigma_vi), decode(vg, so.sigma_vi)
+    v0 = decode(st.vp.astype(np.int32), s.sigma_vi)
+    kick = np.sqrt(np.mean((v_o - v0) ** 2))
+    step = np.abs(decode(vo + 1, so.sigma_vi) - decode(vo - 1, so.sigma_vi))
+    ok = np.abs(v_o - v_g) <= 1e-4 * kick + step
+    assert ok[np.abs(vo) < 32700].all()
     assert sg.dt_fine == pytest.approx(so.dt_fine, rel=1e-4)
     assert sg.dt_coarse == pytest.approx(so.dt_coarse, rel=1e-4)
     assert sg.sigma_vi == so.sigma_vi
