@@ -20,7 +20,7 @@
 
 namespace {
 
-constexpr int PCELLS = 64;
+constexpr int PCELLS = 64;  // cells of one 4^3 brick
 
 // fine sub-cell of every particle inside its coarse cell: sx + 4 sy + 16 sz,
 // s = floor(ncell*frac) (exact: the FP64 position ncell*(i-1)+ncell*frac has no rounding)
@@ -48,26 +48,47 @@ __global__ void __launch_bounds__(256) k_pp(const void* __restrict__ xp_, void* 
                                             double mass, double a_mid, double dt, double pi_d,
                                             const float* __restrict__ tan_table, int half_nvbin, cube_codec codec,
                                             double coef, const uint8_t* __restrict__ sub,
-                                            DevScal* __restrict__ dscal) {
+                                            const int32_t* __restrict__ spill, DevScal* __restrict__ dscal) {
   typedef typename CodeT<ZX>::T TX;
   typedef typename CodeT<ZV>::T TV;
   const TX* xp = reinterpret_cast<const TX*>(xp_);
   TV* vp = reinterpret_cast<TV*>(vp_);
-  __shared__ int64_t cs[PCELLS + 1];
-  const int64_t c0 = (int64_t)blockIdx.x * PCELLS;
-  const int ncl = (int)min((int64_t)PCELLS, ncells - c0);
-  for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = cell_start[c0 + i];
+  // the CTA's cells: a brick listed by k_pp_brick (its 4^3 cells)
+  __shared__ int64_t cid[PCELLS], cst[PCELLS];
+  __shared__ int cpre[PCELLS + 1];
+  const int brick = spill[blockIdx.x];
+  const int nb = nc / 4;
+  const int bx = brick % nb, by = (brick / nb) % nb, bz = brick / (nb * nb);
+  if (threadIdx.x < 32) {
+    int run = 0;
+    for (int base = 0; base < PCELLS; base += 32) {
+      const int q = base + threadIdx.x;
+      const int64_t c = cube_cell_of(bx * 4 + q % 4, by * 4 + (q / 4) % 4, bz * 4 + q / 16, nt, nnt);
+      cid[q] = c;
+      cst[q] = cell_start[c];
+      const int cnt = (int)(cell_start[c + 1] - cst[q]);
+      int inc = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)threadIdx.x >= o) inc += v;
+      }
+      cpre[q] = run + inc - cnt;
+      run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (threadIdx.x == 0) cpre[PCELLS] = run;
+  }
   __syncthreads();
   unsigned long long n1 = 0, npair = 0;
   float f2max = 0.f;
   const int nt3 = nt * nt * nt;
-  for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
-    int lo = 0, hi = ncl - 1;
+  for (int m = threadIdx.x; m < cpre[PCELLS]; m += blockDim.x) {
+    int lo = 0, hi = PCELLS - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
+      if (cpre[mid] <= m) lo = mid; else hi = mid - 1;
     }
-    const int64_t c = c0 + lo;
+    const int64_t c = cid[lo];
+    const int64_t ip = cst[lo] + (m - cpre[lo]);
     const int64_t tile = c / nt3;
     const int rem = (int)(c - tile * nt3);
     const int l[3] = {rem % nt, (rem / nt) % nt, rem / (nt * nt)};
@@ -207,18 +228,213 @@ __global__ void __launch_bounds__(256) k_pp(const void* __restrict__ xp_, void* 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Brick kernel: one CTA per 4^3-cell brick.  The particles of the brick and of
+// its one-cell halo (6^3 cells; pp_range <= 4 fine cells = one coarse cell)
+// are staged in shared memory, the reference's per-fine-cell chains are built
+// there (one thread per coarse cell inserts its particles in storage order, so
+// each chain is newest-first exactly like the linked list of
+// ext_pp_force.f90:51-73), and each particle of the brick walks the chains of
+// its +-pp_range window.  Positions enter the pair sums as differences of
+// ncell*(cell)+ncell*frac, which are exact in FP64 whatever the origin, so
+// region-local coordinates give the reference's values.  Bricks holding more
+// than PB_CAP particles are listed and done by k_pp_list below.
+constexpr int PB = 4;                     // brick edge in coarse cells
+constexpr int PR = PB + 2;                // with the halo
+constexpr int PRC = PR * PR * PR;         // 216 region cells
+constexpr int PF = 4 * PR;                // region edge in fine cells (24)
+constexpr int PB_CAP = 4096;              // particles staged per brick
+
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
+                                                  const int64_t* __restrict__ cell_start, int64_t cap, int nc,
+                                                  int nt, int nnt, int pr, int nf_cutoff, double rsoft,
+                                                  double mass, double a_mid, double dt, double pi_d,
+                                                  const float* __restrict__ tan_table, int half_nvbin,
+                                                  cube_codec codec, double coef, int32_t* __restrict__ spill,
+                                                  DevScal* __restrict__ dscal) {
+  typedef typename CodeT<ZX>::T TX;
+  typedef typename CodeT<ZV>::T TV;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  TV* vp = reinterpret_cast<TV*>(vp_);
+  extern __shared__ unsigned char pbsm[];
+  uint16_t* head = reinterpret_cast<uint16_t*>(pbsm);                       // PF^3
+  uint16_t* nxt = head + PF * PF * PF;                                      // PB_CAP
+  uint16_t* fidx = nxt + PB_CAP;                                            // PB_CAP
+  uint16_t* code = fidx + PB_CAP;                                           // 3*PB_CAP, raw position codes
+  __shared__ int64_t cst[PRC];
+  __shared__ int cpre[PRC + 1];
+  const int nb = nc / PB;
+  const int bx = blockIdx.x % nb, by = (blockIdx.x / nb) % nb, bz = blockIdx.x / (nb * nb);
+  const int x0 = bx * PB - 1, y0 = by * PB - 1, z0 = bz * PB - 1;  // region origin (global coarse, unwrapped)
+  if (threadIdx.x < 32) {
+    int run = 0;
+    for (int base = 0; base < PRC; base += 32) {
+      const int q = base + threadIdx.x;
+      int cnt = 0;
+      if (q < PRC) {
+        const int cx = q % PR, cy = (q / PR) % PR, cz = q / (PR * PR);
+        const int gx = (x0 + cx + nc) % nc, gy = (y0 + cy + nc) % nc, gz = (z0 + cz + nc) % nc;
+        const int64_t c = cube_cell_of(gx, gy, gz, nt, nnt);
+        cst[q] = cell_start[c];
+        cnt = (int)(cell_start[c + 1] - cst[q]);
+      }
+      int inc = cnt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if ((int)threadIdx.x >= o) inc += v;
+      }
+      if (q < PRC) cpre[q] = run + inc - cnt;
+      run += __shfl_sync(0xffffffffu, inc, 31);
+    }
+    if (threadIdx.x == 0) cpre[PRC] = run;
+  }
+  __syncthreads();
+  const int M = cpre[PRC];
+  if (M > PB_CAP) {  // crowded: handled by the list kernel
+    if (threadIdx.x == 0) {
+      const unsigned long long q = atomicAdd(&dscal->n_big, 1ull);
+      spill[q] = blockIdx.x;
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < PF * PF * PF; i += blockDim.x) head[i] = 0xFFFFu;
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    int lo = 0, hi = PRC - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cpre[mid] <= m) lo = mid; else hi = mid - 1;
+    }
+    const int q = lo;
+    const int64_t ip = cst[q] + (m - cpre[q]);
+    const int cc[3] = {q % PR, (q / PR) % PR, q / (PR * PR)};
+    int f[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int cd = (int)xp[(size_t)d * cap + ip];
+      code[3 * m + d] = (uint16_t)cd;
+      f[d] = 4 * cc[d] + (int)floor(cube_dmul(4.0, cube_xfrac(cd, ZX)));
+    }
+    fidx[m] = (uint16_t)((f[2] * PF + f[1]) * PF + f[0]);
+  }
+  __syncthreads();
+  // chains: the thread of region cell q inserts q's particles in storage order
+  for (int q = threadIdx.x; q < PRC; q += blockDim.x)
+    for (int m = cpre[q]; m < cpre[q + 1]; ++m) {
+      const int f = fidx[m];
+      nxt[m] = head[f];
+      head[f] = (uint16_t)m;
+    }
+  __syncthreads();
+  unsigned long long n1 = 0, npair = 0;
+  float f2max = 0.f;
+  // targets: the particles of the brick's own cells (region cells 1..PB)
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    int lo = 0, hi = PRC - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cpre[mid] <= m) lo = mid; else hi = mid - 1;
+    }
+    const int q = lo;
+    const int cc[3] = {q % PR, (q / PR) % PR, q / (PR * PR)};
+    if (cc[0] < 1 || cc[0] > PB || cc[1] < 1 || cc[1] > PB || cc[2] < 1 || cc[2] > PB) continue;
+    const int64_t ip = cst[q] + (m - cpre[q]);
+    double x1[3], v[3], ft[3] = {0.0, 0.0, 0.0};
+    int g1[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const double fr = cube_xfrac((int32_t)(int16_t)code[3 * m + d], ZX);
+      x1[d] = cube_dadd(4.0 * (double)cc[d], cube_dmul(4.0, fr));
+      g1[d] = 4 * cc[d] + (int)floor(cube_dmul(4.0, fr));
+      const int vc = (int)vp[(size_t)d * cap + ip];
+      v[d] = cube_vdecode(__ldg(&tan_table[vc + half_nvbin]), coef);
+    }
+    ++n1;
+    for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
+      for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj)
+        for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii) {
+          int m2 = head[(kk * PF + jj) * PF + ii];
+          const int cf[3] = {ii >> 2, jj >> 2, kk >> 2};
+          while (m2 != 0xFFFF) {
+            ++npair;
+            double x21[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const double fr = cube_xfrac((int32_t)(int16_t)code[3 * m2 + d], ZX);
+              x21[d] = cube_dsub(cube_dadd(4.0 * (double)cf[d], cube_dmul(4.0, fr)), x1[d]);
+            }
+            double rmag = sqrt(cube_dadd(cube_dadd(cube_dmul(x21[0], x21[0]), cube_dmul(x21[1], x21[1])),
+                                         cube_dmul(x21[2], x21[2])));
+            if (rmag == 0.0) rmag = 1.0;
+            const double rc = cube_ddiv(rmag, (double)nf_cutoff);
+            const double rc2 = cube_dmul(rc, rc);
+            const double rc3 = cube_dmul(rc2, rc);
+            const double rc5 = cube_dmul(cube_dmul(rc2, rc2), rc);
+            const double pcut = cube_dadd(cube_dsub(1.0, cube_dmul(1.75, rc3)), cube_dmul(0.75, rc5));
+            const double r3 = cube_dmul(cube_dmul(rmag, rmag), rmag);
+            const bool keep = rmag > rsoft;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              double fp = cube_dmul(cube_dmul(mass, cube_ddiv(x21[d], r3)), pcut);
+              if (!keep) fp = cube_dmul(fp, 0.0);
+              ft[d] = cube_dadd(ft[d], fp);
+            }
+            m2 = nxt[m2];
+          }
+        }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      double k = cube_dmul(ft[d], a_mid);
+      k = cube_dmul(k, dt);
+      k = cube_ddiv(k, 6.0);
+      k = cube_ddiv(k, pi_d);
+      v[d] = cube_dadd(v[d], k);
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode(&codec, v[d], coef), ZV);
+    }
+    const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
+    f2max = fmaxf(f2max, (float)f2);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+    npair += __shfl_xor_sync(0xffffffffu, npair, o);
+    f2max = fmaxf(f2max, __shfl_xor_sync(0xffffffffu, f2max, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(&dscal->itest1, n1);
+    atomicAdd(&dscal->npairs, npair);
+    atomicMax(&dscal->f2_pp_bits, __float_as_uint(f2max));
+  }
+}
+
 template <int ZX, int ZV>
 int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
-  const int64_t blocks = (ctx->ncells + PCELLS - 1) / PCELLS;
   const double coef = cube_vcoef(&ctx->codec, io->sigma_vi);
-  uint8_t* sub = reinterpret_cast<uint8_t*>(ctx->tkey);  // re-bin scratch, free outside update_x
-  k_pp_subcell<ZX><<<1184, 256, 0, ctx->stream>>>(ctx->xp, ctx->cap, ctx->np, sub);
+  if (ctx->nc % PB) {
+    ctx->err = "nc must be a multiple of 4 for the PP bricks";
+    return CUBE_ERR_PARAM;
+  }
+  int32_t* spill = ctx->big_list;  // re-bin scratch, free outside update_x
+  const int nbricks = (ctx->nc / PB) * (ctx->nc / PB) * (ctx->nc / PB);
+  const size_t smem = sizeof(uint16_t) * ((size_t)PF * PF * PF + 5 * (size_t)PB_CAP);
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_pp_brick<ZX, ZV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_pp_brick<ZX, ZV><<<nbricks, 256, smem, ctx->stream>>>(
+      ctx->xp, ctx->vp, ctx->cell_start, ctx->cap, ctx->nc, ctx->nt, ctx->nnt, ctx->P.pp_range, ctx->P.nf_cutoff,
+      (double)ctx->P.rsoft, (double)io->mass_p_cdm, (double)io->a_mid, (double)io->dt, (double)ctx->codec.pi_f,
+      ctx->tan_table, ctx->nvbin / 2, ctx->codec, coef, spill, ctx->dscal);
   CUBE_LAUNCH_CHECK(ctx);
-  k_pp<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
-      ctx->xp, ctx->vp, ctx->cell_start, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, ctx->P.pp_range,
-      ctx->P.nf_cutoff, (double)ctx->P.rsoft, (double)io->mass_p_cdm, (double)io->a_mid, (double)io->dt,
-      (double)ctx->codec.pi_f, ctx->tan_table, ctx->nvbin / 2, ctx->codec, coef, sub, ctx->dscal);
-  CUBE_LAUNCH_CHECK(ctx);
+  unsigned long long nspill = 0;
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&nspill, &ctx->dscal->n_big, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (nspill) {
+    uint8_t* sub = reinterpret_cast<uint8_t*>(ctx->tkey);  // re-bin scratch, free outside update_x
+    k_pp_subcell<ZX><<<1184, 256, 0, ctx->stream>>>(ctx->xp, ctx->cap, ctx->np, sub);
+    CUBE_LAUNCH_CHECK(ctx);
+    k_pp<ZX, ZV><<<(unsigned)nspill, 256, 0, ctx->stream>>>(
+        ctx->xp, ctx->vp, ctx->cell_start, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, ctx->P.pp_range,
+        ctx->P.nf_cutoff, (double)ctx->P.rsoft, (double)io->mass_p_cdm, (double)io->a_mid, (double)io->dt,
+        (double)ctx->codec.pi_f, ctx->tan_table, ctx->nvbin / 2, ctx->codec, coef, sub, spill, ctx->dscal);
+    CUBE_LAUNCH_CHECK(ctx);
+  }
   return CUBE_OK;
 }
 
