@@ -235,7 +235,9 @@ def run_ours(args, cfg, rank, world, local_rank):
 
 def cpu_sample(threads: int):
     """The CPU oracle on a bounded sample: one step (update_x + PP + particle_mesh)
-    of a 64^3-particle box with the workload's method settings."""
+    of a 64^3-particle box with the workload's method settings, OpenMP over all
+    host threads where the reference's loops are parallel (its nlayer scheme)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_ref import Oracle
     from cube_nufluid_b200 import ic, tables, make_params, scalars_from_ic
@@ -254,7 +256,7 @@ def cpu_sample(threads: int):
     dt = time.perf_counter() - t0
     return {"value": st.np / dt, "unit": "particle-updates/s", "cores": threads, "kind": "port",
             "sample": f"1 step (update_x + ext_pp_force + particle_mesh, FP32 reference-order deposit, FP64 FFT) "
-                      f"of a {st.np}-particle box (nc=32, nf=128, 2^3 tiles) on {threads} host thread; "
+                      f"of a {st.np}-particle box (nc=32, nf=128, 2^3 tiles) on {threads} host threads; "
                       f"{dt:.1f} s"}
 
 
@@ -280,7 +282,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        base = cpu_sample(1)
+        base = cpu_sample(os.cpu_count() or 1)
         line = {"impl": "reference", "metric": metric, "value": base["value"], "unit": "particle-updates/s",
                 "n_gpus": args.gpus, "steps": 1, "warmup": 0, "higher_is_better": True, "config": config,
                 "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "particle-updates/s",
@@ -321,7 +323,7 @@ def main():
         "phases_ms": phases, "phase_gbs": phase_gbs, "clocks": r["clocks"],
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(1)
+        line["cpu_baseline"] = cpu_sample(os.cpu_count() or 1)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

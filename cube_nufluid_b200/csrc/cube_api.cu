@@ -177,6 +177,12 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
     return fail(CUBE_ERR_CUDA);
   }
   ctx->own_stream = 1;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || ctx->num_sms <= 0)
+      ctx->num_sms = 148;
+  }
   for (int i = 0; i < 16; ++i)
     if (cudaEventCreate(&ctx->ev[i]) != cudaSuccess) { ctx->err = "cudaEventCreate failed"; return fail(CUBE_ERR_CUDA); }
   const int64_t cap = ctx->cap, nce = ctx->ncells;

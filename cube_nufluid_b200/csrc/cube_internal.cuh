@@ -66,6 +66,7 @@ struct cube_ctx {
   int own_stream;
   int64_t np, cap;
   int state_loaded;
+  int num_sms;
   // particles (double-buffered for the re-bin)
   void* xp;  void* vp;  int32_t* pid;
   void* xp2; void* vp2; int32_t* pid2;

@@ -21,6 +21,7 @@
  */
 #include "cube_internal.cuh"
 
+#include <algorithm>
 #include <utility>
 
 namespace {
@@ -69,6 +70,8 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <int L, int I>
 struct BitRev {
@@ -186,6 +189,57 @@ __global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_
   }
 }
 
+// Persistent column pass: each CTA walks tiles (TK columns x N, one y or z
+// line set) with two shared buffers, prefetching tile i+1 with cp.async while
+// it transforms and stores tile i.
+template <int N, int R, int T, int TK, int SIGN>
+__global__ void __launch_bounds__(T * TK) k_col_pipe(float2* __restrict__ base, size_t comp_stride, int ncol,
+                                                     long long jstride, long long ostride, int nother, int ncomp,
+                                                     const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  constexpr int P = TK + 1;
+  const int ntx = (ncol + TK - 1) / TK;
+  const int ntiles = ntx * nother * ncomp;
+  auto tile_ptr = [&](int tl, int& nk) -> float2* {
+    const int cx = tl % ntx, rest = tl / ntx;
+    const int o = rest % nother, comp = rest / nother;
+    nk = min(TK, ncol - cx * TK);
+    return base + comp * comp_stride + (size_t)o * ostride + cx * TK;
+  };
+  auto issue = [&](int tl, float2* dst) {
+    int nk;
+    const float2* b = tile_ptr(tl, nk);
+    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+      const int j = i / TK, c = i - j * TK;
+      cp_async8(&dst[j * P + c], c < nk ? &b[(size_t)j * jstride + c] : b, c < nk);
+    }
+  };
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  int cur = 0;
+  int tile = blockIdx.x;
+  if (tile < ntiles) issue(tile, sm);
+  cp_async_commit();
+  for (; tile < ntiles; tile += gridDim.x) {
+    const int next = tile + gridDim.x;
+    if (next < ntiles) issue(next, sm + (cur ^ 1) * N * P);
+    cp_async_commit();
+    cp_async_wait_one();
+    __syncthreads();
+    float2* buf = sm + cur * N * P;
+    fft_seq<N, R, T, SIGN, false>(buf + g, P, t, tw);
+    __syncthreads();
+    int nk;
+    float2* b = tile_ptr(tile, nk);
+    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+      const int j = i / TK, c = i - j * TK;
+      if (c < nk) b[(size_t)j * jstride + c] = buf[j * P + c];
+    }
+    __syncthreads();
+    cur ^= 1;
+  }
+  cp_async_wait_all();
+}
+
 // fused z pass with the Green multiply (kernel octant [d][ky][kx][kz], kz fastest)
 template <int N, int R, int T, int TK>
 __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in, float2* __restrict__ out0,
@@ -288,27 +342,33 @@ __global__ void __launch_bounds__(3 * T * RB) k_xc2r3(float* __restrict__ data, 
   const int cp = rp / 2;
   constexpr int nh = N / 2;
   const int g = threadIdx.x / T, t = threadIdx.x % T;
-  float2* stage = sm + 3 * RB * CS;  // raw half rows A,B of each (component, pair): 2*(nh+1)
-  constexpr int SS = 2 * (nh + 1);
-  for (int i = threadIdx.x; i < 3 * RB * SS; i += NT) {
-    const int cq = i / SS, k = i - cq * SS;
+  // cp.async the half rows into the sequence slots: A[k] -> slot k, B[k] -> slot
+  // N-k (1 <= k < nh), A[0], A[nh] -> slots 0, nh; B[0], B[nh] -> spare slots
+  // N, N+1; then unfold in place (Z[k] = A + iB, Z[N-k] = conj(A) + i conj(B))
+  for (int i = threadIdx.x; i < 3 * RB * (N + 2); i += NT) {
+    const int cq = i / (N + 2), r = i - cq * (N + 2);
     const int c = cq / RB, q = cq - c * RB;
     const float2* cb = reinterpret_cast<const float2*>(data + c * comp_stride);
     const int pr = min(pair0 + q, npairs - 1);
-    const size_t ra = (size_t)(2 * pr) * cp + (k <= nh ? k : cp + (k - nh - 1));
-    cp_async8(&stage[i], &cb[ra], true);
+    const size_t ra = (size_t)(2 * pr) * cp;
+    const bool isA = r <= nh;
+    const int k = isA ? r : r - nh - 1;
+    const int slot = isA ? k : (k == 0 ? N : (k == nh ? N + 1 : N - k));
+    cp_async8(&sm[cq * CS + slot], &cb[ra + (isA ? 0 : cp) + k], true);
   }
   cp_async_wait_all();
   __syncthreads();
-  for (int i = threadIdx.x; i < 3 * RB * N; i += NT) {
-    const int cq = i / N, k = i - cq * N;
-    const int kk = k <= nh ? k : N - k;
-    const float2 A = stage[cq * SS + kk], B = stage[cq * SS + nh + 1 + kk];
-    float2 z;
-    if (k == 0 || k == nh) z = make_float2(A.x, B.x);
-    else if (k < nh) z = make_float2(A.x - B.y, A.y + B.x);
-    else z = make_float2(A.x + B.y, B.x - A.y);
-    sm[cq * CS + k] = z;
+  for (int i = threadIdx.x; i < 3 * RB * (nh + 1); i += NT) {
+    const int cq = i / (nh + 1), k = i - cq * (nh + 1);
+    float2* z = sm + cq * CS;
+    if (k == 0 || k == nh) {
+      const float2 A = z[k], B = z[k == 0 ? N : N + 1];
+      z[k] = make_float2(A.x, B.x);
+    } else {
+      const float2 A = z[k], B = z[N - k];
+      z[k] = make_float2(A.x - B.y, A.y + B.x);
+      z[N - k] = make_float2(A.x + B.y, B.x - A.y);
+    }
   }
   __syncthreads();
   fft_seq<N, R, T, 1, true>(sm + g * CS, 1, t, tw);
@@ -358,9 +418,15 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen<N, R, T, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   const dim3 g1((ncol + TK - 1) / TK, N, 1), g3((ncol + TK - 1) / TK, N, 3);
-  // y forward
-  k_col<N, R, T, TK, -1><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.rho), cstride, ncol, cp,
-                                                             (long long)N * cp, tw);
+  // y forward (persistent, double-buffered)
+  const size_t psm = 2 * csm;
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col_pipe<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col_pipe<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
+  int per_sm = 0;
+  CUBE_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_col_pipe<N, R, T, TK, -1>, T * TK, psm));
+  const int pgrid = std::max(1, per_sm) * ctx->num_sms;
+  k_col_pipe<N, R, T, TK, -1><<<pgrid, T * TK, psm, ctx->stream>>>(reinterpret_cast<float2*>(L.rho), cstride, ncol, cp,
+                                                                   (long long)N * cp, N, 1, tw);
   CUBE_LAUNCH_CHECK(ctx);
   // z forward, Green, z inverse
   k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
@@ -368,13 +434,13 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
                                                             (long long)N * cp, cp, tw, L.kern, L.kern_pitch);
   CUBE_LAUNCH_CHECK(ctx);
   // y inverse, three components
-  k_col<N, R, T, TK, 1><<<g3, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.force), cstride, ncol, cp,
-                                                            (long long)N * cp, tw);
+  k_col_pipe<N, R, T, TK, 1><<<pgrid, T * TK, psm, ctx->stream>>>(reinterpret_cast<float2*>(L.force), cstride, ncol,
+                                                                  cp, (long long)N * cp, N, 3, tw);
   CUBE_LAUNCH_CHECK(ctx);
   // x c2r, three components, max f^2
   {
     const int npairs = N * N / 2;
-    const size_t smem = sizeof(float2) * 3 * RB3 * ((N + R + 8) + (N + 2));
+    const size_t smem = sizeof(float2) * 3 * RB3 * (N + R + 8);
     CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, smem, ctx->stream>>>(L.force, (size_t)N * L.plane,
                                                                                     L.rp, npairs, tw, f2_bits);

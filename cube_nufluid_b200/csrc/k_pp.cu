@@ -228,6 +228,29 @@ __global__ void __launch_bounds__(256) k_pp(const void* __restrict__ xp_, void* 
   }
 }
 
+// FP64 pair term of ext_pp_force.f90:99-107 for a separation x21 (exact in FP64).
+// rc = rmag/nf_cutoff is evaluated as rmag*(1/nf_cutoff) only when nf_cutoff is
+// a power of two, where both are the same exact scaling.
+__device__ __forceinline__ void pp_pair(const double x21[3], double mass, double rsoft, int nf_cutoff,
+                                        bool pow2_cut, double inv_cut, double fp[3]) {
+  double rmag = sqrt(cube_dadd(cube_dadd(cube_dmul(x21[0], x21[0]), cube_dmul(x21[1], x21[1])),
+                               cube_dmul(x21[2], x21[2])));
+  if (rmag == 0.0) rmag = 1.0;
+  const double rc = pow2_cut ? cube_dmul(rmag, inv_cut) : cube_ddiv(rmag, (double)nf_cutoff);
+  const double rc2 = cube_dmul(rc, rc);
+  const double rc3 = cube_dmul(rc2, rc);
+  const double rc5 = cube_dmul(cube_dmul(rc2, rc2), rc);
+  const double pcut = cube_dadd(cube_dsub(1.0, cube_dmul(1.75, rc3)), cube_dmul(0.75, rc5));
+  const double r3 = cube_dmul(cube_dmul(rmag, rmag), rmag);
+  const bool keep = rmag > rsoft;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double f = cube_dmul(cube_dmul(mass, cube_ddiv(x21[d], r3)), pcut);
+    if (!keep) f = cube_dmul(f, 0.0);
+    fp[d] = f;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Brick kernel: one CTA per 4^3-cell brick.  The particles of the brick and of
 // its one-cell halo (6^3 cells; pp_range <= 4 fine cells = one coarse cell)
@@ -246,7 +269,7 @@ constexpr int PF = 4 * PR;                // region edge in fine cells (24)
 constexpr int PB_CAP = 4096;              // particles staged per brick
 
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(256) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
+__global__ void __launch_bounds__(256, 2) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                                   const int64_t* __restrict__ cell_start, int64_t cap, int nc,
                                                   int nt, int nnt, int pr, int nf_cutoff, double rsoft,
                                                   double mass, double a_mid, double dt, double pi_d,
@@ -350,38 +373,51 @@ __global__ void __launch_bounds__(256) k_pp_brick(const void* __restrict__ xp_, 
       v[d] = cube_vdecode(__ldg(&tan_table[vc + half_nvbin]), coef);
     }
     ++n1;
+    // members of the window in the reference order, evaluated four at a time
+    // (independent FP64 chains) and added to ft in that order
+    const bool pow2_cut = (nf_cutoff & (nf_cutoff - 1)) == 0;
+    const double inv_cut = 1.0 / (double)nf_cutoff;
+    int mb[4];
+    int nbuf = 0;
+    auto flush = [&]() {
+      double fp[4][3];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (u < nbuf) {
+          const int m2 = mb[u];
+          const int f = fidx[m2];
+          const int cf[3] = {(f % PF) >> 2, ((f / PF) % PF) >> 2, (f / (PF * PF)) >> 2};
+          double x21[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double fr = cube_xfrac((int32_t)(int16_t)code[3 * m2 + d], ZX);
+            x21[d] = cube_dsub(cube_dadd(4.0 * (double)cf[d], cube_dmul(4.0, fr)), x1[d]);
+          }
+          pp_pair(x21, mass, rsoft, nf_cutoff, pow2_cut, inv_cut, fp[u]);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (u < nbuf)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], fp[u][d]);
+      nbuf = 0;
+    };
     for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
       for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj)
         for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii) {
           int m2 = head[(kk * PF + jj) * PF + ii];
-          const int cf[3] = {ii >> 2, jj >> 2, kk >> 2};
           while (m2 != 0xFFFF) {
             ++npair;
-            double x21[3];
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const double fr = cube_xfrac((int32_t)(int16_t)code[3 * m2 + d], ZX);
-              x21[d] = cube_dsub(cube_dadd(4.0 * (double)cf[d], cube_dmul(4.0, fr)), x1[d]);
-            }
-            double rmag = sqrt(cube_dadd(cube_dadd(cube_dmul(x21[0], x21[0]), cube_dmul(x21[1], x21[1])),
-                                         cube_dmul(x21[2], x21[2])));
-            if (rmag == 0.0) rmag = 1.0;
-            const double rc = cube_ddiv(rmag, (double)nf_cutoff);
-            const double rc2 = cube_dmul(rc, rc);
-            const double rc3 = cube_dmul(rc2, rc);
-            const double rc5 = cube_dmul(cube_dmul(rc2, rc2), rc);
-            const double pcut = cube_dadd(cube_dsub(1.0, cube_dmul(1.75, rc3)), cube_dmul(0.75, rc5));
-            const double r3 = cube_dmul(cube_dmul(rmag, rmag), rmag);
-            const bool keep = rmag > rsoft;
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              double fp = cube_dmul(cube_dmul(mass, cube_ddiv(x21[d], r3)), pcut);
-              if (!keep) fp = cube_dmul(fp, 0.0);
-              ft[d] = cube_dadd(ft[d], fp);
-            }
+            if (nbuf == 0) mb[0] = m2;
+            else if (nbuf == 1) mb[1] = m2;
+            else if (nbuf == 2) mb[2] = m2;
+            else mb[3] = m2;
+            if (++nbuf == 4) flush();
             m2 = nxt[m2];
           }
         }
+    flush();
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       double k = cube_dmul(ft[d], a_mid);

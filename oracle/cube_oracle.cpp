@@ -464,8 +464,10 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
         std::fill(rho_f.begin(), rho_f.end(), 0.f);
         if (deposit_mode == 1) rho_q.assign(rho_f.size(), 0);
         auto fat = [&](int i, int j, int k) -> size_t { return ((size_t)(k - 1) * nfe + (j - 1)) * nfe + (i - 1); };
-        // fine_cic_mass (pm.f90:76-107)
+        // fine_cic_mass (pm.f90:76-107): three layers of k-planes, each layer's planes
+        // are CIC-disjoint, so the threads of a layer never touch the same node
         for (int il = 0; il < 3; ++il)
+#pragma omp parallel for schedule(static, 2)
           for (int k = 2 - ncb + il; k <= nt + ncb - 1; k += 3)
             for (int j = 2 - ncb; j <= nt + ncb - 1; ++j)
               for (int i = 2 - ncb; i <= nt + ncb - 1; ++i) {
@@ -547,6 +549,7 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
             }
         // fine velocity (pm.f90:131-155)
         const float kfac_a = a_mid, kfac_dt = dt;
+#pragma omp parallel for schedule(static, 2)
         for (int k = 1; k <= nt; ++k)
           for (int j = 1; j <= nt; ++j)
             for (int i = 1; i <= nt; ++i) {
@@ -598,6 +601,7 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
         if (deposit_mode == 1) r3q.assign(r3t.size(), 0);
         auto tat = [&](int i, int j, int k) { return ((size_t)(k + 1) * n3 + (j + 1)) * n3 + (i + 1); };
         for (int il = 0; il < 3; ++il)
+#pragma omp parallel for schedule(static, 2)
           for (int k = 0 + il; k <= nt + 1; k += 3)
             for (int j = 0; j <= nt + 1; ++j)
               for (int i = 0; i <= nt + 1; ++i) {
@@ -661,9 +665,11 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
   s->f2_max_coarse = f2c;
   // coarse velocity (pm.f90:335-372)
   const double coef = cube_vcoef(&o.codec, s->sigma_vi);
+  double vmx0 = 0, vmx1 = 0, vmx2 = 0;
   for (int tz = 0; tz < o.nnt; ++tz)
     for (int ty = 0; ty < o.nnt; ++ty)
       for (int tx = 0; tx < o.nnt; ++tx)
+#pragma omp parallel for schedule(static, 2) reduction(max : vmx0, vmx1, vmx2)
         for (int k = 1; k <= nt; ++k)
           for (int j = 1; j <= nt; ++j)
             for (int i = 1; i <= nt; ++i) {
@@ -697,11 +703,15 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                     t = cube_fmul(t, cx[c8][2] ? dx2[2] : dx1[2]);
                     v = cube_dadd(v, (double)t);
                   }
-                  vmax[d] = std::max(vmax[d], fabs(cube_dadd(v, (double)o.vfield[3 * c + d])));
+                  const double am = fabs(cube_dadd(v, (double)o.vfield[3 * c + d]));
+                  if (d == 0) vmx0 = std::max(vmx0, am);
+                  else if (d == 1) vmx1 = std::max(vmx1, am);
+                  else vmx2 = std::max(vmx2, am);
                   o.vp[3 * ip + d] = cube_wrap_code(cube_vencode(&o.codec, v, coef), o.izipv);
                 }
               }
             }
+  vmax[0] = vmx0; vmax[1] = vmx1; vmax[2] = vmx2;
   for (int d = 0; d < 3; ++d) s->vmax[d] = (float)vmax[d];
   s->testrhof = testrhof;
   s->testrhoc = testrhoc;
@@ -755,6 +765,7 @@ int ext_pp_force(Orc& o, cube_scalars* s) {
           const int cidx = (int)floorf(cube_fdiv((float)(fi - 1), 4.f));
           return cube_dadd((double)ncell * (double)cidx, cube_dmul((double)ncell, cube_xfrac(code, o.izipx)));
         };
+#pragma omp parallel for schedule(static, 2) reduction(+ : itest1, npairs) reduction(max : ftemp)
         for (int igz = 1; igz <= nft; ++igz)
           for (int igy = 1; igy <= nft; ++igy)
             for (int igx = 1; igx <= nft; ++igx) {

@@ -1,10 +1,11 @@
 /*
  * oracle_fft.h -- TEST INFRASTRUCTURE ONLY (the CPU oracle of the parity tests).
  *
- * Mixed-radix complex DFT for any length (recursive decimation in time, radix
- * = smallest prime factor, naive DFT inside each butterfly) and 3-D real
- * transforms built on it.  This stands in for FFTW 3.x (single precision in
- * the reference: sfftw_plan_dft_r2c_3d / c2r_3d, CUBE_v2.0/work/main/cubefft.f90:25-26,
+ * Mixed-radix complex DFT for any length (Stockham autosort passes, radix =
+ * prime factors of n, a plain DFT inside each butterfly, twiddles computed in
+ * long double) and 3-D real transforms built on it, threaded over lines with
+ * OpenMP.  This stands in for FFTW 3.x (single precision in the reference:
+ * sfftw_plan_dft_r2c_3d / c2r_3d, CUBE_v2.0/work/main/cubefft.f90:25-26,
  * pencil_fft.f90:178-189), which is not vendored with the reference.  Sign
  * conventions follow FFTW: the forward transform uses exp(-2 pi i jk/N), the
  * backward transform exp(+2 pi i jk/N), both unnormalised.  The results are
@@ -23,10 +24,9 @@ template <typename R>
 struct Dft1 {
   int n;
   int sign;
-  std::vector<std::complex<R>> w;  // w[j] = exp(sign*2 pi i j/n), computed in long double
+  std::vector<std::complex<R>> w;  // w[j] = exp(sign*2 pi i j/n)
   std::vector<int> fac;
-  std::vector<std::complex<R>> tmp;
-  Dft1(int n_, int sign_) : n(n_), sign(sign_), w(n_), tmp(n_) {
+  Dft1(int n_, int sign_) : n(n_), sign(sign_), w(n_) {
     for (int j = 0; j < n; ++j) {
       long double ang = (long double)sign * 2.0L * 3.14159265358979323846264338327950288L * (long double)j / (long double)n;
       w[j] = std::complex<R>((R)cosl(ang), (R)sinl(ang));
@@ -36,31 +36,31 @@ struct Dft1 {
       while (m % p == 0) { fac.push_back(p); m /= p; }
     if (m > 1) fac.push_back(m);
   }
-  // out[k] = sum_j in[j*stride] w^{jk}
-  void rec(const std::complex<R>* in, long stride, std::complex<R>* out, int len, int lvl,
-           int wstep) {
-    if (len == 1) { out[0] = in[0]; return; }
-    const int p = fac[lvl];
-    const int m = len / p;
-    for (int r = 0; r < p; ++r) rec(in + r * stride, stride * p, out + r * m, m, lvl + 1, wstep * p);
-    std::complex<R> t[64];
-    std::vector<std::complex<R>> big;
-    std::complex<R>* tt = t;
-    if (p > 64) { big.resize(p); tt = big.data(); }
-    std::vector<std::complex<R>> res(len);
-    for (int k = 0; k < m; ++k) {
-      for (int r = 0; r < p; ++r) tt[r] = out[r * m + k] * w[((long)r * k * wstep) % n];
-      for (int s = 0; s < p; ++s) {
-        std::complex<R> acc(0, 0);
-        for (int r = 0; r < p; ++r) acc += tt[r] * w[((long)r * s * m * wstep) % n];
-        res[k + m * s] = acc;
+  // in place on x with scratch y (both length n)
+  void run(std::complex<R>* x, std::complex<R>* y) const {
+    int T = 1;
+    std::complex<R>* a = x;
+    std::complex<R>* b = y;
+    std::complex<R> v[64];
+    for (size_t st = 0; st < fac.size(); ++st) {
+      const int p = fac[st];
+      const int nb = n / p;
+      const int tstep = n / (p * T);
+      for (int i = 0; i < nb; ++i) {
+        const int k = i % T;
+        for (int r = 0; r < p; ++r) v[r] = a[i + r * nb] * w[(size_t)r * k * tstep];
+        const int j0 = (i - k) * p + k;
+        for (int s = 0; s < p; ++s) {
+          std::complex<R> acc(0, 0);
+          for (int r = 0; r < p; ++r) acc += v[r] * w[((size_t)r * s * nb) % n];
+          b[j0 + s * T] = acc;
+        }
       }
+      std::swap(a, b);
+      T *= p;
     }
-    for (int i = 0; i < len; ++i) out[i] = res[i];
-  }
-  void run(std::complex<R>* data) {  // in place on contiguous data
-    std::vector<std::complex<R>> in(data, data + n);
-    rec(in.data(), 1, data, n, 0, 1);
+    if (a != x)
+      for (int i = 0; i < n; ++i) x[i] = a[i];
   }
 };
 
@@ -69,32 +69,44 @@ template <typename R>
 void cfft3(std::vector<std::complex<R>>& c, int nx, int ny, int nz, int sign) {
   {
     Dft1<R> d(nx, sign);
-    std::vector<std::complex<R>> line(nx);
-    for (long r = 0; r < (long)ny * nz; ++r) {
-      for (int i = 0; i < nx; ++i) line[i] = c[r * nx + i];
-      d.run(line.data());
-      for (int i = 0; i < nx; ++i) c[r * nx + i] = line[i];
+#pragma omp parallel
+    {
+      std::vector<std::complex<R>> line(nx), tmp(nx);
+#pragma omp for schedule(static)
+      for (long r = 0; r < (long)ny * nz; ++r) {
+        for (int i = 0; i < nx; ++i) line[i] = c[r * nx + i];
+        d.run(line.data(), tmp.data());
+        for (int i = 0; i < nx; ++i) c[r * nx + i] = line[i];
+      }
     }
   }
   {
     Dft1<R> d(ny, sign);
-    std::vector<std::complex<R>> line(ny);
-    for (int k = 0; k < nz; ++k)
-      for (int i = 0; i < nx; ++i) {
+#pragma omp parallel
+    {
+      std::vector<std::complex<R>> line(ny), tmp(ny);
+#pragma omp for schedule(static)
+      for (long r = 0; r < (long)nz * nx; ++r) {
+        const long k = r / nx, i = r % nx;
         for (int j = 0; j < ny; ++j) line[j] = c[((long)k * ny + j) * nx + i];
-        d.run(line.data());
+        d.run(line.data(), tmp.data());
         for (int j = 0; j < ny; ++j) c[((long)k * ny + j) * nx + i] = line[j];
       }
+    }
   }
   {
     Dft1<R> d(nz, sign);
-    std::vector<std::complex<R>> line(nz);
-    for (int j = 0; j < ny; ++j)
-      for (int i = 0; i < nx; ++i) {
+#pragma omp parallel
+    {
+      std::vector<std::complex<R>> line(nz), tmp(nz);
+#pragma omp for schedule(static)
+      for (long r = 0; r < (long)ny * nx; ++r) {
+        const long j = r / nx, i = r % nx;
         for (int k = 0; k < nz; ++k) line[k] = c[((long)k * ny + j) * nx + i];
-        d.run(line.data());
+        d.run(line.data(), tmp.data());
         for (int k = 0; k < nz; ++k) c[((long)k * ny + j) * nx + i] = line[k];
       }
+    }
   }
 }
 
