@@ -124,7 +124,8 @@ void cube_destroy(cube_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   void* ptrs[] = {ctx->xp, ctx->vp, ctx->pid, ctx->xp2, ctx->vp2, ctx->pid2, ctx->rhoc, ctx->rhoc2,
                   ctx->cell_start, ctx->cell_start2, ctx->vfield, ctx->vfield2, ctx->tcell, ctx->tkey,
-                  ctx->perm, ctx->pkey, ctx->cursor, ctx->big_list, ctx->cell_stats, ctx->red_tmp,
+                  ctx->perm, ctx->pkey, ctx->cursor, ctx->big_list, ctx->cell_stats, ctx->slot_r2, ctx->slot_s2,
+                  ctx->red_tmp,
                   ctx->scan_tmp, ctx->fine.rho, ctx->fine.force, ctx->fine.kern, ctx->fine.plan.tw,
                   ctx->coarse.rho, ctx->coarse.force, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->rho_c_acc,
                   ctx->tan_table, ctx->dscal};
@@ -201,6 +202,7 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
             A((void**)&ctx->tcell, 4 * cap) && A((void**)&ctx->tkey, 4 * cap) && A((void**)&ctx->perm, 4 * cap) &&
             A((void**)&ctx->pkey, 4 * cap) && A((void**)&ctx->cursor, 4 * nce) &&
             A((void**)&ctx->big_list, 4 * nce) && A((void**)&ctx->cell_stats, 24 * nce) &&
+            A((void**)&ctx->slot_r2, 8 * cap) && A((void**)&ctx->slot_s2, 8 * cap) &&
             A((void**)&ctx->red_tmp, 8 * (2 * (nce / 1024 + 64) + 64)) &&
             A((void**)&ctx->scan_tmp, 8 * (nce / 2048 + 64)) &&
             A((void**)&ctx->rho_c_acc, 8 * nce) && A((void**)&ctx->tan_table, 4 * ctx->nvbin) &&

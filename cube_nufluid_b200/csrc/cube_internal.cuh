@@ -77,6 +77,7 @@ struct cube_ctx {
   int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
   int32_t* big_list;
   double* cell_stats;   // [3][ncells]
+  double* slot_r2; double* slot_s2;  // per-slot statistics terms of the re-bin
   double* red_tmp;      // scratch for tree sums
   int64_t* scan_tmp;
   // meshes

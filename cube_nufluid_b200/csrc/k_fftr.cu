@@ -70,8 +70,7 @@ __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
 
 template <int L, int I>
 struct BitRev {
@@ -187,57 +186,6 @@ __global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_
     const int j = i / TK, c = i - j * TK;
     if (c < nk) b[(size_t)j * jstride + c] = sm[j * P + c];
   }
-}
-
-// Persistent column pass: each CTA walks tiles (TK columns x N, one y or z
-// line set) with two shared buffers, prefetching tile i+1 with cp.async while
-// it transforms and stores tile i.
-template <int N, int R, int T, int TK, int SIGN>
-__global__ void __launch_bounds__(T * TK) k_col_pipe(float2* __restrict__ base, size_t comp_stride, int ncol,
-                                                     long long jstride, long long ostride, int nother, int ncomp,
-                                                     const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  constexpr int P = TK + 1;
-  const int ntx = (ncol + TK - 1) / TK;
-  const int ntiles = ntx * nother * ncomp;
-  auto tile_ptr = [&](int tl, int& nk) -> float2* {
-    const int cx = tl % ntx, rest = tl / ntx;
-    const int o = rest % nother, comp = rest / nother;
-    nk = min(TK, ncol - cx * TK);
-    return base + comp * comp_stride + (size_t)o * ostride + cx * TK;
-  };
-  auto issue = [&](int tl, float2* dst) {
-    int nk;
-    const float2* b = tile_ptr(tl, nk);
-    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-      const int j = i / TK, c = i - j * TK;
-      cp_async8(&dst[j * P + c], c < nk ? &b[(size_t)j * jstride + c] : b, c < nk);
-    }
-  };
-  const int g = threadIdx.x / T, t = threadIdx.x % T;
-  int cur = 0;
-  int tile = blockIdx.x;
-  if (tile < ntiles) issue(tile, sm);
-  cp_async_commit();
-  for (; tile < ntiles; tile += gridDim.x) {
-    const int next = tile + gridDim.x;
-    if (next < ntiles) issue(next, sm + (cur ^ 1) * N * P);
-    cp_async_commit();
-    cp_async_wait_one();
-    __syncthreads();
-    float2* buf = sm + cur * N * P;
-    fft_seq<N, R, T, SIGN, false>(buf + g, P, t, tw);
-    __syncthreads();
-    int nk;
-    float2* b = tile_ptr(tile, nk);
-    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-      const int j = i / TK, c = i - j * TK;
-      if (c < nk) b[(size_t)j * jstride + c] = buf[j * P + c];
-    }
-    __syncthreads();
-    cur ^= 1;
-  }
-  cp_async_wait_all();
 }
 
 // fused z pass with the Green multiply (kernel octant [d][ky][kx][kz], kz fastest)
@@ -418,15 +366,9 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen<N, R, T, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   const dim3 g1((ncol + TK - 1) / TK, N, 1), g3((ncol + TK - 1) / TK, N, 3);
-  // y forward (persistent, double-buffered)
-  const size_t psm = 2 * csm;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col_pipe<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col_pipe<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm));
-  int per_sm = 0;
-  CUBE_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_col_pipe<N, R, T, TK, -1>, T * TK, psm));
-  const int pgrid = std::max(1, per_sm) * ctx->num_sms;
-  k_col_pipe<N, R, T, TK, -1><<<pgrid, T * TK, psm, ctx->stream>>>(reinterpret_cast<float2*>(L.rho), cstride, ncol, cp,
-                                                                   (long long)N * cp, N, 1, tw);
+  // y forward
+  k_col<N, R, T, TK, -1><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.rho), cstride, ncol, cp,
+                                                             (long long)N * cp, tw);
   CUBE_LAUNCH_CHECK(ctx);
   // z forward, Green, z inverse
   k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
@@ -434,8 +376,8 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
                                                             (long long)N * cp, cp, tw, L.kern, L.kern_pitch);
   CUBE_LAUNCH_CHECK(ctx);
   // y inverse, three components
-  k_col_pipe<N, R, T, TK, 1><<<pgrid, T * TK, psm, ctx->stream>>>(reinterpret_cast<float2*>(L.force), cstride, ncol,
-                                                                  cp, (long long)N * cp, N, 3, tw);
+  k_col<N, R, T, TK, 1><<<g3, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.force), cstride, ncol, cp,
+                                                            (long long)N * cp, tw);
   CUBE_LAUNCH_CHECK(ctx);
   // x c2r, three components, max f^2
   {

@@ -269,7 +269,7 @@ constexpr int PF = 4 * PR;                // region edge in fine cells (24)
 constexpr int PB_CAP = 4096;              // particles staged per brick
 
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(256, 2) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
+__global__ void __launch_bounds__(256, 3) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                                   const int64_t* __restrict__ cell_start, int64_t cap, int nc,
                                                   int nt, int nnt, int pr, int nf_cutoff, double rsoft,
                                                   double mass, double a_mid, double dt, double pi_d,
@@ -373,51 +373,27 @@ __global__ void __launch_bounds__(256, 2) k_pp_brick(const void* __restrict__ xp
       v[d] = cube_vdecode(__ldg(&tan_table[vc + half_nvbin]), coef);
     }
     ++n1;
-    // members of the window in the reference order, evaluated four at a time
-    // (independent FP64 chains) and added to ft in that order
     const bool pow2_cut = (nf_cutoff & (nf_cutoff - 1)) == 0;
     const double inv_cut = 1.0 / (double)nf_cutoff;
-    int mb[4];
-    int nbuf = 0;
-    auto flush = [&]() {
-      double fp[4][3];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        if (u < nbuf) {
-          const int m2 = mb[u];
-          const int f = fidx[m2];
-          const int cf[3] = {(f % PF) >> 2, ((f / PF) % PF) >> 2, (f / (PF * PF)) >> 2};
-          double x21[3];
-#pragma unroll
-          for (int d = 0; d < 3; ++d) {
-            const double fr = cube_xfrac((int32_t)(int16_t)code[3 * m2 + d], ZX);
-            x21[d] = cube_dsub(cube_dadd(4.0 * (double)cf[d], cube_dmul(4.0, fr)), x1[d]);
-          }
-          pp_pair(x21, mass, rsoft, nf_cutoff, pow2_cut, inv_cut, fp[u]);
-        }
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        if (u < nbuf)
-#pragma unroll
-          for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], fp[u][d]);
-      nbuf = 0;
-    };
     for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
       for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj)
         for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii) {
           int m2 = head[(kk * PF + jj) * PF + ii];
+          const int cf[3] = {ii >> 2, jj >> 2, kk >> 2};
           while (m2 != 0xFFFF) {
             ++npair;
-            if (nbuf == 0) mb[0] = m2;
-            else if (nbuf == 1) mb[1] = m2;
-            else if (nbuf == 2) mb[2] = m2;
-            else mb[3] = m2;
-            if (++nbuf == 4) flush();
+            double x21[3], fp[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const double fr = cube_xfrac((int32_t)(int16_t)code[3 * m2 + d], ZX);
+              x21[d] = cube_dsub(cube_dadd(4.0 * (double)cf[d], cube_dmul(4.0, fr)), x1[d]);
+            }
+            pp_pair(x21, mass, rsoft, nf_cutoff, pow2_cut, inv_cut, fp);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], fp[d]);
             m2 = nxt[m2];
           }
         }
-    flush();
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       double k = cube_dmul(ft[d], a_mid);

@@ -15,15 +15,19 @@
  *             coordinates; count per target cell
  *   scan    : cell starts
  *   place   : slot = start + atomic cursor (arbitrary order inside the cell)
- *   finalize: per target cell, sort its entries by (key, source index) --
+ *   sortsum : per target cell, sort its entries by (key, source index) --
  *             the reference order -- then run the FP32 velocity sum in that
- *             order, the division by (n + weight_v), and write x, v, pid in
- *             order; per-cell velocity statistics for the fixed-tree sums.
- *             Cells with more than 32 particles go to a block-wide sorter.
+ *             order and the division by (n + weight_v); cells with more than
+ *             32 particles go to a block-wide sorter
+ *   emit    : per slot (fully parallel), re-encode, move and copy the PID
+ *   stats   : per cell, the velocity statistics terms summed in slot order,
+ *             for the fixed-tree sums
  * Positions move by nint(dt_mid*v/(x_resolution*ncell)) with the integer
  * wrap of the 1- or 2-byte store (update_particle.f90:117).
  */
 #include "cube_internal.cuh"
+
+#include <algorithm>
 
 namespace {
 
@@ -37,7 +41,7 @@ struct RebinArgs {
   void* xp2; void* vp2; int32_t* pid2;
   int32_t* cnt2; int64_t* start2; float* vfield2;
   int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
-  int32_t* big_list; double* stats;
+  int32_t* big_list; double* stats; double* slot_r2; double* slot_s2;
   const float* tan_table; int half_nvbin;
   cube_codec codec; double coef;
   int64_t cap, ncells;
@@ -168,8 +172,11 @@ __device__ __forceinline__ void cell_tile(const RebinArgs& A, int64_t c, int tt[
   tt[2] = (int)(tile / ((int64_t)A.nnt * A.nnt));
 }
 
+// F1: per target cell, sort its entries into the reference order and run the
+// cell's FP32 velocity sum in that order (update_particle.f90:74,83-85).
+// Cells with more than SMALL entries go to k_rebin_big.
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(256) k_rebin_finalize(RebinArgs A) {
+__global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= A.ncells) return;
   const int n = A.cnt2[c];
@@ -210,35 +217,18 @@ __global__ void __launch_bounds__(256) k_rebin_finalize(RebinArgs A) {
       acc[d] = (float)cube_dadd((double)acc[d], v);
     }
   }
-  float vfn[3];
   const double den = cube_dadd((double)n, 0.1);
 #pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    vfn[d] = (float)cube_ddiv((double)acc[d], den);
-    A.vfield2[(size_t)d * A.ncells + c] = vfn[d];
-  }
-  double sr = 0.0, ss = 0.0;
-  for (int r = 0; r < n; ++r) {
-    const int64_t ip = A.perm[s + r];
-    const int64_t sc = src_cell(A, A.pkey[s + r], tt);
-    double v[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d)
-      v[d] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
-    emit<ZX, ZV>(A, s + r, ip, v, vfn, sr, ss);
-  }
-  const float f2 = cube_fadd(cube_fadd(cube_fmul(vfn[0], vfn[0]), cube_fmul(vfn[1], vfn[1])), cube_fmul(vfn[2], vfn[2]));
-  A.stats[c] = (double)f2;
-  A.stats[A.ncells + c] = sr;
-  A.stats[2 * A.ncells + c] = ss;
+  for (int d = 0; d < 3; ++d) A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc[d], den);
 }
 
-// one CTA per crowded cell: bitonic sort of (key<<32|source) in shared memory
+// F1 for crowded cells: one CTA per cell, bitonic sort of (key<<32|source) in
+// shared memory, per-particle velocities in parallel, the sum by one thread per
+// component in order
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
   extern __shared__ unsigned long long sk[];
-  double* sv = reinterpret_cast<double*>(sk + BIG_MAX);  // [3][BIG_MAX] velocities, later stats
-  __shared__ float vfn_s[3];
+  double* sv = reinterpret_cast<double*>(sk + BIG_MAX);  // [3][BIG_MAX] velocities
   const unsigned long long nbig = A.dscal->n_big;
   for (unsigned long long b = blockIdx.x; b < nbig; b += gridDim.x) {
     const int64_t c = A.big_list[b];
@@ -268,8 +258,11 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
     int tt[3];
     cell_tile(A, c, tt);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const int64_t ip = (int64_t)(uint32_t)(sk[i] & 0xffffffffu);
-      const int64_t sc = src_cell(A, (uint32_t)(sk[i] >> 32), tt);
+      const uint32_t key = (uint32_t)(sk[i] >> 32);
+      const int32_t ip = (int32_t)(uint32_t)(sk[i] & 0xffffffffu);
+      A.pkey[s + i] = key;  // sorted order back to the slots for the emit pass
+      A.perm[s + i] = ip;
+      const int64_t sc = src_cell(A, key, tt);
       for (int d = 0; d < 3; ++d)
         sv[d * BIG_MAX + i] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
     }
@@ -278,34 +271,54 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
       const int d = threadIdx.x;
       float acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
       for (int i = 0; i < n; ++i) acc = (float)cube_dadd((double)acc, sv[d * BIG_MAX + i]);
-      const float v = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
-      vfn_s[d] = v;
-      A.vfield2[(size_t)d * A.ncells + c] = v;
-    }
-    __syncthreads();
-    const float vfn[3] = {vfn_s[0], vfn_s[1], vfn_s[2]};
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const int64_t ip = (int64_t)(uint32_t)(sk[i] & 0xffffffffu);
-      const double v[3] = {sv[i], sv[BIG_MAX + i], sv[2 * BIG_MAX + i]};
-      double sr = 0.0, ss = 0.0;
-      emit<ZX, ZV>(A, s + i, ip, v, vfn, sr, ss);
-      sv[i] = sr;  // per-particle terms, summed in order below
-      sv[BIG_MAX + i] = ss;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double sr = 0.0, ss = 0.0;
-      for (int i = 0; i < n; ++i) {
-        sr = cube_dadd(sr, sv[i]);
-        ss = cube_dadd(ss, sv[BIG_MAX + i]);
-      }
-      const float f2 = cube_fadd(cube_fadd(cube_fmul(vfn[0], vfn[0]), cube_fmul(vfn[1], vfn[1])), cube_fmul(vfn[2], vfn[2]));
-      A.stats[c] = (double)f2;
-      A.stats[A.ncells + c] = sr;
-      A.stats[2 * A.ncells + c] = ss;
+      A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
     }
     __syncthreads();
   }
+}
+
+// F2: one thread per slot of the new layout: re-encode, move, copy the PID,
+// and keep the particle's two statistics terms for the in-order cell sums
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256) k_rebin_emit(RebinArgs A, int64_t np) {
+  for (int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; slot < np;
+       slot += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ip = A.perm[slot];
+    const int64_t c = A.tcell[ip];
+    int tt[3];
+    cell_tile(A, c, tt);
+    const int64_t sc = src_cell(A, A.pkey[slot], tt);
+    double v[3];
+    float vfn[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      v[d] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
+      vfn[d] = A.vfield2[(size_t)d * A.ncells + c];
+    }
+    double sr = 0.0, ss = 0.0;
+    emit<ZX, ZV>(A, slot, ip, v, vfn, sr, ss);
+    A.slot_r2[slot] = sr;
+    A.slot_s2[slot] = ss;
+  }
+}
+
+// F3: per cell, the statistics terms summed in slot order
+__global__ void k_rebin_stats(RebinArgs A) {
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= A.ncells) return;
+  const int64_t s0 = A.start2[c], s1 = s0 + A.cnt2[c];
+  double sr = 0.0, ss = 0.0;
+  for (int64_t q = s0; q < s1; ++q) {
+    sr = cube_dadd(sr, A.slot_r2[q]);
+    ss = cube_dadd(ss, A.slot_s2[q]);
+  }
+  float vfn[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) vfn[d] = A.vfield2[(size_t)d * A.ncells + c];
+  const float f2 = cube_fadd(cube_fadd(cube_fmul(vfn[0], vfn[0]), cube_fmul(vfn[1], vfn[1])), cube_fmul(vfn[2], vfn[2]));
+  A.stats[c] = (double)f2;
+  A.stats[A.ncells + c] = sr;
+  A.stats[2 * A.ncells + c] = ss;
 }
 
 template <int ZX, int ZV>
@@ -317,11 +330,16 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
   if (rc) return rc;
   k_rebin_place<<<1184, 256, 0, ctx->stream>>>(A, ctx->np);
   CUBE_LAUNCH_CHECK(ctx);
-  k_rebin_finalize<ZX, ZV><<<(unsigned)((ctx->ncells + 255) / 256), 256, 0, ctx->stream>>>(A);
+  const unsigned cb = (unsigned)((ctx->ncells + 255) / 256);
+  k_rebin_sortsum<ZX, ZV><<<cb, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
   const size_t smem = sizeof(unsigned long long) * BIG_MAX + sizeof(double) * 3 * BIG_MAX;
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rebin_big<ZX, ZV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_rebin_big<ZX, ZV><<<296, 512, smem, ctx->stream>>>(A);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_rebin_emit<ZX, ZV><<<(unsigned)std::min<int64_t>((ctx->np + 255) / 256, 148 * 64), 256, 0, ctx->stream>>>(A, ctx->np);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_rebin_stats<<<cb, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }
@@ -340,6 +358,7 @@ int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
   A.cnt2 = ctx->rhoc2; A.start2 = ctx->cell_start2; A.vfield2 = ctx->vfield2;
   A.tcell = ctx->tcell; A.tkey = ctx->tkey; A.perm = ctx->perm; A.pkey = ctx->pkey; A.cursor = ctx->cursor;
   A.big_list = ctx->big_list; A.stats = ctx->cell_stats;
+  A.slot_r2 = ctx->slot_r2; A.slot_s2 = ctx->slot_s2;
   A.tan_table = ctx->tan_table; A.half_nvbin = ctx->nvbin / 2;
   A.codec = ctx->codec; A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
   A.cap = ctx->cap; A.ncells = ctx->ncells;
