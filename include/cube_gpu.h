@@ -199,6 +199,24 @@ int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io);
 int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float* fine_force,
                                    const float* coarse_force);
 
+/* ---- allocation-free coarse density ------------------------------------------
+ * No counterpart in the reference.  For hosts that may not allocate device memory
+ * during a run (their HBM is owned by another allocator, or a fixed budget per box
+ * was handed out at start-up): computes the coarse CIC density of pm.f90:192-278,
+ * bit-identical to the coarse density of cube_particle_mesh, from caller-owned
+ * device buffers, and allocates nothing.
+ *   xp         device, int8|int16 [3][np_capacity] position codes (structure of arrays)
+ *   cell_start device, int64 [nc^3+1] first particle of each cell, tile-major order
+ *   rho        device, float [nc^3] output (x fastest), overwritten
+ *   stream     cudaStream_t (may be NULL) the kernels are launched on
+ * Its 64-bit accumulator is a static device array sized for nc <= 64 (2 MiB, held
+ * by every GPU that loads the library until exit); larger nc returns
+ * CUBE_ERR_CAPACITY.  Every call shares that array and clears it first, so calls
+ * that overlap on the GPU race.  The first call on a device looks up the array's
+ * address and should come before any stream capture. */
+int32_t cube_coarse_density_noalloc(int32_t nc, int32_t nnt, int32_t izipx, int64_t np_capacity, const void* xp,
+                                    const int64_t* cell_start, float mass_p_cdm, float* rho, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
