@@ -134,6 +134,27 @@ __device__ __forceinline__ int64_t cube_cell_of(int gx, int gy, int gz, int nt, 
   return ((((int64_t)tz * nnt + ty) * nnt + tx) * nt + lz) * (int64_t)nt * nt + (int64_t)ly * nt + lx;
 }
 
+// periodic wrap of an index that lies in [-n, 2n)
+__device__ __forceinline__ int cube_wrap(int x, int n) {
+  x += (x < 0) ? n : 0;
+  return x - ((x >= n) ? n : 0);
+}
+
+// tile-major cell id -> coordinates inside its tile (l) and the tile's first
+// global coarse cell per dimension (tb = tile index * nt)
+__device__ __forceinline__ void cube_cell_coords(int64_t c, int nt, int nnt, int l[3], int tb[3]) {
+  const int nt3 = nt * nt * nt;
+  const int64_t tile = c / nt3;
+  const int rem = (int)(c - tile * nt3);
+  const int t2 = (int)tile;  // < nnt^3 < 2^31
+  l[0] = rem % nt;
+  l[1] = (rem / nt) % nt;
+  l[2] = rem / (nt * nt);
+  tb[0] = (t2 % nnt) * nt;
+  tb[1] = ((t2 / nnt) % nnt) * nt;
+  tb[2] = (t2 / (nnt * nnt)) * nt;
+}
+
 // ---- launchers (implemented in the k_*.cu files) -----------------------------
 int cube_rebin(cube_ctx* ctx, cube_scalars* io);
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);

@@ -42,6 +42,7 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
   unsigned long long* cacc = facc + FX * FY * FZ;      // CX*CY*CZ
   __shared__ int64_t cst[NHC];
   __shared__ int cpre[NHC + 1];
+  __shared__ int lt[3][HX];  // in-tile coordinate of region cell -1..B-1 per dimension
 
   const int nbx = nc / BX, nby = nc / BY;
   const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
@@ -49,6 +50,11 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
 
   for (int i = threadIdx.x; i < FX * FY * FZ; i += blockDim.x) facc[i] = 0ull;
   for (int i = threadIdx.x; i < CX * CY * CZ; i += blockDim.x) cacc[i] = 0ull;
+  if (threadIdx.x >= 32 && threadIdx.x < 32 + 3 * HX) {
+    const int d = (threadIdx.x - 32) / HX, c = (threadIdx.x - 32) % HX;
+    const int base = d == 0 ? x0 : d == 1 ? y0 : z0;
+    lt[d][c] = cube_wrap(base + c - 1, nc) % nt;
+  }
   if (threadIdx.x < 32) {
     // cell table of the (B+1)^3 region in (z,y,x) order; warp 0 builds the prefix
     int run = 0;
@@ -57,8 +63,7 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
       int cnt = 0;
       if (q < NHC) {
         const int cx = q % HX - 1, cy = (q / HX) % HY - 1, cz = q / (HX * HY) - 1;
-        const int gx = (x0 + cx + nc) % nc, gy = (y0 + cy + nc) % nc, gz = (z0 + cz + nc) % nc;
-        const int64_t c = cube_cell_of(gx, gy, gz, nt, nnt);
+        const int64_t c = cube_cell_of(cube_wrap(x0 + cx, nc), cube_wrap(y0 + cy, nc), cube_wrap(z0 + cz, nc), nt, nnt);
         const int64_t s0 = cell_start[c];
         cst[q] = s0;
         cnt = (int)(cell_start[c + 1] - s0);
@@ -85,13 +90,13 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
     const int64_t ip = cst[q] + (t - cpre[q]);
     const int cx = q % HX - 1, cy = (q / HX) % HY - 1, cz = q / (HX * HY) - 1;
     const int cu[3] = {x0 + cx, y0 + cy, z0 + cz};     // unwrapped global coarse cell
+    const int cr[3] = {cx + 1, cy + 1, cz + 1};        // region index
     const int own = (cx >= 0 && cy >= 0 && cz >= 0);
     int o1[3], c1[3];
     float dx1[3], dx2[3], cd1[3], cd2[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const int g = (cu[d] + nc) % nc;
-      const int l = g % nt;
+      const int l = lt[d][cr[d]];
       const double fr = cube_xfrac((int32_t)xp[(size_t)d * cap + ip], ZX);
       // fine: tempx = ncell*(i-1) + ncell*frac (tile-relative), FP64 -> FP32
       const float tf = (float)cube_dadd(4.0 * (double)l, cube_dmul(4.0, fr));
@@ -137,7 +142,7 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
     const unsigned long long a = cacc[i];
     if (a) {
       const int nx = i % CX - 1, ny = (i / CX) % CY - 1, nz = i / (CX * CY) - 1;
-      const int gx = (x0 + nx + nc) % nc, gy = (y0 + ny + nc) % nc, gz = (z0 + nz + nc) % nc;
+      const int gx = cube_wrap(x0 + nx, nc), gy = cube_wrap(y0 + ny, nc), gz = cube_wrap(z0 + nz, nc);
       atomicAdd(&rho_c_acc[((size_t)gz * nc + gy) * nc + gx], a);
     }
   }

@@ -41,19 +41,21 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
   const TX* xp = reinterpret_cast<const TX*>(xp_);
   TV* vp = reinterpret_cast<TV*>(vp_);
   __shared__ int64_t cs[KCELLS + 1];
+  __shared__ int cl[KCELLS][3], ctb[KCELLS][3];  // per cell: local coords, tile base
   __shared__ unsigned int vmx_s[3];
   const int64_t c0 = (int64_t)blockIdx.x * KCELLS;
   const int ncl = (int)min((int64_t)KCELLS, ncells - c0);
   for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = cell_start[c0 + i];
+  if (threadIdx.x < ncl) cube_cell_coords(c0 + threadIdx.x, nt, nnt, cl[threadIdx.x], ctb[threadIdx.x]);
   if (threadIdx.x < 3) vmx_s[threadIdx.x] = 0u;
   __syncthreads();
   const int nf = 4 * nc;
   const float pi_f = codec.pi_f;
   const int64_t p0 = cs[0];
   const int npb = (int)(cs[ncl] - p0);
-  const int nt3 = nt * nt * nt;
   // reference corner order: 111,211,121,112,122,212,221,222
   const int ox[8] = {0, 1, 0, 0, 0, 1, 1, 1}, oy[8] = {0, 0, 1, 0, 1, 0, 1, 1}, oz[8] = {0, 0, 0, 1, 1, 1, 0, 1};
+  float vm[3] = {0.f, 0.f, 0.f};  // per-thread |v+vfield| maxima (non-negative)
   for (int i = threadIdx.x; i < 3 * npb; i += blockDim.x) {
     const int d = i / npb;
     const int64_t ip = p0 + (i - d * npb);
@@ -63,39 +65,41 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
       if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
     }
     const int64_t c = c0 + lo;
-    const int64_t tile = c / nt3;
-    const int rem = (int)(c - tile * nt3);
-    const int l[3] = {rem % nt, (rem / nt) % nt, rem / (nt * nt)};
-    const int t[3] = {(int)(tile % nnt), (int)((tile / nnt) % nnt), (int)(tile / ((int64_t)nnt * nnt))};
     const int code = (int)vp[(size_t)d * cap + ip];
     const float tan0 = __ldg(&tan_table[code + half_nvbin]);
     const float vf = __ldg(&vfield[(size_t)d * ncells + c]);
-    int n1[3], m1[3];
+    int fi[3][2], gi[3][2];
     float dx1[3], dx2[3], cx1[3], cx2[3];
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
+      const int l = cl[lo][e], tb = ctb[lo][e];
       const double fr = cube_xfrac((int32_t)xp[(size_t)e * cap + ip], ZX);
-      const float tf = (float)cube_dadd(4.0 * (double)l[e], cube_dmul(4.0, fr));
+      const float tf = (float)cube_dadd(4.0 * (double)l, cube_dmul(4.0, fr));
       const float f = floorf(tf) + 1.f;
       dx1[e] = cube_fsub(f, tf);
       dx2[e] = cube_fsub(1.f, dx1[e]);
-      n1[e] = 4 * t[e] * nt + (int)f - 1;  // global fine node of idx1 (0-based), < nf
-      const double g = cube_dadd((double)(t[e] * nt + l[e]), fr);
+      const int n1 = 4 * tb + (int)f - 1;  // global fine node of idx1 (0-based), <= nf
+      fi[e][0] = cube_wrap(n1, nf);
+      fi[e][1] = cube_wrap(n1 + 1, nf);
+      const double g = cube_dadd((double)(tb + l), fr);
       const float tc = (float)cube_dsub(g, 0.5);
       const float ci = floorf(tc) + 1.f;
       cx1[e] = cube_fsub(ci, tc);
       cx2[e] = cube_fsub(1.f, cx1[e]);
-      m1[e] = (int)ci - 1;  // global coarse node of idx1, may be -1
+      const int m1 = (int)ci - 1;  // global coarse node of idx1, may be -1
+      gi[e][0] = cube_wrap(m1, nc);
+      gi[e][1] = cube_wrap(m1 + 1, nc);
     }
     const float* F = ff + d * fcomp;
     const float* G = fc + d * ccomp;
+    const size_t fz[2] = {(size_t)fi[2][0] * fplane, (size_t)fi[2][1] * fplane};
+    const size_t gz[2] = {(size_t)gi[2][0] * cplane, (size_t)gi[2][1] * cplane};
+    const int fy[2] = {fi[1][0] * frp, fi[1][1] * frp}, gy[2] = {gi[1][0] * crp, gi[1][1] * crp};
     float fv[8], gv[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int fx = (n1[0] + ox[k]) % nf, fy = (n1[1] + oy[k]) % nf, fz = (n1[2] + oz[k]) % nf;
-      fv[k] = __ldg(&F[(size_t)fz * fplane + (size_t)fy * frp + fx]);
-      const int gx = (m1[0] + ox[k] + nc) % nc, gy = (m1[1] + oy[k] + nc) % nc, gz = (m1[2] + oz[k] + nc) % nc;
-      gv[k] = __ldg(&G[(size_t)gz * cplane + (size_t)gy * crp + gx]);
+      fv[k] = __ldg(&F[fz[oz[k]] + (size_t)(fy[oy[k]] + fi[0][ox[k]])]);
+      gv[k] = __ldg(&G[gz[oz[k]] + (size_t)(gy[oy[k]] + gi[0][ox[k]])]);
     }
     double v = cube_vdecode(tan0, coef_old);
 #pragma unroll
@@ -123,8 +127,16 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
       v = cube_dadd(v, (double)q);
     }
     const float am = (float)fabs(cube_dadd(v, (double)vf));
-    atomicMax(&vmx_s[d], __float_as_uint(am));
+    vm[0] = (d == 0) ? fmaxf(vm[0], am) : vm[0];
+    vm[1] = (d == 1) ? fmaxf(vm[1], am) : vm[1];
+    vm[2] = (d == 2) ? fmaxf(vm[2], am) : vm[2];
     vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
+  }
+  // every thread reaches here: warp maxima, then one shared atomic per warp and component
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const unsigned int w = __reduce_max_sync(0xffffffffu, __float_as_uint(vm[e]));
+    if ((threadIdx.x & 31) == 0 && w) atomicMax(&vmx_s[e], w);
   }
   __syncthreads();
   if (threadIdx.x < 3) atomicMax(&dscal->vmax_bits[threadIdx.x], vmx_s[threadIdx.x]);

@@ -65,12 +65,19 @@ __global__ void __launch_bounds__(256) k_rebin_count(RebinArgs A) {
   typedef typename CodeT<ZX>::T TX;
   const TX* xp = reinterpret_cast<const TX*>(A.xp);
   __shared__ int64_t cs[RCELLS + 1];
+  __shared__ int cl[RCELLS][3], ctt[RCELLS][3];  // per cell: local coords, tile coords
   const int64_t c0 = (int64_t)blockIdx.x * RCELLS;
   const int ncl = (int)min((int64_t)RCELLS, A.ncells - c0);
-  for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = A.cell_start[c0 + i];
-  __syncthreads();
   const int nt = A.nt, nnt = A.nnt, ncb = A.ncb, nte = A.nte;
-  const int nt3 = nt * nt * nt;
+  for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = A.cell_start[c0 + i];
+  for (int i = threadIdx.x; i < ncl; i += blockDim.x) {
+    int tb[3];
+    cube_cell_coords(c0 + i, nt, nnt, cl[i], tb);
+    ctt[i][0] = tb[0] / nt;
+    ctt[i][1] = tb[1] / nt;
+    ctt[i][2] = tb[2] / nt;
+  }
+  __syncthreads();
   for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
     int lo = 0, hi = ncl - 1;
     while (lo < hi) {
@@ -78,10 +85,8 @@ __global__ void __launch_bounds__(256) k_rebin_count(RebinArgs A) {
       if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
     }
     const int64_t c = c0 + lo;
-    const int64_t tile = c / nt3;
-    const int rem = (int)(c - tile * nt3);
-    const int l[3] = {rem % nt, (rem / nt) % nt, rem / (nt * nt)};
-    const int t[3] = {(int)(tile % nnt), (int)((tile / nnt) % nnt), (int)(tile / ((int64_t)nnt * nnt))};
+    const int l[3] = {cl[lo][0], cl[lo][1], cl[lo][2]};
+    const int t[3] = {ctt[lo][0], ctt[lo][1], ctt[lo][2]};
     int tg[3], src[3];
     bool bad = false;
 #pragma unroll
@@ -132,9 +137,9 @@ __global__ void k_rebin_place(RebinArgs A, int64_t np) {
 __device__ __forceinline__ int64_t src_cell(const RebinArgs& A, uint32_t key, const int tt[3]) {
   const int nte = A.nte, nt = A.nt, nc = A.nc, ncb = A.ncb;
   const int i = key % nte, j = (key / nte) % nte, k = (key / (nte * nte)) % nte;
-  const int gx = ((tt[0] * nt + i - ncb) % nc + nc) % nc;
-  const int gy = ((tt[1] * nt + j - ncb) % nc + nc) % nc;
-  const int gz = ((tt[2] * nt + k - ncb) % nc + nc) % nc;
+  const int gx = cube_wrap(tt[0] * nt + i - ncb, nc);
+  const int gy = cube_wrap(tt[1] * nt + j - ncb, nc);
+  const int gz = cube_wrap(tt[2] * nt + k - ncb, nc);
   return cube_cell_of(gx, gy, gz, nt, A.nnt);
 }
 
