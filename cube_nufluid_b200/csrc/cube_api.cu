@@ -84,6 +84,12 @@ float uint_as_float(unsigned int u) {
   return f;
 }
 
+unsigned int float_as_uint(float f) {
+  unsigned int u;
+  memcpy(&u, &f, 4);
+  return u;
+}
+
 /* dt constraints of particle_mesh (pm.f90:427-443), FP32 as the reference */
 void dt_constraints(const cube_ctx* ctx, cube_scalars* s) {
   const float pi_f = ctx->codec.pi_f;
@@ -99,6 +105,66 @@ void dt_constraints(const cube_ctx* ctx, cube_scalars* s) {
   const float vm = std::max(s->vmax[0], std::max(s->vmax[1], s->vmax[2]));
   s->dt_vmax = cube_fdiv(cube_fmul(ctx->P.vbuf, 20.f), vm);
   s->vz_max = s->vmax[2];
+  // vmax_nu is zeroed at pm.f90:40 and nothing raises it in the fluid model
+  if (ctx->nu.on) s->dt_vmax_nu = cube_fdiv(cube_fmul(ctx->P.vbuf, 20.f), 0.f);
+}
+
+// dfld_setup / hg_setup (hydrodf.f90:53-84, hydrogr.f90:39-90) for one species of
+// mass m_nu_ev with gamma = 5/3 (main.f90:38), on the host in FP32 with the C
+// library's expf, then the device arrays in their initial state
+int setup_neutrinos(cube_ctx* ctx) {
+  const cube_params& P = ctx->P;
+  NuState& N = ctx->nu;
+  const int nf = ctx->nf;
+  const float GLv[3] = {0.41577456f, 2.29428036f, 6.28994508f};
+  const float GLw[3] = {0.71109301f, 0.27851773f, 0.01038926f};
+  N.g = 5.f / 3.f;
+  N.beta = cube_fmul(5966.34f, P.m_nu_ev);
+  N.ai = cube_fdiv(1.f, cube_fadd(1.f, P.z_i_nu));  // NEUTRINO_IC: ai = ai_max (hydrodf.f90:13-15,96-97)
+  const float hg_dv = cube_fdiv((float)(2 * nf), cube_fmul(cube_fmul(300.f, sqrtf(P.omega_m)), P.box));
+  const int hg_nfb = P.ncb * P.ncell;
+  float wsum = 0.f;
+  for (int k = 0; k < 3; ++k) {
+    NuFluid& F = N.fl[k];
+    F.n = P.nu_nc[k] > 0 ? P.nu_nc[k] : nf >> (k + 1);
+    if (F.n < 4 || nf % F.n || (nf / F.n != 2 && nf / F.n != 4 && nf / F.n != 8) || nf % 32) {
+      ctx->err = "fluid meshes must be nf/2, nf/4 or nf/8 cells per side (>= 4), with nf a multiple of 32";
+      return CUBE_ERR_PARAM;
+    }
+    F.dx = cube_fdiv(cube_fmul(1.f, (float)nf), (float)F.n);
+    F.dv = hg_dv;
+    F.ncb = std::max(2, 1 + (int)floorf(cube_fdiv((float)hg_nfb, F.dx)));
+    const float v = cube_fmul(cube_fdiv(GLv[k], N.beta), 2.998e5f);
+    const float t = cube_fmul(v, F.dv);
+    F.cs2 = std::max(1e-6f, cube_fmul(t, t));
+    const float f0 = cube_fdiv(cube_fmul(GLv[k], GLv[k]), cube_fadd(expf(GLv[k]), 1.f));
+    N.dwgts[k] = cube_fmul(cube_fmul(GLw[k], f0), expf(GLv[k]));
+    wsum = (k == 0) ? N.dwgts[0] : cube_fadd(wsum, N.dwgts[k]);
+  }
+  for (int k = 0; k < 3; ++k) N.dwgts[k] = cube_fdiv(N.dwgts[k], wsum);
+  for (int k = 0; k < 3; ++k) {
+    NuFluid& F = N.fl[k];
+    const size_t n3 = (size_t)F.n * F.n * F.n;
+    if (cudaMalloc((void**)&F.block[0], 4 * 5 * n3) != cudaSuccess ||
+        cudaMalloc((void**)&F.block[1], 4 * 5 * n3) != cudaSuccess ||
+        cudaMalloc((void**)&F.xy, 4 * (size_t)5 * (nf + 4) * F.n * F.n) != cudaSuccess) {
+      ctx->err = "cudaMalloc of the fluid arrays failed";
+      return CUBE_ERR_CUDA;
+    }
+    for (int c = 0; c < 5; ++c) {
+      F.a[c] = F.block[0] + c * n3;
+      F.b[c] = F.block[1] + c * n3;
+    }
+    int rc = cube_nu_init(ctx, F);
+    if (rc) return rc;
+  }
+  N.nparts = ctx->num_sms * 8;
+  if (cudaMalloc((void**)&N.partial, 8 * (size_t)N.nparts) != cudaSuccess) {
+    ctx->err = "cudaMalloc failed";
+    return CUBE_ERR_CUDA;
+  }
+  N.on = true;
+  return CUBE_OK;
 }
 
 }  // namespace
@@ -131,6 +197,12 @@ void cube_destroy(cube_ctx* ctx) {
                   ctx->tan_table, ctx->dscal};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (int k = 0; k < 3; ++k) {
+    NuFluid& F = ctx->nu.fl[k];
+    for (float* q : {F.block[0], F.block[1], F.xy})
+      if (q) cudaFree(q);
+  }
+  if (ctx->nu.partial) cudaFree(ctx->nu.partial);
   if (ctx->hscal) cudaFreeHost(ctx->hscal);
   for (int i = 0; i < 16; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
@@ -223,6 +295,7 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
     return fail(CUBE_ERR_CUDA);
   }
   if ((rc = cube_build_green(ctx, fk_table, ck_table))) return fail(rc);
+  if (P.neutrino && (rc = setup_neutrinos(ctx))) return fail(rc);
   if (cudaDeviceSynchronize() != cudaSuccess) { ctx->err = "setup failed"; return fail(CUBE_ERR_CUDA); }
   *out = ctx;
   return CUBE_OK;
@@ -356,11 +429,21 @@ int32_t cube_particle_mesh(cube_ctx* ctx, cube_scalars* io) {
   CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[5], ctx->stream));
   if ((rc = cube_kick(ctx, io))) return rc;
   CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[6], ctx->stream));
+  if (ctx->nu.on) {
+    if ((rc = cube_nu_gravity(ctx, io))) return rc;
+    CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[9], ctx->stream));
+  }
   unsigned long long mt[2];
   CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(mt, ctx->red_tmp, 16, cudaMemcpyDeviceToHost, ctx->stream));
   if ((rc = check_device_error(ctx))) return rc;
   io->testrhof = (double)mt[0] * (1.0 / 4294967296.0);
   io->testrhoc = (double)mt[1] * (1.0 / 4294967296.0);
+  if (ctx->nu.on) {
+    double nus = 0.0;
+    if ((rc = cube_tree_sum_dev(ctx, ctx->nu.partial, ctx->nu.nparts, &nus))) return rc;
+    io->testrhof += nus;
+    cudaEventElapsedTime(&ctx->phase_ms[6], ctx->ev[6], ctx->ev[9]);
+  }
   io->f2_max_fine = uint_as_float(ctx->hscal->f2_fine_bits);
   io->f2_max_coarse = uint_as_float(ctx->hscal->f2_coarse_bits);
   for (int d = 0; d < 3; ++d) io->vmax[d] = uint_as_float(ctx->hscal->vmax_bits[d]);
@@ -467,10 +550,71 @@ int32_t cube_timestep(const cube_params* p, cube_scalars* s, float a_next, int32
 }
 
 int32_t cube_nu_evolve(cube_ctx* ctx, float dt, float* dtg, int32_t dir, float a) {
-  (void)dt; (void)dtg; (void)dir; (void)a;
-  if (!ctx) return CUBE_ERR_PARAM;
-  ctx->err = "fluid neutrinos are not enabled in this context";
-  return CUBE_ERR_PARAM;
+  if (!ctx || !dtg || (dir != 1 && dir != -1)) return CUBE_ERR_PARAM;
+  if (!ctx->nu.on) {
+    ctx->err = "fluid neutrinos are not enabled in this context";
+    return CUBE_ERR_STATE;
+  }
+  NuState& N = ctx->nu;
+  if (!(a >= N.ai)) return CUBE_OK;  // dfld_evolve: before the turn-on nothing moves
+  CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[10], ctx->stream));
+  const unsigned int big = float_as_uint(1e9f);
+  const unsigned int init[3] = {big, big, big};
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->dscal->nu_dt_bits, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+  for (int k = 0; k < 3; ++k) {
+    int rc = cube_nu_sweeps(ctx, N.fl[k], dt, dir);
+    if (rc) return rc;
+    if ((rc = cube_nu_timestep(ctx, N.fl[k], &ctx->dscal->nu_dt_bits[k]))) return rc;
+  }
+  CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[11], ctx->stream));
+  unsigned int bits[3];
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(bits, ctx->dscal->nu_dt_bits, sizeof(bits), cudaMemcpyDeviceToHost, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < 3; ++k) {  // hg_timestep: dt = min(dtg, h3_timestep) per fluid
+    float d = uint_as_float(bits[k]);
+    if (d == 1e9f) d = 1.f;
+    *dtg = std::min(*dtg, d);
+  }
+  cudaEventElapsedTime(&ctx->phase_ms[6], ctx->ev[10], ctx->ev[11]);
+  return CUBE_OK;
+}
+
+int32_t cube_nu_load(cube_ctx* ctx, int32_t fluid, const float* fld) {
+  if (!ctx || !fld || fluid < 0 || fluid > 2) return CUBE_ERR_PARAM;
+  if (!ctx->nu.on) { ctx->err = "fluid neutrinos are not enabled in this context"; return CUBE_ERR_STATE; }
+  NuFluid& F = ctx->nu.fl[fluid];
+  const size_t n3 = (size_t)F.n * F.n * F.n;
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(F.b[0], fld, 4 * 5 * n3, cudaMemcpyHostToDevice, ctx->stream));
+  int rc = cube_nu_transpose(ctx, F, 1);
+  if (rc) return rc;
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return CUBE_OK;
+}
+
+int32_t cube_nu_store(cube_ctx* ctx, int32_t fluid, float* fld) {
+  if (!ctx || !fld || fluid < 0 || fluid > 2) return CUBE_ERR_PARAM;
+  if (!ctx->nu.on) { ctx->err = "fluid neutrinos are not enabled in this context"; return CUBE_ERR_STATE; }
+  NuFluid& F = ctx->nu.fl[fluid];
+  const size_t n3 = (size_t)F.n * F.n * F.n;
+  int rc = cube_nu_transpose(ctx, F, 0);
+  if (rc) return rc;
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(fld, F.b[0], 4 * 5 * n3, cudaMemcpyDeviceToHost, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  return CUBE_OK;
+}
+
+int32_t cube_nu_info(cube_ctx* ctx, float* out) {
+  if (!ctx || !out) return CUBE_ERR_PARAM;
+  if (!ctx->nu.on) { ctx->err = "fluid neutrinos are not enabled in this context"; return CUBE_ERR_STATE; }
+  const NuState& N = ctx->nu;
+  out[0] = N.beta;
+  for (int k = 0; k < 3; ++k) out[1 + k] = N.dwgts[k];
+  for (int k = 0; k < 3; ++k) {
+    const NuFluid& F = N.fl[k];
+    float* q = out + 4 + 5 * k;
+    q[0] = (float)F.n; q[1] = (float)F.ncb; q[2] = F.dx; q[3] = F.cs2; q[4] = F.dv;
+  }
+  return CUBE_OK;
 }
 
 int32_t cube_phase_times(cube_ctx* ctx, float* ms8) {
@@ -523,6 +667,11 @@ int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io) {
   if ((rc = check_device_error(ctx))) return rc;
   io->testrhof = (double)mt[0] * (1.0 / 4294967296.0);
   io->testrhoc = (double)mt[1] * (1.0 / 4294967296.0);
+  if (ctx->nu.on) {
+    double nus = 0.0;
+    if ((rc = cube_tree_sum_dev(ctx, ctx->nu.partial, ctx->nu.nparts, &nus))) return rc;
+    io->testrhof += nus;
+  }
   return CUBE_OK;
 }
 
@@ -545,6 +694,7 @@ int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float*
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dscal, 0, sizeof(DevScal), ctx->stream));
   int rc = cube_kick(ctx, io);
   if (rc) return rc;
+  if (ctx->nu.on && (rc = cube_nu_gravity(ctx, io))) return rc;
   if ((rc = check_device_error(ctx))) return rc;
   for (int d = 0; d < 3; ++d) io->vmax[d] = uint_as_float(ctx->hscal->vmax_bits[d]);
   io->sigma_vi = io->sigma_vi_new;

@@ -54,6 +54,29 @@ struct DevScal {
   unsigned long long n_big;    // re-bin cells needing the block sorter
   unsigned long long itest1, npairs;
   unsigned long long moved_far;
+  unsigned int nu_dt_bits[3];  // per-fluid CFL step as float bits
+};
+
+// one isothermal fluid of the dispersive sum (hydrogr.f90 type hydro): five FP32
+// arrays of n^3 cells, x fastest, periodic; a = current state, b = the other
+// half of the ping-pong (each is one contiguous block of 5 n^3)
+struct NuFluid {
+  int n = 0, ncb = 0;              // cells per side; halo width of the reference layout
+  float dx = 0.f, cs2 = 0.f, dv = 0.f;
+  float* a[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float* b[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float* block[2] = {nullptr, nullptr};
+  float* xy = nullptr;             // gravity scratch [5][nf+4][n][n]
+};
+
+// fluid neutrinos of one species (hydrodf.f90 type dfld)
+struct NuState {
+  bool on = false;
+  float beta = 0.f, g = 0.f, ai = 0.f;
+  float dwgts[3] = {0.f, 0.f, 0.f};
+  NuFluid fl[3];
+  double* partial = nullptr;       // per-CTA sums of the fine neutrino density
+  int nparts = 0;
 };
 
 struct cube_ctx {
@@ -80,6 +103,7 @@ struct cube_ctx {
   double* slot_r2; double* slot_s2;  // per-slot statistics terms of the re-bin
   double* red_tmp;      // scratch for tree sums
   int64_t* scan_tmp;
+  NuState nu;
   // meshes
   MeshLevel fine, coarse;
   unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator
@@ -166,6 +190,12 @@ int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table
 int cube_tree_sum_dev(cube_ctx* ctx, const double* in, int64_t n, double* out_host);
 int cube_exclusive_scan(cube_ctx* ctx, const int32_t* in, int64_t n, int64_t* out);
 int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n);
+int cube_nu_init(cube_ctx* ctx, NuFluid& F);
+int cube_nu_sweeps(cube_ctx* ctx, NuFluid& F, float dt, int dir);
+int cube_nu_timestep(cube_ctx* ctx, NuFluid& F, unsigned int* dt_bits);
+int cube_nu_transpose(cube_ctx* ctx, NuFluid& F, int to_soa);
+int cube_nu_density(cube_ctx* ctx, cube_scalars* io);
+int cube_nu_gravity(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int ncomp, unsigned int* f2_bits);
 
 #endif

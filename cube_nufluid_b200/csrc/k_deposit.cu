@@ -190,6 +190,10 @@ int cube_deposit(cube_ctx* ctx, cube_scalars* io) {
                                                      ctx->rho_c_acc, mtot);
   }
   CUBE_LAUNCH_CHECK(ctx);
+  if (ctx->nu.on) {  // neutrino density into both meshes (pm.f90:55-74, :198-242)
+    const int rc = cube_nu_density(ctx, io);
+    if (rc) return rc;
+  }
   k_coarse_finalize<<<592, 256, 0, ctx->stream>>>(ctx->rho_c_acc, ctx->coarse.rho, nc, ctx->coarse.rp, mtot + 1);
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;

@@ -65,6 +65,11 @@ def load_library():
     L.cube_expansion.restype = None
     L.cube_nu_evolve.argtypes = [vp, C.c_float, C.POINTER(C.c_float), C.c_int32, C.c_float]
     L.cube_nu_evolve.restype = C.c_int32
+    for name in ("cube_nu_load", "cube_nu_store"):
+        getattr(L, name).argtypes = [vp, C.c_int32, vp]
+        getattr(L, name).restype = C.c_int32
+    L.cube_nu_info.argtypes = [vp, vp]
+    L.cube_nu_info.restype = C.c_int32
     L.cube_phase_times.argtypes = [vp, C.POINTER(C.c_float)]
     L.cube_phase_times.restype = C.c_int32
     L.cube_launch_count.argtypes = [vp]
@@ -179,13 +184,46 @@ class Cube:
         self._check(self.L.cube_particle_mesh(self.h, C.byref(s)))
 
     def step(self, s: CubeScalars, a_next: float = 0.0) -> bool:
-        """One pass of main.f90:49-64 (without the neutrino half steps)."""
+        """One pass of main.f90:49-64: timestep, neutrino half step, drift, PP,
+        particle mesh, neutrino half step."""
         hit = self.timestep(s, a_next)
+        if self.p.neutrino:
+            s.dt_neu = self.nu_evolve(s.dt / 2.0, s.dt_neu, 1, s.a_mid)
         self.update_x(s)
         if self.p.ext_pp_force:
             self.ext_pp_force(s)
         self.particle_mesh(s)
+        if self.p.neutrino:
+            s.dt_neu = self.nu_evolve(s.dt / 2.0, s.dt_neu, -1, s.a_mid)
         return hit
+
+    # ---- fluid neutrinos (hydrodf.f90) ---------------------------------------
+    def nu_evolve(self, dt: float, dtg: float, direction: int, a: float) -> float:
+        """neu%evolve(dt, dtg, dir, a); returns the lowered dtg."""
+        g = C.c_float(dtg)
+        self._check(self.L.cube_nu_evolve(self.h, float(np.float32(dt)), C.byref(g), int(direction), float(a)))
+        return g.value
+
+    def nu_info(self) -> dict:
+        out = np.zeros(19, np.float32)
+        self._check(self.L.cube_nu_info(self.h, _ptr(out)))
+        fl = out[4:].reshape(3, 5)
+        return {"beta": float(out[0]), "dwgts": out[1:4].copy(), "nc": fl[:, 0].astype(int),
+                "ncb": fl[:, 1].astype(int), "dx": fl[:, 2].copy(), "cs2": fl[:, 3].copy(), "dv": fl[:, 4].copy()}
+
+    def nu_load(self, fluid: int, fld: np.ndarray):
+        """fld: float32 [n,n,n,5] = the reference's fld(1:5,1:n,1:n,1:n)."""
+        a = np.ascontiguousarray(fld, dtype=np.float32)
+        n = int(self.nu_info()["nc"][fluid])
+        if a.shape != (n, n, n, 5):
+            raise ValueError(f"fluid {fluid} expects shape {(n, n, n, 5)}")
+        self._check(self.L.cube_nu_load(self.h, int(fluid), _ptr(a)))
+
+    def nu_store(self, fluid: int) -> np.ndarray:
+        n = int(self.nu_info()["nc"][fluid])
+        a = np.zeros((n, n, n, 5), np.float32)
+        self._check(self.L.cube_nu_store(self.h, int(fluid), _ptr(a)))
+        return a
 
     # ---- inspection --------------------------------------------------------
     def phase_times(self) -> list[float]:

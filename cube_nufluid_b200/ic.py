@@ -257,3 +257,33 @@ def pack(x: np.ndarray, vel: np.ndarray, nc: int, nnt: int, *, ncell: int = 4, i
     return ICState(nc=nc, nnt=nnt, izipx=izipx, izipv=izipv, xp=np.ascontiguousarray(xp),
                    vp=np.ascontiguousarray(vp), pid=pid, rhoc=rhoc, vfield=vfield, a=a,
                    sigma_vi=sigma_vi, mass_p_cdm=mass_p, vmax=vmax.astype(np.float32), vsim2phys=vsim2phys)
+
+
+def nu_fluid_perturbed(nc: int, seed: int, *, cs2: float, gamma: float = np.float32(5.0) / np.float32(3.0),
+                       amp_rho: float = 0.2, amp_v: float = 0.5) -> np.ndarray:
+    """A smooth seeded fluid state fld(1:5,1:nc,1:nc,1:nc) as float32 [nc,nc,nc,5]
+    (z, y, x, component): rho = 1 + amp_rho*s, momentum = rho*v with
+    v = amp_v*sqrt(cs2)*s', energy = rho*cs2/(g-1) + |m|^2/(2 rho) -- the
+    composition neutrino_ic.f90 builds (density, isotropic stress, kinetic
+    energy), on a band-limited random field instead of the linear one."""
+    f32 = np.float32
+    k = np.fft.fftfreq(nc) * nc
+    kk = np.sqrt(k[:, None, None] ** 2 + k[None, :, None] ** 2 + k[None, None, :] ** 2)
+    filt = np.exp(-(kk / max(nc / 8.0, 1.0)) ** 2)
+
+    def field(s):
+        w = np.fft.ifftn(np.fft.fftn(gaussian_noise(nc, s)) * filt).real
+        return (w / max(np.abs(w).max(), 1e-30)).astype(f32)
+
+    rho = (f32(1.0) + f32(amp_rho) * field(seed)).astype(f32)
+    cs = f32(np.sqrt(f32(cs2)))
+    out = np.zeros((nc, nc, nc, 5), f32)
+    out[..., 0] = rho
+    e = rho * f32(cs2) / (f32(gamma) - f32(1.0))
+    for d in range(3):
+        v = (f32(amp_v) * cs * field(seed + 1 + d)).astype(f32)
+        m = (rho * v).astype(f32)
+        out[..., 1 + d] = m
+        e = (e + f32(0.5) * m * m / rho).astype(f32)
+    out[..., 4] = e
+    return out

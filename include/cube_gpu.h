@@ -11,6 +11,8 @@
  *                                          keeps every particle once and reads
  *                                          neighbour cells by periodic index
  *   neu(nu)%evolve (hydrodf.f90:86)     -> cube_nu_evolve
+ *   neu(nu)%gravity / %density (hydrodf.f90:111,209) -> inside cube_particle_mesh
+ *   neu(nu)%restart / %checkpoint (hydrodf.f90:158,134) -> cube_nu_load / cube_nu_store
  *   timestep       (timestep.f90:1)     -> cube_timestep (host arithmetic)
  *   kernel_f / kernel_c (kernel_f.f90:2, kernel_c.f90:2) -> inside cube_create
  *
@@ -158,8 +160,28 @@ int32_t cube_timestep(const cube_params* params, cube_scalars* io, float a_next,
 /* Friedmann expansion of timestep.f90:136-180 (real(4) interface, FP64 inside). */
 void cube_expansion(const cube_params* params, float a0, float dt0, float* da1, float* da2);
 
-/* Fluid-neutrino half step (hydrodf.f90:86-109). dir=+1 sweeps x,y,z; -1 z,y,x. */
+/* ---- fluid neutrinos (params.neutrino = 1) ------------------------------------
+ * One species of mass m_nu_ev (Nneu = 1, parameters.f90:80) as the dispersive sum
+ * of three isothermal fluids (hydrodf.f90:22-49) on meshes of nu_nc[k] cells per
+ * side (0 = nf/2, nf/4, nf/8), gamma = 5/3.  cube_create sets them to hg_setup's
+ * rest state; cube_particle_mesh adds their density to both meshes and applies
+ * the mesh forces to them (pm.f90:55-74, :157-171, :198-242, :374-422).
+ *
+ * Half step neu(nu)%evolve(dt,dtg,dir,a) (hydrodf.f90:86-109): dir = +1 sweeps
+ * x,y,z, -1 sweeps z,y,x; no-op while a < 1/(1+z_i_nu); *dtg is lowered to each
+ * fluid's CFL step (hydrogr.f90:92-108). */
 int32_t cube_nu_evolve(cube_ctx* ctx, float dt, float* dtg, int32_t dir, float a);
+
+/* Fluid k (0..2) to / from the host as fld(1:5,1:n,1:n,1:n): float [n][n][n][5],
+ * component fastest (rho, rho*vx, rho*vy, rho*vz, E), the physical cells of the
+ * reference's fld array (hydrogr.f90:21; its checkpoint adds the halo cells,
+ * hydrodf.f90:134-156). */
+int32_t cube_nu_load(cube_ctx* ctx, int32_t fluid, const float* fld);
+int32_t cube_nu_store(cube_ctx* ctx, int32_t fluid, float* fld);
+
+/* Set-up constants, 19 floats: beta = m/T, the three normalised weights, then
+ * per fluid (n, ncb of the reference layout, dx, cs2, hg_dv). */
+int32_t cube_nu_info(cube_ctx* ctx, float* out);
 
 /* Device time of the phases of the last step call, milliseconds:
  * [0] update_x, [1] ext_pp_force, [2] deposit, [3] fine FFT+Green, [4] coarse

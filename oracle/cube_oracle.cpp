@@ -42,6 +42,7 @@
 #include "../include/cube_gpu.h"
 #include "../cube_nufluid_b200/csrc/cube_codec.h"
 #include "oracle_fft.h"
+#include "oracle_nu.h"
 
 namespace {
 
@@ -69,6 +70,9 @@ struct Orc {
   std::vector<float> force_f_global;  // [3][nf^3]
   std::vector<float> r3;              // [nc^3]
   std::vector<float> force_c;         // [3][nc^3]
+  // fluid neutrinos (one species, hydrodf.f90 type dfld)
+  bool nu_on = false;
+  orcnu::Dfld nu;
   std::string err;
 };
 
@@ -425,6 +429,8 @@ void dt_constraints(const Orc& o, cube_scalars* s) {
   const float vm = std::max(s->vmax[0], std::max(s->vmax[1], s->vmax[2]));
   s->dt_vmax = cube_fdiv(cube_fmul(o.P.vbuf, 20.f), vm);
   s->vz_max = s->vmax[2];
+  // vmax_nu is zeroed at pm.f90:40 and never raised by the fluid: dt_vmax_nu = +Inf
+  if (o.nu_on) s->dt_vmax_nu = cube_fdiv(cube_fmul(o.P.vbuf, 20.f), 0.f);
 }
 
 struct KickIn {
@@ -464,6 +470,24 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
         std::fill(rho_f.begin(), rho_f.end(), 0.f);
         if (deposit_mode == 1) rho_q.assign(rho_f.size(), 0);
         auto fat = [&](int i, int j, int k) -> size_t { return ((size_t)(k - 1) * nfe + (j - 1)) * nfe + (i - 1); };
+        // neutrino density into the fine mesh (pm.f90:55-74), before the particles
+        std::vector<float> nu_t;
+        if (o.nu_on) {
+          nu_t.assign(rho_f.size(), 0.f);
+          if (1.f / a_mid - 1.f > o.P.z_i_nu) {
+            for (size_t q = 0; q < nu_t.size(); ++q) nu_t[q] = 0.f + o.P.f_neu;
+          } else {
+#pragma omp parallel for schedule(static)
+            for (int k = 1; k <= nfe; ++k)
+              for (int j = 1; j <= nfe; ++j)
+                for (int i = 1; i <= nfe; ++i) {
+                  const float x[3] = {(float)(tx * nt * ncell + i - nfb) - 0.5f, (float)(ty * nt * ncell + j - nfb) - 0.5f,
+                                      (float)(tz * nt * ncell + k - nfb) - 0.5f};
+                  nu_t[fat(i, j, k)] = 0.f + orcnu::dfld_density(o.nu, x) * o.P.f_neu;
+                }
+          }
+          if (deposit_mode == 0) rho_f = nu_t;
+        }
         // fine_cic_mass (pm.f90:76-107): three layers of k-planes, each layer's planes
         // are CIC-disjoint, so the threads of a layer never touch the same node
         for (int il = 0; il < 3; ++il)
@@ -497,7 +521,10 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                 }
               }
         if (deposit_mode == 1)
-          for (size_t q = 0; q < rho_f.size(); ++q) rho_f[q] = (float)((double)rho_q[q] * (1.0 / 4294967296.0));
+          for (size_t q = 0; q < rho_f.size(); ++q) {
+            rho_f[q] = (float)((double)rho_q[q] * (1.0 / 4294967296.0));
+            if (o.nu_on) rho_f[q] = cube_fadd(rho_f[q], nu_t[q]);
+          }
         for (int k = nfb + 1; k <= nft + nfb; ++k)
           for (int j = nfb + 1; j <= nft + nfb; ++j)
             for (int i = nfb + 1; i <= nft + nfb; ++i) {
@@ -585,6 +612,26 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                 }
               }
             }
+        // neutrino gravity from the fine force (pm.f90:157-171), sequential in the
+        // reference's (k,j,i,kk,jj,ii) order: the scatter is order-dependent
+        if (o.nu_on)
+          for (int k = 1; k <= nt; ++k)
+            for (int j = 1; j <= nt; ++j)
+              for (int i = 1; i <= nt; ++i)
+                for (int kk = 1; kk <= ncell; ++kk)
+                  for (int jj = 1; jj <= ncell; ++jj)
+                    for (int ii = 1; ii <= ncell; ++ii) {
+                      const int m[3] = {ncell * (i - 1) + ii, ncell * (j - 1) + jj, ncell * (k - 1) + kk};
+                      // idx1 = floor(tempx)+1+nfb -> force_f offset m+1 from rho index nfb
+                      const float* f = &force_f[(((size_t)(m[2] + 1) * nfo + (m[1] + 1)) * nfo + (m[0] + 1)) * 3];
+                      double acc[3];
+                      for (int d = 0; d < 3; ++d)
+                        acc[d] = (double)cube_fdiv(cube_fdiv(cube_fmul(cube_fmul(f[d], a_mid), dt), 6.f), pi_f);
+                      const int tt[3] = {tx, ty, tz};
+                      float x[3];
+                      for (int d = 0; d < 3; ++d) x[d] = (float)(tt[d] * nt * ncell + m[d]) - 0.5f;
+                      orcnu::dfld_gravity(o.nu, x, acc, a_mid, o.P.z_i_nu);
+                    }
       }
   s->f2_max_fine = f2_max_fine;
   s->sigma_vi = s->sigma_vi_new;
@@ -600,6 +647,44 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
         std::vector<int64_t> r3q;
         if (deposit_mode == 1) r3q.assign(r3t.size(), 0);
         auto tat = [&](int i, int j, int k) { return ((size_t)(k + 1) * n3 + (j + 1)) * n3 + (i + 1); };
+        // neutrino density into the coarse mesh (pm.f90:198-242), buffer cells included
+        auto r3add = [&](size_t q, float w) {
+          if (deposit_mode == 1) r3q[q] += (int64_t)llrint((double)w * 4294967296.0);
+          else r3t[q] = cube_fadd(r3t[q], w);
+        };
+        if (o.nu_on) {
+          if (1.f / a_mid - 1.f > o.P.z_i_nu) {
+            const float hom = o.P.f_neu * (float)(ncell * ncell * ncell);
+            for (size_t q = 0; q < r3t.size(); ++q) r3add(q, hom);
+          } else {
+            for (int k = 0; k <= nt + 1; ++k)
+              for (int j = 0; j <= nt + 1; ++j)
+                for (int i = 0; i <= nt + 1; ++i)
+                  for (int kk = 1; kk <= ncell; ++kk)
+                    for (int jj = 1; jj <= ncell; ++jj)
+                      for (int ii = 1; ii <= ncell; ++ii) {
+                        const int ijk[3] = {i, j, k}, sub[3] = {ii, jj, kk}, tt[3] = {tx, ty, tz};
+                        float x[3], c1[3], c2[3];
+                        int i1[3];
+                        for (int d = 0; d < 3; ++d) {
+                          x[d] = (float)(tt[d] * nt * ncell + (ijk[d] - 1) * ncell + sub[d]) - 0.5f;
+                          float xc = ((float)((ijk[d] - 1) * ncell + sub[d]) - 0.5f) / (float)ncell;
+                          xc = xc - 0.5f;
+                          i1[d] = 1 + (int)floorf(xc);
+                          c1[d] = (float)i1[d] - xc;
+                          c2[d] = 1.f - c1[d];
+                        }
+                        const float rho_nu = orcnu::dfld_density(o.nu, x) * o.P.f_neu;
+                        const int ox[8] = {0, 1, 0, 1, 0, 1, 0, 1}, oy[8] = {0, 0, 1, 1, 0, 0, 1, 1},
+                                  oz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+                        for (int c8 = 0; c8 < 8; ++c8) {
+                          const float w = cube_fmul(cube_fmul(cube_fmul(rho_nu, ox[c8] ? c2[0] : c1[0]), oy[c8] ? c2[1] : c1[1]),
+                                                    oz[c8] ? c2[2] : c1[2]);
+                          r3add(tat(i1[0] + ox[c8], i1[1] + oy[c8], i1[2] + oz[c8]), w);
+                        }
+                      }
+          }
+        }
         for (int il = 0; il < 3; ++il)
 #pragma omp parallel for schedule(static, 2)
           for (int k = 0 + il; k <= nt + 1; k += 3)
@@ -711,6 +796,43 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                 }
               }
             }
+  // neutrino gravity from the coarse force (pm.f90:374-422), sequential
+  if (o.nu_on)
+    for (int k = 0; k <= nc + 1; ++k)
+      for (int j = 0; j <= nc + 1; ++j)
+        for (int i = 0; i <= nc + 1; ++i)
+          for (int kk = 1; kk <= ncell; ++kk)
+            for (int jj = 1; jj <= ncell; ++jj)
+              for (int ii = 1; ii <= ncell; ++ii) {
+                const int m[3] = {(i - 1) * ncell + ii, (j - 1) * ncell + jj, (k - 1) * ncell + kk};
+                if (std::min(std::min(m[0], m[1]), m[2]) < -1 || std::max(std::max(m[0], m[1]), m[2]) > nf + 2) continue;
+                float x[3], c1[3], c2[3];
+                int i1[3];
+                for (int d = 0; d < 3; ++d) {
+                  x[d] = (float)m[d] - 0.5f;
+                  float xc = x[d] / (float)ncell;
+                  xc = xc - 0.5f;
+                  i1[d] = 1 + (int)floorf(xc);
+                  c1[d] = (float)i1[d] - xc;
+                  c2[d] = 1.f - c1[d];
+                }
+                const int ox[8] = {0, 1, 0, 1, 0, 1, 0, 1}, oy[8] = {0, 0, 1, 1, 0, 0, 1, 1}, oz[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+                double acc[3] = {0.0, 0.0, 0.0};
+                for (int c8 = 0; c8 < 8; ++c8) {
+                  // force_c(:,0:nc+1) with its periodic halo
+                  const int fi = ((i1[0] + ox[c8] - 1) % nc + nc) % nc, fj = ((i1[1] + oy[c8] - 1) % nc + nc) % nc,
+                            fk = ((i1[2] + oz[c8] - 1) % nc + nc) % nc;
+                  for (int d = 0; d < 3; ++d) {
+                    const float fv = o.force_c[(size_t)d * nc * nc * nc + ((size_t)fk * nc + fj) * nc + fi];
+                    float t = cube_fdiv(cube_fdiv(cube_fmul(cube_fmul(fv, a_mid), dt), 6.f), pi_f);
+                    t = cube_fmul(t, ox[c8] ? c2[0] : c1[0]);
+                    t = cube_fmul(t, oy[c8] ? c2[1] : c1[1]);
+                    t = cube_fmul(t, oz[c8] ? c2[2] : c1[2]);
+                    acc[d] = cube_dadd(acc[d], (double)t);
+                  }
+                }
+                orcnu::dfld_gravity(o.nu, x, acc, a_mid, o.P.z_i_nu);
+              }
   vmax[0] = vmx0; vmax[1] = vmx1; vmax[2] = vmx2;
   for (int d = 0; d < 3; ++d) s->vmax[d] = (float)vmax[d];
   s->testrhof = testrhof;
@@ -861,7 +983,62 @@ void* orc_create(const cube_params* p, const float* fk_table, const float* ck_ta
   o->ck_table.assign(ck_table, ck_table + 3 * 64);
   o->np = 0;
   if (build_kernels) { kernel_f(*o); kernel_c(*o); }
+  if (p->neutrino) {
+    // one species (Nneu=1, parameters.f90:80-93); gamma = 5/3 (main.f90:38)
+    o->nu_on = true;
+    const int nf = o->nf;
+    const int nc_n[3] = {p->nu_nc[0] > 0 ? p->nu_nc[0] : nf / 2, p->nu_nc[1] > 0 ? p->nu_nc[1] : nf / 4,
+                         p->nu_nc[2] > 0 ? p->nu_nc[2] : nf / 8};
+    const float hg_dv = (float)(2 * nf) / ((300.f * sqrtf(p->omega_m)) * p->box);  // hydrogr.f90:13
+    orcnu::dfld_setup(o->nu, 5.f / 3.f, p->m_nu_ev, nc_n, nf, p->ncb * p->ncell, hg_dv);
+  }
   return o;
+}
+
+/* fluid n (0..2) interior as fld(1:5,1:nc,1:nc,1:nc), component fastest */
+int orc_nu_load(void* h, int n, const float* fld) {
+  Orc& o = *(Orc*)h;
+  if (!o.nu_on || n < 0 || n > 2) return CUBE_ERR_STATE;
+  orcnu::Hydro& y = o.nu.h[n];
+  size_t q = 0;
+  for (int k = 1; k <= y.nc; ++k)
+    for (int j = 1; j <= y.nc; ++j)
+      for (int i = 1; i <= y.nc; ++i)
+        for (int c = 1; c <= 5; ++c) y.f(c, i, j, k) = fld[q++];
+  orcnu::hg_buffer(y);
+  return CUBE_OK;
+}
+
+int orc_nu_store(void* h, int n, float* fld) {
+  Orc& o = *(Orc*)h;
+  if (!o.nu_on || n < 0 || n > 2) return CUBE_ERR_STATE;
+  const orcnu::Hydro& y = o.nu.h[n];
+  size_t q = 0;
+  for (int k = 1; k <= y.nc; ++k)
+    for (int j = 1; j <= y.nc; ++j)
+      for (int i = 1; i <= y.nc; ++i)
+        for (int c = 1; c <= 5; ++c) fld[q++] = y.f(c, i, j, k);
+  return CUBE_OK;
+}
+
+/* neu%evolve(dt,dtg,dir,a) (hydrodf.f90:86-109) */
+int orc_nu_evolve(void* h, float dt, float* dtg, int dir, float a) {
+  Orc& o = *(Orc*)h;
+  if (!o.nu_on) return CUBE_ERR_STATE;
+  orcnu::dfld_evolve(o.nu, dt, *dtg, dir, a, o.P.z_i_nu);
+  return CUBE_OK;
+}
+
+/* beta, dwgts[3], then per fluid: nc, ncb, dx, cs2, dv (3 x 5) */
+void orc_nu_info(void* h, float* out) {
+  const Orc& o = *(Orc*)h;
+  out[0] = o.nu.beta;
+  for (int n = 0; n < 3; ++n) out[1 + n] = o.nu.dwgts[n];
+  for (int n = 0; n < 3; ++n) {
+    const orcnu::Hydro& y = o.nu.h[n];
+    float* q = out + 4 + 5 * n;
+    q[0] = (float)y.nc; q[1] = (float)y.ncb; q[2] = y.dx; q[3] = y.cs2; q[4] = y.dv;
+  }
 }
 
 void orc_destroy(void* h) { delete (Orc*)h; }

@@ -40,3 +40,15 @@ def rel_rms(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b ** 2)), 1e-300))
+
+
+# fluid neutrinos: 3 x 0.1 eV at h=0.67 (parameters.f90:80-93), FP32 as there
+_F32 = np.float32
+OMEGA_NU = _F32(3.0) * _F32(0.1) * _F32(1.0) / _F32(93.14) / (_F32(0.67) ** 2)
+F_NEU = float(OMEGA_NU / (_F32(0.27 + 0.05) + OMEGA_NU))
+
+
+def nu_params(nc=16, nnt=2, box=300.0, **kw):
+    """Parameters with the fluid neutrinos of the reference's defaults."""
+    return make_params(nc, nnt, box=box, neutrino=True, f_neu=F_NEU, m_nu_ev=0.1, z_i_nu=10.0,
+                       omega_m=float(_F32(0.32) + OMEGA_NU), h0=0.67, **kw)

@@ -59,6 +59,10 @@ def lib():
         L.orc_vdecode.argtypes = [vp, C.c_int, C.c_float]
         L.orc_tree_sum.restype = C.c_double
         L.orc_tree_sum.argtypes = [vp, C.c_int64]
+        L.orc_nu_load.argtypes = [vp, C.c_int, vp]
+        L.orc_nu_store.argtypes = [vp, C.c_int, vp]
+        L.orc_nu_evolve.argtypes = [vp, C.c_float, C.POINTER(C.c_float), C.c_int, C.c_float]
+        L.orc_nu_info.argtypes = [vp, vp]
         _lib = L
     return _lib
 
@@ -134,3 +138,27 @@ class Oracle:
         if got < 0:
             raise RuntimeError("orc_fetch failed")
         return out[:got]
+
+    # ---- fluid neutrinos (hydrodf.f90) ----------------------------------------
+    def nu_info(self) -> dict:
+        out = np.zeros(4 + 15, np.float32)
+        lib().orc_nu_info(self.h, _ptr(out))
+        fl = out[4:].reshape(3, 5)
+        return {"beta": float(out[0]), "dwgts": out[1:4].copy(), "nc": fl[:, 0].astype(int), "ncb": fl[:, 1].astype(int),
+                "dx": fl[:, 2].copy(), "cs2": fl[:, 3].copy(), "dv": fl[:, 4].copy()}
+
+    def nu_load(self, n: int, fld: np.ndarray):
+        """fld: float32 [nc,nc,nc,5] (z,y,x,component) = the reference's fld(1:5,1:nc,1:nc,1:nc)."""
+        a = np.ascontiguousarray(fld, dtype=np.float32)
+        self._check(lib().orc_nu_load(self.h, n, _ptr(a)))
+
+    def nu_store(self, n: int) -> np.ndarray:
+        nc = int(self.nu_info()["nc"][n])
+        a = np.zeros((nc, nc, nc, 5), np.float32)
+        self._check(lib().orc_nu_store(self.h, n, _ptr(a)))
+        return a
+
+    def nu_evolve(self, dt: float, dtg: float, direction: int, a: float) -> float:
+        g = C.c_float(dtg)
+        self._check(lib().orc_nu_evolve(self.h, dt, C.byref(g), direction, a))
+        return g.value
