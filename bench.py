@@ -42,7 +42,21 @@ CONFIGS = {
                 workload="256^3 particles, 500 Mpc/h, fine 512^3, coarse 128^3, int2 x/v, PP on (profiling size)"),
     "c1": dict(nc=32, nnt=2, box=200.0, izip=2, pp=False, z_i=49.0,
                workload="64^3 particles, 200 Mpc/h, fine 128^3, coarse 32^3, int2 x/v, PP off"),
+    # CDM + fluid neutrinos, started at the neutrino turn-on z_i_nu = 10 (the redshift
+    # neutrino_ic.f90 builds the fluids at), so every timed step evolves the fluids
+    "c3": dict(nc=256, nnt=8, box=500.0, izip=2, pp=True, z_i=10.0, nu=True,
+               workload="512^3 CDM particles + fluid neutrinos (1 species, 3 x 0.1 eV; Gauss-Laguerre fluids "
+                        "512^3, 256^3, 128^3), 500 Mpc/h, fine 1024^3, coarse 256^3, int2 x/v, PP on, from z=10"),
+    "c3s": dict(nc=128, nnt=4, box=250.0, izip=2, pp=True, z_i=10.0, nu=True,
+                workload="256^3 CDM particles + fluid neutrinos (fluids 256^3, 128^3, 64^3), 250 Mpc/h, "
+                         "fine 512^3, coarse 128^3, int2 x/v, PP on, from z=10 (profiling size)"),
 }
+
+# fluid neutrinos of the C3 workload: one species of 0.1 eV, degeneracy 3, in a
+# total Omega_m = 0.3 with h = 0.7 (Omega_cdm reduced by Omega_nu)
+NU_M_EV, NU_DEG, NU_H = 0.1, 3.0, 0.7
+NU_F = float(np.float32(NU_DEG * NU_M_EV / 93.14 / NU_H ** 2) / np.float32(0.3))
+GL_V = (0.41577456, 2.29428036, 6.28994508)
 
 
 def read_peaks():
@@ -106,13 +120,25 @@ def make_state(cfg, seed):
     import pickle
     import tempfile
     from cube_nufluid_b200 import ic
-    key = f"cube_ic_{cfg['nc']}_{cfg['nnt']}_{cfg['box']}_{cfg['z_i']}_{cfg['izip']}_{seed}.pkl"
+    nu = bool(cfg.get("nu"))
+    key = f"cube_ic_{cfg['nc']}_{cfg['nnt']}_{cfg['box']}_{cfg['z_i']}_{cfg['izip']}_{seed}_{int(nu)}.pkl"
     path = os.path.join(tempfile.gettempdir(), key)
     if os.path.exists(path):
         with open(path, "rb") as f:
             return pickle.load(f)
     st = ic.zeldovich(cfg["nc"], cfg["nnt"], box=cfg["box"], z_i=cfg["z_i"], seed=seed,
-                      izipx=cfg["izip"], izipv=cfg["izip"])
+                      izipx=cfg["izip"], izipv=cfg["izip"], f_cdm=(1.0 - NU_F) if nu else 1.0)
+    if nu:
+        # fluid meshes nf/2, nf/4, nf/8 and hg_setup's cs2 = (u/beta*c * hg_dv)^2 (hydrogr.f90:66)
+        f32 = np.float32
+        nf = 4 * cfg["nc"]
+        hg_dv = f32(2 * nf) / ((f32(300.0) * np.sqrt(f32(0.3))) * f32(cfg["box"]))
+        beta = f32(5966.34) * f32(NU_M_EV)
+        st.nu_fluids = []
+        for k in range(3):
+            cs = (f32(GL_V[k]) / beta) * f32(2.998e5) * hg_dv
+            st.nu_fluids.append(ic.nu_fluid_linear(cfg["nc"], cfg["box"], cfg["z_i"], seed, fluid_n=nf >> (k + 1),
+                                                   gl_v=GL_V[k], m_nu_ev=NU_M_EV, cs2=float(cs * cs)))
     try:
         with open(path + ".tmp", "wb") as f:
             pickle.dump(st, f, protocol=4)
@@ -120,6 +146,13 @@ def make_state(cfg, seed):
     except OSError:
         pass
     return st
+
+
+def nu_params_for(cfg):
+    from cube_nufluid_b200 import make_params
+    return make_params(cfg["nc"], cfg["nnt"], box=cfg["box"], izipx=cfg["izip"], izipv=cfg["izip"],
+                       ext_pp_force=cfg["pp"], neutrino=True, f_neu=NU_F, m_nu_ev=NU_M_EV, deg_nu=NU_DEG,
+                       z_i_nu=10.0, omega_m=0.3, omega_l=0.7, h0=NU_H)
 
 
 def algorithmic_bytes(cfg, npart):
@@ -130,7 +163,7 @@ def algorithmic_bytes(cfg, npart):
     bx = bv = 3 * cfg["izip"]
     kf = 3 * (nf // 2 + 1) ** 3 * 4
     kc = 3 * (nc // 2 + 1) ** 3 * 4
-    return {
+    out = {
         "update_x": npart * (2 * bx + 2 * bv + 8),
         "ext_pp_force": npart * (bx + 2 * bv),
         "deposit": npart * bx + Nc * 4 + Nf * 4 + Nc * 4,
@@ -138,6 +171,14 @@ def algorithmic_bytes(cfg, npart):
         "coarse_fft_green": 4 * 8 * Nc + kc,
         "kick": npart * (bx + 2 * bv) + Nf * 12 + Nc * 12 + Nc * 12 + Nc * 8,
     }
+    if cfg.get("nu"):
+        # two half steps of 3 sweeps (5 floats in, 5 out per cell) and a CFL pass (5 in),
+        # plus the gravity coupling: fine force once, the x/y restriction out and back
+        # in, and 5 in + 4 out per fluid cell
+        cells = sum((nf >> k) ** 3 for k in (1, 2, 3))
+        planes = sum((nf >> k) ** 2 for k in (1, 2, 3))
+        out["nu_fluid"] = 2 * (3 * 40 + 20) * cells + 12 * Nf + 2 * 20 * (nf + 4) * planes + 36 * cells
+    return out
 
 
 PHASES = ["update_x", "ext_pp_force", "deposit", "fine_fft_green", "coarse_fft_green", "kick"]
@@ -150,24 +191,41 @@ def run_ours(args, cfg, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     st = make_state(cfg, seed=1000 + rank)
-    p = make_params(cfg["nc"], cfg["nnt"], box=cfg["box"], izipx=cfg["izip"], izipv=cfg["izip"],
-                    ext_pp_force=cfg["pp"])
+    nu = bool(cfg.get("nu"))
+    if nu:
+        p = nu_params_for(cfg)
+    else:
+        p = make_params(cfg["nc"], cfg["nnt"], box=cfg["box"], izipx=cfg["izip"], izipv=cfg["izip"],
+                        ext_pp_force=cfg["pp"])
     cube = Cube(p, np_capacity=st.np)
     stream = torch.cuda.Stream()
     cube.L.cube_set_stream(cube.h, stream.cuda_stream)
     cube.load_state(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    if nu:
+        for k in range(3):
+            cube.nu_load(k, st.nu_fluids[k])
     s = scalars_from_ic(st)
     npart = st.np
+    nu_ms = [0.0]
 
     def step():
+        # main.f90:49-64: timestep, neutrino half step, drift, PP, PM, neutrino half step
         cube.timestep(s)
+        if nu:
+            s.dt_neu = cube.nu_evolve(s.dt / 2.0, s.dt_neu, 1, s.a_mid)
+            nu_ms[0] += cube.phase_times()[6]
         cube.update_x(s)
         if cfg["pp"]:
             cube.ext_pp_force(s)
         cube.particle_mesh(s)
+        if nu:
+            nu_ms[0] += cube.phase_times()[6]  # gravity on the fluids
+            s.dt_neu = cube.nu_evolve(s.dt / 2.0, s.dt_neu, -1, s.a_mid)
+            nu_ms[0] += cube.phase_times()[6]
 
     for _ in range(args.warmup):
         step()
+    nu_ms[0] = 0.0
     phase_sum = np.zeros(len(PHASES))
     if world > 1:
         dist.barrier()
@@ -229,6 +287,8 @@ def run_ours(args, cfg, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(t2, op=dist.ReduceOp.MAX)
     e2e_ms = float(t2.item())
+    if nu:
+        phase_sum = np.append(phase_sum, nu_ms[0])
     return dict(ms=ms_max, npart=npart, launches=launches, phase_ms=phase_sum / args.steps, clocks=clk.summary(),
                 e2e_ms=e2e_ms, e2e_steps=e2e_steps, h2d=h2d, d2h=h2d, scal=s.as_dict())
 
@@ -306,10 +366,11 @@ def main():
     e2e = r["npart"] * world * r["e2e_steps"] / (r["e2e_ms"] / 1e3)
     peak, peak_kind = read_peaks()
     ab = algorithmic_bytes(cfg, r["npart"])
-    phases = {k: float(v) for k, v in zip(PHASES, r["phase_ms"])}
+    names = PHASES + (["nu_fluid"] if cfg.get("nu") else [])
+    phases = {k: float(v) for k, v in zip(names, r["phase_ms"])}
     dom = max(phases, key=lambda k: phases[k])
     ach = ab[dom] / (phases[dom] / 1e3) / 1e9
-    phase_gbs = {k: (ab[k] / (phases[k] / 1e3) / 1e9 if phases[k] > 0 else None) for k in PHASES}
+    phase_gbs = {k: (ab[k] / (phases[k] / 1e3) / 1e9 if phases[k] > 0 else None) for k in names}
     line = {
         "metric": metric, "value": value, "unit": "particle-updates/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True, "scaling": "weak",

@@ -158,7 +158,7 @@ int setup_neutrinos(cube_ctx* ctx) {
     int rc = cube_nu_init(ctx, F);
     if (rc) return rc;
   }
-  N.nparts = ctx->num_sms * 8;
+  N.nparts = (nf / 32) * (nf / 8) * (nf / 8);  // one partial sum per k_nu_fine_density brick
   if (cudaMalloc((void**)&N.partial, 8 * (size_t)N.nparts) != cudaSuccess) {
     ctx->err = "cudaMalloc failed";
     return CUBE_ERR_CUDA;
@@ -194,7 +194,7 @@ void cube_destroy(cube_ctx* ctx) {
                   ctx->red_tmp,
                   ctx->scan_tmp, ctx->fine.rho, ctx->fine.force, ctx->fine.kern, ctx->fine.plan.tw,
                   ctx->coarse.rho, ctx->coarse.force, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->rho_c_acc,
-                  ctx->tan_table, ctx->dscal};
+                  ctx->tan_table, ctx->dscal, ctx->pk_bins};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 3; ++k) {
@@ -278,7 +278,8 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
             A((void**)&ctx->red_tmp, 8 * (2 * (nce / 1024 + 64) + 64)) &&
             A((void**)&ctx->scan_tmp, 8 * (nce / 2048 + 64)) &&
             A((void**)&ctx->rho_c_acc, 8 * nce) && A((void**)&ctx->tan_table, 4 * ctx->nvbin) &&
-            A((void**)&ctx->dscal, sizeof(DevScal));
+            A((void**)&ctx->dscal, sizeof(DevScal)) &&
+            A((void**)&ctx->pk_bins, 8 * 7 * (size_t)(cube_pk_nbin(ctx->nf, 0) + 1));
   if (!ok) return fail(CUBE_ERR_CUDA);
   if (cudaMallocHost((void**)&ctx->hscal, sizeof(DevScal)) != cudaSuccess) { ctx->err = "cudaMallocHost failed"; return fail(CUBE_ERR_CUDA); }
   cudaMemset(ctx->rho_c_acc, 0, 8 * nce);
@@ -423,9 +424,10 @@ int32_t cube_particle_mesh(cube_ctx* ctx, cube_scalars* io) {
   int rc = cube_deposit(ctx, io);
   if (rc) return rc;
   CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[3], ctx->stream));
-  if ((rc = cube_fft_poisson(ctx, ctx->fine, &ctx->dscal->f2_fine_bits))) return rc;
+  const KickScale ks = {io->a_mid, io->dt, ctx->codec.pi_f, 1, 1.0f / 6.0f, 1.0f / ctx->codec.pi_f};
+  if ((rc = cube_fft_poisson(ctx, ctx->fine, &ctx->dscal->f2_fine_bits, ks))) return rc;
   CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[4], ctx->stream));
-  if ((rc = cube_fft_poisson(ctx, ctx->coarse, &ctx->dscal->f2_coarse_bits))) return rc;
+  if ((rc = cube_fft_poisson(ctx, ctx->coarse, &ctx->dscal->f2_coarse_bits, ks))) return rc;
   CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[5], ctx->stream));
   if ((rc = cube_kick(ctx, io))) return rc;
   CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[6], ctx->stream));
@@ -444,8 +446,10 @@ int32_t cube_particle_mesh(cube_ctx* ctx, cube_scalars* io) {
     io->testrhof += nus;
     cudaEventElapsedTime(&ctx->phase_ms[6], ctx->ev[6], ctx->ev[9]);
   }
-  io->f2_max_fine = uint_as_float(ctx->hscal->f2_fine_bits);
-  io->f2_max_coarse = uint_as_float(ctx->hscal->f2_coarse_bits);
+  // the meshes hold force*s; max f^2 in force units
+  const double s2 = (double)cube_kick_scalar(ks) * (double)cube_kick_scalar(ks);
+  io->f2_max_fine = (float)((double)uint_as_float(ctx->hscal->f2_fine_bits) / s2);
+  io->f2_max_coarse = (float)((double)uint_as_float(ctx->hscal->f2_coarse_bits) / s2);
   for (int d = 0; d < 3; ++d) io->vmax[d] = uint_as_float(ctx->hscal->vmax_bits[d]);
   io->sigma_vi = io->sigma_vi_new;  // pm.f90:180
   dt_constraints(ctx, io);
@@ -603,6 +607,35 @@ int32_t cube_nu_store(cube_ctx* ctx, int32_t fluid, float* fld) {
   return CUBE_OK;
 }
 
+int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t capacity, int32_t* nbin) {
+  if (!ctx || !xip || !nbin) return CUBE_ERR_PARAM;
+  if (!ctx->state_loaded) return CUBE_ERR_STATE;
+  const int need = cube_pk_nbin(ctx->nf, log_bins ? 1 : 0);
+  *nbin = need;
+  if (capacity < need) {
+    ctx->err = "xip holds fewer bins than the mesh has";
+    return CUBE_ERR_CAPACITY;
+  }
+  std::vector<double> b;
+  int nb = 0;
+  int rc = cube_power_spectrum_dev(ctx, log_bins ? 1 : 0, b, &nb);
+  if (rc) return rc;
+  // powerspectrum.f90:113-135 for bins 1..nbin (bin 0 holds only modes with |k| < 1/2)
+  const int W = nb + 1;
+  const double two_pi_box = 2.0 * 3.14159265358979323846 / (double)ctx->P.box;
+  for (int i = 1; i <= nb; ++i) {
+    const double n = b[0 * W + i];
+    float* o = xip + (size_t)(i - 1) * 10;
+    o[0] = (float)n;
+    o[1] = (float)(b[1 * W + i] / n * two_pi_box);
+    for (int q = 2; q < 7; ++q) o[q] = (float)(b[q * W + i] / n);
+    o[7] = o[4] / sqrtf(o[2] * o[3]);
+    o[8] = sqrtf(o[3] / o[2]);
+    o[9] = powf(o[7], 4.f) / powf(o[8], 2.f) * o[3];
+  }
+  return CUBE_OK;
+}
+
 int32_t cube_nu_info(cube_ctx* ctx, float* out) {
   if (!ctx || !out) return CUBE_ERR_PARAM;
   if (!ctx->nu.on) { ctx->err = "fluid neutrinos are not enabled in this context"; return CUBE_ERR_STATE; }
@@ -692,8 +725,11 @@ int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float*
     cudaFree(tmp);
   }
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dscal, 0, sizeof(DevScal), ctx->stream));
-  int rc = cube_kick(ctx, io);
-  if (rc) return rc;
+  // the meshes hold kick increments once particle_mesh has run: scale the raw forces
+  const KickScale ks = {io->a_mid, io->dt, ctx->codec.pi_f, 1, 1.0f / 6.0f, 1.0f / ctx->codec.pi_f};
+  int rc = cube_force_scale(ctx, ctx->fine, ks);
+  if (rc || (rc = cube_force_scale(ctx, ctx->coarse, ks))) return rc;
+  if ((rc = cube_kick(ctx, io))) return rc;
   if (ctx->nu.on && (rc = cube_nu_gravity(ctx, io))) return rc;
   if ((rc = check_device_error(ctx))) return rc;
   for (int d = 0; d < 3; ++d) io->vmax[d] = uint_as_float(ctx->hscal->vmax_bits[d]);

@@ -104,6 +104,7 @@ struct cube_ctx {
   double* red_tmp;      // scratch for tree sums
   int64_t* scan_tmp;
   NuState nu;
+  double* pk_bins;  // power-spectrum bin sums, 7 * (bins of the fine mesh + 1)
   // meshes
   MeshLevel fine, coarse;
   unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator
@@ -179,11 +180,50 @@ __device__ __forceinline__ void cube_cell_coords(int64_t c, int nt, int nnt, int
   tb[2] = (t2 / (nnt * nnt)) * nt;
 }
 
+// The kick chain of the reference, (((f*a_mid)*dt)/6)/pi (pm.f90:146,163,358,393),
+// is the same for every particle that reads a force node.  cube_particle_mesh folds
+// the scalar ((a_mid*dt)/6)/pi into the Green multiply, so the force meshes come
+// out of the inverse FFT as kick increments (to FP32 rounding, like the force
+// itself); forces given from outside (cube_debug_kick_with_force) get the exact
+// per-node chain below.
+struct KickScale {
+  float a_mid, dt, pi_f;
+  int on;
+  float inv6, inv_pi;  // RN(1/6), RN(1/pi_f)
+};
+
+// RN(x/y) for a constant y with z = RN(1/y): q0 = RN(x z), r = fma(-q0, y, x),
+// q = fma(r, z, q0) (Brisebarre, Muller and Raina, IEEE Trans. Computers 53(8),
+// 2004).  For y = 6 and y = pi_f the result equals IEEE division for every finite
+// FP32 x with |x| >= 2^-100 (checked over all 2^32 inputs by the CPU tests); smaller
+// and non-finite x take the IEEE division.
+__device__ __forceinline__ float cube_div_const(float x, float y, float z) {
+  const float ax = fabsf(x);
+  if (!(ax >= 7.88860905e-31f && ax <= 3.40282347e38f)) return __fdiv_rn(x, y);
+  const float q0 = __fmul_rn(x, z);
+  const float r = __fmaf_rn(-q0, y, x);
+  return __fmaf_rn(r, z, q0);
+}
+
+inline float cube_kick_scalar(const KickScale& k) {
+  return k.on ? cube_fdiv(cube_fdiv(cube_fmul(k.a_mid, k.dt), 6.f), k.pi_f) : 1.f;
+}
+
+__device__ __forceinline__ float cube_kick_scale(float f, const KickScale& k) {
+  const float t = __fmul_rn(__fmul_rn(f, k.a_mid), k.dt);
+  return cube_div_const(cube_div_const(t, 6.f, k.inv6), k.pi_f, k.inv_pi);
+}
+
 // ---- launchers (implemented in the k_*.cu files) -----------------------------
 int cube_rebin(cube_ctx* ctx, cube_scalars* io);
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);
-int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits);
-int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, int* rc);
+int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks);
+int cube_force_scale(cube_ctx* ctx, MeshLevel& L, KickScale ks);
+int cube_fft_forward3(cube_ctx* ctx, MeshLevel& L, float* data);
+int cube_pk_nbin(int ng, int logbins);
+int cube_power_spectrum_dev(cube_ctx* ctx, int logbins, std::vector<double>& bins, int* nbin_out);
+int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc);
+int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks, int* rc);
 int cube_kick(cube_ctx* ctx, cube_scalars* io);
 int cube_pp(cube_ctx* ctx, cube_scalars* io);
 int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table);

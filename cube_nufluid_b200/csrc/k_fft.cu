@@ -248,7 +248,7 @@ __global__ void k_fft_col(float2* __restrict__ base, size_t comp_stride, int n, 
 template <int MAXIT>
 __global__ void k_fft_z_green(const float2* __restrict__ in, float2* __restrict__ out0, size_t comp_stride,
                               int n, int ncol, int tk, long long jstride, long long ostride, FftPlan pl,
-                              const float* __restrict__ kern, int kp) {
+                              const float* __restrict__ kern, int kp, float ksc) {
   extern __shared__ float2 sm[];
   float2* A = sm;
   float2* B = sm + (size_t)n * tk;
@@ -277,6 +277,7 @@ __global__ void k_fft_z_green(const float2* __restrict__ in, float2* __restrict_
         kv = __ldg(&K[((size_t)fy * kp + kx) * kp + fz]);
         if (d == 1) kv *= sy;
         if (d == 2 && kz > nh) kv = -kv;
+        kv *= ksc;
       }
       const float2 a = A[kz * tk + c];
       B[kz * tk + c] = make_float2(-a.y * kv, a.x * kv);
@@ -358,10 +359,26 @@ static int col_pass(cube_ctx* ctx, MeshLevel& L, float* data, int ncomp, int alo
   return CUBE_OK;
 }
 
-int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
+__global__ void k_force_scale(float* __restrict__ f, int n, int rp, KickScale ks) {
+  const int64_t tot = 3ll * n * n * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % n);
+    const int64_t row = i / n;  // (c*n + z)*n + y
+    float* p = f + row * rp + x;
+    *p = cube_kick_scale(*p, ks);
+  }
+}
+
+int cube_force_scale(cube_ctx* ctx, MeshLevel& L, KickScale ks) {
+  k_force_scale<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(L.force, L.n, L.rp, ks);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
+int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks) {
   const int n = L.n;
   int rc;
-  if (!ctx->P.reserved[0] && cube_fft_poisson_fast(ctx, L, f2_bits, &rc)) return rc;
+  if (!ctx->P.reserved[0] && cube_fft_poisson_fast(ctx, L, f2_bits, ks, &rc)) return rc;
   // forward r2c of the density, in place
   if ((rc = cube_fft_r2c_x(ctx, L, L.rho, 0, 1, nullptr))) return rc;
   if ((rc = col_pass(ctx, L, L.rho, 1, 0, -1.f))) return rc;
@@ -375,10 +392,18 @@ int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
     CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fft_z_green<MAXIT_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_fft_z_green<MAXIT_C><<<grid, thr, smem, ctx->stream>>>(
         reinterpret_cast<const float2*>(L.rho), reinterpret_cast<float2*>(L.force), (size_t)n * L.plane / 2, n,
-        ncol, tk, (long long)n * cp, cp, L.plan, L.kern, L.kern_pitch);
+        ncol, tk, (long long)n * cp, cp, L.plan, L.kern, L.kern_pitch, cube_kick_scalar(ks));
     CUBE_LAUNCH_CHECK(ctx);
   }
   if ((rc = col_pass(ctx, L, L.force, 3, 0, 1.f))) return rc;
-  if ((rc = cube_fft_r2c_x(ctx, L, L.force, 1, 3, f2_bits))) return rc;
-  return CUBE_OK;
+  return cube_fft_r2c_x(ctx, L, L.force, 1, 3, f2_bits);
+}
+
+// forward 3-D r2c in place (x, y, z), unnormalised
+int cube_fft_forward3(cube_ctx* ctx, MeshLevel& L, float* data) {
+  int rc;
+  if (!ctx->P.reserved[0] && cube_fft_forward3_fast(ctx, L, data, &rc)) return rc;
+  if ((rc = cube_fft_r2c_x(ctx, L, data, 0, 1, nullptr))) return rc;
+  if ((rc = col_pass(ctx, L, data, 1, 0, -1.f))) return rc;
+  return col_pass(ctx, L, data, 1, 1, -1.f);
 }

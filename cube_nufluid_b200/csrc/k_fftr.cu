@@ -193,7 +193,7 @@ template <int N, int R, int T, int TK>
 __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in, float2* __restrict__ out0,
                                                    size_t comp_stride, int ncol, long long jstride,
                                                    long long ostride, const float2* __restrict__ tw,
-                                                   const float* __restrict__ kern, int kp) {
+                                                   const float* __restrict__ kern, int kp, float ksc) {
   extern __shared__ float2 sm[];
   constexpr int P = TK + 1;
   const int kx0 = blockIdx.x * TK;
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in
     for (int q = 0; q < R; ++q) {
       const int kz = t + T * q;
       const int fz = kz <= nh ? kz : N - kz;
-      float kv = __ldg(&K[fz]);
+      float kv = __ldg(&K[fz]) * ksc;
       if (d == 1) kv *= sy;
       if (d == 2 && kz > nh) kv = -kv;
       v[q] = make_float2(-keep[q].y * kv, keep[q].x * kv);
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(3 * T * RB) k_xc2r3(float* __restrict__ data, 
 }
 
 template <int N, int R, int T>
-int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
+int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks) {
   constexpr int TK = (T >= 16) ? 8 : 16;
   constexpr int RB = (T >= 32) ? 4 : (T >= 16 ? 8 : 16);
   constexpr int RB3 = (T >= 32) ? 2 : (T >= 16 ? 4 : 8);
@@ -353,55 +353,112 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits) {
   const long long cp = L.cp;
   const size_t cstride = (size_t)N * L.plane / 2;
   const float2* tw = L.plan.tw;
-  // x r2c
-  {
-    const int npairs = N * N / 2;
-    const size_t smem = sizeof(float2) * RB * (N + R + 8);
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, smem, ctx->stream>>>(L.rho, L.rp, npairs, tw);
-    CUBE_LAUNCH_CHECK(ctx);
-  }
+  const size_t xsm = sizeof(float2) * RB * (N + R + 8);
+  const size_t x3sm = sizeof(float2) * 3 * RB3 * (N + R + 8);
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)x3sm));
   const size_t csm = sizeof(float2) * (size_t)N * (TK + 1);
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen<N, R, T, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-  const dim3 g1((ncol + TK - 1) / TK, N, 1), g3((ncol + TK - 1) / TK, N, 3);
-  // y forward
-  k_col<N, R, T, TK, -1><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.rho), cstride, ncol, cp,
-                                                             (long long)N * cp, tw);
-  CUBE_LAUNCH_CHECK(ctx);
-  // z forward, Green, z inverse
+  // The x and y passes can run slab by slab over z (params.reserved[1] / [2] planes
+  // per slab for the forward / inverse passes), which keeps a slab's intermediate
+  // in L2 between the two passes; measured at nf = 1024 every slab size was slower
+  // than whole-mesh passes (the short launches lose more to partial waves than the
+  // L2 reuse saves), so whole-mesh passes are the default.
+  int szf = N, szi = N;
+  if (ctx->P.reserved[1] > 0) szf = ctx->P.reserved[1];
+  if (ctx->P.reserved[2] > 0) szi = ctx->P.reserved[2];
+  szf = std::min(szf, N);
+  szi = std::min(szi, N);
+  float2* spec = reinterpret_cast<float2*>(L.rho);
+  const long long pstride = (long long)N * cp;  // float2 per plane
+  for (int z0 = 0; z0 < N; z0 += szf) {
+    const int nz = std::min(szf, N - z0);
+    // x r2c of the slab's rows (two real rows per complex transform)
+    const int npairs = nz * N / 2;
+    k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, xsm, ctx->stream>>>(L.rho + (size_t)z0 * L.plane, L.rp,
+                                                                              npairs, tw);
+    CUBE_LAUNCH_CHECK(ctx);
+    // y forward of the slab's columns
+    const dim3 g((ncol + TK - 1) / TK, nz, 1);
+    k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec + (size_t)z0 * pstride, cstride, ncol, cp, pstride,
+                                                             tw);
+    CUBE_LAUNCH_CHECK(ctx);
+  }
+  // z forward, Green, z inverse (whole mesh: z columns span every slab)
+  const dim3 g1((ncol + TK - 1) / TK, N, 1);
   k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
                                                             reinterpret_cast<float2*>(L.force), cstride, ncol,
-                                                            (long long)N * cp, cp, tw, L.kern, L.kern_pitch);
+                                                            pstride, cp, tw, L.kern, L.kern_pitch,
+                                                            cube_kick_scalar(ks));
   CUBE_LAUNCH_CHECK(ctx);
-  // y inverse, three components
-  k_col<N, R, T, TK, 1><<<g3, T * TK, csm, ctx->stream>>>(reinterpret_cast<float2*>(L.force), cstride, ncol, cp,
-                                                            (long long)N * cp, tw);
-  CUBE_LAUNCH_CHECK(ctx);
-  // x c2r, three components, max f^2
-  {
-    const int npairs = N * N / 2;
-    const size_t smem = sizeof(float2) * 3 * RB3 * (N + R + 8);
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, smem, ctx->stream>>>(L.force, (size_t)N * L.plane,
-                                                                                    L.rp, npairs, tw, f2_bits);
+  float2* fspec = reinterpret_cast<float2*>(L.force);
+  for (int z0 = 0; z0 < N; z0 += szi) {
+    const int nz = std::min(szi, N - z0);
+    // y inverse, three components
+    const dim3 g((ncol + TK - 1) / TK, nz, 3);
+    k_col<N, R, T, TK, 1><<<g, T * TK, csm, ctx->stream>>>(fspec + (size_t)z0 * pstride, cstride, ncol, cp, pstride,
+                                                            tw);
+    CUBE_LAUNCH_CHECK(ctx);
+    // x c2r, three components, max f^2
+    const int npairs = nz * N / 2;
+    k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, x3sm, ctx->stream>>>(
+        L.force + (size_t)z0 * L.plane, (size_t)N * L.plane, L.rp, npairs, tw, f2_bits);
     CUBE_LAUNCH_CHECK(ctx);
   }
   return CUBE_OK;
 }
 
+// forward 3-D r2c of data in place (x r2c, y, z), unnormalised: the half spectrum
+// c[z][y][kx] at pitch cp
+template <int N, int R, int T>
+int run_forward3(cube_ctx* ctx, MeshLevel& L, float* data) {
+  constexpr int TK = (T >= 16) ? 8 : 16;
+  constexpr int RB = (T >= 32) ? 4 : (T >= 16 ? 8 : 16);
+  const int ncol = N / 2 + 1;
+  const long long cp = L.cp;
+  const float2* tw = L.plan.tw;
+  const size_t xsm = sizeof(float2) * RB * (N + R + 8);
+  const size_t csm = sizeof(float2) * (size_t)N * (TK + 1);
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  const int npairs = N * N / 2;
+  k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, xsm, ctx->stream>>>(data, L.rp, npairs, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  float2* spec = reinterpret_cast<float2*>(data);
+  const size_t cstride = (size_t)N * L.plane / 2;
+  const dim3 g((ncol + TK - 1) / TK, N, 1);
+  k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec, cstride, ncol, cp, (long long)N * cp, tw);  // y
+  CUBE_LAUNCH_CHECK(ctx);
+  k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec, cstride, ncol, (long long)N * cp, cp, tw);  // z
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
 }  // namespace
 
-// returns 1 if handled by a register-resident path
-int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, int* rc) {
+int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc) {
   switch (L.n) {
-    case 1024: *rc = run_poisson<1024, 32, 32>(ctx, L, f2_bits); return 1;
-    case 512: *rc = run_poisson<512, 32, 16>(ctx, L, f2_bits); return 1;
-    case 256: *rc = run_poisson<256, 16, 16>(ctx, L, f2_bits); return 1;
-    case 128: *rc = run_poisson<128, 16, 8>(ctx, L, f2_bits); return 1;
-    case 64: *rc = run_poisson<64, 8, 8>(ctx, L, f2_bits); return 1;
-    case 32: *rc = run_poisson<32, 8, 4>(ctx, L, f2_bits); return 1;
+    case 1024: *rc = run_forward3<1024, 32, 32>(ctx, L, data); return 1;
+    case 512: *rc = run_forward3<512, 32, 16>(ctx, L, data); return 1;
+    case 256: *rc = run_forward3<256, 16, 16>(ctx, L, data); return 1;
+    case 128: *rc = run_forward3<128, 16, 8>(ctx, L, data); return 1;
+    case 64: *rc = run_forward3<64, 8, 8>(ctx, L, data); return 1;
+    case 32: *rc = run_forward3<32, 8, 4>(ctx, L, data); return 1;
+    default: return 0;
+  }
+}
+
+// returns 1 if handled by a register-resident path
+int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks, int* rc) {
+  switch (L.n) {
+    case 1024: *rc = run_poisson<1024, 32, 32>(ctx, L, f2_bits, ks); return 1;
+    case 512: *rc = run_poisson<512, 32, 16>(ctx, L, f2_bits, ks); return 1;
+    case 256: *rc = run_poisson<256, 16, 16>(ctx, L, f2_bits, ks); return 1;
+    case 128: *rc = run_poisson<128, 16, 8>(ctx, L, f2_bits, ks); return 1;
+    case 64: *rc = run_poisson<64, 8, 8>(ctx, L, f2_bits, ks); return 1;
+    case 32: *rc = run_poisson<32, 8, 4>(ctx, L, f2_bits, ks); return 1;
     default: return 0;
   }
 }

@@ -4,7 +4,9 @@
  *
  * Per particle and component the arithmetic is the reference's, in its
  * order: decode with sigma_vi, add the eight fine CIC terms
- * force*a_mid*dt/6/pi*dx*dy*dz (FP32 products, FP64 accumulation), encode
+ * force*a_mid*dt/6/pi*dx*dy*dz (FP32 products, FP64 accumulation; the first four
+ * factors are the same for every particle reading a node, so the c2r pass of the
+ * FFT has applied them to the mesh already), encode
  * with sigma_vi_new; decode that code again with sigma_vi_new, add the
  * eight coarse terms, record |v+vfield| for vmax, encode.  The intermediate
  * quantisation between the two kicks is kept, so the result is bit-identical
@@ -50,7 +52,6 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
   if (threadIdx.x < 3) vmx_s[threadIdx.x] = 0u;
   __syncthreads();
   const int nf = 4 * nc;
-  const float pi_f = codec.pi_f;
   const int64_t p0 = cs[0];
   const int npb = (int)(cs[ncl] - p0);
   // reference corner order: 111,211,121,112,122,212,221,222
@@ -104,10 +105,7 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
     double v = cube_vdecode(tan0, coef_old);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      float q = cube_fmul(fv[k], a_mid);
-      q = cube_fmul(q, dt);
-      q = cube_fdiv(q, 6.f);
-      q = cube_fdiv(q, pi_f);
+      float q = fv[k];  // force*a_mid*dt/6/pi of the node, applied by the c2r pass
       q = cube_fmul(q, ox[k] ? dx2[0] : dx1[0]);
       q = cube_fmul(q, oy[k] ? dx2[1] : dx1[1]);
       q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
@@ -117,10 +115,7 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
     v = cube_vdecode(__ldg(&tan_table[code1 + half_nvbin]), coef_new);
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      float q = cube_fmul(gv[k], a_mid);
-      q = cube_fmul(q, dt);
-      q = cube_fdiv(q, 6.f);
-      q = cube_fdiv(q, pi_f);
+      float q = gv[k];
       q = cube_fmul(q, ox[k] ? cx2[0] : cx1[0]);
       q = cube_fmul(q, oy[k] ? cx2[1] : cx1[1]);
       q = cube_fmul(q, oz[k] ? cx2[2] : cx1[2]);

@@ -79,7 +79,7 @@ struct SweepArgs {
   const float* in[5];
   float* out[5];
   int n, ts, tx;       // cells per side, tile length along the sweep, lines per tile
-  float gm1, dt, dx;   // g-1, half-step dt, cell size
+  float gm1, dt, inv_dx;  // g-1, half-step dt, 1/cell size (a power of two)
 };
 
 // slot order of the momentum components seen by the 1-D solver: the normal
@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(256) k_nu_sweep(SweepArgs A) {
     for (int v = 0; v < 5; ++v) {
       const float* f = flux + (v * TX + l) * NI + s;  // f[0] = f(i-1), f[1] = f(i)
       const float r = FA(-f[1], f[0]);
-      A.out[comp[v]][g] = FA(A.in[comp[v]][g], FD(FM(A.dt, r), A.dx));
+      A.out[comp[v]][g] = FA(A.in[comp[v]][g], FM(FM(A.dt, r), A.inv_dx));  // x/dx = x*(1/dx) exactly
     }
   }
 }
@@ -250,7 +250,7 @@ __device__ __forceinline__ float fluid_density(const float* __restrict__ r, int 
   float d1[3], d2[3];
 #pragma unroll
   for (int e = 0; e < 3; ++e) {
-    const float xx = FS(FD(x[e], dx), 0.5f);
+    const float xx = FS(FM(x[e], 1.f / dx), 0.5f);  // dx is a power of two: exact
     const int lo = (int)floorf(xx);  // 0-based index of idx1
     d1[e] = FS((float)(lo + 1), xx);
     d2[e] = FS(1.f, d1[e]);
@@ -271,24 +271,84 @@ __device__ __forceinline__ float fluid_density(const float* __restrict__ r, int 
 
 // neutrino density at every fine node (pm.f90:55-74): nu = 0 + f_neu*sum_k w_k rho_k(n+1/2)
 // (or 0 + f_neu before z_i_nu); added to the fine mesh, kept in `scratch` for the
-// coarse deposit, and summed in FP64 per thread/CTA for testrhof.
+// coarse deposit, and summed in FP64 per CTA for testrhof.  One CTA per brick of
+// 32x8x8 fine nodes: each fluid's cells under the brick (plus one on each side)
+// are staged in shared memory, and each node runs hg_density's CIC in its order.
+constexpr int DBX = 32, DBY = 8, DBZ = 8;
+constexpr int DPATCH = 3 * (DBX / 2 + 2) * (DBY / 2 + 2) * (DBZ / 2 + 2);  // three fluids, dx >= 2
+
 __global__ void __launch_bounds__(256) k_nu_fine_density(Rho3 F, int homogeneous, float f_neu, int nf, float* __restrict__ rho,
                                                         int rp, size_t plane, float* __restrict__ scratch,
                                                         double* __restrict__ partial) {
-  const int64_t total = (int64_t)nf * nf * nf;
+  __shared__ float patch[DPATCH];
+  __shared__ double red[256];
+  const int nbx = nf / DBX, nby = nf / DBY;
+  const int x0 = (blockIdx.x % nbx) * DBX, y0 = ((blockIdx.x / nbx) % nby) * DBY, z0 = (blockIdx.x / (nbx * nby)) * DBZ;
+  int off[3], px[3], py[3], pz[3], lo0[3][3];
+  {
+    int o = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int dx = (int)F.dx[k];  // 2, 4 or 8
+      px[k] = DBX / dx + 2; py[k] = DBY / dx + 2; pz[k] = DBZ / dx + 2;
+      lo0[k][0] = x0 / dx - 1; lo0[k][1] = y0 / dx - 1; lo0[k][2] = z0 / dx - 1;
+      off[k] = o;
+      o += px[k] * py[k] * pz[k];
+    }
+  }
+  if (!homogeneous) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int n = F.n[k];
+      for (int e = threadIdx.x; e < px[k] * py[k] * pz[k]; e += blockDim.x) {
+        const int ix = e % px[k], iy = (e / px[k]) % py[k], iz = e / (px[k] * py[k]);
+        const int gx = cube_wrap(lo0[k][0] + ix, n), gy = cube_wrap(lo0[k][1] + iy, n), gz = cube_wrap(lo0[k][2] + iz, n);
+        patch[off[k] + e] = __ldg(&F.r[k][((size_t)gz * n + gy) * n + gx]);
+      }
+    }
+  }
+  __syncthreads();
+  const int lx = threadIdx.x & 31;
+  const int x = x0 + lx;
+  // x weights of this thread's column, per fluid (hg_density, hydrogr.f90:328-333)
+  float wx1[3], wx2[3];
+  int ix0[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    const float xx = FS(FM(FA((float)x, 0.5f), 1.f / F.dx[k]), 0.5f);
+    const int lo = (int)floorf(xx);
+    wx1[k] = FS((float)(lo + 1), xx);
+    wx2[k] = FS(1.f, wx1[k]);
+    ix0[k] = lo - lo0[k][0];
+  }
   double acc = 0.0;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x) {
-    const int x = (int)(i % nf);
-    const int64_t yz = i / nf;
-    const int y = (int)(yz % nf), z = (int)(yz / nf);
+  for (int yz = threadIdx.x >> 5; yz < DBY * DBZ; yz += 8) {
+    const int y = y0 + (yz & (DBY - 1)), z = z0 + yz / DBY;
     float val;
     if (homogeneous) {
       val = FA(0.f, f_neu);
     } else {
-      const float X[3] = {FA((float)x, 0.5f), FA((float)y, 0.5f), FA((float)z, 0.5f)};
       float den = 0.f;
 #pragma unroll
-      for (int k = 0; k < 3; ++k) den = FA(den, FM(F.w[k], fluid_density(F.r[k], F.n[k], F.dx[k], X)));
+      for (int k = 0; k < 3; ++k) {
+        const float inv = 1.f / F.dx[k];
+        const float yy = FS(FM(FA((float)y, 0.5f), inv), 0.5f), zz = FS(FM(FA((float)z, 0.5f), inv), 0.5f);
+        const int ylo = (int)floorf(yy), zlo = (int)floorf(zz);
+        const float wy1 = FS((float)(ylo + 1), yy), wz1 = FS((float)(zlo + 1), zz);
+        const float wy2 = FS(1.f, wy1), wz2 = FS(1.f, wz1);
+        const float* P = patch + off[k] + ((zlo - lo0[k][2]) * py[k] + (ylo - lo0[k][1])) * px[k] + ix0[k];
+        const int sy = px[k], sz = px[k] * py[k];
+        // term order 111,211,121,221,112,212,122,222 (hydrogr.f90:335-342)
+        float d = FM(FM(FM(P[0], wx1[k]), wy1), wz1);
+        d = FA(d, FM(FM(FM(P[1], wx2[k]), wy1), wz1));
+        d = FA(d, FM(FM(FM(P[sy], wx1[k]), wy2), wz1));
+        d = FA(d, FM(FM(FM(P[sy + 1], wx2[k]), wy2), wz1));
+        d = FA(d, FM(FM(FM(P[sz], wx1[k]), wy1), wz2));
+        d = FA(d, FM(FM(FM(P[sz + 1], wx2[k]), wy1), wz2));
+        d = FA(d, FM(FM(FM(P[sz + sy], wx1[k]), wy2), wz2));
+        d = FA(d, FM(FM(FM(P[sz + sy + 1], wx2[k]), wy2), wz2));
+        den = FA(den, FM(F.w[k], d));
+      }
       val = FA(0.f, FM(den, f_neu));
     }
     const size_t g = (size_t)z * plane + (size_t)y * rp + x;
@@ -296,7 +356,6 @@ __global__ void __launch_bounds__(256) k_nu_fine_density(Rho3 F, int homogeneous
     scratch[g] = val;
     acc += (double)val;
   }
-  __shared__ double red[256];
   red[threadIdx.x] = acc;
   __syncthreads();
   for (int s = 128; s > 0; s >>= 1) {
@@ -345,8 +404,10 @@ constexpr int GT = 32;          // fine cells per side of a k_nu_src_xy tile
 constexpr int GW = GT + 8;      // source window per side (dx <= 8: dx/2 either side)
 constexpr int GCN = 12;         // coarse nodes per side the window's CIC reads
 
+// the force meshes hold kick increments (((f*a_mid)*dt)/6)/pi per node (the
+// chain of pm.f90:163, :393, applied by the c2r pass)
 struct GravArgs {
-  const float* ff;   // fine force [3][nf planes], pitch frp, plane fplane
+  const float* ff;   // fine kick increments [3][nf planes], pitch frp, plane fplane
   size_t fcomp, fplane;
   int frp;
   const float* fc;   // coarse force
@@ -359,103 +420,117 @@ struct GravArgs {
   float* xy[3];      // [5][nf+4][n][n] per fluid
 };
 
-// the scale chain of the reference, (((f*a_mid)*dt)/6)/pi (pm.f90:163, :393)
-__device__ __forceinline__ float kick_scale(float f, float a_mid, float dt, float pi_f) {
-  return FD(FD(FM(FM(f, a_mid), dt), 6.f), pi_f);
-}
-
 // per fine z-plane qz in [-2, nf+2) and 32x32 tile of fine cells: source terms of
-// the window, then their x/y restriction onto each fluid's cells of the tile
+// the window, then their x/y restriction onto each fluid's cells of the tile.
+// A and B are FP32 sums in a fixed order (deterministic); the coarse
+// acceleration at the fine-cell centres is the trilinear CIC of the coarse kick
+// increments evaluated separably (z per plane, then y and x), which agrees with
+// the reference's FP64 sum of its eight FP32 terms to FP32 rounding.
 __global__ void __launch_bounds__(256) k_nu_src_xy(GravArgs G) {
-  __shared__ float src[4][GW][GW];        // A.x, A.y, A.z, |a_f|^2 + |a_c|^2
-  __shared__ float gc[3][2][GCN][GCN];    // scaled coarse force of the nodes read
+  __shared__ float src[4][GW][GW + 1];   // A.x, A.y, A.z, |a_f|^2 + |a_c|^2 (rows padded)
+  __shared__ float gz[3][GCN][GCN + 1];  // coarse increments interpolated to this plane
+  __shared__ float rx[5][GW][GT / 2 + 1];  // x-restricted rows, [v][window row][target x]
+  __shared__ float wt[2][GT / 2][16];     // per axis: weight of source i of target t
   const int nf = G.nf, nc = G.nc, ntx = nf / GT;
   const int x0 = (blockIdx.x % ntx) * GT, y0 = (blockIdx.x / ntx) * GT;
   const int qz = (int)blockIdx.y - 2;
   // coarse CIC along z for this plane (x = qz + 1/2): xc = x/4 - 0.5
-  const float zc = FS(FD(FA((float)qz, 0.5f), 4.f), 0.5f);
+  const float zc = FS(FM(FA((float)qz, 0.5f), 0.25f), 0.5f);
   const int zlo = (int)floorf(zc);
   const float cz1 = FS((float)(zlo + 1), zc), cz2 = FS(1.f, cz1);
   const int nbx = (x0 >> 2) - 2, nby = (y0 >> 2) - 2;  // first coarse node of the window
-  for (int e = threadIdx.x; e < 3 * 2 * GCN * GCN; e += blockDim.x) {
-    const int ix = e % GCN, iy = (e / GCN) % GCN, iz = (e / (GCN * GCN)) % 2, d = e / (2 * GCN * GCN);
-    const int gx = cube_wrap(nbx + ix, nc), gy = cube_wrap(nby + iy, nc), gz = cube_wrap(zlo + iz, nc);
-    gc[d][iz][iy][ix] = kick_scale(__ldg(&G.fc[d * G.ccomp + (size_t)gz * G.cplane + (size_t)gy * G.crp + gx]),
-                                   G.a_mid, G.dt, G.pi_f);
+  const int gz0 = cube_wrap(zlo, nc), gz1 = cube_wrap(zlo + 1, nc);
+  for (int e = threadIdx.x; e < 3 * GCN * GCN; e += blockDim.x) {
+    const int ix = e % GCN, iy = (e / GCN) % GCN, d = e / (GCN * GCN);
+    const int gx = cube_wrap(nbx + ix, nc), gy = cube_wrap(nby + iy, nc);
+    const float* c = G.fc + d * G.ccomp + (size_t)gy * G.crp + gx;
+    gz[d][iy][ix] = cz1 * __ldg(c + (size_t)gz0 * G.cplane) + cz2 * __ldg(c + (size_t)gz1 * G.cplane);
   }
   __syncthreads();
   const bool zf = (qz >= 0 && qz < nf);  // fine sources exist on this plane
+  const bool zc_in = (qz >= -2 && qz <= nf + 1);
   for (int e = threadIdx.x; e < GW * GW; e += blockDim.x) {
     const int wx = e % GW, wy = e / GW;
     const int qx = x0 - 4 + wx, qy = y0 - 4 + wy;
     float af[3] = {0.f, 0.f, 0.f}, ac[3] = {0.f, 0.f, 0.f};
-    const bool cin = qx >= -2 && qx <= nf + 1 && qy >= -2 && qy <= nf + 1;
     if (zf && qx >= 0 && qx < nf && qy >= 0 && qy < nf) {
-      // fine force at node q+1 (pm.f90:160-163: idx1 = floor(tempx)+1+nfb)
+      // fine increment at node q+1 (pm.f90:160-163: idx1 = floor(tempx)+1+nfb)
       const int fx = cube_wrap(qx + 1, nf), fy = cube_wrap(qy + 1, nf), fz = cube_wrap(qz + 1, nf);
       const size_t o = (size_t)fz * G.fplane + (size_t)fy * G.frp + fx;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) af[d] = kick_scale(__ldg(&G.ff[d * G.fcomp + o]), G.a_mid, G.dt, G.pi_f);
+      for (int d = 0; d < 3; ++d) af[d] = __ldg(&G.ff[d * G.fcomp + o]);
     }
-    if (cin) {
-      // coarse force CIC at the fine-cell centre, FP64 sum of FP32 terms in the
-      // reference order 111,211,121,221,112,212,122,222 (pm.f90:393-400)
-      const float xc = FS(FD(FA((float)qx, 0.5f), 4.f), 0.5f), yc = FS(FD(FA((float)qy, 0.5f), 4.f), 0.5f);
+    if (zc_in && qx >= -2 && qx <= nf + 1 && qy >= -2 && qy <= nf + 1) {
+      // coarse sources also on the two buffer layers beyond each face (pm.f90:382-385)
+      const float xc = FS(FM(FA((float)qx, 0.5f), 0.25f), 0.5f), yc = FS(FM(FA((float)qy, 0.5f), 0.25f), 0.5f);
       const int xl = (int)floorf(xc), yl = (int)floorf(yc);
       const float cx1 = FS((float)(xl + 1), xc), cx2 = FS(1.f, cx1);
       const float cy1 = FS((float)(yl + 1), yc), cy2 = FS(1.f, cy1);
       const int ix = xl - nbx, iy = yl - nby;
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        double v = 0.0;
+      for (int d = 0; d < 3; ++d)
+        ac[d] = cy1 * (cx1 * gz[d][iy][ix] + cx2 * gz[d][iy][ix + 1]) +
+                cy2 * (cx1 * gz[d][iy + 1][ix] + cx2 * gz[d][iy + 1][ix + 1]);
+    }
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          const int ox = c & 1, oy = (c >> 1) & 1, oz = c >> 2;
-          const float t = FM(FM(FM(gc[d][oz][iy + oy][ix + ox], ox ? cx2 : cx1), oy ? cy2 : cy1), oz ? cz2 : cz1);
-          v = __dadd_rn(v, (double)t);
-        }
-        ac[d] = (float)v;
-      }
-    }
-    src[0][wy][wx] = FA(af[0], ac[0]);
-    src[1][wy][wx] = FA(af[1], ac[1]);
-    src[2][wy][wx] = FA(af[2], ac[2]);
-    const float f2 = FA(FA(FM(af[0], af[0]), FM(af[1], af[1])), FM(af[2], af[2]));
-    const float c2 = FA(FA(FM(ac[0], ac[0]), FM(ac[1], ac[1])), FM(ac[2], ac[2]));
-    src[3][wy][wx] = FA(f2, c2);
+    for (int d = 0; d < 3; ++d) src[d][wy][wx] = af[d] + ac[d];
+    src[3][wy][wx] = (af[0] * af[0] + af[1] * af[1] + af[2] * af[2]) + (ac[0] * ac[0] + ac[1] * ac[1] + ac[2] * ac[2]);
   }
-  __syncthreads();
-  // restriction onto each fluid's cells: target t gets sources dx*t - dx/2 .. dx*t + 3dx/2 - 1
+  // Restriction onto each fluid's cells: target t gets the 2dx sources from window
+  // index b0 + dx t (lower target floor((q+1/2)/dx - 1/2) with weight w1 = that + 1
+  // - ((q+1/2)/dx - 1/2), the upper one 1 - w1).  A (3 components), C1 = sum w|a|^2
+  // and C2 = sum w^2 |a|^2; x first (one thread per window row and target), then y.
   for (int k = 0; k < G.nfl; ++k) {
-    const int dx = G.fdx[k], n = G.fn[k], tb = GT / dx;
-    const float dxf = (float)dx;
-    for (int e = threadIdx.x; e < tb * tb * 5; e += blockDim.x) {
-      const int v = e / (tb * tb), tt = e - v * tb * tb;
-      const int ty = tt / tb, tx = tt - ty * tb;
-      const int gtx = x0 / dx + tx, gty = y0 / dx + ty;
-      const int sx0 = dx * gtx - dx / 2, sy0 = dx * gty - dx / 2;
-      float acc = 0.f;
-      for (int j = 0; j < 2 * dx; ++j) {
-        const int qy = sy0 + j;
-        // weight of source qy on target gty: xx = (q+1/2)/dx - 1/2, lower target floor(xx)
-        const float yy = FS(FD(FA((float)qy, 0.5f), dxf), 0.5f);
-        const int yl = (int)floorf(yy);
-        const float wy1 = FS((float)(yl + 1), yy);
-        const float wy = (yl == gty) ? wy1 : FS(1.f, wy1);
-        float row = 0.f;
-        for (int i = 0; i < 2 * dx; ++i) {
-          const int qx = sx0 + i;
-          const float xx = FS(FD(FA((float)qx, 0.5f), dxf), 0.5f);
-          const int xl = (int)floorf(xx);
-          const float wx1 = FS((float)(xl + 1), xx);
-          const float wx = (xl == gtx) ? wx1 : FS(1.f, wx1);
-          const float s = src[v < 3 ? v : 3][qy - (y0 - 4)][qx - (x0 - 4)];
-          row = FA(row, FM(v == 4 ? FM(wx, wx) : wx, s));
-        }
-        acc = FA(acc, FM(v == 4 ? FM(wy, wy) : wy, row));
-      }
-      G.xy[k][(((size_t)v * (nf + 4) + (qz + 2)) * n + gty) * n + gtx] = acc;
+    const int dx = G.fdx[k], n = G.fn[k], tb = GT / dx, nw = 2 * dx;
+    const float inv_dx = 1.f / (float)dx;  // exact: dx is a power of two
+    const int b0 = 4 - dx / 2;             // window index of target 0's first source
+    for (int e = threadIdx.x; e < 2 * tb * nw; e += blockDim.x) {
+      const int ax = e / (tb * nw), r = e - ax * tb * nw, t = r / nw, i = r - t * nw;
+      const int q = (ax == 0 ? x0 : y0) - 4 + b0 + dx * t + i;
+      const float xx = FS(FM(FA((float)q, 0.5f), inv_dx), 0.5f);
+      const int lo = (int)floorf(xx);
+      const float w1 = FS((float)(lo + 1), xx);
+      wt[ax][t][i] = (lo - (ax == 0 ? x0 : y0) / dx == t) ? w1 : FS(1.f, w1);
     }
+    __syncthreads();
+    for (int e = threadIdx.x; e < tb * GW; e += blockDim.x) {
+      const int tx = e / GW, wy = e - tx * GW;
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f, c1 = 0.f, c2 = 0.f;
+      for (int i = 0; i < nw; ++i) {
+        const int wx = b0 + dx * tx + i;
+        const float w = wt[0][tx][i];
+        a0 += w * src[0][wy][wx];
+        a1 += w * src[1][wy][wx];
+        a2 += w * src[2][wy][wx];
+        const float q2 = src[3][wy][wx];
+        c1 += w * q2;
+        c2 += (w * w) * q2;
+      }
+      rx[0][wy][tx] = a0; rx[1][wy][tx] = a1; rx[2][wy][tx] = a2; rx[3][wy][tx] = c1; rx[4][wy][tx] = c2;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < tb * tb; e += blockDim.x) {
+      const int ty = e / tb, tx = e - ty * tb;
+      float a0 = 0.f, a1 = 0.f, a2 = 0.f, c1 = 0.f, c2 = 0.f;
+      for (int j = 0; j < nw; ++j) {
+        const int wy = b0 + dx * ty + j;
+        const float w = wt[1][ty][j];
+        a0 += w * rx[0][wy][tx];
+        a1 += w * rx[1][wy][tx];
+        a2 += w * rx[2][wy][tx];
+        c1 += w * rx[3][wy][tx];
+        c2 += (w * w) * rx[4][wy][tx];
+      }
+      const int gtx = x0 / dx + tx, gty = y0 / dx + ty;
+      const size_t vs = (size_t)(nf + 4) * n * n;
+      const size_t o = ((size_t)(qz + 2) * n + gty) * n + gtx;
+      G.xy[k][o] = a0;
+      G.xy[k][vs + o] = a1;
+      G.xy[k][2 * vs + o] = a2;
+      G.xy[k][3 * vs + o] = c1;
+      G.xy[k][4 * vs + o] = c2;
+    }
+    __syncthreads();
   }
 }
 
@@ -477,7 +552,7 @@ __global__ void __launch_bounds__(256) k_nu_grav_z(const float* __restrict__ xy,
     for (int j = 0; j < 2 * dx; ++j) {
       const int qz = q0 + j;
       if (qz < -2 || qz > nf + 1) continue;
-      const float zz = FS(FD(FA((float)qz, 0.5f), dxf), 0.5f);
+      const float zz = FS(FM(FA((float)qz, 0.5f), 1.f / dxf), 0.5f);
       const int zl = (int)floorf(zz);
       const float wz1 = FS((float)(zl + 1), zz);
       const float wz = (zl == tz) ? wz1 : FS(1.f, wz1);
@@ -541,7 +616,7 @@ int cube_nu_sweeps(cube_ctx* ctx, NuFluid& F, float dt, int dir) {
     A.n = n;
     A.gm1 = cube_fsub(ctx->nu.g, 1.f);
     A.dt = dt;
-    A.dx = F.dx;
+    A.inv_dx = 1.f / F.dx;
     if (ax == 0) { A.ts = pick_tile(n, 64); A.tx = pick_tile(n, 16); }
     else { A.ts = pick_tile(n, 32); A.tx = pick_tile(n, 32); }
     const size_t smem = sizeof(float) * (size_t)5 * A.tx * ((A.ts + 4) + (A.ts + 1));
@@ -591,7 +666,8 @@ int cube_nu_density(cube_ctx* ctx, cube_scalars* io) {
     R.w[k] = N.dwgts[k];
   }
   float* scratch = L.force;  // free until the force is computed
-  k_nu_fine_density<<<N.nparts, 256, 0, ctx->stream>>>(R, homogeneous, ctx->P.f_neu, L.n, L.rho, L.rp, L.plane,
+  const int nbricks = (L.n / DBX) * (L.n / DBY) * (L.n / DBZ);
+  k_nu_fine_density<<<nbricks, 256, 0, ctx->stream>>>(R, homogeneous, ctx->P.f_neu, L.n, L.rho, L.rp, L.plane,
                                                       scratch, N.partial);
   CUBE_LAUNCH_CHECK(ctx);
   const float hom = cube_fmul(ctx->P.f_neu, (float)(ctx->ncell * ctx->ncell * ctx->ncell));

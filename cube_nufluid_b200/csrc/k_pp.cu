@@ -287,6 +287,7 @@ __global__ void __launch_bounds__(256, 3) k_pp_brick(const void* __restrict__ xp
   uint16_t* code = fidx + PB_CAP;                                           // 3*PB_CAP, raw position codes
   __shared__ int64_t cst[PRC];
   __shared__ int cpre[PRC + 1];
+  __shared__ int tpre[PB * PB * PB + 1];  // prefix of the brick's own cells (targets)
   const int nb = nc / PB;
   const int bx = blockIdx.x % nb, by = (blockIdx.x / nb) % nb, bz = blockIdx.x / (nb * nb);
   const int x0 = bx * PB - 1, y0 = by * PB - 1, z0 = bz * PB - 1;  // region origin (global coarse, unwrapped)
@@ -311,6 +312,25 @@ __global__ void __launch_bounds__(256, 3) k_pp_brick(const void* __restrict__ xp
       run += __shfl_sync(0xffffffffu, inc, 31);
     }
     if (threadIdx.x == 0) cpre[PRC] = run;
+    __syncwarp();
+    // the 64 own cells in (z,y,x) order, two per lane
+    int c2[2], n2[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int t = 2 * threadIdx.x + h;
+      const int q = (((t >> 4) + 1) * PR + ((t >> 2) & 3) + 1) * PR + (t & 3) + 1;
+      c2[h] = q;
+      n2[h] = cpre[q + 1] - cpre[q];
+    }
+    int inc = n2[0] + n2[1];
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, inc, o);
+      if ((int)threadIdx.x >= o) inc += v;
+    }
+    tpre[2 * threadIdx.x] = inc - n2[0] - n2[1];
+    tpre[2 * threadIdx.x + 1] = inc - n2[1];
+    if (threadIdx.x == 31) tpre[PB * PB * PB] = inc;
+    (void)c2;
   }
   __syncthreads();
   const int M = cpre[PRC];
@@ -351,16 +371,17 @@ __global__ void __launch_bounds__(256, 3) k_pp_brick(const void* __restrict__ xp
   __syncthreads();
   unsigned long long n1 = 0, npair = 0;
   float f2max = 0.f;
-  // targets: the particles of the brick's own cells (region cells 1..PB)
-  for (int m = threadIdx.x; m < M; m += blockDim.x) {
-    int lo = 0, hi = PRC - 1;
+  // targets: the particles of the brick's own cells (region cells 1..PB), compacted
+  const int T = tpre[PB * PB * PB];
+  for (int t = threadIdx.x; t < T; t += blockDim.x) {
+    int lo = 0, hi = PB * PB * PB - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
-      if (cpre[mid] <= m) lo = mid; else hi = mid - 1;
+      if (tpre[mid] <= t) lo = mid; else hi = mid - 1;
     }
-    const int q = lo;
-    const int cc[3] = {q % PR, (q / PR) % PR, q / (PR * PR)};
-    if (cc[0] < 1 || cc[0] > PB || cc[1] < 1 || cc[1] > PB || cc[2] < 1 || cc[2] > PB) continue;
+    const int cc[3] = {(lo & 3) + 1, ((lo >> 2) & 3) + 1, (lo >> 4) + 1};
+    const int q = (cc[2] * PR + cc[1]) * PR + cc[0];
+    const int m = cpre[q] + (t - tpre[lo]);
     const int64_t ip = cst[q] + (m - cpre[q]);
     double x1[3], v[3], ft[3] = {0.0, 0.0, 0.0};
     int g1[3];

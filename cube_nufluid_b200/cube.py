@@ -70,6 +70,8 @@ def load_library():
         getattr(L, name).restype = C.c_int32
     L.cube_nu_info.argtypes = [vp, vp]
     L.cube_nu_info.restype = C.c_int32
+    L.cube_power_spectrum.argtypes = [vp, C.c_int32, vp, C.c_int32, C.POINTER(C.c_int32)]
+    L.cube_power_spectrum.restype = C.c_int32
     L.cube_phase_times.argtypes = [vp, C.POINTER(C.c_float)]
     L.cube_phase_times.restype = C.c_int32
     L.cube_launch_count.argtypes = [vp]
@@ -196,6 +198,14 @@ class Cube:
         if self.p.neutrino:
             s.dt_neu = self.nu_evolve(s.dt / 2.0, s.dt_neu, -1, s.a_mid)
         return hit
+
+    def power_spectrum(self, log_bins: bool = False) -> np.ndarray:
+        """xip(10, nbin) of cicpower / powerspectrum as float32 [nbin, 10]."""
+        nb = C.c_int32(0)
+        cap = 4096
+        out = np.zeros((cap, 10), np.float32)
+        self._check(self.L.cube_power_spectrum(self.h, int(log_bins), _ptr(out), cap, C.byref(nb)))
+        return out[:nb.value].copy()
 
     # ---- fluid neutrinos (hydrodf.f90) ---------------------------------------
     def nu_evolve(self, dt: float, dtg: float, direction: int, a: float) -> float:

@@ -160,15 +160,11 @@ def tile_major_cell_id(g: np.ndarray, nc: int, nnt: int) -> np.ndarray:
     return ((tile * nt + l[..., 2]) * nt + l[..., 1]) * nt + l[..., 0]
 
 
-def zeldovich(nc: int, nnt: int, box: float, z_i: float, seed: int, *, np_nc: int = 2,
-              ncell: int = 4, izipx: int = 2, izipv: int = 2, cosmo: Cosmology | None = None,
-              f_cdm: float = 1.0, amplitude: float = 1.0) -> ICState:
-    """Build a seeded Zel'dovich state at z_i in checkpoint layout."""
-    c = cosmo or Cosmology()
-    npd = nc * np_nc
-    a = 1.0 / (1.0 + z_i)
-    noise = gaussian_noise(npd, seed)  # [z][y][x]
+def _linear_delta_k(npd: int, box: float, a: float, seed: int, c: Cosmology, amplitude: float):
+    """Linear density contrast in Fourier space on an npd^3 grid from the seeded
+    noise (initial_conditions.f90:320-420): noise * sqrt(P(k)) at scale factor a."""
     import scipy.fft as sfft
+    noise = gaussian_noise(npd, seed)  # [z][y][x]
     wk = sfft.rfftn(noise, workers=-1)
     del noise
     kx = np.fft.rfftfreq(npd, d=1.0 / npd).astype(np.float32)
@@ -180,7 +176,18 @@ def zeldovich(nc: int, nnt: int, box: float, z_i: float, seed: int, *, np_nc: in
     amp = np.sqrt(d2 / (4 * math.pi) * (npd / kr)) * (npd / kr) * amplitude
     dk = wk * amp
     dk[0, 0, 0] = 0
-    del wk, amp, d2
+    return dk, kx, ky, kz, kr2
+
+
+def zeldovich(nc: int, nnt: int, box: float, z_i: float, seed: int, *, np_nc: int = 2,
+              ncell: int = 4, izipx: int = 2, izipv: int = 2, cosmo: Cosmology | None = None,
+              f_cdm: float = 1.0, amplitude: float = 1.0) -> ICState:
+    """Build a seeded Zel'dovich state at z_i in checkpoint layout."""
+    c = cosmo or Cosmology()
+    npd = nc * np_nc
+    a = 1.0 / (1.0 + z_i)
+    import scipy.fft as sfft
+    dk, kx, ky, kz, kr2 = _linear_delta_k(npd, box, a, seed, c, amplitude)
     kgrid = 2 * math.pi / npd
     inv = np.where(kr2 > 0, 1.0 / (kgrid * kgrid * np.maximum(kr2, 1e-30)), 0.0).astype(np.float32)
     disp = np.empty((3, npd, npd, npd), dtype=np.float32)
@@ -285,5 +292,52 @@ def nu_fluid_perturbed(nc: int, seed: int, *, cs2: float, gamma: float = np.floa
         m = (rho * v).astype(f32)
         out[..., 1 + d] = m
         e = (e + f32(0.5) * m * m / rho).astype(f32)
+    out[..., 4] = e
+    return out
+
+
+def nu_fluid_linear(nc: int, box: float, z: float, seed: int, *, fluid_n: int, gl_v: float, m_nu_ev: float,
+                    cs2: float, z_i_nu: float = 10.0, np_nc: int = 2, ncell: int = 4,
+                    cosmo: Cosmology | None = None, amplitude: float = 1.0,
+                    gamma: float = np.float32(5.0) / np.float32(3.0)) -> np.ndarray:
+    """One Gauss-Laguerre fluid's initial state fld(1:5,1:n,1:n,1:n) as float32
+    [n,n,n,5], following neutrino_ic.f90:46-181 on the seeded field of zeldovich():
+    delta_nu = delta_L * 1/(1+l+l^2), v_nu = v_L * (1+1.5l+2l^2)/(1+l+l^2)^2 with
+    l = k/k_fs, k_fs = sqrt(1.5 Om/(1+z_i_nu))*100 / v_nu and v_nu = u c/(beta m)
+    (:11,:52-58,:77,:147); the fields are built on the particle grid and averaged
+    to the fluid's n^3 cells (hydrogr.f90:288-308 set_fld); rho = 1 + delta,
+    E = rho cs2/(g-1) + sum m_d^2/(2 rho) (:91-94,:162-166)."""
+    import scipy.fft as sfft
+    c = cosmo or Cosmology()
+    npd = nc * np_nc
+    a = 1.0 / (1.0 + z)
+    dk, kx, ky, kz, kr2 = _linear_delta_k(npd, box, a, seed, c, amplitude)
+    kgrid = 2 * math.pi / npd
+    kphys = np.sqrt(kr2) * (2 * math.pi / box)
+    kfs1 = math.sqrt(1.5 * c.omega_m / (1.0 + z_i_nu)) * 100.0
+    vneu = gl_v / 5966.34 * 2.998e5 / m_nu_ev
+    ll = (kphys / (kfs1 / vneu)).astype(np.float32)
+    t_rho = 1.0 / (1.0 + ll + ll * ll)
+    t_v = (1.0 + 1.5 * ll + 2.0 * ll * ll) * t_rho * t_rho
+    if fluid_n <= 0 or npd % fluid_n:
+        raise ValueError("the fluid mesh must divide the particle grid")
+    r = npd // fluid_n
+
+    def down(f):
+        f = f.reshape(fluid_n, r, fluid_n, r, fluid_n, r).astype(np.float64)
+        return f.mean(axis=(1, 3, 5)).astype(np.float32)
+
+    rho = (1.0 + down(sfft.irfftn(dk * t_rho, s=(npd,) * 3, workers=-1))).astype(np.float32)
+    out = np.zeros((fluid_n, fluid_n, fluid_n, 5), np.float32)
+    out[..., 0] = rho
+    e = (rho * np.float32(cs2) / (np.float32(gamma) - np.float32(1.0))).astype(np.float32)
+    inv = np.where(kr2 > 0, 1.0 / (kgrid * kgrid * np.maximum(kr2, 1e-30)), 0.0).astype(np.float32)
+    vf = vfactor(a, c.omega_m, c.omega_l) * ncell / np_nc  # displacement (grid cells) -> fine cells / time
+    for d, kk in enumerate((kx[None, None, :], ky[None, :, None], kz[:, None, None])):
+        vk = (1j * (kgrid * kk) * inv * dk) * (t_v * np.float32(vf))
+        v = down(sfft.irfftn(vk, s=(npd,) * 3, workers=-1))
+        m = (rho * v).astype(np.float32)
+        out[..., 1 + d] = m
+        e = (e + np.float32(0.5) * m * m / rho).astype(np.float32)
     out[..., 4] = e
     return out

@@ -75,6 +75,36 @@ module cube_gpu
       type(c_ptr), value :: ctx
       type(c_ptr) :: cube_last_error
     end function
+    ! neu(nu)%evolve(dt,dtg,dir,a) (hydrodf.f90:86)
+    integer(c_int32_t) function cube_nu_evolve(ctx, dt, dtg, dir, a) bind(c, name="cube_nu_evolve")
+      import :: c_int32_t, c_ptr, c_float
+      type(c_ptr), value :: ctx
+      real(c_float), value :: dt, a
+      real(c_float), intent(inout) :: dtg
+      integer(c_int32_t), value :: dir
+    end function
+    ! one fluid's physical cells fld(1:5,1:n,1:n,1:n)
+    integer(c_int32_t) function cube_nu_load(ctx, fluid, fld) bind(c, name="cube_nu_load")
+      import :: c_int32_t, c_ptr, c_float
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: fluid
+      real(c_float), intent(in) :: fld(*)
+    end function
+    integer(c_int32_t) function cube_nu_store(ctx, fluid, fld) bind(c, name="cube_nu_store")
+      import :: c_int32_t, c_ptr, c_float
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: fluid
+      real(c_float), intent(out) :: fld(*)
+    end function
+    ! cicpower analysis into xip(10,nbin)
+    integer(c_int32_t) function cube_power_spectrum(ctx, log_bins, xip, capacity, nbin) &
+        bind(c, name="cube_power_spectrum")
+      import :: c_int32_t, c_ptr, c_float
+      type(c_ptr), value :: ctx
+      integer(c_int32_t), value :: log_bins, capacity
+      real(c_float), intent(out) :: xip(10, *)
+      integer(c_int32_t), intent(out) :: nbin
+    end function
   end interface
 
   type(c_ptr), save :: gpu_ctx = c_null_ptr
@@ -113,3 +143,7 @@ end module cube_gpu
 !     sigma_vi = gpu_s%sigma_vi; sim%dt_fine = gpu_s%dt_fine; sim%dt_coarse = gpu_s%dt_coarse
 !     sim%dt_vmax = gpu_s%dt_vmax; sim%vz_max = gpu_s%vz_max; sim%vsim2phys = gpu_s%vsim2phys
 !   end subroutine
+!
+! and the neutrino half steps of main.f90:51-54, 66-69:
+!
+!     call gpu_check(cube_nu_evolve(gpu_ctx, dt/2., dt_neu, 1, a_mid), 'nu evolve')

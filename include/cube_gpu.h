@@ -179,6 +179,18 @@ int32_t cube_nu_evolve(cube_ctx* ctx, float dt, float* dtg, int32_t dir, float a
 int32_t cube_nu_load(cube_ctx* ctx, int32_t fluid, const float* fld);
 int32_t cube_nu_store(cube_ctx* ctx, int32_t fluid, float* fld);
 
+/* Power spectrum of the resident particles on the fine mesh (ng = nf), the
+ * checkpoint analysis of cicpower.f90:84-255 + powerspectrum.f90:27-137: CIC
+ * with unit mass at pos*ng/nc - 1/2, delta = rho/mean - 1, forward FFT, modes
+ * binned by nint(|k|) (log_bins = 0, the reference's linear_kbin) or 4 per
+ * octave from 0.95 (log_bins = 1).  With fluid neutrinos the second field is
+ * their density contrast (cross power), else zero.  Writes xip(10,nbin) as
+ * float [nbin][10]: count, k (h/Mpc), Delta^2_cc, Delta^2_nn, Delta^2_cn,
+ * <1/sinc^2>, <1/sinc^4>, r, b, reconstruction; *nbin = bins of the mesh
+ * (CUBE_ERR_CAPACITY if capacity < *nbin).  Uses the fine meshes as scratch:
+ * call it between steps, not inside one. */
+int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t capacity, int32_t* nbin);
+
 /* Set-up constants, 19 floats: beta = m/T, the three normalised weights, then
  * per fluid (n, ncb of the reference layout, dx, cs2, hg_dv). */
 int32_t cube_nu_info(cube_ctx* ctx, float* out);

@@ -1151,3 +1151,35 @@ void orc_rfft3(const double* in, int n, double* out) {
   memcpy(out, h.data(), sizeof(cd) * h.size());
 }
 }
+
+/* ------------------------------------------------------------------------- */
+/* Division by a constant y with a precomputed reciprocal z = RN(1/y) and one  */
+/* FMA correction (Brisebarre, Muller and Raina, "Accelerating correctly       */
+/* rounded floating-point division when the divisor is known in advance",     */
+/* IEEE Trans. Computers 53(8), 2004):                                          */
+/*     q0 = RN(x z),  r = RN(x - q0 y) (fma, exact),  q = RN(q0 + r z) (fma).   */
+/* Whether q = RN(x/y) for every x depends on y; this counts the FP32 inputs    */
+/* where it differs from IEEE division (NaN/Inf inputs skipped), over all 2^32  */
+/* bit patterns, and reports the largest |x| among the failures.                */
+extern "C" int64_t orc_check_const_div(float y, float* worst_abs_x) {
+  const float z = 1.0f / y;
+  int64_t nfail = 0;
+  float worst = 0.f;
+#pragma omp parallel for reduction(+ : nfail) reduction(max : worst) schedule(static)
+  for (int64_t b = 0; b < (1ll << 32); ++b) {
+    const uint32_t u = (uint32_t)b;
+    float x;
+    memcpy(&x, &u, 4);
+    if (!std::isfinite(x)) continue;
+    const float q0 = x * z;
+    const float r = fmaf(-q0, y, x);
+    const float q = fmaf(r, z, q0);
+    const float ref = x / y;
+    if (memcmp(&q, &ref, 4) != 0) {
+      ++nfail;
+      worst = std::max(worst, fabsf(x));
+    }
+  }
+  *worst_abs_x = worst;
+  return nfail;
+}

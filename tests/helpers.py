@@ -52,3 +52,11 @@ def nu_params(nc=16, nnt=2, box=300.0, **kw):
     """Parameters with the fluid neutrinos of the reference's defaults."""
     return make_params(nc, nnt, box=box, neutrino=True, f_neu=F_NEU, m_nu_ev=0.1, z_i_nu=10.0,
                        omega_m=float(_F32(0.32) + OMEGA_NU), h0=0.67, **kw)
+
+
+def kick_chain(force, a_mid, dt):
+    """(((f*a_mid)*dt)/6)/pi in FP32 (pm.f90:146): what the library's force meshes
+    hold after particle_mesh."""
+    f32 = np.float32
+    pif = f32(4.0) * np.arctan(f32(1.0))
+    return ((((np.asarray(force, f32) * f32(a_mid)) * f32(dt)) / f32(6.0)) / pif).astype(f32)

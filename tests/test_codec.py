@@ -101,3 +101,19 @@ def test_position_code_matches_reference_expression(izip):
     ours = ((codes & (2 ** bits - 1)) + 0.5) * 2.0 ** (-bits)
     assert np.array_equal(ref, ours)
     assert ref.min() > 0 and ref.max() < 1
+
+
+def test_constant_division_is_exact():
+    """The force meshes divide by 6 and by pi_f with a precomputed reciprocal and one
+    FMA correction (Brisebarre-Muller-Raina); over all 2^32 FP32 inputs it must equal
+    IEEE division wherever the library uses it (|x| >= 2^-100)."""
+    import ctypes as C
+    from oracle_ref import lib
+    L = lib()
+    L.orc_check_const_div.restype = C.c_int64
+    L.orc_check_const_div.argtypes = [C.c_float, C.POINTER(C.c_float)]
+    pif = np.float32(4.0) * np.arctan(np.float32(1.0))
+    for y in (6.0, float(pif)):
+        worst = C.c_float(0.0)
+        L.orc_check_const_div(y, C.byref(worst))
+        assert worst.value < 2.0 ** -100, (y, worst.value)

@@ -108,9 +108,9 @@ def test_nu_gravity_matches_sequential_scatter(tables):
     for x in (so, sg):
         x.a_mid = 0.5
         x.dt = 0.05
-    g.particle_mesh(sg)
-    fine, coarse = g.fetch(2), g.fetch(3)
-    o.particle_mesh_with_force(so, fine, coarse, 1)
+    # the oracle's own step, then the GPU's kick + gravity on the oracle's forces
+    o.particle_mesh(so, 1)
+    g.kick_with_force(sg, o.fetch(2), o.fetch(3))
     info = g.nu_info()
     for k in range(3):
         fo = o.nu_store(k).astype(np.float64)
