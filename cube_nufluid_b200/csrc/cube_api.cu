@@ -607,6 +607,23 @@ int32_t cube_nu_store(cube_ctx* ctx, int32_t fluid, float* fld) {
   return CUBE_OK;
 }
 
+int32_t cube_debug_time_poisson(cube_ctx* ctx, int32_t reps, float* ms) {
+  if (!ctx || !ms || reps <= 0) return CUBE_ERR_PARAM;
+  const KickScale ks = {0.5f, 0.01f, ctx->codec.pi_f, 1, 1.0f / 6.0f, 1.0f / ctx->codec.pi_f};
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dscal, 0, sizeof(DevScal), ctx->stream));
+  int rc = cube_fft_poisson(ctx, ctx->fine, &ctx->dscal->f2_fine_bits, ks);  // warm-up
+  if (rc) return rc;
+  CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[12], ctx->stream));
+  for (int r = 0; r < reps; ++r)
+    if ((rc = cube_fft_poisson(ctx, ctx->fine, &ctx->dscal->f2_fine_bits, ks))) return rc;
+  CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[13], ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev[13]));
+  float t = 0.f;
+  cudaEventElapsedTime(&t, ctx->ev[12], ctx->ev[13]);
+  *ms = t / (float)reps;
+  return CUBE_OK;
+}
+
 int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t capacity, int32_t* nbin) {
   if (!ctx || !xip || !nbin) return CUBE_ERR_PARAM;
   if (!ctx->state_loaded) return CUBE_ERR_STATE;

@@ -217,6 +217,7 @@ __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in
   const float sy = ky <= nh ? 1.f : -1.f;
   const int kx = min(kx0 + g, ncol - 1);
   const size_t ksz = (size_t)kp * kp * kp;
+#pragma unroll 1
   for (int d = 0; d < 3; ++d) {
     const float* K = kern + d * ksz + ((size_t)fy * kp + kx) * kp;
     float2 v[R];
@@ -228,6 +229,62 @@ __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in
       if (d == 1) kv *= sy;
       if (d == 2 && kz > nh) kv = -kv;
       v[q] = make_float2(-keep[q].y * kv, keep[q].x * kv);
+    }
+    __syncwarp();
+    fft_from_regs<N, R, T, 1, false>(v, s, P, t, tw);
+    __syncthreads();
+    float2* bo = out0 + d * comp_stride + (size_t)ky * ostride + kx0;
+    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+      const int j = i / TK, c = i - j * TK;
+      if (c < nk) bo[(size_t)j * jstride + c] = sm[j * P + c];
+    }
+    __syncthreads();
+  }
+}
+
+// k_zgreen with the forward spectrum kept in a second shared buffer instead of
+// registers (fewer registers per thread, more resident columns per SM)
+template <int N, int R, int T, int TK>
+__global__ void __launch_bounds__(T * TK, 512 / (T * TK)) k_zgreen_s(const float2* __restrict__ in, float2* __restrict__ out0,
+                                                     size_t comp_stride, int ncol, long long jstride,
+                                                     long long ostride, const float2* __restrict__ tw,
+                                                     const float* __restrict__ kern, int kp, float ksc) {
+  extern __shared__ float2 sm[];
+  constexpr int P = TK + 1;
+  float2* spec = sm + (size_t)N * P;  // forward spectrum, same layout
+  const int kx0 = blockIdx.x * TK;
+  const int nk = min(TK, ncol - kx0);
+  const int ky = blockIdx.y;
+  const float2* bi = in + (size_t)ky * ostride + kx0;
+  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
+    const int j = i / TK, c = i - j * TK;
+    cp_async8(&sm[j * P + c], c < nk ? &bi[(size_t)j * jstride + c] : bi, c < nk);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  float2* s = sm + g;
+  fft_seq<N, R, T, -1, false>(s, P, t, tw);
+#pragma unroll
+  for (int q = 0; q < R; ++q) spec[(t + T * q) * P + g] = s[(t + T * q) * P];
+  constexpr int nh = N / 2;
+  const int fy = ky <= nh ? ky : N - ky;
+  const float sy = ky <= nh ? 1.f : -1.f;
+  const int kx = min(kx0 + g, ncol - 1);
+  const size_t ksz = (size_t)kp * kp * kp;
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d) {
+    const float* K = kern + d * ksz + ((size_t)fy * kp + kx) * kp;
+    float2 v[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int kz = t + T * q;
+      const int fz = kz <= nh ? kz : N - kz;
+      float kv = __ldg(&K[fz]) * ksc;
+      if (d == 1) kv *= sy;
+      if (d == 2 && kz > nh) kv = -kv;
+      const float2 a = spec[kz * P + g];
+      v[q] = make_float2(-a.y * kv, a.x * kv);
     }
     __syncwarp();
     fft_from_regs<N, R, T, 1, false>(v, s, P, t, tw);
@@ -361,6 +418,15 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen<N, R, T, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+  // y passes with twice the columns per CTA (longer contiguous row segments, fewer
+  // CTAs per SM), selected by params.reserved[3] = 16 where T*16 <= 1024 threads
+  constexpr int TKW = (T * 2 * TK <= 1024) ? 2 * TK : TK;
+  const size_t csmw = sizeof(float2) * (size_t)N * (TKW + 1);
+  const bool wide = ctx->P.reserved[3] == 16 && TKW != TK && csmw <= 227 * 1024;
+  if (wide) {
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TKW, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmw));
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TKW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmw));
+  }
   // The x and y passes can run slab by slab over z (params.reserved[1] / [2] planes
   // per slab for the forward / inverse passes), which keeps a slab's intermediate
   // in L2 between the two passes; measured at nf = 1024 every slab size was slower
@@ -381,25 +447,49 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks
                                                                               npairs, tw);
     CUBE_LAUNCH_CHECK(ctx);
     // y forward of the slab's columns
-    const dim3 g((ncol + TK - 1) / TK, nz, 1);
-    k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec + (size_t)z0 * pstride, cstride, ncol, cp, pstride,
-                                                             tw);
+    if (wide) {
+      const dim3 g((ncol + TKW - 1) / TKW, nz, 1);
+      k_col<N, R, T, TKW, -1><<<g, T * TKW, csmw, ctx->stream>>>(spec + (size_t)z0 * pstride, cstride, ncol, cp,
+                                                                  pstride, tw);
+    } else {
+      const dim3 g((ncol + TK - 1) / TK, nz, 1);
+      k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec + (size_t)z0 * pstride, cstride, ncol, cp,
+                                                               pstride, tw);
+    }
     CUBE_LAUNCH_CHECK(ctx);
   }
-  // z forward, Green, z inverse (whole mesh: z columns span every slab)
-  const dim3 g1((ncol + TK - 1) / TK, N, 1);
-  k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
-                                                            reinterpret_cast<float2*>(L.force), cstride, ncol,
-                                                            pstride, cp, tw, L.kern, L.kern_pitch,
-                                                            cube_kick_scalar(ks));
+  // z forward, Green, z inverse (whole mesh: z columns span every slab); with
+  // params.reserved[4] = 1 the spectrum stays in shared memory (k_zgreen_s, 2 columns per CTA)
+  if (ctx->P.reserved[4] == 1) {
+    constexpr int TKS = 2;
+    const size_t ssm = 2 * sizeof(float2) * (size_t)N * (TKS + 1);
+    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen_s<N, R, T, TKS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+    const dim3 gs((ncol + TKS - 1) / TKS, N, 1);
+    k_zgreen_s<N, R, T, TKS><<<gs, T * TKS, ssm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
+                                                                 reinterpret_cast<float2*>(L.force), cstride, ncol,
+                                                                 pstride, cp, tw, L.kern, L.kern_pitch,
+                                                                 cube_kick_scalar(ks));
+  } else {
+    const dim3 g1((ncol + TK - 1) / TK, N, 1);
+    k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
+                                                              reinterpret_cast<float2*>(L.force), cstride, ncol,
+                                                              pstride, cp, tw, L.kern, L.kern_pitch,
+                                                              cube_kick_scalar(ks));
+  }
   CUBE_LAUNCH_CHECK(ctx);
   float2* fspec = reinterpret_cast<float2*>(L.force);
   for (int z0 = 0; z0 < N; z0 += szi) {
     const int nz = std::min(szi, N - z0);
     // y inverse, three components
-    const dim3 g((ncol + TK - 1) / TK, nz, 3);
-    k_col<N, R, T, TK, 1><<<g, T * TK, csm, ctx->stream>>>(fspec + (size_t)z0 * pstride, cstride, ncol, cp, pstride,
-                                                            tw);
+    if (wide) {
+      const dim3 g((ncol + TKW - 1) / TKW, nz, 3);
+      k_col<N, R, T, TKW, 1><<<g, T * TKW, csmw, ctx->stream>>>(fspec + (size_t)z0 * pstride, cstride, ncol, cp,
+                                                                 pstride, tw);
+    } else {
+      const dim3 g((ncol + TK - 1) / TK, nz, 3);
+      k_col<N, R, T, TK, 1><<<g, T * TK, csm, ctx->stream>>>(fspec + (size_t)z0 * pstride, cstride, ncol, cp,
+                                                              pstride, tw);
+    }
     CUBE_LAUNCH_CHECK(ctx);
     // x c2r, three components, max f^2
     const int npairs = nz * N / 2;

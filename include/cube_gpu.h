@@ -233,6 +233,10 @@ int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io);
 int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float* fine_force,
                                    const float* coarse_force);
 
+/* Device time of the fine-mesh Poisson solve (FFT passes + Green multiply) on
+ * whatever the fine density array holds, averaged over reps runs, in *ms. */
+int32_t cube_debug_time_poisson(cube_ctx* ctx, int32_t reps, float* ms);
+
 /* ---- allocation-free coarse density ------------------------------------------
  * No counterpart in the reference.  For hosts that may not allocate device memory
  * during a run (their HBM is owned by another allocator, or a fixed budget per box
