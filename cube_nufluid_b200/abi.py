@@ -56,6 +56,16 @@ class CubeScalars(C.Structure):
         return d
 
 
+class CubeIcParams(C.Structure):
+    """cube_ic_params of include/cube_gpu.h."""
+    _fields_ = [
+        ("seed", C.c_int64), ("np_nc", C.c_int32), ("pad0", C.c_int32),
+        ("a", C.c_double), ("norm_d2", C.c_double), ("n_s", C.c_double), ("h", C.c_double),
+        ("eh_s", C.c_double), ("eh_alpha", C.c_double), ("eh_omh", C.c_double), ("eh_theta2", C.c_double),
+        ("vf", C.c_double), ("amplitude", C.c_double), ("f_cdm", C.c_double),
+    ]
+
+
 def make_params(nc: int, nnt: int, *, ncell: int = 4, ncb: int = 6, np_nc: int = 2, izipx: int = 2,
                 izipv: int = 2, nf_cutoff: int = 16, pp_range: int = 1, ext_pp_force: bool = False,
                 use_pid: bool = True, neutrino: bool = False, box: float = 200.0, h0: float = 0.7,

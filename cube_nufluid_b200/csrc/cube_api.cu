@@ -90,16 +90,21 @@ unsigned int float_as_uint(float f) {
   return u;
 }
 
-/* dt constraints of particle_mesh (pm.f90:427-443), FP32 as the reference */
-void dt_constraints(const cube_ctx* ctx, cube_scalars* s) {
-  const float pi_f = ctx->codec.pi_f;
-  const float GG = cube_fdiv(cube_fdiv(1.0f, 6.0f), pi_f);  // variables.f90:22
-  float v = cube_fdiv(1.5f, s->a);
+/* sim%vsim2phys of particle_mesh (pm.f90:427), FP32 as the reference */
+float vsim2phys(const cube_ctx* ctx, float a) {
+  float v = cube_fdiv(1.5f, a);
   v = cube_fmul(v, ctx->P.box);
   v = cube_fmul(v, ctx->P.h0);
   v = cube_fmul(v, 100.f);
   v = cube_fmul(v, sqrtf(ctx->P.omega_m));
-  s->vsim2phys = cube_fdiv(v, (float)ctx->nf);
+  return cube_fdiv(v, (float)ctx->nf);
+}
+
+/* dt constraints of particle_mesh (pm.f90:427-443), FP32 as the reference */
+void dt_constraints(const cube_ctx* ctx, cube_scalars* s) {
+  const float pi_f = ctx->codec.pi_f;
+  const float GG = cube_fdiv(cube_fdiv(1.0f, 6.0f), pi_f);  // variables.f90:22
+  s->vsim2phys = vsim2phys(ctx, s->a);
   s->dt_fine = sqrtf(cube_fdiv(1.0f, cube_fmul(cube_fmul(sqrtf(s->f2_max_fine), s->a_mid), GG)));
   s->dt_coarse = sqrtf(cube_fdiv((float)ctx->ncell, cube_fmul(cube_fmul(sqrtf(s->f2_max_coarse), s->a_mid), GG)));
   const float vm = std::max(s->vmax[0], std::max(s->vmax[1], s->vmax[2]));
@@ -622,6 +627,13 @@ int32_t cube_debug_time_poisson(cube_ctx* ctx, int32_t reps, float* ms) {
   cudaEventElapsedTime(&t, ctx->ev[12], ctx->ev[13]);
   *ms = t / (float)reps;
   return CUBE_OK;
+}
+
+int32_t cube_make_ic(cube_ctx* ctx, const cube_ic_params* ic, cube_scalars* io) {
+  if (!ctx || !ic || !io) return CUBE_ERR_PARAM;
+  const int rc = cube_make_ic_dev(ctx, ic, io);
+  if (rc == CUBE_OK) io->vsim2phys = vsim2phys(ctx, io->a);
+  return rc;
 }
 
 int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t capacity, int32_t* nbin) {

@@ -237,5 +237,6 @@ int cube_nu_transpose(cube_ctx* ctx, NuFluid& F, int to_soa);
 int cube_nu_density(cube_ctx* ctx, cube_scalars* io);
 int cube_nu_gravity(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int ncomp, unsigned int* f2_bits);
+int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io);
 
 #endif

@@ -21,7 +21,7 @@ import os
 
 import numpy as np
 
-from .abi import ABI_VERSION, CubeParams, CubeScalars
+from .abi import ABI_VERSION, CubeIcParams, CubeParams, CubeScalars
 from . import tables
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -70,6 +70,8 @@ def load_library():
         getattr(L, name).restype = C.c_int32
     L.cube_nu_info.argtypes = [vp, vp]
     L.cube_nu_info.restype = C.c_int32
+    L.cube_make_ic.argtypes = [vp, C.POINTER(CubeIcParams), S]
+    L.cube_make_ic.restype = C.c_int32
     L.cube_power_spectrum.argtypes = [vp, C.c_int32, vp, C.c_int32, C.POINTER(C.c_int32)]
     L.cube_power_spectrum.restype = C.c_int32
     L.cube_phase_times.argtypes = [vp, C.POINTER(C.c_float)]
@@ -198,6 +200,19 @@ class Cube:
         if self.p.neutrino:
             s.dt_neu = self.nu_evolve(s.dt / 2.0, s.dt_neu, -1, s.a_mid)
         return hit
+
+    def make_ic(self, ic: dict, seed: int, *, f_cdm: float = 1.0) -> CubeScalars:
+        """Zel'dovich state made on the device (cube_make_ic) from the scalars of
+        ic.device_ic_params; returns the initial scalar block."""
+        q = CubeIcParams()
+        q.seed = int(seed)
+        q.np_nc = int(ic["np_nc"])
+        for k in ("a", "norm_d2", "n_s", "h", "eh_s", "eh_alpha", "eh_omh", "eh_theta2", "vf", "amplitude"):
+            setattr(q, k, float(ic[k]))
+        q.f_cdm = float(f_cdm)
+        s = CubeScalars()
+        self._check(self.L.cube_make_ic(self.h, C.byref(q), C.byref(s)))
+        return s
 
     def power_spectrum(self, log_bins: bool = False) -> np.ndarray:
         """xip(10, nbin) of cicpower / powerspectrum as float32 [nbin, 10]."""

@@ -57,13 +57,52 @@ def eh_nowiggle(k_hmpc: np.ndarray, c: Cosmology) -> np.ndarray:
     return l0 / (l0 + c0 * q * q)
 
 
+# Philox4x32-10 (Salmon, Moraes, Dror and Shaw, "Parallel random numbers: as easy as
+# 1, 2, 3", SC 2011): the counter-based generator shared by the host and the device
+# initial conditions.  Word i of the noise grid is output word i mod 4 of the block
+# with counter (i div 4 low 32 bits, high 32 bits, 0, 0) and key (seed low, seed high).
+PHILOX_M0, PHILOX_M1 = 0xD2511F53, 0xCD9E8D57
+PHILOX_W0, PHILOX_W1 = 0x9E3779B9, 0xBB67AE85
+
+
+def philox4x32_10(ctr: np.ndarray, key: tuple[int, int]) -> np.ndarray:
+    """ctr: uint32 [..., 4]; returns the uint32 [..., 4] output block."""
+    c = [ctr[..., i].astype(np.uint64) for i in range(4)]
+    k0, k1 = np.uint64(key[0] & 0xFFFFFFFF), np.uint64(key[1] & 0xFFFFFFFF)
+    m32 = np.uint64(0xFFFFFFFF)
+    for r in range(10):
+        p0 = np.uint64(PHILOX_M0) * c[0]
+        p1 = np.uint64(PHILOX_M1) * c[2]
+        hi0, lo0 = p0 >> np.uint64(32), p0 & m32
+        hi1, lo1 = p1 >> np.uint64(32), p1 & m32
+        c = [(hi1 ^ c[1] ^ k0) & m32, lo1, (hi0 ^ c[3] ^ k1) & m32, lo0]
+        k0 = (k0 + np.uint64(PHILOX_W0)) & m32
+        k1 = (k1 + np.uint64(PHILOX_W1)) & m32
+    return np.stack([x.astype(np.uint32) for x in c], axis=-1)
+
+
+def uniform_noise(n: int, seed: int) -> np.ndarray:
+    """Uniforms in [0,1) on an n^3 grid [z][y][x]: (word >> 8) * 2^-24 of the Philox stream."""
+    total = n ** 3
+    blocks = (total + 3) // 4
+    out = np.empty(blocks * 4, np.float32)
+    step = 1 << 22
+    for b0 in range(0, blocks, step):
+        b = np.arange(b0, min(blocks, b0 + step), dtype=np.uint64)
+        ctr = np.zeros((len(b), 4), np.uint32)
+        ctr[:, 0] = (b & np.uint64(0xFFFFFFFF)).astype(np.uint32)
+        ctr[:, 1] = (b >> np.uint64(32)).astype(np.uint32)
+        w = philox4x32_10(ctr, (seed & 0xFFFFFFFF, (seed >> 32) & 0xFFFFFFFF))
+        out[4 * b0:4 * b0 + 4 * len(b)] = (w >> np.uint32(8)).astype(np.float32).reshape(-1) * np.float32(2.0 ** -24)
+    return out[:total].reshape(n, n, n)
+
+
 def gaussian_noise(n: int, seed: int) -> np.ndarray:
     """Unit Gaussian noise [z][y][x] (float32): Philox4x32-10 uniforms through the
     reference's Box-Muller pairing along x (initial_conditions.f90:320-336)."""
     if n % 2:
         raise ValueError("noise grid must be even along x")
-    rng = np.random.Generator(np.random.Philox(seed))
-    u = rng.random((n, n, n), dtype=np.float32)
+    u = uniform_noise(n, seed)
     pif = pi_f32()
     theta = np.float32(2.0) * pif * u[..., 0::2]
     r = np.sqrt(np.float32(-2.0) * np.log(np.float32(1.0) - u[..., 1::2]))
@@ -192,7 +231,8 @@ def zeldovich(nc: int, nnt: int, box: float, z_i: float, seed: int, *, np_nc: in
     inv = np.where(kr2 > 0, 1.0 / (kgrid * kgrid * np.maximum(kr2, 1e-30)), 0.0).astype(np.float32)
     disp = np.empty((3, npd, npd, npd), dtype=np.float32)
     for d, kk in enumerate((kx[None, None, :], ky[None, :, None], kz[:, None, None])):
-        psi_k = 1j * (kgrid * kk) * inv * dk
+        # odd in its own wavenumber: zero on that dimension's Nyquist plane
+        psi_k = 1j * (kgrid * kk) * inv * dk * (np.abs(kk) != npd // 2)
         disp[d] = sfft.irfftn(psi_k, s=(npd, npd, npd), workers=-1)
         del psi_k
     del dk, inv
@@ -341,3 +381,27 @@ def nu_fluid_linear(nc: int, box: float, z: float, seed: int, *, fluid_n: int, g
         e = (e + np.float32(0.5) * m * m / rho).astype(np.float32)
     out[..., 4] = e
     return out
+
+
+def device_ic_params(c: Cosmology, z_i: float, nc: int, *, np_nc: int = 2, ncell: int = 4,
+                     box: float = 200.0, amplitude: float = 1.0) -> dict:
+    """The scalars the device initial conditions need (cube_make_ic): the linear power
+    normalisation sigma8^2/v8 * D(a)^2 and the Eisenstein-Hu constants, so the device
+    evaluates Delta^2(k) = norm * T(k)^2 * k^(3+n_s) per mode exactly as delta2() does."""
+    a = 1.0 / (1.0 + z_i)
+    kk = np.logspace(-4, 2, 4000)
+    t = eh_nowiggle(kk, c)
+    w = _tophat(kk * 8.0)
+    v8 = np.trapezoid(t * t * kk ** (3 + c.n_s) * w * w / kk, kk)
+    d = dgrow(a, c.omega_m, c.omega_l)
+    om = c.omega_m * c.h * c.h
+    ob = c.omega_b * c.h * c.h
+    fb = c.omega_b / c.omega_m
+    return {
+        "norm_d2": c.sigma8 ** 2 / v8 * d * d, "n_s": c.n_s, "h": c.h,
+        "eh_s": 44.5 * math.log(9.83 / om) / math.sqrt(1.0 + 10.0 * ob ** 0.75),
+        "eh_alpha": 1.0 - 0.328 * math.log(431.0 * om) * fb + 0.38 * math.log(22.3 * om) * fb * fb,
+        "eh_omh": c.omega_m * c.h, "eh_theta2": (c.t_cmb / 2.7) ** 2,
+        "vf": vfactor(a, c.omega_m, c.omega_l), "a": a, "box": box, "amplitude": amplitude,
+        "np_nc": np_nc, "ncell": ncell, "omega_m": c.omega_m,
+    }

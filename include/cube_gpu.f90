@@ -33,6 +33,13 @@ module cube_gpu
     integer(c_int32_t) :: reserved(16)
   end type
 
+  ! cube_make_ic arguments (in place of running ic.x and reading its files)
+  type, bind(c) :: cube_ic_params_t
+    integer(c_int64_t) :: seed
+    integer(c_int32_t) :: np_nc, pad0
+    real(c_double) :: a, norm_d2, n_s, h, eh_s, eh_alpha, eh_omh, eh_theta2, vf, amplitude, f_cdm
+  end type
+
   interface
     integer(c_int32_t) function cube_create(p, cap, fk, ck, ctx) bind(c, name="cube_create")
       import :: c_int32_t, c_int64_t, c_float, c_ptr, cube_params_t
@@ -97,6 +104,13 @@ module cube_gpu
       real(c_float), intent(out) :: fld(*)
     end function
     ! cicpower analysis into xip(10,nbin)
+    integer(c_int32_t) function cube_make_ic(ctx, ic, s) bind(c, name="cube_make_ic")
+      import :: c_int32_t, c_ptr, cube_ic_params_t, cube_scalars_t
+      type(c_ptr), value :: ctx
+      type(cube_ic_params_t), intent(in) :: ic
+      type(cube_scalars_t), intent(inout) :: s
+    end function
+
     integer(c_int32_t) function cube_power_spectrum(ctx, log_bins, xip, capacity, nbin) &
         bind(c, name="cube_power_spectrum")
       import :: c_int32_t, c_ptr, c_float

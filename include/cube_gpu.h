@@ -191,6 +191,39 @@ int32_t cube_nu_store(cube_ctx* ctx, int32_t fluid, float* fld);
  * call it between steps, not inside one. */
 int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t capacity, int32_t* nbin);
 
+/* ---- initial conditions on the device -----------------------------------------
+ * Replaces running the ic.x program (initial_conditions.f90:268-900) and loading
+ * its files with cube_load_state: a Zel'dovich state on the np_nc*nc particle
+ * lattice, made in place.  The linear power is Delta^2(k) = norm_d2 * T(k)^2 *
+ * k^(3+n_s) with the Eisenstein-Hu (1998) no-wiggle transfer T (k in h/Mpc; the
+ * host precomputes the sigma8 normalisation times D(a)^2 and the EH constants);
+ * the noise is Philox4x32-10 under `seed` through the reference's Box-Muller
+ * pairing along x (initial_conditions.f90:320-336).  Particles are packed as the
+ * reference packs them (:797-838): sorted by coarse cell, lattice order within a
+ * cell, PID = lattice index + 1, vfield = cell-mean velocity, velocity codes
+ * relative to it with sigma_vi from the residuals. */
+typedef struct cube_ic_params {
+  int64_t seed;
+  int32_t np_nc;        /* particles per coarse cell per dimension; np_nc*nc even */
+  int32_t pad0;
+  double a;             /* initial scale factor 1/(1+z_i) */
+  double norm_d2;       /* sigma8^2/v8 * D(a)^2 */
+  double n_s, h;
+  double eh_s;          /* sound horizon, Mpc */
+  double eh_alpha;      /* alpha_Gamma */
+  double eh_omh;        /* Omega_m h */
+  double eh_theta2;     /* (T_cmb/2.7)^2 */
+  double vf;            /* a^2 H(a) f(a), simulation units (initial_conditions.f90:1068-1079) */
+  double amplitude;     /* extra scale of the displacement (1) */
+  double f_cdm;         /* CDM share of the matter: mass_p_cdm = f_cdm*nf^3/np */
+} cube_ic_params;
+
+/* Generates the state above for the context's box (params.box, nc, nnt, ncell,
+ * izipx, izipv) and sets the scalar block as particle_initialization.f90:37-39
+ * does after reading it (a, sigma_vi, mass_p_cdm, vmax, vz_max, dt_vmax, np).
+ * Uses the fine meshes as scratch (np_nc <= ncell); needs np <= np_capacity. */
+int32_t cube_make_ic(cube_ctx* ctx, const cube_ic_params* ic, cube_scalars* io);
+
 /* Set-up constants, 19 floats: beta = m/T, the three normalised weights, then
  * per fluid (n, ncb of the reference layout, dx, cs2, hg_dv). */
 int32_t cube_nu_info(cube_ctx* ctx, float* out);
