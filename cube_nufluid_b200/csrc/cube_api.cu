@@ -58,6 +58,7 @@ int alloc_level(cube_ctx* ctx, MeshLevel& L, int n) {
   const size_t vol = (size_t)n * L.plane;
   CUBE_CUDA_TRY(ctx, cudaMalloc(&L.rho, sizeof(float) * vol));
   CUBE_CUDA_TRY(ctx, cudaMalloc(&L.force, sizeof(float) * 3 * vol));
+  CUBE_CUDA_TRY(ctx, cudaMalloc(&L.ext, sizeof(float) * vol));
   const int kp = n / 2 + 1;
   L.kern_octant = 1;
   L.kern_pitch = kp;
@@ -197,8 +198,9 @@ void cube_destroy(cube_ctx* ctx) {
                   ctx->cell_start, ctx->cell_start2, ctx->vfield, ctx->vfield2, ctx->tcell, ctx->tkey,
                   ctx->perm, ctx->pkey, ctx->cursor, ctx->big_list, ctx->cell_stats, ctx->slot_r2, ctx->slot_s2,
                   ctx->red_tmp,
-                  ctx->scan_tmp, ctx->fine.rho, ctx->fine.force, ctx->fine.kern, ctx->fine.plan.tw,
-                  ctx->coarse.rho, ctx->coarse.force, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->rho_c_acc,
+                  ctx->scan_tmp, ctx->fine.rho, ctx->fine.force, ctx->fine.ext, ctx->fine.kern, ctx->fine.plan.tw, ctx->fine.plan.tw2,
+                  ctx->coarse.rho, ctx->coarse.force, ctx->coarse.ext, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->coarse.plan.tw2,
+                  ctx->rho_c_acc,
                   ctx->tan_table, ctx->dscal, ctx->pk_bins};
   for (void* p : ptrs)
     if (p) cudaFree(p);

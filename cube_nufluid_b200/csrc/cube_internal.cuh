@@ -29,7 +29,22 @@ struct FftPlan {
   int nst;                        // number of stages
   int radix[CUBE_MAX_RADIX_STAGES];
   float2* tw;                     // device twiddles exp(-2 pi i j/n), j < n
+  float2* tw2;                    // register-FFT twiddles tw[(t*k1) mod n] at [k1*T + t] (n = R*T)
 };
+
+// R x T split of the register-resident transforms (T threads of one warp, R
+// points each); false for lengths they do not cover
+inline bool cube_fast_rt(int n, int* R, int* T) {
+  switch (n) {
+    case 1024: *R = 32; *T = 32; return true;
+    case 512: *R = 32; *T = 16; return true;
+    case 256: *R = 16; *T = 16; return true;
+    case 128: *R = 16; *T = 8; return true;
+    case 64: *R = 8; *T = 8; return true;
+    case 32: *R = 8; *T = 4; return true;
+    default: return false;
+  }
+}
 
 struct MeshLevel {
   int n;          // mesh points per dimension
@@ -38,6 +53,7 @@ struct MeshLevel {
   size_t plane;   // floats per z-plane = n*rp
   float* rho;     // density, in place as the forward half spectrum
   float* force;   // [3] force meshes, each n*plane floats, in place as spectra
+  float* ext;     // scratch mesh (n*plane floats) for the transposed passes
   float* kern;    // Green multiplier (imaginary parts, /n^3)
   int kern_octant;  // 1: kern is [3][(n/2+1)^3] octant; 0: [3][n][n][cp_k]
   int kern_pitch;   // inner pitch of kern (n/2+1)
@@ -219,10 +235,10 @@ int cube_rebin(cube_ctx* ctx, cube_scalars* io);
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks);
 int cube_force_scale(cube_ctx* ctx, MeshLevel& L, KickScale ks);
-int cube_fft_forward3(cube_ctx* ctx, MeshLevel& L, float* data);
+int cube_fft_forward3(cube_ctx* ctx, MeshLevel& L, float* data, int* kx_major);
 int cube_pk_nbin(int ng, int logbins);
 int cube_power_spectrum_dev(cube_ctx* ctx, int logbins, std::vector<double>& bins, int* nbin_out);
-int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc);
+int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc, int* kx_major);
 int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks, int* rc);
 int cube_kick(cube_ctx* ctx, cube_scalars* io);
 int cube_pp(cube_ctx* ctx, cube_scalars* io);

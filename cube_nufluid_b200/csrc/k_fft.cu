@@ -305,6 +305,7 @@ int pick_threads(int butterflies4, int maxit) {
 int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n) {
   p.n = n;
   p.nst = 0;
+  p.tw = p.tw2 = nullptr;
   int m = n;
   while (m % 4 == 0) { p.radix[p.nst++] = 4; m /= 4; }
   while (m % 2 == 0) { p.radix[p.nst++] = 2; m /= 2; }
@@ -321,6 +322,16 @@ int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n) {
   }
   CUBE_CUDA_TRY(ctx, cudaMalloc(&p.tw, sizeof(float2) * n));
   CUBE_CUDA_TRY(ctx, cudaMemcpy(p.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  int R, T;
+  if (cube_fast_rt(n, &R, &T)) {
+    // the twiddles thread t of a register transform multiplies its k1-th value by,
+    // laid out so that a warp's loads are contiguous
+    std::vector<float2> tw2((size_t)R * T);
+    for (int k1 = 0; k1 < R; ++k1)
+      for (int t = 0; t < T; ++t) tw2[(size_t)k1 * T + t] = tw[(t * k1) & (n - 1)];
+    CUBE_CUDA_TRY(ctx, cudaMalloc(&p.tw2, sizeof(float2) * R * T));
+    CUBE_CUDA_TRY(ctx, cudaMemcpy(p.tw2, tw2.data(), sizeof(float2) * R * T, cudaMemcpyHostToDevice));
+  }
   return CUBE_OK;
 }
 
@@ -400,9 +411,10 @@ int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickSca
 }
 
 // forward 3-D r2c in place (x, y, z), unnormalised
-int cube_fft_forward3(cube_ctx* ctx, MeshLevel& L, float* data) {
+int cube_fft_forward3(cube_ctx* ctx, MeshLevel& L, float* data, int* kx_major) {
   int rc;
-  if (!ctx->P.reserved[0] && cube_fft_forward3_fast(ctx, L, data, &rc)) return rc;
+  if (!ctx->P.reserved[0] && cube_fft_forward3_fast(ctx, L, data, &rc, kx_major)) return rc;
+  *kx_major = 0;
   if ((rc = cube_fft_r2c_x(ctx, L, data, 0, 1, nullptr))) return rc;
   if ((rc = col_pass(ctx, L, data, 1, 0, -1.f))) return rc;
   return col_pass(ctx, L, data, 1, 1, -1.f);

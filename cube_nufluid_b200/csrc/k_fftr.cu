@@ -131,7 +131,7 @@ __device__ __forceinline__ void fft_from_regs(float2* v, float2* s, int es, int 
   dft_reg<R, SIGN>(v);
 #pragma unroll
   for (int k1 = 1; k1 < R; ++k1) {
-    float2 w = __ldg(&tw[(t * k1) & (N - 1)]);
+    float2 w = __ldg(&tw[k1 * T + t]);  // = exp(-2 pi i ((t k1) mod N)/N)
     if (SIGN > 0) w.y = -w.y;
     v[k1] = cmul(v[k1], w);
   }
@@ -188,6 +188,232 @@ __global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_
   }
 }
 
+// ---------------------------------------------------------------------------
+// Transposed-layout passes.  Every transform runs along contiguous memory: a
+// group of T threads loads its row straight into registers (coalesced), and the
+// pass writes its output with the next transform's dimension innermost (through
+// the natural-order result in shared memory, read across the CTA's 8 rows).
+// Per complex point that is two shared-memory round trips (the in-warp exchange
+// and the transpose) instead of three, and no global->shared copy.  Layouts of
+// a level with n = N, H = N/2 + 1, cp = complex row pitch:
+//   S1 [z][kx][y]  after x r2c           (in L.ext)
+//   S2 [kx][ky][z] after y forward       (in L.rho)
+//   S3 [z][kx][ky] after z+Green+z^-1    (components 0,1,2 in force 1, force 2, L.ext)
+//   S4 [z][y][kx]  after y^-1, pitch cp  (components 0,1,2 in force 0, 1, 2)
+// then x c2r in place gives the real force meshes.  The arithmetic of every
+// transform is that of the column kernels above, so results are bit-identical.
+
+// group stride in float2 for RT rows per CTA: >= N + R + 8 and == 16/RT (mod 16),
+// so that reading one column across the RT rows (two rows per thread) is free of
+// bank conflicts
+template <int N, int R, int RT>
+constexpr int cs_row() {
+  return ((N + R + 8 + 15) / 16) * 16 + 16 / RT;
+}
+
+// x r2c of 8 rows (4 packed complex transforms) of one z-plane -> S1
+template <int N, int R, int T>
+__global__ void __launch_bounds__(4 * T) k_xr2c_t(const float* __restrict__ rho, int rp, float2* __restrict__ out,
+                                                  const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  constexpr int CS = cs_row<N, R, 4>();
+  constexpr int H = N / 2 + 1;
+  constexpr int YB = N / 8;
+  const int z = blockIdx.x / YB, y0 = (blockIdx.x - z * YB) * 8;
+  const int g = threadIdx.x / T, t = threadIdx.x - g * T;
+  const float* ra = rho + ((size_t)z * N + y0 + 2 * g) * rp;
+  const float* rb = ra + rp;
+  float2 v[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) v[q] = make_float2(__ldg(&ra[t + T * q]), __ldg(&rb[t + T * q]));
+  fft_from_regs<N, R, T, -1, true>(v, sm + g * CS, 1, t, tw);
+  __syncthreads();
+  float2* o = out + (size_t)z * H * N + y0;
+  for (int i = threadIdx.x; i < 4 * H; i += 4 * T) {
+    const int k = i >> 2, p = i & 3;
+    const float2 Zk = sm[p * CS + k];
+    const float2 Zm = sm[p * CS + ((N - k) & (N - 1))];
+    const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
+    const float2 B = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
+    *reinterpret_cast<float4*>(o + (size_t)k * N + 2 * p) = make_float4(A.x, A.y, B.x, B.y);
+  }
+}
+
+// natural-order results of the CTA's 8 rows (group stride CS) -> out + B0 + k*B1 + r,
+// two rows per thread (16-byte stores), rows r >= nrows skipped
+template <int N, int T, int CS>
+__device__ __forceinline__ void store_transposed(const float2* sm, float2* __restrict__ out, size_t B0, size_t B1,
+                                                 int nrows) {
+  for (int i = threadIdx.x; i < 4 * N; i += 8 * T) {
+    const int k = i >> 2, r = 2 * (i & 3);
+    const float2 a = sm[r * CS + k], b = sm[(r + 1) * CS + k];
+    float2* o = out + B0 + (size_t)k * B1 + r;
+    if (r + 1 < nrows) *reinterpret_cast<float4*>(o) = make_float4(a.x, a.y, b.x, b.y);
+    else if (r < nrows) *o = a;
+  }
+}
+
+// one transform along rows of 8 consecutive row indices, transposed output:
+//   MODE 0  y forward : S1 rows (z, kx), CTA = (kx, 8 z)  -> S2 [kx][ky][z]
+//   MODE 1  y inverse : S3 rows (z, kx), CTA = (z, 8 kx)  -> S4 [z][y][kx] (pitch cp)
+template <int N, int R, int T, int SIGN, int MODE>
+__global__ void __launch_bounds__(8 * T) k_row_t(const float2* __restrict__ in, float2* __restrict__ out, int cp,
+                                                 const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  constexpr int CS = cs_row<N, R, 8>();
+  constexpr int H = N / 2 + 1;
+  const int g = threadIdx.x / T, t = threadIdx.x - g * T;
+  size_t row, B0, B1;
+  int nrows = 8;
+  if (MODE == 0) {
+    constexpr int ZB = N / 8;
+    const int kx = blockIdx.x / ZB, z0 = (blockIdx.x - kx * ZB) * 8;
+    row = ((size_t)(z0 + g) * H + kx) * N;
+    B0 = (size_t)kx * N * N + z0;
+    B1 = N;
+  } else {
+    constexpr int KB = (H + 7) / 8;
+    const int z = blockIdx.x / KB, kx0 = (blockIdx.x - z * KB) * 8;
+    nrows = min(8, H - kx0);
+    row = ((size_t)z * H + min(kx0 + g, H - 1)) * N;
+    B0 = (size_t)z * N * cp + kx0;
+    B1 = cp;
+  }
+  float2 v[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) v[q] = __ldg(&in[row + t + T * q]);
+  fft_from_regs<N, R, T, SIGN, true>(v, sm + g * CS, 1, t, tw);
+  __syncthreads();
+  store_transposed<N, T, CS>(sm, out, B0, B1, nrows);
+}
+
+// z forward, Green multiply, z inverse on S2 rows (kx, ky), CTA = (kx, 8 ky);
+// the three components go out transposed to S3 in o0, o1, o2
+template <int N, int R, int T>
+__global__ void __launch_bounds__(8 * T) k_zgreen_t(const float2* __restrict__ in, float2* __restrict__ o0,
+                                                    float2* __restrict__ o1, float2* __restrict__ o2,
+                                                    const float2* __restrict__ tw, const float* __restrict__ kern,
+                                                    int kp, float ksc) {
+  extern __shared__ float2 sm[];
+  constexpr int CS = cs_row<N, R, 8>();
+  constexpr int H = N / 2 + 1;
+  constexpr int nh = N / 2;
+  constexpr int YB = N / 8;
+  const int kx = blockIdx.x / YB, ky0 = (blockIdx.x - kx * YB) * 8;
+  const int g = threadIdx.x / T, t = threadIdx.x - g * T;
+  const int ky = ky0 + g;
+  const float2* bi = in + ((size_t)kx * N + ky) * N;
+  float2 v[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) v[q] = __ldg(&bi[t + T * q]);
+  float2* s = sm + g * CS;
+  fft_from_regs<N, R, T, -1, true>(v, s, 1, t, tw);
+  float2 keep[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) keep[q] = s[t + T * q];
+  const int fy = ky <= nh ? ky : N - ky;
+  const float sy = ky <= nh ? 1.f : -1.f;
+  const size_t ksz = (size_t)kp * kp * kp;
+  const size_t B0 = (size_t)kx * N + ky0, B1 = (size_t)H * N;
+#pragma unroll 1
+  for (int d = 0; d < 3; ++d) {
+    const float* K = kern + d * ksz + ((size_t)fy * kp + kx) * kp;
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int kz = t + T * q;
+      const int fz = kz <= nh ? kz : N - kz;
+      float kv = __ldg(&K[fz]) * ksc;
+      if (d == 1) kv *= sy;
+      if (d == 2 && kz > nh) kv = -kv;
+      v[q] = make_float2(-keep[q].y * kv, keep[q].x * kv);
+    }
+    __syncwarp();
+    fft_from_regs<N, R, T, 1, true>(v, s, 1, t, tw);
+    __syncthreads();
+    store_transposed<N, T, CS>(sm, d == 0 ? o0 : (d == 1 ? o1 : o2), B0, B1, 8);
+    __syncthreads();
+  }
+}
+
+// in-place transform of 8 contiguous rows of length N (the z pass of the forward
+// 3-D transform on S2)
+template <int N, int R, int T, int SIGN>
+__global__ void __launch_bounds__(8 * T) k_row_inplace(float2* __restrict__ data, long long nrows,
+                                                       const float2* __restrict__ tw) {
+  extern __shared__ float2 sm[];
+  constexpr int CS = cs_row<N, R, 8>();
+  const int g = threadIdx.x / T, t = threadIdx.x - g * T;
+  const long long row = min((long long)blockIdx.x * 8 + g, nrows - 1);
+  float2* b = data + (size_t)row * N;
+  float2 v[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) v[q] = b[t + T * q];
+  float2* s = sm + g * CS;
+  fft_from_regs<N, R, T, SIGN, true>(v, s, 1, t, tw);
+  if ((long long)blockIdx.x * 8 + g < nrows) {
+#pragma unroll
+    for (int q = 0; q < R; ++q) b[t + T * q] = s[t + T * q];
+  }
+}
+
+// x c2r of the three force components (S4 rows of RB row pairs, in place) with
+// max f^2, as k_xc2r3 but loading the half spectra straight into registers
+template <int N, int R, int T, int RB>
+__global__ void __launch_bounds__(3 * T * RB) k_xc2r3_t(float* __restrict__ data, size_t comp_stride, int rp,
+                                                        int npairs, const float2* __restrict__ tw,
+                                                        unsigned int* __restrict__ f2_bits) {
+  extern __shared__ float2 sm[];
+  constexpr int CS = N + R + 8;
+  constexpr int NT = 3 * T * RB;
+  constexpr int nh = N / 2;
+  const int pair0 = blockIdx.x * RB;
+  const int cp = rp / 2;
+  const int g = threadIdx.x / T, t = threadIdx.x % T;
+  {
+    const int c = g / RB, q = g - c * RB;
+    const int pr = min(pair0 + q, npairs - 1);
+    const float2* A = reinterpret_cast<const float2*>(data + c * comp_stride) + (size_t)(2 * pr) * cp;
+    const float2* B = A + cp;
+    float2 v[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int n = t + T * k;
+      if (n == 0 || n == nh) {
+        v[k] = make_float2(A[n].x, B[n].x);
+      } else if (n < nh) {
+        const float2 a = A[n], b = B[n];
+        v[k] = make_float2(a.x - b.y, a.y + b.x);
+      } else {
+        const float2 a = A[N - n], b = B[N - n];
+        v[k] = make_float2(a.x + b.y, b.x - a.y);
+      }
+    }
+    fft_from_regs<N, R, T, 1, true>(v, sm + g * CS, 1, t, tw);
+  }
+  __syncthreads();
+  float f2max = 0.f;
+  for (int i = threadIdx.x; i < RB * N; i += NT) {
+    const int q = i / N, j = i - q * N;
+    if (pair0 + q >= npairs) continue;
+    const size_t ra = (size_t)(2 * (pair0 + q)) * rp;
+    float fa[3], fb[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float2 z = sm[(c * RB + q) * CS + j];
+      float* base = data + c * comp_stride;
+      base[ra + j] = z.x;
+      base[ra + rp + j] = z.y;
+      fa[c] = z.x;
+      fb[c] = z.y;
+    }
+    const float a2 = __fadd_rn(__fadd_rn(__fmul_rn(fa[0], fa[0]), __fmul_rn(fa[1], fa[1])), __fmul_rn(fa[2], fa[2]));
+    const float b2 = __fadd_rn(__fadd_rn(__fmul_rn(fb[0], fb[0]), __fmul_rn(fb[1], fb[1])), __fmul_rn(fb[2], fb[2]));
+    f2max = fmaxf(f2max, fmaxf(a2, b2));
+  }
+  for (int o = 16; o > 0; o >>= 1) f2max = fmaxf(f2max, __shfl_xor_sync(0xffffffffu, f2max, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(f2_bits, __float_as_uint(f2max));
+}
+
 // fused z pass with the Green multiply (kernel octant [d][ky][kx][kz], kz fastest)
 template <int N, int R, int T, int TK>
 __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in, float2* __restrict__ out0,
@@ -229,62 +455,6 @@ __global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in
       if (d == 1) kv *= sy;
       if (d == 2 && kz > nh) kv = -kv;
       v[q] = make_float2(-keep[q].y * kv, keep[q].x * kv);
-    }
-    __syncwarp();
-    fft_from_regs<N, R, T, 1, false>(v, s, P, t, tw);
-    __syncthreads();
-    float2* bo = out0 + d * comp_stride + (size_t)ky * ostride + kx0;
-    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-      const int j = i / TK, c = i - j * TK;
-      if (c < nk) bo[(size_t)j * jstride + c] = sm[j * P + c];
-    }
-    __syncthreads();
-  }
-}
-
-// k_zgreen with the forward spectrum kept in a second shared buffer instead of
-// registers (fewer registers per thread, more resident columns per SM)
-template <int N, int R, int T, int TK>
-__global__ void __launch_bounds__(T * TK, 512 / (T * TK)) k_zgreen_s(const float2* __restrict__ in, float2* __restrict__ out0,
-                                                     size_t comp_stride, int ncol, long long jstride,
-                                                     long long ostride, const float2* __restrict__ tw,
-                                                     const float* __restrict__ kern, int kp, float ksc) {
-  extern __shared__ float2 sm[];
-  constexpr int P = TK + 1;
-  float2* spec = sm + (size_t)N * P;  // forward spectrum, same layout
-  const int kx0 = blockIdx.x * TK;
-  const int nk = min(TK, ncol - kx0);
-  const int ky = blockIdx.y;
-  const float2* bi = in + (size_t)ky * ostride + kx0;
-  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-    const int j = i / TK, c = i - j * TK;
-    cp_async8(&sm[j * P + c], c < nk ? &bi[(size_t)j * jstride + c] : bi, c < nk);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  const int g = threadIdx.x / T, t = threadIdx.x % T;
-  float2* s = sm + g;
-  fft_seq<N, R, T, -1, false>(s, P, t, tw);
-#pragma unroll
-  for (int q = 0; q < R; ++q) spec[(t + T * q) * P + g] = s[(t + T * q) * P];
-  constexpr int nh = N / 2;
-  const int fy = ky <= nh ? ky : N - ky;
-  const float sy = ky <= nh ? 1.f : -1.f;
-  const int kx = min(kx0 + g, ncol - 1);
-  const size_t ksz = (size_t)kp * kp * kp;
-#pragma unroll 1
-  for (int d = 0; d < 3; ++d) {
-    const float* K = kern + d * ksz + ((size_t)fy * kp + kx) * kp;
-    float2 v[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int kz = t + T * q;
-      const int fz = kz <= nh ? kz : N - kz;
-      float kv = __ldg(&K[fz]) * ksc;
-      if (d == 1) kv *= sy;
-      if (d == 2 && kz > nh) kv = -kv;
-      const float2 a = spec[kz * P + g];
-      v[q] = make_float2(-a.y * kv, a.x * kv);
     }
     __syncwarp();
     fft_from_regs<N, R, T, 1, false>(v, s, P, t, tw);
@@ -401,6 +571,90 @@ __global__ void __launch_bounds__(3 * T * RB) k_xc2r3(float* __restrict__ data, 
   if ((threadIdx.x & 31) == 0) atomicMax(f2_bits, __float_as_uint(f2max));
 }
 
+// k_col, one CTA per tile (the in-place column passes, params.reserved[5] = 1)
+template <int N, int R, int T, int TK, int SIGN>
+int col_pass_1(cube_ctx* ctx, float2* base, size_t cstride, int ncol, int nplanes, int ncomp, long long jstride,
+               long long ostride, const float2* tw) {
+  const size_t smem = sizeof(float2) * (size_t)N * (TK + 1);
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, SIGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const dim3 g((ncol + TK - 1) / TK, nplanes, ncomp);
+  k_col<N, R, T, TK, SIGN><<<g, T * TK, smem, ctx->stream>>>(base, cstride, ncol, jstride, ostride, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
+template <int N, int R, int T, int TK, int SIGN>
+int col_pass(cube_ctx* ctx, float2* base, size_t cstride, int ncol, int nplanes, int ncomp, long long jstride,
+             long long ostride, const float2* tw) {
+  return col_pass_1<N, R, T, TK, SIGN>(ctx, base, cstride, ncol, nplanes, ncomp, jstride, ostride, tw);
+}
+
+template <int N, int R, int T>
+int run_poisson_t(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks) {
+  constexpr int H = N / 2 + 1;
+  constexpr int RB3 = (T >= 32) ? 2 : (T >= 16 ? 4 : 8);
+  const float2* tw = L.plan.tw2;
+  const size_t cstride = (size_t)N * L.plane;  // floats per force component
+  float* F[3] = {L.force, L.force + cstride, L.force + 2 * cstride};
+  const size_t sm1 = sizeof(float2) * 4 * cs_row<N, R, 4>();
+  const size_t sm8 = sizeof(float2) * 8 * cs_row<N, R, 8>();
+  const size_t sm3 = sizeof(float2) * 3 * RB3 * (N + R + 8);
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3_t<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
+  float2* ext = reinterpret_cast<float2*>(L.ext);
+  float2* rho = reinterpret_cast<float2*>(L.rho);
+  // x r2c: rho -> S1 (ext)
+  k_xr2c_t<N, R, T><<<N * (N / 8), 4 * T, sm1, ctx->stream>>>(L.rho, L.rp, ext, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  // y forward: S1 -> S2 (rho)
+  k_row_t<N, R, T, -1, 0><<<H * (N / 8), 8 * T, sm8, ctx->stream>>>(ext, rho, L.cp, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  // z forward, Green, z inverse: S2 -> S3 of components 0, 1, 2 in force 1, force 2, ext
+  k_zgreen_t<N, R, T><<<H * (N / 8), 8 * T, sm8, ctx->stream>>>(
+      rho, reinterpret_cast<float2*>(F[1]), reinterpret_cast<float2*>(F[2]), ext, tw, L.kern, L.kern_pitch,
+      cube_kick_scalar(ks));
+  CUBE_LAUNCH_CHECK(ctx);
+  // y inverse, component by component into the freed buffers: S3 -> S4 in force 0, 1, 2
+  const float2* s3[3] = {reinterpret_cast<float2*>(F[1]), reinterpret_cast<float2*>(F[2]), ext};
+  for (int d = 0; d < 3; ++d) {
+    k_row_t<N, R, T, 1, 1><<<N * ((H + 7) / 8), 8 * T, sm8, ctx->stream>>>(s3[d], reinterpret_cast<float2*>(F[d]),
+                                                                           L.cp, tw);
+    CUBE_LAUNCH_CHECK(ctx);
+  }
+  // x c2r of the three components in place, max f^2
+  const int npairs = N * N / 2;
+  k_xc2r3_t<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, sm3, ctx->stream>>>(L.force, cstride, L.rp,
+                                                                                       npairs, tw, f2_bits);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
+// forward 3-D r2c: x (data -> ext), y (ext -> data), z in place; the spectrum ends
+// in data as [kx][ky][kz], dense rows of N
+template <int N, int R, int T>
+int run_forward3_t(cube_ctx* ctx, MeshLevel& L, float* data) {
+  constexpr int H = N / 2 + 1;
+  const float2* tw = L.plan.tw2;
+  const size_t sm1 = sizeof(float2) * 4 * cs_row<N, R, 4>();
+  const size_t sm8 = sizeof(float2) * 8 * cs_row<N, R, 8>();
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_inplace<N, R, T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  float2* ext = reinterpret_cast<float2*>(L.ext);
+  float2* d2 = reinterpret_cast<float2*>(data);
+  k_xr2c_t<N, R, T><<<N * (N / 8), 4 * T, sm1, ctx->stream>>>(data, L.rp, ext, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_row_t<N, R, T, -1, 0><<<H * (N / 8), 8 * T, sm8, ctx->stream>>>(ext, d2, L.cp, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  const long long nrows = (long long)H * N;
+  k_row_inplace<N, R, T, -1><<<(unsigned)((nrows + 7) / 8), 8 * T, sm8, ctx->stream>>>(d2, nrows, tw);
+  CUBE_LAUNCH_CHECK(ctx);
+  return CUBE_OK;
+}
+
 template <int N, int R, int T>
 int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks) {
   constexpr int TK = (T >= 16) ? 8 : 16;
@@ -409,94 +663,34 @@ int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks
   const int ncol = N / 2 + 1;
   const long long cp = L.cp;
   const size_t cstride = (size_t)N * L.plane / 2;
-  const float2* tw = L.plan.tw;
+  const float2* tw = L.plan.tw2;
   const size_t xsm = sizeof(float2) * RB * (N + R + 8);
   const size_t x3sm = sizeof(float2) * 3 * RB3 * (N + R + 8);
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)x3sm));
   const size_t csm = sizeof(float2) * (size_t)N * (TK + 1);
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen<N, R, T, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-  // y passes with twice the columns per CTA (longer contiguous row segments, fewer
-  // CTAs per SM), selected by params.reserved[3] = 16 where T*16 <= 1024 threads
-  constexpr int TKW = (T * 2 * TK <= 1024) ? 2 * TK : TK;
-  const size_t csmw = sizeof(float2) * (size_t)N * (TKW + 1);
-  const bool wide = ctx->P.reserved[3] == 16 && TKW != TK && csmw <= 227 * 1024;
-  if (wide) {
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TKW, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmw));
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TKW, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csmw));
-  }
-  // The x and y passes can run slab by slab over z (params.reserved[1] / [2] planes
-  // per slab for the forward / inverse passes), which keeps a slab's intermediate
-  // in L2 between the two passes; measured at nf = 1024 every slab size was slower
-  // than whole-mesh passes (the short launches lose more to partial waves than the
-  // L2 reuse saves), so whole-mesh passes are the default.
-  int szf = N, szi = N;
-  if (ctx->P.reserved[1] > 0) szf = ctx->P.reserved[1];
-  if (ctx->P.reserved[2] > 0) szi = ctx->P.reserved[2];
-  szf = std::min(szf, N);
-  szi = std::min(szi, N);
   float2* spec = reinterpret_cast<float2*>(L.rho);
   const long long pstride = (long long)N * cp;  // float2 per plane
-  for (int z0 = 0; z0 < N; z0 += szf) {
-    const int nz = std::min(szf, N - z0);
-    // x r2c of the slab's rows (two real rows per complex transform)
-    const int npairs = nz * N / 2;
-    k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, xsm, ctx->stream>>>(L.rho + (size_t)z0 * L.plane, L.rp,
-                                                                              npairs, tw);
-    CUBE_LAUNCH_CHECK(ctx);
-    // y forward of the slab's columns
-    if (wide) {
-      const dim3 g((ncol + TKW - 1) / TKW, nz, 1);
-      k_col<N, R, T, TKW, -1><<<g, T * TKW, csmw, ctx->stream>>>(spec + (size_t)z0 * pstride, cstride, ncol, cp,
-                                                                  pstride, tw);
-    } else {
-      const dim3 g((ncol + TK - 1) / TK, nz, 1);
-      k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec + (size_t)z0 * pstride, cstride, ncol, cp,
-                                                               pstride, tw);
-    }
-    CUBE_LAUNCH_CHECK(ctx);
-  }
-  // z forward, Green, z inverse (whole mesh: z columns span every slab); with
-  // params.reserved[4] = 1 the spectrum stays in shared memory (k_zgreen_s, 2 columns per CTA)
-  if (ctx->P.reserved[4] == 1) {
-    constexpr int TKS = 2;
-    const size_t ssm = 2 * sizeof(float2) * (size_t)N * (TKS + 1);
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen_s<N, R, T, TKS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
-    const dim3 gs((ncol + TKS - 1) / TKS, N, 1);
-    k_zgreen_s<N, R, T, TKS><<<gs, T * TKS, ssm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
-                                                                 reinterpret_cast<float2*>(L.force), cstride, ncol,
-                                                                 pstride, cp, tw, L.kern, L.kern_pitch,
-                                                                 cube_kick_scalar(ks));
-  } else {
-    const dim3 g1((ncol + TK - 1) / TK, N, 1);
-    k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
-                                                              reinterpret_cast<float2*>(L.force), cstride, ncol,
-                                                              pstride, cp, tw, L.kern, L.kern_pitch,
-                                                              cube_kick_scalar(ks));
-  }
+  const int npairs = N * N / 2;
+  int rc;
+  // x r2c (two real rows per complex transform), then y forward
+  k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, xsm, ctx->stream>>>(L.rho, L.rp, npairs, tw);
   CUBE_LAUNCH_CHECK(ctx);
-  float2* fspec = reinterpret_cast<float2*>(L.force);
-  for (int z0 = 0; z0 < N; z0 += szi) {
-    const int nz = std::min(szi, N - z0);
-    // y inverse, three components
-    if (wide) {
-      const dim3 g((ncol + TKW - 1) / TKW, nz, 3);
-      k_col<N, R, T, TKW, 1><<<g, T * TKW, csmw, ctx->stream>>>(fspec + (size_t)z0 * pstride, cstride, ncol, cp,
-                                                                 pstride, tw);
-    } else {
-      const dim3 g((ncol + TK - 1) / TK, nz, 3);
-      k_col<N, R, T, TK, 1><<<g, T * TK, csm, ctx->stream>>>(fspec + (size_t)z0 * pstride, cstride, ncol, cp,
-                                                              pstride, tw);
-    }
-    CUBE_LAUNCH_CHECK(ctx);
-    // x c2r, three components, max f^2
-    const int npairs = nz * N / 2;
-    k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, x3sm, ctx->stream>>>(
-        L.force + (size_t)z0 * L.plane, (size_t)N * L.plane, L.rp, npairs, tw, f2_bits);
-    CUBE_LAUNCH_CHECK(ctx);
-  }
+  if ((rc = col_pass<N, R, T, TK, -1>(ctx, spec, cstride, ncol, N, 1, cp, pstride, tw))) return rc;
+  // z forward, Green, z inverse
+  const dim3 g1((ncol + TK - 1) / TK, N, 1);
+  k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
+                                                            reinterpret_cast<float2*>(L.force), cstride, ncol,
+                                                            pstride, cp, tw, L.kern, L.kern_pitch,
+                                                            cube_kick_scalar(ks));
+  CUBE_LAUNCH_CHECK(ctx);
+  // y inverse of the three components, then x c2r with max f^2
+  if ((rc = col_pass<N, R, T, TK, 1>(ctx, reinterpret_cast<float2*>(L.force), cstride, ncol, N, 3, cp, pstride, tw)))
+    return rc;
+  k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, x3sm, ctx->stream>>>(
+      L.force, (size_t)N * L.plane, L.rp, npairs, tw, f2_bits);
+  CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }
 
@@ -508,47 +702,52 @@ int run_forward3(cube_ctx* ctx, MeshLevel& L, float* data) {
   constexpr int RB = (T >= 32) ? 4 : (T >= 16 ? 8 : 16);
   const int ncol = N / 2 + 1;
   const long long cp = L.cp;
-  const float2* tw = L.plan.tw;
+  const float2* tw = L.plan.tw2;
   const size_t xsm = sizeof(float2) * RB * (N + R + 8);
-  const size_t csm = sizeof(float2) * (size_t)N * (TK + 1);
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
   const int npairs = N * N / 2;
   k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, xsm, ctx->stream>>>(data, L.rp, npairs, tw);
   CUBE_LAUNCH_CHECK(ctx);
   float2* spec = reinterpret_cast<float2*>(data);
   const size_t cstride = (size_t)N * L.plane / 2;
-  const dim3 g((ncol + TK - 1) / TK, N, 1);
-  k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec, cstride, ncol, cp, (long long)N * cp, tw);  // y
-  CUBE_LAUNCH_CHECK(ctx);
-  k_col<N, R, T, TK, -1><<<g, T * TK, csm, ctx->stream>>>(spec, cstride, ncol, (long long)N * cp, cp, tw);  // z
-  CUBE_LAUNCH_CHECK(ctx);
-  return CUBE_OK;
+  int rc;
+  if ((rc = col_pass<N, R, T, TK, -1>(ctx, spec, cstride, ncol, N, 1, cp, (long long)N * cp, tw))) return rc;  // y
+  return col_pass<N, R, T, TK, -1>(ctx, spec, cstride, ncol, N, 1, (long long)N * cp, cp, tw);               // z
 }
 
 }  // namespace
 
-int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc) {
+int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc, int* kx_major) {
+  const bool cols = ctx->P.reserved[5] == 1;  // the in-place column passes
+  *kx_major = cols ? 0 : 1;
   switch (L.n) {
-    case 1024: *rc = run_forward3<1024, 32, 32>(ctx, L, data); return 1;
-    case 512: *rc = run_forward3<512, 32, 16>(ctx, L, data); return 1;
-    case 256: *rc = run_forward3<256, 16, 16>(ctx, L, data); return 1;
-    case 128: *rc = run_forward3<128, 16, 8>(ctx, L, data); return 1;
-    case 64: *rc = run_forward3<64, 8, 8>(ctx, L, data); return 1;
-    case 32: *rc = run_forward3<32, 8, 4>(ctx, L, data); return 1;
+#define CUBE_F3(n, r, t) \
+  case n: *rc = cols ? run_forward3<n, r, t>(ctx, L, data) : run_forward3_t<n, r, t>(ctx, L, data); return 1;
+    CUBE_F3(1024, 32, 32)
+    CUBE_F3(512, 32, 16)
+    CUBE_F3(256, 16, 16)
+    CUBE_F3(128, 16, 8)
+    CUBE_F3(64, 8, 8)
+    CUBE_F3(32, 8, 4)
+#undef CUBE_F3
     default: return 0;
   }
 }
 
 // returns 1 if handled by a register-resident path
 int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks, int* rc) {
+  const bool cols = ctx->P.reserved[5] == 1;
   switch (L.n) {
-    case 1024: *rc = run_poisson<1024, 32, 32>(ctx, L, f2_bits, ks); return 1;
-    case 512: *rc = run_poisson<512, 32, 16>(ctx, L, f2_bits, ks); return 1;
-    case 256: *rc = run_poisson<256, 16, 16>(ctx, L, f2_bits, ks); return 1;
-    case 128: *rc = run_poisson<128, 16, 8>(ctx, L, f2_bits, ks); return 1;
-    case 64: *rc = run_poisson<64, 8, 8>(ctx, L, f2_bits, ks); return 1;
-    case 32: *rc = run_poisson<32, 8, 4>(ctx, L, f2_bits, ks); return 1;
+#define CUBE_PS(n, r, t)                                                                                     \
+  case n: *rc = cols ? run_poisson<n, r, t>(ctx, L, f2_bits, ks) : run_poisson_t<n, r, t>(ctx, L, f2_bits, ks); \
+    return 1;
+    CUBE_PS(1024, 32, 32)
+    CUBE_PS(512, 32, 16)
+    CUBE_PS(256, 16, 16)
+    CUBE_PS(128, 16, 8)
+    CUBE_PS(64, 8, 8)
+    CUBE_PS(32, 8, 4)
+#undef CUBE_PS
     default: return 0;
   }
 }

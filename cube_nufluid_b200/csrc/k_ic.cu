@@ -268,9 +268,11 @@ __global__ void k_ic_counts(const int64_t* __restrict__ start, int32_t* __restri
 struct IcScratch {
   float* kern = nullptr;
   float2* tw = nullptr;
+  float2* tw2 = nullptr;
   ~IcScratch() {
     if (kern) cudaFree(kern);
     if (tw) cudaFree(tw);
+    if (tw2) cudaFree(tw2);
   }
 };
 
@@ -295,11 +297,13 @@ int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io)
   M.plane = (size_t)npd * M.rp;
   M.rho = ctx->fine.rho;
   M.force = ctx->fine.force;
+  M.ext = ctx->fine.ext;
   M.kern_octant = 1;
   M.kern_pitch = npd / 2 + 1;
   IcScratch tmp;
   int rc = cube_fft_plan(ctx, M.plan, npd);
   tmp.tw = M.plan.tw;
+  tmp.tw2 = M.plan.tw2;
   if (rc) return rc;
   const size_t ksz = (size_t)M.kern_pitch * M.kern_pitch * M.kern_pitch;
   CUBE_CUDA_TRY(ctx, cudaMalloc((void**)&tmp.kern, sizeof(float) * 3 * ksz));

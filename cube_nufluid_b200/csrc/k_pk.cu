@@ -128,7 +128,7 @@ __global__ void k_pk_delta_nu(Rho3 F, int ng, float* __restrict__ out, int rp) {
 constexpr int NQ = 7;
 
 __global__ void __launch_bounds__(256) k_pk_bin(const float2* __restrict__ c1, const float2* __restrict__ c2, int has2,
-                                               int ng, int cp, int nbin, int logbins, float norm,
+                                               int ng, int cp, int kx_major, int nbin, int logbins, float norm,
                                                double* __restrict__ gbins) {
   extern __shared__ double sb[];  // NQ * (nbin + 1)
   for (int i = threadIdx.x; i < NQ * (nbin + 1); i += blockDim.x) sb[i] = 0.0;
@@ -159,7 +159,8 @@ __global__ void __launch_bounds__(256) k_pk_bin(const float2* __restrict__ c1, c
       ib = (int)roundf(kr);  // Fortran nint: halves away from zero
     }
     if (ib < 0 || ib > nbin) continue;
-    const size_t o = (size_t)k * ng * cp + (size_t)j * cp + i;
+    // spectrum layout: [kz][ky][kx] at row pitch cp, or [kx][ky][kz] dense (kx_major)
+    const size_t o = kx_major ? ((size_t)i * ng + j) * ng + k : (size_t)k * ng * cp + (size_t)j * cp + i;
     const float2 a = c1[o];
     const float ax = a.x * norm, ay = a.y * norm;
     // real(c*conjg(c))/(sinc**4.0)*4*pi*kr**3, left to right
@@ -232,9 +233,10 @@ int cube_power_spectrum_dev(cube_ctx* ctx, int logbins, std::vector<double>& bin
     k_pk_delta_nu<<<g, 256, 0, ctx->stream>>>(R, ng, dnu, L.rp);
     CUBE_LAUNCH_CHECK(ctx);
   }
-  int rc = cube_fft_forward3(ctx, L, L.rho);
+  int kxm = 0, kxm2 = 0;
+  int rc = cube_fft_forward3(ctx, L, L.rho, &kxm);
   if (rc) return rc;
-  if (has2 && (rc = cube_fft_forward3(ctx, L, dnu))) return rc;
+  if (has2 && (rc = cube_fft_forward3(ctx, L, dnu, &kxm2))) return rc;
   double* gb = ctx->pk_bins;  // NQ * (nbin_max + 1), allocated by cube_create
   const size_t nb = (size_t)NQ * (nbin + 1);
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(gb, 0, 8 * nb, ctx->stream));
@@ -242,7 +244,7 @@ int cube_power_spectrum_dev(cube_ctx* ctx, int logbins, std::vector<double>& bin
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_pk_bin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const float norm = (float)(1.0 / ((double)ng * ng * ng));
   k_pk_bin<<<ctx->num_sms * 2, 256, smem, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
-                                                        reinterpret_cast<const float2*>(dnu), has2, ng, L.cp, nbin,
+                                                        reinterpret_cast<const float2*>(dnu), has2, ng, L.cp, kxm, nbin,
                                                         logbins, norm, gb);
   CUBE_LAUNCH_CHECK(ctx);
   bins.assign(nb, 0.0);
