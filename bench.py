@@ -161,10 +161,10 @@ def nu_params_for(cfg):
 #       --clock-control none -c 400 --csv python bench.py --config <c> --steps 1 --warmup 3
 # over the five steps that command runs; the roofline's "traffic" field.
 MEASURED_DRAM_BYTES = {
-    "c2": {"update_x": 21.066e9, "ext_pp_force": 2.529e9, "deposit": 5.921e9, "fine_fft_green": 90.324e9,
-           "coarse_fft_green": 1.199e9, "kick": 15.925e9},
-    "c3": {"update_x": 21.271e9, "ext_pp_force": 2.534e9, "deposit": 28.351e9, "fine_fft_green": 90.322e9,
-           "coarse_fft_green": 1.199e9, "kick": 16.283e9, "nu_fluid": 80.798e9},
+    "c2": {"update_x": 21.063e9, "ext_pp_force": 2.530e9, "deposit": 5.916e9, "fine_fft_green": 87.852e9,
+           "coarse_fft_green": 1.055e9, "kick": 15.925e9},
+    "c3": {"update_x": 21.271e9, "ext_pp_force": 2.534e9, "deposit": 28.351e9, "fine_fft_green": 87.852e9,
+           "coarse_fft_green": 1.055e9, "kick": 16.283e9, "nu_fluid": 80.798e9},
 }
 
 

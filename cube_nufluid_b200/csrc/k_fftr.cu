@@ -5,19 +5,23 @@
  * one warp): with n = t + T*q and k = k1 + R*k2,
  *   X[k1 + R*k2] = sum_t W_N^{t k1} W_T^{t k2} sum_q x[t + T q] W_R^{q k1}
  * so each thread does one R-point DFT in registers (over q), multiplies by
- * W_N^{t k1}, the group exchanges once through shared memory (swizzled so
- * neither side of the transpose has bank conflicts), and each thread does
+ * W_N^{t k1} (a table laid out [k1][t], so a warp's loads are contiguous), the
+ * group exchanges once through shared memory (padded so neither side of the
+ * transpose has bank conflicts), and each thread does
  * R/T T-point DFTs in registers (over t).  Only __syncwarp is needed inside a
  * transform.  Sizes: 1024 = 32*32, 512 = 32*16, 256 = 16*16, 128 = 16*8,
  * 64 = 8*8, 32 = 8*4; other sizes use the shared-memory Stockham passes of
  * k_fft.cu.
  *
- * Passes (same roles as in k_fft.cu):
- *   x r2c   : RB row pairs per CTA packed as complex rows
- *   column  : TK consecutive kx columns per CTA (y or z direction)
- *   z+Green : forward along z, the spectrum kept in registers, then for
- *             each component d: x i*K_d on the way into the inverse FFT
- *   x c2r   : the three force components of RB row pairs, max f^2 fused
+ * Passes of the Poisson solve (the layouts are listed above k_xr2c_t):
+ *   x r2c    : 8 rows of a z-plane per CTA, packed in pairs as complex rows
+ *   y        : 8 rows per CTA, output transposed so that z is innermost
+ *   z+Green  : forward along z, the spectrum kept in registers, then for each
+ *              component d: x i*K_d into the inverse FFT, output transposed
+ *   y^-1     : per component, output transposed back to x innermost
+ *   x c2r    : the three force components of RB row pairs in place, max f^2
+ * The forward 3-D transform of the power spectrum is x r2c, y and an in-place
+ * pass along z.
  */
 #include "cube_internal.cuh"
 
@@ -57,20 +61,6 @@ __host__ __device__ constexpr int bitrev(int L, int i) {
   }
   return r;
 }
-
-// cp.async (LDGSTS) copies: the loads of a pass are all in flight before the
-// first use, instead of one register round trip per element
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  const int n = valid ? 8 : 0;  // 0 bytes read: the 8 destination bytes are zero-filled
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(n));
-}
-__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
 
 template <int L, int I>
 struct BitRev {
@@ -153,41 +143,6 @@ __device__ __forceinline__ void fft_from_regs(float2* v, float2* s, int es, int 
   __syncwarp();
 }
 
-template <int N, int R, int T, int SIGN, bool ROW>
-__device__ __forceinline__ void fft_seq(float2* s, int es, int t, const float2* __restrict__ tw) {
-  float2 v[R];
-  const int e = ROW ? 1 : es;
-#pragma unroll
-  for (int q = 0; q < R; ++q) v[q] = s[(t + T * q) * e];
-  fft_from_regs<N, R, T, SIGN, ROW>(v, s, es, t, tw);
-}
-
-// ---------------------------------------------------------------------------
-// column pass: TK columns (kx0..kx0+TK-1) of length N, element j at b + j*jstride
-template <int N, int R, int T, int TK, int SIGN>
-__global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_t comp_stride, int ncol,
-                                                long long jstride, long long ostride,
-                                                const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  constexpr int P = TK + 1;
-  const int kx0 = blockIdx.x * TK;
-  const int nk = min(TK, ncol - kx0);
-  float2* b = base + blockIdx.z * comp_stride + (size_t)blockIdx.y * ostride + kx0;
-  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-    const int j = i / TK, c = i - j * TK;
-    cp_async8(&sm[j * P + c], c < nk ? &b[(size_t)j * jstride + c] : b, c < nk);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  const int g = threadIdx.x / T, t = threadIdx.x % T;
-  fft_seq<N, R, T, SIGN, false>(sm + g, P, t, tw);
-  __syncthreads();
-  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-    const int j = i / TK, c = i - j * TK;
-    if (c < nk) b[(size_t)j * jstride + c] = sm[j * P + c];
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Transposed-layout passes.  Every transform runs along contiguous memory: a
 // group of T threads loads its row straight into registers (coalesced), and the
@@ -200,8 +155,10 @@ __global__ void __launch_bounds__(T * TK) k_col(float2* __restrict__ base, size_
 //   S2 [kx][ky][z] after y forward       (in L.rho)
 //   S3 [z][kx][ky] after z+Green+z^-1    (components 0,1,2 in force 1, force 2, L.ext)
 //   S4 [z][y][kx]  after y^-1, pitch cp  (components 0,1,2 in force 0, 1, 2)
-// then x c2r in place gives the real force meshes.  The arithmetic of every
-// transform is that of the column kernels above, so results are bit-identical.
+// then x c2r in place gives the real force meshes.  (Same transforms, bit for bit,
+// as in-place column passes over the [z][y][kx] spectrum, which moved the same
+// bytes at 3 TB/s: their global->shared copies and column-wise shared accesses
+// saturated the L1 data path.)
 
 // group stride in float2 for RT rows per CTA: >= N + R + 8 and == 16/RT (mod 16),
 // so that reading one column across the RT rows (two rows per thread) is free of
@@ -239,13 +196,14 @@ __global__ void __launch_bounds__(4 * T) k_xr2c_t(const float* __restrict__ rho,
   }
 }
 
-// natural-order results of the CTA's 8 rows (group stride CS) -> out + B0 + k*B1 + r,
+// natural-order results of the CTA's RT rows (group stride CS) -> out + B0 + k*B1 + r,
 // two rows per thread (16-byte stores), rows r >= nrows skipped
-template <int N, int T, int CS>
+template <int N, int NT, int RT, int CS>
 __device__ __forceinline__ void store_transposed(const float2* sm, float2* __restrict__ out, size_t B0, size_t B1,
                                                  int nrows) {
-  for (int i = threadIdx.x; i < 4 * N; i += 8 * T) {
-    const int k = i >> 2, r = 2 * (i & 3);
+  constexpr int HP = RT / 2;  // row pairs
+  for (int i = threadIdx.x; i < HP * N; i += NT) {
+    const int k = i / HP, r = 2 * (i % HP);
     const float2 a = sm[r * CS + k], b = sm[(r + 1) * CS + k];
     float2* o = out + B0 + (size_t)k * B1 + r;
     if (r + 1 < nrows) *reinterpret_cast<float4*>(o) = make_float4(a.x, a.y, b.x, b.y);
@@ -284,11 +242,13 @@ __global__ void __launch_bounds__(8 * T) k_row_t(const float2* __restrict__ in, 
   for (int q = 0; q < R; ++q) v[q] = __ldg(&in[row + t + T * q]);
   fft_from_regs<N, R, T, SIGN, true>(v, sm + g * CS, 1, t, tw);
   __syncthreads();
-  store_transposed<N, T, CS>(sm, out, B0, B1, nrows);
+  store_transposed<N, 8 * T, 8, CS>(sm, out, B0, B1, nrows);
 }
 
 // z forward, Green multiply, z inverse on S2 rows (kx, ky), CTA = (kx, 8 ky);
-// the three components go out transposed to S3 in o0, o1, o2
+// the three components go out transposed to S3 in o0, o1, o2.  The forward
+// spectrum stays in registers (255 of them: one CTA per SM; staging the Green rows
+// in shared memory, or keeping the spectrum there to fit more CTAs, measured slower).
 template <int N, int R, int T>
 __global__ void __launch_bounds__(8 * T) k_zgreen_t(const float2* __restrict__ in, float2* __restrict__ o0,
                                                     float2* __restrict__ o1, float2* __restrict__ o2,
@@ -302,6 +262,7 @@ __global__ void __launch_bounds__(8 * T) k_zgreen_t(const float2* __restrict__ i
   const int kx = blockIdx.x / YB, ky0 = (blockIdx.x - kx * YB) * 8;
   const int g = threadIdx.x / T, t = threadIdx.x - g * T;
   const int ky = ky0 + g;
+  const size_t ksz = (size_t)kp * kp * kp;
   const float2* bi = in + ((size_t)kx * N + ky) * N;
   float2 v[R];
 #pragma unroll
@@ -313,7 +274,6 @@ __global__ void __launch_bounds__(8 * T) k_zgreen_t(const float2* __restrict__ i
   for (int q = 0; q < R; ++q) keep[q] = s[t + T * q];
   const int fy = ky <= nh ? ky : N - ky;
   const float sy = ky <= nh ? 1.f : -1.f;
-  const size_t ksz = (size_t)kp * kp * kp;
   const size_t B0 = (size_t)kx * N + ky0, B1 = (size_t)H * N;
 #pragma unroll 1
   for (int d = 0; d < 3; ++d) {
@@ -330,7 +290,7 @@ __global__ void __launch_bounds__(8 * T) k_zgreen_t(const float2* __restrict__ i
     __syncwarp();
     fft_from_regs<N, R, T, 1, true>(v, s, 1, t, tw);
     __syncthreads();
-    store_transposed<N, T, CS>(sm, d == 0 ? o0 : (d == 1 ? o1 : o2), B0, B1, 8);
+    store_transposed<N, 8 * T, 8, CS>(sm, d == 0 ? o0 : (d == 1 ? o1 : o2), B0, B1, 8);
     __syncthreads();
   }
 }
@@ -374,220 +334,57 @@ __global__ void __launch_bounds__(3 * T * RB) k_xc2r3_t(float* __restrict__ data
     const int pr = min(pair0 + q, npairs - 1);
     const float2* A = reinterpret_cast<const float2*>(data + c * comp_stride) + (size_t)(2 * pr) * cp;
     const float2* B = A + cp;
+    // Z[n] = A[n] + i B[n] for n <= N/2 and conj(A[N-n]) + i conj(B[N-n]) above; the
+    // imaginary parts of A, B at n = 0 and N/2 are dropped.  n < N/2 exactly when
+    // k < R/2 (n = N/2 is t = 0, k = R/2), so every load is unconditional.
+    float2 a[R], b[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+      const int n = t + T * k;
+      const int m = (k < R / 2) ? n : N - n;
+      a[k] = __ldg(&A[m]);
+      b[k] = __ldg(&B[m]);
+    }
     float2 v[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
       const int n = t + T * k;
-      if (n == 0 || n == nh) {
-        v[k] = make_float2(A[n].x, B[n].x);
-      } else if (n < nh) {
-        const float2 a = A[n], b = B[n];
-        v[k] = make_float2(a.x - b.y, a.y + b.x);
-      } else {
-        const float2 a = A[N - n], b = B[N - n];
-        v[k] = make_float2(a.x + b.y, b.x - a.y);
-      }
+      if (n == 0 || n == nh) v[k] = make_float2(a[k].x, b[k].x);
+      else if (k < R / 2) v[k] = make_float2(a[k].x - b[k].y, a[k].y + b[k].x);
+      else v[k] = make_float2(a[k].x + b[k].y, b[k].x - a[k].y);
     }
     fft_from_regs<N, R, T, 1, true>(v, sm + g * CS, 1, t, tw);
   }
   __syncthreads();
+  // two nodes per thread: one 16-byte shared load and two 8-byte stores per component
   float f2max = 0.f;
-  for (int i = threadIdx.x; i < RB * N; i += NT) {
-    const int q = i / N, j = i - q * N;
+  for (int i = threadIdx.x; i < RB * (N / 2); i += NT) {
+    const int q = i / (N / 2), j = 2 * (i - q * (N / 2));
     if (pair0 + q >= npairs) continue;
     const size_t ra = (size_t)(2 * (pair0 + q)) * rp;
-    float fa[3], fb[3];
+    float fa[3][2], fb[3][2];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const float2 z = sm[(c * RB + q) * CS + j];
+      const float4 z = *reinterpret_cast<const float4*>(&sm[(c * RB + q) * CS + j]);
       float* base = data + c * comp_stride;
-      base[ra + j] = z.x;
-      base[ra + rp + j] = z.y;
-      fa[c] = z.x;
-      fb[c] = z.y;
+      *reinterpret_cast<float2*>(&base[ra + j]) = make_float2(z.x, z.z);
+      *reinterpret_cast<float2*>(&base[ra + rp + j]) = make_float2(z.y, z.w);
+      fa[c][0] = z.x; fa[c][1] = z.z;
+      fb[c][0] = z.y; fb[c][1] = z.w;
     }
-    const float a2 = __fadd_rn(__fadd_rn(__fmul_rn(fa[0], fa[0]), __fmul_rn(fa[1], fa[1])), __fmul_rn(fa[2], fa[2]));
-    const float b2 = __fadd_rn(__fadd_rn(__fmul_rn(fb[0], fb[0]), __fmul_rn(fb[1], fb[1])), __fmul_rn(fb[2], fb[2]));
-    f2max = fmaxf(f2max, fmaxf(a2, b2));
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+      const float a2 = __fadd_rn(__fadd_rn(__fmul_rn(fa[0][e], fa[0][e]), __fmul_rn(fa[1][e], fa[1][e])),
+                                 __fmul_rn(fa[2][e], fa[2][e]));
+      const float b2 = __fadd_rn(__fadd_rn(__fmul_rn(fb[0][e], fb[0][e]), __fmul_rn(fb[1][e], fb[1][e])),
+                                 __fmul_rn(fb[2][e], fb[2][e]));
+      f2max = fmaxf(f2max, fmaxf(a2, b2));
+    }
   }
   for (int o = 16; o > 0; o >>= 1) f2max = fmaxf(f2max, __shfl_xor_sync(0xffffffffu, f2max, o));
   if ((threadIdx.x & 31) == 0) atomicMax(f2_bits, __float_as_uint(f2max));
 }
 
-// fused z pass with the Green multiply (kernel octant [d][ky][kx][kz], kz fastest)
-template <int N, int R, int T, int TK>
-__global__ void __launch_bounds__(T * TK) k_zgreen(const float2* __restrict__ in, float2* __restrict__ out0,
-                                                   size_t comp_stride, int ncol, long long jstride,
-                                                   long long ostride, const float2* __restrict__ tw,
-                                                   const float* __restrict__ kern, int kp, float ksc) {
-  extern __shared__ float2 sm[];
-  constexpr int P = TK + 1;
-  const int kx0 = blockIdx.x * TK;
-  const int nk = min(TK, ncol - kx0);
-  const int ky = blockIdx.y;
-  const float2* bi = in + (size_t)ky * ostride + kx0;
-  for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-    const int j = i / TK, c = i - j * TK;
-    cp_async8(&sm[j * P + c], c < nk ? &bi[(size_t)j * jstride + c] : bi, c < nk);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  const int g = threadIdx.x / T, t = threadIdx.x % T;
-  float2* s = sm + g;
-  fft_seq<N, R, T, -1, false>(s, P, t, tw);
-  float2 keep[R];
-#pragma unroll
-  for (int q = 0; q < R; ++q) keep[q] = s[(t + T * q) * P];
-  constexpr int nh = N / 2;
-  const int fy = ky <= nh ? ky : N - ky;
-  const float sy = ky <= nh ? 1.f : -1.f;
-  const int kx = min(kx0 + g, ncol - 1);
-  const size_t ksz = (size_t)kp * kp * kp;
-#pragma unroll 1
-  for (int d = 0; d < 3; ++d) {
-    const float* K = kern + d * ksz + ((size_t)fy * kp + kx) * kp;
-    float2 v[R];
-#pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int kz = t + T * q;
-      const int fz = kz <= nh ? kz : N - kz;
-      float kv = __ldg(&K[fz]) * ksc;
-      if (d == 1) kv *= sy;
-      if (d == 2 && kz > nh) kv = -kv;
-      v[q] = make_float2(-keep[q].y * kv, keep[q].x * kv);
-    }
-    __syncwarp();
-    fft_from_regs<N, R, T, 1, false>(v, s, P, t, tw);
-    __syncthreads();
-    float2* bo = out0 + d * comp_stride + (size_t)ky * ostride + kx0;
-    for (int i = threadIdx.x; i < N * TK; i += T * TK) {
-      const int j = i / TK, c = i - j * TK;
-      if (c < nk) bo[(size_t)j * jstride + c] = sm[j * P + c];
-    }
-    __syncthreads();
-  }
-}
-
-// x pass, r2c: RB row pairs per CTA, rows (z*N + y) at data + row*rp
-template <int N, int R, int T, int RB>
-__global__ void __launch_bounds__(T * RB) k_xr2c(float* __restrict__ data, int rp, int npairs,
-                                                 const float2* __restrict__ tw) {
-  extern __shared__ float2 sm[];
-  constexpr int CS = N + R + 8;
-  const int pair0 = blockIdx.x * RB;
-  const int cp = rp / 2;
-  for (int i = threadIdx.x; i < RB * N; i += T * RB) {
-    const int q = i / N, j = i - q * N;
-    const int pr = min(pair0 + q, npairs - 1);
-    const size_t ra = (size_t)(2 * pr) * rp;
-    float* dst = reinterpret_cast<float*>(&sm[q * CS + j]);
-    cp_async4(dst, &data[ra + j]);
-    cp_async4(dst + 1, &data[ra + rp + j]);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  const int g = threadIdx.x / T, t = threadIdx.x % T;
-  fft_seq<N, R, T, -1, true>(sm + g * CS, 1, t, tw);
-  __syncthreads();
-  float2* cb = reinterpret_cast<float2*>(data);
-  constexpr int nh = N / 2;
-  for (int i = threadIdx.x; i < RB * (nh + 1); i += T * RB) {
-    const int q = i / (nh + 1), k = i - q * (nh + 1);
-    if (pair0 + q >= npairs) continue;
-    const float2 Zk = sm[q * CS + k];
-    const float2 Zm = sm[q * CS + ((N - k) & (N - 1))];
-    const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
-    const float2 B = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
-    const size_t ra = (size_t)(2 * (pair0 + q)) * cp;
-    cb[ra + k] = A;
-    cb[ra + cp + k] = B;
-  }
-}
-
-// x pass, c2r of the three force components, max f^2 fused; group g handles
-// component g / RB and row pair g % RB, so the three transforms run side by side
-template <int N, int R, int T, int RB>
-__global__ void __launch_bounds__(3 * T * RB) k_xc2r3(float* __restrict__ data, size_t comp_stride, int rp,
-                                                      int npairs, const float2* __restrict__ tw,
-                                                      unsigned int* __restrict__ f2_bits) {
-  extern __shared__ float2 sm[];
-  constexpr int CS = N + R + 8;
-  constexpr int NT = 3 * T * RB;
-  const int pair0 = blockIdx.x * RB;
-  const int cp = rp / 2;
-  constexpr int nh = N / 2;
-  const int g = threadIdx.x / T, t = threadIdx.x % T;
-  // cp.async the half rows into the sequence slots: A[k] -> slot k, B[k] -> slot
-  // N-k (1 <= k < nh), A[0], A[nh] -> slots 0, nh; B[0], B[nh] -> spare slots
-  // N, N+1; then unfold in place (Z[k] = A + iB, Z[N-k] = conj(A) + i conj(B))
-  for (int i = threadIdx.x; i < 3 * RB * (N + 2); i += NT) {
-    const int cq = i / (N + 2), r = i - cq * (N + 2);
-    const int c = cq / RB, q = cq - c * RB;
-    const float2* cb = reinterpret_cast<const float2*>(data + c * comp_stride);
-    const int pr = min(pair0 + q, npairs - 1);
-    const size_t ra = (size_t)(2 * pr) * cp;
-    const bool isA = r <= nh;
-    const int k = isA ? r : r - nh - 1;
-    const int slot = isA ? k : (k == 0 ? N : (k == nh ? N + 1 : N - k));
-    cp_async8(&sm[cq * CS + slot], &cb[ra + (isA ? 0 : cp) + k], true);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  for (int i = threadIdx.x; i < 3 * RB * (nh + 1); i += NT) {
-    const int cq = i / (nh + 1), k = i - cq * (nh + 1);
-    float2* z = sm + cq * CS;
-    if (k == 0 || k == nh) {
-      const float2 A = z[k], B = z[k == 0 ? N : N + 1];
-      z[k] = make_float2(A.x, B.x);
-    } else {
-      const float2 A = z[k], B = z[N - k];
-      z[k] = make_float2(A.x - B.y, A.y + B.x);
-      z[N - k] = make_float2(A.x + B.y, B.x - A.y);
-    }
-  }
-  __syncthreads();
-  fft_seq<N, R, T, 1, true>(sm + g * CS, 1, t, tw);
-  __syncthreads();
-  float f2max = 0.f;
-  for (int i = threadIdx.x; i < RB * N; i += NT) {
-    const int q = i / N, j = i - q * N;
-    if (pair0 + q >= npairs) continue;
-    const size_t ra = (size_t)(2 * (pair0 + q)) * rp;
-    float fa[3], fb[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float2 z = sm[(c * RB + q) * CS + j];
-      float* base = data + c * comp_stride;
-      base[ra + j] = z.x;
-      base[ra + rp + j] = z.y;
-      fa[c] = z.x;
-      fb[c] = z.y;
-    }
-    const float a2 = __fadd_rn(__fadd_rn(__fmul_rn(fa[0], fa[0]), __fmul_rn(fa[1], fa[1])), __fmul_rn(fa[2], fa[2]));
-    const float b2 = __fadd_rn(__fadd_rn(__fmul_rn(fb[0], fb[0]), __fmul_rn(fb[1], fb[1])), __fmul_rn(fb[2], fb[2]));
-    f2max = fmaxf(f2max, fmaxf(a2, b2));
-  }
-  for (int o = 16; o > 0; o >>= 1) f2max = fmaxf(f2max, __shfl_xor_sync(0xffffffffu, f2max, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(f2_bits, __float_as_uint(f2max));
-}
-
-// k_col, one CTA per tile (the in-place column passes, params.reserved[5] = 1)
-template <int N, int R, int T, int TK, int SIGN>
-int col_pass_1(cube_ctx* ctx, float2* base, size_t cstride, int ncol, int nplanes, int ncomp, long long jstride,
-               long long ostride, const float2* tw) {
-  const size_t smem = sizeof(float2) * (size_t)N * (TK + 1);
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_col<N, R, T, TK, SIGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const dim3 g((ncol + TK - 1) / TK, nplanes, ncomp);
-  k_col<N, R, T, TK, SIGN><<<g, T * TK, smem, ctx->stream>>>(base, cstride, ncol, jstride, ostride, tw);
-  CUBE_LAUNCH_CHECK(ctx);
-  return CUBE_OK;
-}
-
-template <int N, int R, int T, int TK, int SIGN>
-int col_pass(cube_ctx* ctx, float2* base, size_t cstride, int ncol, int nplanes, int ncomp, long long jstride,
-             long long ostride, const float2* tw) {
-  return col_pass_1<N, R, T, TK, SIGN>(ctx, base, cstride, ncol, nplanes, ncomp, jstride, ostride, tw);
-}
 
 template <int N, int R, int T>
 int run_poisson_t(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks) {
@@ -602,7 +399,7 @@ int run_poisson_t(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale 
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3_t<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
   float2* ext = reinterpret_cast<float2*>(L.ext);
   float2* rho = reinterpret_cast<float2*>(L.rho);
@@ -613,6 +410,7 @@ int run_poisson_t(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale 
   k_row_t<N, R, T, -1, 0><<<H * (N / 8), 8 * T, sm8, ctx->stream>>>(ext, rho, L.cp, tw);
   CUBE_LAUNCH_CHECK(ctx);
   // z forward, Green, z inverse: S2 -> S3 of components 0, 1, 2 in force 1, force 2, ext
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
   k_zgreen_t<N, R, T><<<H * (N / 8), 8 * T, sm8, ctx->stream>>>(
       rho, reinterpret_cast<float2*>(F[1]), reinterpret_cast<float2*>(F[2]), ext, tw, L.kern, L.kern_pitch,
       cube_kick_scalar(ks));
@@ -655,74 +453,13 @@ int run_forward3_t(cube_ctx* ctx, MeshLevel& L, float* data) {
   return CUBE_OK;
 }
 
-template <int N, int R, int T>
-int run_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks) {
-  constexpr int TK = (T >= 16) ? 8 : 16;
-  constexpr int RB = (T >= 32) ? 4 : (T >= 16 ? 8 : 16);
-  constexpr int RB3 = (T >= 32) ? 2 : (T >= 16 ? 4 : 8);
-  const int ncol = N / 2 + 1;
-  const long long cp = L.cp;
-  const size_t cstride = (size_t)N * L.plane / 2;
-  const float2* tw = L.plan.tw2;
-  const size_t xsm = sizeof(float2) * RB * (N + R + 8);
-  const size_t x3sm = sizeof(float2) * 3 * RB3 * (N + R + 8);
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)x3sm));
-  const size_t csm = sizeof(float2) * (size_t)N * (TK + 1);
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen<N, R, T, TK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
-  float2* spec = reinterpret_cast<float2*>(L.rho);
-  const long long pstride = (long long)N * cp;  // float2 per plane
-  const int npairs = N * N / 2;
-  int rc;
-  // x r2c (two real rows per complex transform), then y forward
-  k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, xsm, ctx->stream>>>(L.rho, L.rp, npairs, tw);
-  CUBE_LAUNCH_CHECK(ctx);
-  if ((rc = col_pass<N, R, T, TK, -1>(ctx, spec, cstride, ncol, N, 1, cp, pstride, tw))) return rc;
-  // z forward, Green, z inverse
-  const dim3 g1((ncol + TK - 1) / TK, N, 1);
-  k_zgreen<N, R, T, TK><<<g1, T * TK, csm, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
-                                                            reinterpret_cast<float2*>(L.force), cstride, ncol,
-                                                            pstride, cp, tw, L.kern, L.kern_pitch,
-                                                            cube_kick_scalar(ks));
-  CUBE_LAUNCH_CHECK(ctx);
-  // y inverse of the three components, then x c2r with max f^2
-  if ((rc = col_pass<N, R, T, TK, 1>(ctx, reinterpret_cast<float2*>(L.force), cstride, ncol, N, 3, cp, pstride, tw)))
-    return rc;
-  k_xc2r3<N, R, T, RB3><<<(npairs + RB3 - 1) / RB3, 3 * T * RB3, x3sm, ctx->stream>>>(
-      L.force, (size_t)N * L.plane, L.rp, npairs, tw, f2_bits);
-  CUBE_LAUNCH_CHECK(ctx);
-  return CUBE_OK;
-}
-
-// forward 3-D r2c of data in place (x r2c, y, z), unnormalised: the half spectrum
-// c[z][y][kx] at pitch cp
-template <int N, int R, int T>
-int run_forward3(cube_ctx* ctx, MeshLevel& L, float* data) {
-  constexpr int TK = (T >= 16) ? 8 : 16;
-  constexpr int RB = (T >= 32) ? 4 : (T >= 16 ? 8 : 16);
-  const int ncol = N / 2 + 1;
-  const long long cp = L.cp;
-  const float2* tw = L.plan.tw2;
-  const size_t xsm = sizeof(float2) * RB * (N + R + 8);
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c<N, R, T, RB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)xsm));
-  const int npairs = N * N / 2;
-  k_xr2c<N, R, T, RB><<<(npairs + RB - 1) / RB, T * RB, xsm, ctx->stream>>>(data, L.rp, npairs, tw);
-  CUBE_LAUNCH_CHECK(ctx);
-  float2* spec = reinterpret_cast<float2*>(data);
-  const size_t cstride = (size_t)N * L.plane / 2;
-  int rc;
-  if ((rc = col_pass<N, R, T, TK, -1>(ctx, spec, cstride, ncol, N, 1, cp, (long long)N * cp, tw))) return rc;  // y
-  return col_pass<N, R, T, TK, -1>(ctx, spec, cstride, ncol, N, 1, (long long)N * cp, cp, tw);               // z
-}
-
 }  // namespace
 
 int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc, int* kx_major) {
-  const bool cols = ctx->P.reserved[5] == 1;  // the in-place column passes
-  *kx_major = cols ? 0 : 1;
+  *kx_major = 1;
   switch (L.n) {
 #define CUBE_F3(n, r, t) \
-  case n: *rc = cols ? run_forward3<n, r, t>(ctx, L, data) : run_forward3_t<n, r, t>(ctx, L, data); return 1;
+  case n: *rc = run_forward3_t<n, r, t>(ctx, L, data); return 1;
     CUBE_F3(1024, 32, 32)
     CUBE_F3(512, 32, 16)
     CUBE_F3(256, 16, 16)
@@ -736,11 +473,9 @@ int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc, in
 
 // returns 1 if handled by a register-resident path
 int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks, int* rc) {
-  const bool cols = ctx->P.reserved[5] == 1;
   switch (L.n) {
-#define CUBE_PS(n, r, t)                                                                                     \
-  case n: *rc = cols ? run_poisson<n, r, t>(ctx, L, f2_bits, ks) : run_poisson_t<n, r, t>(ctx, L, f2_bits, ks); \
-    return 1;
+#define CUBE_PS(n, r, t) \
+  case n: *rc = run_poisson_t<n, r, t>(ctx, L, f2_bits, ks); return 1;
     CUBE_PS(1024, 32, 32)
     CUBE_PS(512, 32, 16)
     CUBE_PS(256, 16, 16)
