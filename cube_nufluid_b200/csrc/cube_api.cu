@@ -210,6 +210,7 @@ void cube_destroy(cube_ctx* ctx) {
       if (q) cudaFree(q);
   }
   if (ctx->nu.partial) cudaFree(ctx->nu.partial);
+  if (ctx->pp_scratch) cudaFree(ctx->pp_scratch);
   if (ctx->hscal) cudaFreeHost(ctx->hscal);
   for (int i = 0; i < 16; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);

@@ -121,6 +121,8 @@ struct cube_ctx {
   int64_t* scan_tmp;
   NuState nu;
   double* pk_bins;  // power-spectrum bin sums, 7 * (bins of the fine mesh + 1)
+  void* pp_scratch = nullptr;     // sorted particles of crowded PP bricks, grown on demand
+  size_t pp_scratch_bytes = 0;
   // meshes
   MeshLevel fine, coarse;
   unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator
