@@ -211,6 +211,8 @@ void cube_destroy(cube_ctx* ctx) {
   }
   if (ctx->nu.partial) cudaFree(ctx->nu.partial);
   if (ctx->pp_scratch) cudaFree(ctx->pp_scratch);
+  for (double* t : ctx->vdec)
+    if (t) cudaFree(t);
   if (ctx->hscal) cudaFreeHost(ctx->hscal);
   for (int i = 0; i < 16; ++i)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);

@@ -121,6 +121,9 @@ struct cube_ctx {
   int64_t* scan_tmp;
   NuState nu;
   double* pk_bins;  // power-spectrum bin sums, 7 * (bins of the fine mesh + 1)
+  double* vdec[2] = {nullptr, nullptr};  // decoded velocity per code, tan(code)/coef, for two coefs
+  double vdec_coef[2] = {0.0, 0.0};
+  int vdec_next = 0;
   void* pp_scratch = nullptr;     // sorted particles of crowded PP bricks, grown on demand
   size_t pp_scratch_bytes = 0;
   // meshes
@@ -232,6 +235,62 @@ __device__ __forceinline__ float cube_kick_scale(float f, const KickScale& k) {
   return cube_div_const(cube_div_const(t, 6.f, k.inv6), k.pi_f, k.inv_pi);
 }
 
+// Velocity encode nint(nvbin_m1*atan(coef*v)/pi) (cube_vencode) with a cheaper
+// first attempt.  The attempt follows cube_atan step by step but forms its two
+// quotients with a reciprocal from an FP32 seed and two Newton steps (relative
+// error below 2^-49) and multiplies by 1/pi instead of dividing.  Propagated
+// through the reduction and the series (Lipschitz 1) that changes atan by less
+// than 2^-48, hence q = nvbin_m1*atan/pi (|q| < 2^15) by less than 1e-10 including
+// the final roundings.  Unless q lies within 1e-9 of a rounding boundary (k + 1/2),
+// both evaluations give the same integer; otherwise the exact evaluation decides.
+__device__ __forceinline__ double cube_rcp_fast(double b) {
+  double y = (double)__fdividef(1.0f, (float)b);
+  double e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-b, y, 1.0);
+  return fma(y, e, y);
+}
+
+__device__ __forceinline__ int32_t cube_vencode_fast(const cube_codec* c, double v, double coef, double inv_pi) {
+  const double x = cube_dmul(coef, v);
+  const double ax = fabs(x);
+  if (!(ax < 1e30)) return cube_vencode(c, v, coef);  // beyond the FP32 seed's range, or NaN
+  double t = ax;
+  const int recip = ax > 1.0;
+  if (recip) t = cube_rcp_fast(ax);
+  const int shift = t > CUBE_TANPIO12;
+  if (shift) {
+    const double num = cube_dfma(CUBE_SQRT3, t, -1.0);
+    const double den = cube_dadd(t, CUBE_SQRT3);
+    t = cube_dmul(num, cube_rcp_fast(den));
+  }
+  const double t2 = cube_dmul(t, t);
+  double p = -1.0 / 29.0;
+  p = cube_dfma(p, t2, 1.0 / 27.0);
+  p = cube_dfma(p, t2, -1.0 / 25.0);
+  p = cube_dfma(p, t2, 1.0 / 23.0);
+  p = cube_dfma(p, t2, -1.0 / 21.0);
+  p = cube_dfma(p, t2, 1.0 / 19.0);
+  p = cube_dfma(p, t2, -1.0 / 17.0);
+  p = cube_dfma(p, t2, 1.0 / 15.0);
+  p = cube_dfma(p, t2, -1.0 / 13.0);
+  p = cube_dfma(p, t2, 1.0 / 11.0);
+  p = cube_dfma(p, t2, -1.0 / 9.0);
+  p = cube_dfma(p, t2, 1.0 / 7.0);
+  p = cube_dfma(p, t2, -1.0 / 5.0);
+  p = cube_dfma(p, t2, 1.0 / 3.0);
+  p = cube_dmul(p, t2);
+  const double sr = cube_dfma(-t, p, t);
+  const double r = shift ? cube_dadd(CUBE_PIO6_HI, cube_dadd(sr, CUBE_PIO6_LO)) : sr;
+  const double res = recip ? cube_dadd(cube_dsub(CUBE_PIO2_HI, r), CUBE_PIO2_LO) : r;
+  const double q = cube_dmul(cube_dmul((double)c->nvbin_m1_f, res), inv_pi);  // |q|, atan >= 0 here
+  const double fl = floor(q);
+  const double fr = q - fl;  // exact
+  if (fabs(fr - 0.5) < 1e-9) return cube_vencode(c, v, coef);
+  const int32_t n = (int32_t)fl + (fr > 0.5 ? 1 : 0);
+  return x < 0.0 ? -n : n;
+}
+
 // ---- launchers (implemented in the k_*.cu files) -----------------------------
 int cube_rebin(cube_ctx* ctx, cube_scalars* io);
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);
@@ -256,5 +315,8 @@ int cube_nu_density(cube_ctx* ctx, cube_scalars* io);
 int cube_nu_gravity(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int ncomp, unsigned int* f2_bits);
 int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io);
+// device table of cube_vdecode(tan_table[c], coef) for every code c (index code + nvbin/2),
+// built on first use of a coefficient; the last two coefficients stay cached
+const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc);
 
 #endif

@@ -5,8 +5,8 @@
  * Per particle and component the arithmetic is the reference's, in its
  * order: decode with sigma_vi, add the eight fine CIC terms
  * force*a_mid*dt/6/pi*dx*dy*dz (FP32 products, FP64 accumulation; the first four
- * factors are the same for every particle reading a node, so the c2r pass of the
- * FFT has applied them to the mesh already), encode
+ * factors are the same for every particle reading a node, so the Green multiply of
+ * the Poisson solve has applied them to the mesh already), encode
  * with sigma_vi_new; decode that code again with sigma_vi_new, add the
  * eight coarse terms, record |v+vfield| for vmax, encode.  The intermediate
  * quantisation between the two kicks is kept, so the result is bit-identical
@@ -23,20 +23,24 @@ namespace {
 
 constexpr int KCELLS = 64;  // cells per CTA
 
-// One thread per (particle, component): the three components of a particle are
-// independent chains (decode, eight fine terms, encode, decode, eight coarse
-// terms, encode), so splitting them triples the threads in flight and keeps
-// each thread's 16 force gathers independent of its FP64 work.  Warps are
-// uniform in the component (d = i / n inside the CTA), so code and force
-// reads of a warp go to one array.
+// One thread per particle: the node indices and CIC weights of a particle are
+// shared by its three components, which then run their chains (decode, eight
+// fine terms, encode, decode, eight coarse terms, encode) one after the other.
+// The position arithmetic is FP32: the reference forms the position in FP64
+// from exact terms (integer cell, code fraction) and rounds it to FP32 once,
+// and the same single rounding of the same exact sum is what the FP32 add gives.
+// Decodes read the per-step tables of tan(code)/coef (bit-identical to the
+// per-particle FP64 division).  (Staging each 4^3-cell brick's force nodes in
+// shared memory first was measured twice as slow: at ~500 particles per brick
+// the copies of 17^3 x 3 nodes outweigh the gathers they replace, which hit L1/L2.)
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                               const int64_t* __restrict__ cell_start, const float* __restrict__ vfield,
                                               int64_t cap, int64_t ncells, int nc, int nt, int nnt,
                                               const float* __restrict__ ff, size_t fcomp, int frp, size_t fplane,
                                               const float* __restrict__ fc, size_t ccomp, int crp, size_t cplane,
-                                              const float* __restrict__ tan_table, int half_nvbin, cube_codec codec,
-                                              double coef_old, double coef_new, float a_mid, float dt,
+                                              const double* __restrict__ dec_old, const double* __restrict__ dec_new,
+                                              int half_nvbin, cube_codec codec, double coef_new, double inv_pi,
                                               DevScal* __restrict__ dscal) {
   typedef typename CodeT<ZX>::T TX;
   typedef typename CodeT<ZV>::T TV;
@@ -54,36 +58,33 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
   const int nf = 4 * nc;
   const int64_t p0 = cs[0];
   const int npb = (int)(cs[ncl] - p0);
+  const float xres = ZX == 1 ? 0.00390625f : 1.52587890625e-05f;  // 2^-8, 2^-16
   // reference corner order: 111,211,121,112,122,212,221,222
   const int ox[8] = {0, 1, 0, 0, 0, 1, 1, 1}, oy[8] = {0, 0, 1, 0, 1, 0, 1, 1}, oz[8] = {0, 0, 0, 1, 1, 1, 0, 1};
   float vm[3] = {0.f, 0.f, 0.f};  // per-thread |v+vfield| maxima (non-negative)
-  for (int i = threadIdx.x; i < 3 * npb; i += blockDim.x) {
-    const int d = i / npb;
-    const int64_t ip = p0 + (i - d * npb);
+  for (int i = threadIdx.x; i < npb; i += blockDim.x) {
+    const int64_t ip = p0 + i;
     int lo = 0, hi = ncl - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
     }
     const int64_t c = c0 + lo;
-    const int code = (int)vp[(size_t)d * cap + ip];
-    const float tan0 = __ldg(&tan_table[code + half_nvbin]);
-    const float vf = __ldg(&vfield[(size_t)d * ncells + c]);
     int fi[3][2], gi[3][2];
     float dx1[3], dx2[3], cx1[3], cx2[3];
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
       const int l = cl[lo][e], tb = ctb[lo][e];
-      const double fr = cube_xfrac((int32_t)xp[(size_t)e * cap + ip], ZX);
-      const float tf = (float)cube_dadd(4.0 * (double)l, cube_dmul(4.0, fr));
+      const uint32_t u = (uint32_t)(int32_t)xp[(size_t)e * cap + ip] & (ZX == 1 ? 0xFFu : 0xFFFFu);
+      const float fr = __fmul_rn((float)u + 0.5f, xres);                  // exact
+      const float tf = __fadd_rn(4.f * (float)l, __fmul_rn(4.f, fr));   // RN(4l + 4 fr)
       const float f = floorf(tf) + 1.f;
       dx1[e] = cube_fsub(f, tf);
       dx2[e] = cube_fsub(1.f, dx1[e]);
       const int n1 = 4 * tb + (int)f - 1;  // global fine node of idx1 (0-based), <= nf
       fi[e][0] = cube_wrap(n1, nf);
       fi[e][1] = cube_wrap(n1 + 1, nf);
-      const double g = cube_dadd((double)(tb + l), fr);
-      const float tc = (float)cube_dsub(g, 0.5);
+      const float tc = __fadd_rn((float)(tb + l) - 0.5f, fr);            // RN(cell + fr - 1/2)
       const float ci = floorf(tc) + 1.f;
       cx1[e] = cube_fsub(ci, tc);
       cx2[e] = cube_fsub(1.f, cx1[e]);
@@ -91,41 +92,46 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
       gi[e][0] = cube_wrap(m1, nc);
       gi[e][1] = cube_wrap(m1 + 1, nc);
     }
-    const float* F = ff + d * fcomp;
-    const float* G = fc + d * ccomp;
     const size_t fz[2] = {(size_t)fi[2][0] * fplane, (size_t)fi[2][1] * fplane};
     const size_t gz[2] = {(size_t)gi[2][0] * cplane, (size_t)gi[2][1] * cplane};
     const int fy[2] = {fi[1][0] * frp, fi[1][1] * frp}, gy[2] = {gi[1][0] * crp, gi[1][1] * crp};
-    float fv[8], gv[8];
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+      const float* F = ff + d * fcomp;
+      const float* G = fc + d * ccomp;
+      const int code = (int)vp[(size_t)d * cap + ip];
+      float fv[8], gv[8];
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      fv[k] = __ldg(&F[fz[oz[k]] + (size_t)(fy[oy[k]] + fi[0][ox[k]])]);
-      gv[k] = __ldg(&G[gz[oz[k]] + (size_t)(gy[oy[k]] + gi[0][ox[k]])]);
-    }
-    double v = cube_vdecode(tan0, coef_old);
+      for (int k = 0; k < 8; ++k) {
+        fv[k] = __ldg(&F[fz[oz[k]] + (size_t)(fy[oy[k]] + fi[0][ox[k]])]);
+        gv[k] = __ldg(&G[gz[oz[k]] + (size_t)(gy[oy[k]] + gi[0][ox[k]])]);
+      }
+      const float vf = __ldg(&vfield[(size_t)d * ncells + c]);
+      double v = __ldg(&dec_old[code + half_nvbin]);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      float q = fv[k];  // force*a_mid*dt/6/pi of the node, applied by the c2r pass
-      q = cube_fmul(q, ox[k] ? dx2[0] : dx1[0]);
-      q = cube_fmul(q, oy[k] ? dx2[1] : dx1[1]);
-      q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
-      v = cube_dadd(v, (double)q);
-    }
-    const int code1 = cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
-    v = cube_vdecode(__ldg(&tan_table[code1 + half_nvbin]), coef_new);
+      for (int k = 0; k < 8; ++k) {
+        float q = fv[k];  // force*a_mid*dt/6/pi of the node, applied by the Green multiply
+        q = cube_fmul(q, ox[k] ? dx2[0] : dx1[0]);
+        q = cube_fmul(q, oy[k] ? dx2[1] : dx1[1]);
+        q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
+        v = cube_dadd(v, (double)q);
+      }
+      const int code1 = cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
+      v = __ldg(&dec_new[code1 + half_nvbin]);
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      float q = gv[k];
-      q = cube_fmul(q, ox[k] ? cx2[0] : cx1[0]);
-      q = cube_fmul(q, oy[k] ? cx2[1] : cx1[1]);
-      q = cube_fmul(q, oz[k] ? cx2[2] : cx1[2]);
-      v = cube_dadd(v, (double)q);
+      for (int k = 0; k < 8; ++k) {
+        float q = gv[k];
+        q = cube_fmul(q, ox[k] ? cx2[0] : cx1[0]);
+        q = cube_fmul(q, oy[k] ? cx2[1] : cx1[1]);
+        q = cube_fmul(q, oz[k] ? cx2[2] : cx1[2]);
+        v = cube_dadd(v, (double)q);
+      }
+      const float am = (float)fabs(cube_dadd(v, (double)vf));
+      vm[0] = (d == 0) ? fmaxf(vm[0], am) : vm[0];
+      vm[1] = (d == 1) ? fmaxf(vm[1], am) : vm[1];
+      vm[2] = (d == 2) ? fmaxf(vm[2], am) : vm[2];
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
     }
-    const float am = (float)fabs(cube_dadd(v, (double)vf));
-    vm[0] = (d == 0) ? fmaxf(vm[0], am) : vm[0];
-    vm[1] = (d == 1) ? fmaxf(vm[1], am) : vm[1];
-    vm[2] = (d == 2) ? fmaxf(vm[2], am) : vm[2];
-    vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode(&codec, v, coef_new), ZV);
   }
   // every thread reaches here: warp maxima, then one shared atomic per warp and component
 #pragma unroll
@@ -142,12 +148,17 @@ int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
   const int64_t blocks = (ctx->ncells + KCELLS - 1) / KCELLS;
   const double coef_old = cube_vcoef(&ctx->codec, io->sigma_vi);
   const double coef_new = cube_vcoef(&ctx->codec, io->sigma_vi_new);
+  int rc;
+  const double* dec_old = cube_vdec_table(ctx, coef_old, &rc);
+  if (rc) return rc;
+  const double* dec_new = cube_vdec_table(ctx, coef_new, &rc);
+  if (rc) return rc;
   MeshLevel& F = ctx->fine;
   MeshLevel& Cc = ctx->coarse;
   k_kick<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
       ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, F.force,
-      (size_t)F.n * F.plane, F.rp, F.plane, Cc.force, (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, ctx->tan_table,
-      ctx->nvbin / 2, ctx->codec, coef_old, coef_new, io->a_mid, io->dt, ctx->dscal);
+      (size_t)F.n * F.plane, F.rp, F.plane, Cc.force, (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, dec_old, dec_new,
+      ctx->nvbin / 2, ctx->codec, coef_new, 1.0 / (double)ctx->codec.pi_f, ctx->dscal);
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }

@@ -85,8 +85,8 @@ __device__ __forceinline__ void pp_pair(const double x21[3], double mass, double
 
 struct PPArgs {
   int pr, nf_cutoff;
-  double rsoft, mass, a_mid, dt, pi_d, coef;
-  const float* tan_table;
+  double rsoft, mass, a_mid, dt, pi_d, coef, inv_pi;
+  const double* dec;  // tan(code)/coef per code (cube_vdec_table)
   int half_nvbin;
   cube_codec codec;
   int64_t cap;
@@ -132,7 +132,7 @@ __device__ __forceinline__ void pp_target(const Sorted<OffT>& S, const Chains& H
     x1[d] = cube_dadd(4.0 * (double)cc[d], cube_dmul(4.0, fr));
     g1[d] = 4 * cc[d] + (int)floor(cube_dmul(4.0, fr));
     const int vc = (int)vp[(size_t)d * A.cap + ip];
-    v[d] = cube_vdecode(__ldg(&A.tan_table[vc + A.half_nvbin]), A.coef);
+    v[d] = __ldg(&A.dec[vc + A.half_nvbin]);
   }
   ++acc.n1;
   const bool pow2_cut = (A.nf_cutoff & (A.nf_cutoff - 1)) == 0;
@@ -195,7 +195,7 @@ __device__ __forceinline__ void pp_target(const Sorted<OffT>& S, const Chains& H
     k = cube_ddiv(k, 6.0);
     k = cube_ddiv(k, A.pi_d);
     v[d] = cube_dadd(v[d], k);
-    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode(&A.codec, v[d], A.coef), ZV);
+    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&A.codec, v[d], A.coef, A.inv_pi), ZV);
   }
   const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
   acc.f2max = fmaxf(acc.f2max, (float)f2);
@@ -566,8 +566,11 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   A.a_mid = (double)io->a_mid;
   A.dt = (double)io->dt;
   A.pi_d = (double)ctx->codec.pi_f;
+  A.inv_pi = 1.0 / A.pi_d;
   A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
-  A.tan_table = ctx->tan_table;
+  int rc;
+  A.dec = cube_vdec_table(ctx, A.coef, &rc);
+  if (rc) return rc;
   A.half_nvbin = ctx->nvbin / 2;
   A.codec = ctx->codec;
   A.cap = ctx->cap;

@@ -42,8 +42,8 @@ struct RebinArgs {
   int32_t* cnt2; int64_t* start2; float* vfield2;
   int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
   int32_t* big_list; double* stats; double* slot_r2; double* slot_s2;
-  const float* tan_table; int half_nvbin;
-  cube_codec codec; double coef;
+  const double* dec; int half_nvbin;  // tan(code)/coef per code (cube_vdec_table)
+  cube_codec codec; double coef, inv_pi;
   int64_t cap, ncells;
   int nc, nt, nnt, ncb, nte, ncell, nlayer, use_pid;
   float dt_mid;
@@ -57,7 +57,7 @@ __device__ __forceinline__ double decode_v(const RebinArgs& A, int64_t ip, int d
   typedef typename CodeT<ZV>::T TV;
   const TV* vp = reinterpret_cast<const TV*>(A.vp);
   const int code = (int)vp[(size_t)d * A.cap + ip];
-  return cube_vdecode(__ldg(&A.tan_table[code + A.half_nvbin]), A.coef);
+  return __ldg(&A.dec[code + A.half_nvbin]);
 }
 
 template <int ZX, int ZV>
@@ -157,9 +157,9 @@ __device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t i
   for (int d = 0; d < 3; ++d) {
     const int64_t mv = cube_nint(cube_ddiv(cube_dmul((double)A.dt_mid, v[d]), xstep));
     xp2[(size_t)d * A.cap + slot] = (TX)cube_wrap_code((int64_t)xp[(size_t)d * A.cap + ip] + (int32_t)mv, ZX);
-    const int code = cube_wrap_code(cube_vencode(&A.codec, cube_dsub(v[d], (double)vfn[d]), A.coef), ZV);
+    const int code = cube_wrap_code(cube_vencode_fast(&A.codec, cube_dsub(v[d], (double)vfn[d]), A.coef, A.inv_pi), ZV);
     vp2[(size_t)d * A.cap + slot] = (TV)code;
-    const double vr = cube_vdecode(__ldg(&A.tan_table[code + A.half_nvbin]), A.coef);
+    const double vr = __ldg(&A.dec[code + A.half_nvbin]);
     const double vs = cube_dadd(vr, (double)vfn[d]);
     r2 = cube_dadd(r2, cube_dmul(vr, vr));
     s2 = cube_dadd(s2, cube_dmul(vs, vs));
@@ -364,8 +364,14 @@ int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
   A.tcell = ctx->tcell; A.tkey = ctx->tkey; A.perm = ctx->perm; A.pkey = ctx->pkey; A.cursor = ctx->cursor;
   A.big_list = ctx->big_list; A.stats = ctx->cell_stats;
   A.slot_r2 = ctx->slot_r2; A.slot_s2 = ctx->slot_s2;
-  A.tan_table = ctx->tan_table; A.half_nvbin = ctx->nvbin / 2;
+  A.half_nvbin = ctx->nvbin / 2;
   A.codec = ctx->codec; A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
+  A.inv_pi = 1.0 / (double)ctx->codec.pi_f;
+  {
+    int trc;
+    A.dec = cube_vdec_table(ctx, A.coef, &trc);
+    if (trc) return trc;
+  }
   A.cap = ctx->cap; A.ncells = ctx->ncells;
   A.nc = ctx->nc; A.nt = ctx->nt; A.nnt = ctx->nnt; A.ncb = ctx->ncb; A.nte = ctx->nte; A.ncell = ctx->ncell;
   A.nlayer = nlayer; A.use_pid = ctx->P.use_pid; A.dt_mid = io->dt_mid; A.dscal = ctx->dscal;

@@ -163,3 +163,74 @@ int cube_exclusive_scan(cube_ctx* ctx, const int32_t* in, int64_t n, int64_t* ou
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }
+
+namespace {
+__global__ void k_vdec_build(const float* __restrict__ tan_table, double coef, double* __restrict__ out, int nvbin) {
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nvbin; c += gridDim.x * blockDim.x)
+    out[c] = cube_vdecode(tan_table[c], coef);
+}
+}  // namespace
+
+// decode table for coef: the velocity decode tan(pi*code/(nvbin-1))/coef of every
+// code, computed by the same FP32 table and FP64 division as a per-particle decode,
+// so a lookup is bit-identical to it
+const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc) {
+  *rc = CUBE_OK;
+  for (int i = 0; i < 2; ++i)
+    if (ctx->vdec[i] && ctx->vdec_coef[i] == coef) return ctx->vdec[i];
+  const int i = ctx->vdec_next;
+  ctx->vdec_next ^= 1;
+  if (!ctx->vdec[i] && cudaMalloc((void**)&ctx->vdec[i], sizeof(double) * ctx->nvbin) != cudaSuccess) {
+    ctx->err = "cudaMalloc of the velocity decode table failed";
+    *rc = CUBE_ERR_CUDA;
+    return nullptr;
+  }
+  k_vdec_build<<<(ctx->nvbin + 255) / 256, 256, 0, ctx->stream>>>(ctx->tan_table, coef, ctx->vdec[i], ctx->nvbin);
+  ctx->launches++;
+  if (cudaGetLastError() != cudaSuccess) {
+    ctx->err = "velocity decode table launch failed";
+    *rc = CUBE_ERR_CUDA;
+    return nullptr;
+  }
+  ctx->vdec_coef[i] = coef;
+  return ctx->vdec[i];
+}
+
+namespace {
+// velocities spread over the code range: v = tan(pi*(code + off)/(nvbin-1))/coef with
+// off in (-1, 1) drawn from a hash of the index, so that many land near the
+// rounding boundaries code +- 1/2
+__global__ void k_encode_check(cube_codec codec, double coef, double inv_pi, int64_t n, uint64_t seed,
+                               unsigned long long* __restrict__ bad) {
+  unsigned long long nb = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t h = (uint64_t)i * 0x9E3779B97F4A7C15ull + seed;
+    h ^= h >> 31; h *= 0xBF58476D1CE4E5B9ull; h ^= h >> 27; h *= 0x94D049BB133111EBull; h ^= h >> 31;
+    const double u = (double)(h >> 11) * 0x1p-53;                        // [0,1)
+    const double half = 0.5 * (double)codec.nvbin_m1_f;
+    const double code = floor(u * (double)codec.nvbin_m1_f) - half;       // whole code range
+    const double off = ((h & 7) < 4) ? ((double)((h >> 3) & 0xFF) - 128.0) * 1e-10 + 0.5  // near x.5
+                                     : ((double)((h >> 3) & 0xFFFF) / 65536.0 - 0.5);      // anywhere
+    const double ang = 3.141592653589793 * (code + off) / (double)codec.nvbin_m1_f;
+    if (fabs(ang) >= 1.5707963) continue;
+    const double v = tan(ang) / coef;
+    nb += cube_vencode_fast(&codec, v, coef, inv_pi) != cube_vencode(&codec, v, coef);
+  }
+  if (nb) atomicAdd(bad, nb);
+}
+}  // namespace
+
+int32_t cube_debug_encode_check(cube_ctx* ctx, int64_t n, uint64_t seed, float sigma, int64_t* mismatches) {
+  if (!ctx || !mismatches || n < 0) return CUBE_ERR_PARAM;
+  unsigned long long* bad = reinterpret_cast<unsigned long long*>(ctx->red_tmp);
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, 8, ctx->stream));
+  const double coef = cube_vcoef(&ctx->codec, sigma);
+  k_encode_check<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->codec, coef, 1.0 / (double)ctx->codec.pi_f, n,
+                                                            seed, bad);
+  CUBE_LAUNCH_CHECK(ctx);
+  unsigned long long h = 0;
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&h, bad, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *mismatches = (int64_t)h;
+  return CUBE_OK;
+}

@@ -70,6 +70,8 @@ def load_library():
         getattr(L, name).restype = C.c_int32
     L.cube_nu_info.argtypes = [vp, vp]
     L.cube_nu_info.restype = C.c_int32
+    L.cube_debug_encode_check.argtypes = [vp, C.c_int64, C.c_uint64, C.c_float, C.POINTER(C.c_int64)]
+    L.cube_debug_encode_check.restype = C.c_int32
     L.cube_make_ic.argtypes = [vp, C.POINTER(CubeIcParams), S]
     L.cube_make_ic.restype = C.c_int32
     L.cube_power_spectrum.argtypes = [vp, C.c_int32, vp, C.c_int32, C.POINTER(C.c_int32)]
@@ -200,6 +202,12 @@ class Cube:
         if self.p.neutrino:
             s.dt_neu = self.nu_evolve(s.dt / 2.0, s.dt_neu, -1, s.a_mid)
         return hit
+
+    def debug_encode_check(self, n: int, seed: int, sigma: float) -> int:
+        """Disagreements between the fast and the exact velocity encode over n velocities."""
+        bad = C.c_int64(0)
+        self._check(self.L.cube_debug_encode_check(self.h, int(n), int(seed), float(sigma), C.byref(bad)))
+        return bad.value
 
     def make_ic(self, ic: dict, seed: int, *, f_cdm: float = 1.0) -> CubeScalars:
         """Zel'dovich state made on the device (cube_make_ic) from the scalars of

@@ -266,6 +266,12 @@ int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io);
 int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float* fine_force,
                                    const float* coarse_force);
 
+/* Compares, for n velocities spread over every code and concentrated at the
+ * rounding boundaries, the step's fast velocity encode (reciprocal-based, with an
+ * exact fallback near ties) with the exact FP64 encode under sigma; *mismatches
+ * counts the disagreements (0 expected). */
+int32_t cube_debug_encode_check(cube_ctx* ctx, int64_t n, uint64_t seed, float sigma, int64_t* mismatches);
+
 /* Device time of the fine-mesh Poisson solve (FFT passes + Green multiply) on
  * whatever the fine density array holds, averaged over reps runs, in *ms. */
 int32_t cube_debug_time_poisson(cube_ctx* ctx, int32_t reps, float* ms);

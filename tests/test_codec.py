@@ -117,3 +117,16 @@ def test_constant_division_is_exact():
         worst = C.c_float(0.0)
         L.orc_check_const_div(y, C.byref(worst))
         assert worst.value < 2.0 ** -100, (y, worst.value)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("izipv", [2, 1])
+def test_gpu_fast_encode_matches_exact(tables, izipv):
+    # the reciprocal-based encode used by the kick, PP and re-bin falls back to the
+    # exact FP64 encode within 1e-9 of a rounding boundary; it must never disagree
+    from cube_nufluid_b200 import Cube
+    from cube_nufluid_b200.abi import make_params
+    fk, ck = tables
+    g = Cube(make_params(16, 2, izipv=izipv), np_capacity=1024, fk_table=fk, ck_table=ck)
+    for sigma in (0.00287, 0.05, 1.7):
+        assert g.debug_encode_check(1 << 26, 12345, sigma) == 0
