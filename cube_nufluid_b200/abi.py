@@ -3,6 +3,8 @@ from __future__ import annotations
 
 import ctypes as C
 
+import numpy as np
+
 ABI_VERSION = 1
 
 
@@ -64,6 +66,37 @@ class CubeIcParams(C.Structure):
         ("eh_s", C.c_double), ("eh_alpha", C.c_double), ("eh_omh", C.c_double), ("eh_theta2", C.c_double),
         ("vf", C.c_double), ("amplitude", C.c_double), ("f_cdm", C.c_double),
     ]
+
+
+class CubeHalo(C.Structure):
+    """cube_halo of include/cube_gpu.h: type_halo_info (halofind.f90:10-15), 42 floats."""
+    _fields_ = [
+        ("hpos", C.c_float * 3), ("mass_odc", C.c_float), ("radius_odc", C.c_float), ("v_disp", C.c_float),
+        ("x_mean", C.c_float * 3), ("v_mean", C.c_float * 3), ("ang_mom", C.c_float * 3), ("var_x", C.c_float * 3),
+        ("inertia", C.c_float * 9), ("q_mean", C.c_float * 3), ("inertia_q", C.c_float * 9), ("s_mean", C.c_float * 3),
+    ]
+
+
+class CubeHaloArgs(C.Structure):
+    """cube_halo_args of include/cube_gpu.h."""
+    _fields_ = [
+        ("den_odc", C.c_float), ("capacity", C.c_int32), ("halos", C.c_void_p),
+        ("member_pid", C.c_void_p), ("member_capacity", C.c_int64),
+        ("hid", C.c_void_p), ("hid_len", C.c_int64),
+    ]
+
+
+class CubeHaloResult(C.Structure):
+    """cube_halo_result of include/cube_gpu.h."""
+    _fields_ = [("nhalo", C.c_int32), ("npeak", C.c_int32), ("nmember", C.c_int64)]
+
+
+# numpy view of one cube_halo record
+HALO_DTYPE = np.dtype([
+    ("hpos", "<f4", 3), ("mass_odc", "<f4"), ("radius_odc", "<f4"), ("v_disp", "<f4"),
+    ("x_mean", "<f4", 3), ("v_mean", "<f4", 3), ("ang_mom", "<f4", 3), ("var_x", "<f4", 3),
+    ("inertia", "<f4", 9), ("q_mean", "<f4", 3), ("inertia_q", "<f4", 9), ("s_mean", "<f4", 3),
+])
 
 
 def make_params(nc: int, nnt: int, *, ncell: int = 4, ncb: int = 6, np_nc: int = 2, izipx: int = 2,

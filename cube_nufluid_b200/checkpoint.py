@@ -27,7 +27,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .abi import CubeScalars
+from .abi import HALO_DTYPE, CubeScalars
 
 # sim_header (parameters.f90:129-153): 17 integer(8) then 22 real(4), no padding
 SIM_HEADER = np.dtype([
@@ -202,3 +202,67 @@ def restore(cube, opath: str, z: float, image: int = 1) -> CubeScalars:
         for k in range(3):
             cube.nu_load(k, fl[k])
     return scalars_from_header(r.header, z)
+
+
+# ---- halo catalogue (halofind.f90:113-127, :417-513, :566-580) ---------------
+HALO_HEADER = np.dtype([("nhalo_tot", "<i4"), ("nhalo", "<i4"), ("den_odc", "<f4")])
+
+
+def write_halos(opath: str, z: float, halos: np.ndarray, members: np.ndarray | None, hid: np.ndarray | None,
+                den_odc: float = 200.0, image: int = 1) -> list[str]:
+    """The halofind output files of one image at redshift z:
+
+    halo      nhalo_tot, nhalo (int32), den_odc (float32), then one type_halo_info
+              record (42 float32, HALO_DTYPE) per halo;
+    halo_pid  per halo: int32 i_odc, its i_odc PIDs by increasing radius, int32 0;
+    hid       int16 per PID - 1 (halo number, 0 if none), nf^3 entries as the
+              reference writes them (its integer(2) wraps above 32767).
+    `members` is the concatenated PID list of cube_halofind (halos in order)."""
+    os.makedirs(os.path.join(opath, f"image{image}"), exist_ok=True)
+    files = []
+    head = np.zeros(1, HALO_HEADER)
+    head["nhalo_tot"] = head["nhalo"] = len(halos)
+    head["den_odc"] = den_odc
+    fn = file_name(opath, z, "halo", image)
+    with open(fn, "wb") as f:
+        f.write(head.tobytes())
+        f.write(np.ascontiguousarray(halos).tobytes())
+    files.append(fn)
+    if members is not None:
+        fn = file_name(opath, z, "halo_pid", image)
+        counts = np.asarray(halos["mass_odc"], np.int64)
+        if int(counts.sum()) != len(members):
+            raise ValueError("member list does not match the halos' particle counts")
+        with open(fn, "wb") as f:
+            off = 0
+            for n in counts:
+                f.write(np.int32(n).tobytes())
+                f.write(np.ascontiguousarray(members[off:off + n], dtype=np.int32).tobytes())
+                f.write(np.int32(0).tobytes())
+                off += int(n)
+        files.append(fn)
+    if hid is not None:
+        fn = file_name(opath, z, "hid", image)
+        with open(fn, "wb") as f:
+            f.write(np.asarray(hid).astype(np.int16).tobytes())
+        files.append(fn)
+    return files
+
+
+def read_halos(opath: str, z: float, image: int = 1):
+    """(header, halos, list of per-halo PID arrays or None) of write_halos' files."""
+    raw = np.fromfile(file_name(opath, z, "halo", image), dtype=np.uint8)
+    head = raw[:HALO_HEADER.itemsize].view(HALO_HEADER)[0]
+    halos = raw[HALO_HEADER.itemsize:].view(HALO_DTYPE)
+    members = None
+    fn = file_name(opath, z, "halo_pid", image)
+    if os.path.exists(fn):
+        w = np.fromfile(fn, dtype=np.int32)
+        members, off = [], 0
+        while off < len(w):
+            n = int(w[off])
+            members.append(w[off + 1:off + 1 + n].copy())
+            if w[off + 1 + n] != 0:
+                raise ValueError("halo_pid record does not end in 0")
+            off += n + 2
+    return head, halos, members

@@ -641,6 +641,13 @@ int32_t cube_make_ic(cube_ctx* ctx, const cube_ic_params* ic, cube_scalars* io) 
   return rc;
 }
 
+int32_t cube_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* args, cube_halo_result* result) {
+  if (!ctx || !io || !args || !result || (args->capacity > 0 && !args->halos)) return CUBE_ERR_PARAM;
+  if (!ctx->state_loaded) return CUBE_ERR_STATE;
+  *result = cube_halo_result{0, 0, 0};
+  return cube_halofind_dev(ctx, io, args, result);
+}
+
 int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t capacity, int32_t* nbin) {
   if (!ctx || !xip || !nbin) return CUBE_ERR_PARAM;
   if (!ctx->state_loaded) return CUBE_ERR_STATE;

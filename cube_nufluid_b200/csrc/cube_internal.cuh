@@ -315,6 +315,7 @@ int cube_nu_density(cube_ctx* ctx, cube_scalars* io);
 int cube_nu_gravity(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int ncomp, unsigned int* f2_bits);
 int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io);
+int cube_halofind_dev(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* ha, cube_halo_result* res);
 // device table of cube_vdecode(tan_table[c], coef) for every code c (index code + nvbin/2),
 // built on first use of a coefficient; the last two coefficients stay cached
 const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc);

@@ -16,7 +16,8 @@
  *              plane);
  *   particles  lattice q = i/np_nc + 1/(2 ncell) (coarse units), x = q + psi/np_nc,
  *              v = psi/np_nc * ncell * vf; sorted by tile-major cell, in lattice
- *              order inside a cell (PID = lattice index + 1); per cell the mean
+ *              order inside a cell; PID = 1 + the fine-mesh index of the lattice
+ *              point, iq = (ncell/np_nc)*lattice index per dimension (:834-836); per cell the mean
  *              velocity (vfield), the residuals' dispersion sigma_vi, and the codes
  *              (initial_conditions.f90:797-838).
  */
@@ -247,7 +248,10 @@ __global__ void k_ic_emit(PartArgs A, const int32_t* __restrict__ perm, const in
       vp[(size_t)d * cap + s] = (TV)cube_wrap_code(cube_vencode(&codec, r, coef), ZV);
       vm[d] = fmaxf(vm[d], (float)fabs(v[d]));
     }
-    pid[s] = i + 1;
+    {
+      const int64_t n = A.npd, nf = (int64_t)A.nc * A.ncell, st = A.ncell / A.np_nc;
+      pid[s] = (int32_t)(st * (i % n) + nf * (st * ((i / n) % n)) + nf * nf * (st * (i / (n * n))) + 1);
+    }
   }
   for (int d = 0; d < 3; ++d) {
     float m = vm[d];
@@ -287,6 +291,10 @@ int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io)
   if (np > ctx->cap || np >= (1ll << 31)) {
     ctx->err = "initial conditions: np_nc^3 nc^3 particles exceed the context capacity";
     return CUBE_ERR_CAPACITY;
+  }
+  if ((int64_t)ctx->nf * ctx->nf * ctx->nf >= (1ll << 31)) {
+    ctx->err = "initial conditions: PIDs are fine-mesh indices + 1 and need nf^3 < 2^31";
+    return CUBE_ERR_PARAM;
   }
   // the particle grid borrows the fine mesh's arrays (free outside particle_mesh);
   // npd <= nf, so it fits with its own pitch

@@ -21,7 +21,7 @@ import os
 
 import numpy as np
 
-from .abi import ABI_VERSION, CubeIcParams, CubeParams, CubeScalars
+from .abi import ABI_VERSION, HALO_DTYPE, CubeHaloArgs, CubeHaloResult, CubeIcParams, CubeParams, CubeScalars
 from . import tables
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
@@ -74,6 +74,8 @@ def load_library():
     L.cube_debug_encode_check.restype = C.c_int32
     L.cube_make_ic.argtypes = [vp, C.POINTER(CubeIcParams), S]
     L.cube_make_ic.restype = C.c_int32
+    L.cube_halofind.argtypes = [vp, S, C.POINTER(CubeHaloArgs), C.POINTER(CubeHaloResult)]
+    L.cube_halofind.restype = C.c_int32
     L.cube_power_spectrum.argtypes = [vp, C.c_int32, vp, C.c_int32, C.POINTER(C.c_int32)]
     L.cube_power_spectrum.restype = C.c_int32
     L.cube_phase_times.argtypes = [vp, C.POINTER(C.c_float)]
@@ -126,6 +128,7 @@ class Cube:
         if rc:
             raise CubeError(rc, self.L.cube_last_error(None).decode())
         self.h = h
+        self.np_capacity = int(np_capacity)
         self.nc = params.nc
         self.nf = params.nc * params.ncell
 
@@ -221,6 +224,30 @@ class Cube:
         s = CubeScalars()
         self._check(self.L.cube_make_ic(self.h, C.byref(q), C.byref(s)))
         return s
+
+    def halofind(self, s: CubeScalars, *, den_odc: float = 200.0, capacity: int = 1 << 16,
+                 members: bool = True, hid_len: int = 0):
+        """Run-time halo finder (cube_halofind, halofind.f90:18-598) on the resident
+        state.  Returns (halos as a HALO_DTYPE array, member PIDs by halo in radius
+        order, hid array or None, number of density peaks)."""
+        while True:
+            halos = np.zeros(capacity, HALO_DTYPE)
+            mcap = int(max(self.np_capacity, 1)) if members else 0
+            mem = np.zeros(max(mcap, 1), np.int32)
+            hid = np.zeros(hid_len, np.int32) if hid_len > 0 else None
+            a = CubeHaloArgs()
+            a.den_odc, a.capacity, a.halos = float(den_odc), int(capacity), halos.ctypes.data
+            a.member_pid = mem.ctypes.data if members else None
+            a.member_capacity = mcap
+            a.hid = hid.ctypes.data if hid is not None else None
+            a.hid_len = int(hid_len)
+            r = CubeHaloResult()
+            rc = self.L.cube_halofind(self.h, C.byref(s), C.byref(a), C.byref(r))
+            if rc == 2 and r.nhalo > capacity:
+                capacity = int(r.nhalo)
+                continue
+            self._check(rc)
+            return halos[:r.nhalo].copy(), mem[:r.nmember].copy(), hid, int(r.npeak)
 
     def power_spectrum(self, log_bins: bool = False) -> np.ndarray:
         """xip(10, nbin) of cicpower / powerspectrum as float32 [nbin, 10]."""

@@ -14,7 +14,9 @@ on a host with numpy:
   velocity v = psi * vfactor(a) (initial_conditions.f90:705,799, vfactor :1068-1079);
 * zip packing as at initial_conditions.f90:797-838: cell g = ceiling(x),
   xp = floor(x/x_resolution) wrapped to the code width, vfield = mean particle
-  velocity of the cell, vp = arctan code of v - vfield, pid = lattice index + 1.
+  velocity of the cell, vp = arctan code of v - vfield, pid = 1 + the fine-mesh
+  index of the lattice point, iq = (ncell/np_nc)*lattice index per dimension,
+  pid = iq_x + nf*iq_y + nf^2*iq_z + 1 (initial_conditions.f90:834-836).
 
 The reference computes the potential on the fine mesh with a discrete
 Laplacian and central differences; this harness uses the continuous-k
@@ -248,7 +250,17 @@ def zeldovich(nc: int, nnt: int, box: float, z_i: float, seed: int, *, np_nc: in
     vel = dsp * (ncell * vf)  # fine cells per unit time
     del pos, dsp
     return pack(x, vel, nc, nnt, ncell=ncell, izipx=izipx, izipv=izipv, a=a, box=box, omega_m=c.omega_m,
-                f_cdm=f_cdm)
+                f_cdm=f_cdm, pid_of=lattice_pid(nc, np_nc, ncell))
+
+
+def lattice_pid(nc: int, np_nc: int, ncell: int = 4) -> np.ndarray:
+    """PID of each lattice point (x fastest): 1 + its fine-mesh index on the nf^3
+    mesh, iq = (ncell/np_nc)*(lattice index) per dimension (initial_conditions.f90:834-836)."""
+    npd = nc * np_nc
+    nf = nc * ncell
+    iq = (ncell // np_nc) * np.arange(npd, dtype=np.int64)
+    z, y, x = np.meshgrid(iq, iq, iq, indexing="ij")
+    return (x + nf * y + nf * nf * z + 1).reshape(-1).astype(np.int32)
 
 
 
@@ -275,8 +287,10 @@ def clustered(nc: int, nnt: int, npart: int, seed: int, *, ncell: int = 4, izipx
 
 
 def pack(x: np.ndarray, vel: np.ndarray, nc: int, nnt: int, *, ncell: int = 4, izipx: int = 2, izipv: int = 2,
-         a: float = 0.02, box: float = 100.0, omega_m: float = 0.3, f_cdm: float = 1.0) -> ICState:
-    """Zip packing of initial_conditions.f90:797-838 for positions x (coarse units) and velocities."""
+         a: float = 0.02, box: float = 100.0, omega_m: float = 0.3, f_cdm: float = 1.0,
+         pid_of: np.ndarray | None = None) -> ICState:
+    """Zip packing of initial_conditions.f90:797-838 for positions x (coarse units) and velocities;
+    pid_of[i] is particle i's PID (default i + 1)."""
     g = np.ceil(x).astype(np.int64) - 1
     g %= nc
     cid = tile_major_cell_id(g, nc, nnt)
@@ -284,7 +298,7 @@ def pack(x: np.ndarray, vel: np.ndarray, nc: int, nnt: int, *, ncell: int = 4, i
     cid = cid[order]
     x = x[order]
     vel = vel[order]
-    pid = (order + 1).astype(np.int32)
+    pid = (order + 1).astype(np.int32) if pid_of is None else np.asarray(pid_of, np.int32)[order]
     ncells = nc ** 3
     rhoc = np.bincount(cid, minlength=ncells).astype(np.int32)
     vsum = np.stack([np.bincount(cid, weights=vel[:, d], minlength=ncells) for d in range(3)], axis=-1)

@@ -200,7 +200,9 @@ int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t
  * the noise is Philox4x32-10 under `seed` through the reference's Box-Muller
  * pairing along x (initial_conditions.f90:320-336).  Particles are packed as the
  * reference packs them (:797-838): sorted by coarse cell, lattice order within a
- * cell, PID = lattice index + 1, vfield = cell-mean velocity, velocity codes
+ * cell, PID = 1 + the fine-mesh index of the lattice point (iq = (ncell/np_nc)*
+ * lattice index per dimension, PID = iq_x + nf iq_y + nf^2 iq_z + 1, :834-836; needs
+ * nf^3 < 2^31), vfield = cell-mean velocity, velocity codes
  * relative to it with sigma_vi from the residuals. */
 typedef struct cube_ic_params {
   int64_t seed;
@@ -223,6 +225,50 @@ typedef struct cube_ic_params {
  * does after reading it (a, sigma_vi, mass_p_cdm, vmax, vz_max, dt_vmax, np).
  * Uses the fine meshes as scratch (np_nc <= ncell); needs np <= np_capacity. */
 int32_t cube_make_ic(cube_ctx* ctx, const cube_ic_params* ic, cube_scalars* io);
+
+/* ---- run-time halo finder ------------------------------------------------------
+ * halofind (halofind.f90:18-598) on the resident particles: spherical-overdensity
+ * halos grown from the peaks of the fine CIC density, densest first, each taking
+ * the untagged particles inside the radius where the enclosed density falls below
+ * den_odc, kept with at least 100 particles.  One record per halo, the reference's
+ * type_halo_info (halofind.f90:10-15), 42 floats: */
+typedef struct cube_halo {
+  float hpos[3];          /* refined density peak, fine units, in [0, nf) */
+  float mass_odc;         /* particles inside radius_odc */
+  float radius_odc;       /* fine units */
+  float v_disp;           /* 3-D velocity dispersion, simulation units */
+  float x_mean[3], v_mean[3], ang_mom[3], var_x[3];
+  float inertia[9];       /* (3,3), column-major, about x_mean */
+  float q_mean[3];        /* Lagrangian mean position from the PIDs */
+  float inertia_q[9];
+  float s_mean[3];        /* redshift-space mean position (viewer at cen/500*nc) */
+} cube_halo;
+
+typedef struct cube_halo_args {
+  float den_odc;          /* overdensity threshold; <= 0 selects 200 (halofind.f90:96-104) */
+  int32_t capacity;       /* records `halos` holds */
+  cube_halo* halos;       /* host, in order of discovery (decreasing peak density) */
+  int32_t* member_pid;    /* host or NULL: each halo's PIDs by increasing radius, halos
+                             concatenated (the halo_pid file without its counts) */
+  int64_t member_capacity;
+  int32_t* hid;           /* host or NULL: hid[pid-1] = 1-based halo number, 0 if none */
+  int64_t hid_len;        /* entries of hid (nf^3 for the IC's PIDs) */
+} cube_halo_args;
+
+typedef struct cube_halo_result {
+  int32_t nhalo;          /* halos found (may exceed capacity: CUBE_ERR_CAPACITY) */
+  int32_t npeak;          /* density peaks examined */
+  int64_t nmember;        /* PIDs written to member_pid (with params.use_pid) */
+} cube_halo_result;
+
+/* Finds the halos of the resident state.  Reads a, sigma_vi, mass_p_cdm and
+ * vsim2phys (set by cube_particle_mesh or cube_make_ic) from io.  Without
+ * params.use_pid the q-space fields are zero and no PIDs are written.  Uses the
+ * fine force meshes as scratch: call it between steps.  CUBE_ERR_CAPACITY when
+ * a halo's refined grid would exceed 300 cells per dimension (the reference's
+ * newbox_max stop) or an output array is too small (the counts are still set). */
+int32_t cube_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* args,
+                      cube_halo_result* result);
 
 /* Set-up constants, 19 floats: beta = m/T, the three normalised weights, then
  * per fluid (n, ncb of the reference layout, dx, cs2, hg_dv). */

@@ -17,6 +17,7 @@
  *   particle_mesh      pm.f90:2-451 (fine per tile, then coarse)
  *   ext_pp_force       ext_pp_force.f90:9-160
  *   kernel_f/kernel_c  kernel_f.f90:2-43, kernel_c.f90:2-134 (FP64 here)
+ *   halofind           halofind.f90:18-598 (global periodic box, namespace hf)
  *
  * Precision: FP32 where the reference is FP32 (rho_f, force_f, vfield, ...),
  * FP64 where it is real(8).  The FFTs run in FP64 (FFTW single precision is
@@ -953,6 +954,351 @@ int ext_pp_force(Orc& o, cube_scalars* s) {
   return CUBE_OK;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Run-time halo finder, halofind.f90:18-598, on the global periodic box of   */
+/* one image instead of tile by tile (every halo is then found once).  The    */
+/* reference's FP32 meshes become 64-bit fixed point (weights * 2^32), ties   */
+/* it leaves to its unstable quicksort are broken by index, and the moment    */
+/* accumulators start from zero for each halo; see the library's k_halo.cu    */
+/* for the list.  Plain sequential loops in the reference's step order.       */
+namespace hf {
+
+const double FIX = 4294967296.0;
+const int RMAX = 64, NB_MAX = 300, MIN_NP = 100;
+
+struct Cand {
+  int64_t node;
+  uint64_t acc;
+  double mass;
+  double pos[3];
+  double rp;
+};
+
+inline int wrapn(int64_t x, int64_t n) { x %= n; return (int)(x < 0 ? x + n : x); }
+inline double pmod(double a, double p) { return a - floor(a / p) * p; }  /* Fortran modulo */
+inline double dist3(const double a[3], const double b[3]) {
+  const double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
+  return sqrt((d0 * d0 + d1 * d1) + d2 * d2);
+}
+inline double parab(int64_t m, int64_t p, int64_t den) { return (0.5 * (double)(p - m)) / (double)den; }
+
+void cell_xyz(const Orc& o, int64_t c, int g[3]) {
+  const int64_t nt3 = (int64_t)o.nt * o.nt * o.nt;
+  const int64_t t = c / nt3, r = c % nt3;
+  g[0] = (int)(t % o.nnt) * o.nt + (int)(r % o.nt);
+  g[1] = (int)((t / o.nnt) % o.nnt) * o.nt + (int)((r / o.nt) % o.nt);
+  g[2] = (int)(t / ((int64_t)o.nnt * o.nnt)) * o.nt + (int)(r / ((int64_t)o.nt * o.nt));
+}
+
+/* distance-ordered offsets (:68-87) with exact r^2 and a stable order */
+struct Off { int dx, dy, dz, r2; };
+std::vector<Off> shell_list() {
+  std::vector<Off> L;
+  for (int i = -RMAX; i <= RMAX; ++i)
+    for (int j = -RMAX; j <= RMAX; ++j)
+      for (int k = -RMAX; k <= RMAX; ++k) {
+        const int r2 = i * i + j * j + k * k;
+        if (r2 <= RMAX * RMAX) L.push_back(Off{i, j, k, r2});
+      }
+  std::stable_sort(L.begin(), L.end(), [](const Off& a, const Off& b) { return a.r2 < b.r2; });
+  return L;
+}
+
+int halofind(Orc& o, const cube_scalars* s, const cube_halo_args* ha, cube_halo_result* res) {
+  const int nf = o.nf, nc = o.nc, ncell = o.ncell;
+  const int64_t n3 = (int64_t)nf * nf * nf;
+  const double den_odc = ha->den_odc > 0.f ? (double)ha->den_odc : 200.0;
+  const double mass = (double)s->mass_p_cdm, unit = mass / FIX, pi = (double)o.codec.pi_f;
+  const double coef = cube_vcoef(&o.codec, s->sigma_vi);
+  const std::vector<int64_t> cs = compact_cell_start(o);
+  const int64_t ncells = (int64_t)nc * nc * nc;
+  *res = cube_halo_result{0, 0, 0};
+  /* fine mass assignment, CIC at pos - 1/2 (:144-177) */
+  std::vector<uint64_t> rhof((size_t)n3, 0);
+  for (int64_t c = 0; c < ncells; ++c) {
+    int g[3];
+    cell_xyz(o, c, g);
+    for (int64_t ip = cs[c]; ip < cs[c + 1]; ++ip) {
+      int i1[3];
+      double w1[3], w2[3];
+      for (int d = 0; d < 3; ++d) {
+        const double p = 4.0 * ((double)g[d] + cube_xfrac(o.xp[3 * ip + d], o.izipx)) - 0.5;
+        const double f = floor(p);
+        w1[d] = (f + 1.0) - p;
+        w2[d] = 1.0 - w1[d];
+        i1[d] = (int)f;
+      }
+      for (int cc = 0; cc < 8; ++cc) {
+        const int ox = cc & 1, oy = (cc >> 1) & 1, oz = cc >> 2;
+        const double w = ((ox ? w2[0] : w1[0]) * (oy ? w2[1] : w1[1])) * (oz ? w2[2] : w1[2]);
+        const size_t q = ((size_t)wrapn(i1[2] + oz, nf) * nf + wrapn(i1[1] + oy, nf)) * nf + wrapn(i1[0] + ox, nf);
+        rhof[q] += (uint64_t)llrint(w * FIX);
+      }
+    }
+  }
+  /* density peaks, their mesh mass and parabolic position (:179-208) */
+  const std::vector<Off> sl = shell_list();
+  std::vector<Cand> cand;
+  auto at = [&](int x, int y, int z) { return (int64_t)rhof[((size_t)wrapn(z, nf) * nf + wrapn(y, nf)) * nf + wrapn(x, nf)]; };
+  for (int z = 0; z < nf; ++z)
+    for (int y = 0; y < nf; ++y)
+      for (int x = 0; x < nf; ++x) {
+        const uint64_t a0 = rhof[((size_t)z * nf + y) * nf + x];
+        if (!((double)a0 * unit > 100.0)) continue;
+        bool peak = true;
+        for (int dz = -1; dz <= 1; ++dz)
+          for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx)
+              if ((uint64_t)at(x + dx, y + dy, z + dz) > a0) peak = false;
+        if (!peak) continue;
+        uint64_t m = 0;
+        for (size_t i = 0; i < sl.size(); ++i) {
+          m += (uint64_t)at(x + sl[i].dx, y + sl[i].dy, z + sl[i].dz);
+          if (i + 1 < sl.size() && sl[i + 1].r2 == sl[i].r2) continue;
+          if (i + 1 >= 19 && (double)m * unit / (double)(i + 1) < den_odc) break;
+        }
+        const double mm = (double)m * unit;
+        if (!(mm > mass * 50.0)) continue;
+        Cand h;
+        h.node = ((int64_t)z * nf + y) * nf + x;
+        h.acc = a0;
+        h.mass = mm;
+        const int c3[3] = {x, y, z};
+        for (int d = 0; d < 3; ++d) {
+          const int e0 = d == 0, e1 = d == 1, e2 = d == 2;
+          const int64_t am = at(x - e0, y - e1, z - e2), ap = at(x + e0, y + e1, z + e2);
+          const int64_t den = 2 * (int64_t)a0 - am - ap;
+          h.pos[d] = ((double)c3[d] + 0.5) + (den != 0 ? parab(am, ap, den) : 0.0);
+        }
+        cand.push_back(h);
+      }
+  std::sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) {
+    return a.acc != b.acc ? a.acc > b.acc : a.node < b.node;
+  });
+  for (Cand& h : cand) h.rp = cbrt(0.75 / pi / den_odc * h.mass);
+  res->npeak = (int32_t)cand.size();
+  /* halos, densest peak first (:231-513) */
+  std::vector<uint8_t> tag((size_t)o.np, 0);
+  if (ha->hid && ha->hid_len > 0) std::fill(ha->hid, ha->hid + ha->hid_len, 0);
+  const double ng = 1.0 / 3.0, half_ng = 0.5 / 3.0, hnf = (double)(nf / 2);
+  const bool use_pid = o.P.use_pid && !o.pid.empty();
+  int nhalo = 0;
+  int64_t nmem = 0;
+  std::vector<double> gx, gv;
+  std::vector<int64_t> gip;
+  std::vector<uint64_t> grid;
+  for (const Cand& h : cand) {
+    double hpos[3] = {h.pos[0], h.pos[1], h.pos[2]};
+    const double rp = h.rp, rs = fmin(2.0 * rp, (double)((o.ncb - 1) * ncell));
+    int clo[3], cn[3], flo[3], nb[3], mx[3];
+    for (int d = 0; d < 3; ++d) {
+      clo[d] = (int)floor((hpos[d] - rs) / ncell);
+      cn[d] = (int)floor((hpos[d] + rs) / ncell) - clo[d] + 1;
+      const int rlo = (int)floor((hpos[d] - rp) / ncell), rhi = (int)floor((hpos[d] + rp) / ncell);
+      flo[d] = ncell * rlo;
+      nb[d] = 3 * ncell * (rhi - rlo + 1);
+      mx[d] = std::min(nb[d] + 1, NB_MAX);
+      if (nb[d] > NB_MAX) { o.err = "halofind: newbox > newbox_max"; return CUBE_ERR_CAPACITY; }
+      if (cn[d] > nc) { o.err = "halofind: search box wraps onto itself"; return CUBE_ERR_PARAM; }
+    }
+    const int gxn = nb[0] + 3, gyn = nb[1] + 3, gzn = nb[2] + 3;
+    grid.assign((size_t)gxn * gyn * gzn, 0);
+    gx.clear(); gv.clear(); gip.clear();
+    for (int q = 0; q < cn[0] * cn[1] * cn[2]; ++q) {
+      const int cu[3] = {clo[0] + q % cn[0], clo[1] + (q / cn[0]) % cn[1], clo[2] + q / (cn[0] * cn[1])};
+      const int gw[3] = {wrapn(cu[0], nc), wrapn(cu[1], nc), wrapn(cu[2], nc)};
+      const int64_t c = cell_id(o, gw[0] / o.nt, gw[1] / o.nt, gw[2] / o.nt, gw[0] % o.nt, gw[1] % o.nt, gw[2] % o.nt);
+      for (int64_t ip = cs[c]; ip < cs[c + 1]; ++ip) {
+        if (tag[ip]) continue;
+        double x[3];
+        for (int d = 0; d < 3; ++d) x[d] = 4.0 * ((double)cu[d] + cube_xfrac(o.xp[3 * ip + d], o.izipx));
+        const double r = dist3(x, hpos);
+        if (!(r < rs)) continue;
+        for (int d = 0; d < 3; ++d) {
+          gx.push_back(x[d]);
+          gv.push_back(cube_dadd(cube_vdecode(tanf_code(o, o.vp[3 * ip + d]), coef), (double)o.vfield[3 * c + d]));
+        }
+        gip.push_back(ip);
+        if (r < rp) {
+          int i1[3];
+          double w1[3], w2[3];
+          for (int d = 0; d < 3; ++d) {
+            const double p = ((x[d] - half_ng) - (double)flo[d]) / ng;
+            const double f = floor(p);
+            w1[d] = (f + 1.0) - p;
+            w2[d] = 1.0 - w1[d];
+            i1[d] = (int)f + 1;
+          }
+          for (int cc = 0; cc < 8; ++cc) {
+            const int ox = cc & 1, oy = (cc >> 1) & 1, oz = cc >> 2;
+            const int ix = i1[0] + ox, iy = i1[1] + oy, iz = i1[2] + oz;
+            if (ix < 0 || iy < 0 || iz < 0 || ix >= gxn || iy >= gyn || iz >= gzn) continue;
+            const double w = ((ox ? w2[0] : w1[0]) * (oy ? w2[1] : w1[1])) * (oz ? w2[2] : w1[2]);
+            grid[((size_t)iz * gyn + iy) * gxn + ix] += (uint64_t)llrint(w * FIX);
+          }
+        }
+      }
+    }
+    const int n = (int)gip.size();
+    /* refined maximum, maxloc(finegrid(1:newbox_max,...)) (:347) */
+    auto g = [&](int a, int b, int c) { return (int64_t)grid[((size_t)c * gyn + b) * gxn + a]; };
+    int i0 = 1, j0 = 1, k0 = 1;
+    int64_t best = g(1, 1, 1);
+    for (int iz = 1; iz <= mx[2]; ++iz)
+      for (int iy = 1; iy <= mx[1]; ++iy)
+        for (int ix = 1; ix <= mx[0]; ++ix)
+          if (g(ix, iy, iz) > best) { best = g(ix, iy, iz); i0 = ix; j0 = iy; k0 = iz; }
+    const int64_t g0 = g(i0, j0, k0);
+    const int64_t dxn = 2 * g0 - g(i0 - 1, j0, k0) - g(i0 + 1, j0, k0);
+    const int64_t dyn = 2 * g0 - g(i0, j0 - 1, k0) - g(i0, j0 + 1, k0);
+    const int64_t dzn = 2 * g0 - g(i0, j0, k0 - 1) - g(i0, j0, k0 - 1);  /* as :354-355 */
+    if (dxn == 0 || dyn == 0 || dzn == 0) continue;
+    const double hr[3] = {(i0 - 0.5) + parab(g(i0 - 1, j0, k0), g(i0 + 1, j0, k0), dxn),
+                          (j0 - 0.5) + parab(g(i0, j0 - 1, k0), g(i0, j0 + 1, k0), dyn),
+                          (k0 - 0.5) + parab(g(i0, j0, k0 - 1), g(i0, j0, k0 + 1), dzn)};
+    for (int d = 0; d < 3; ++d) hpos[d] = (double)flo[d] + ng * hr[d];
+    /* sort by radius (:361-369), ties by storage index */
+    std::vector<double> key(n);
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; ++i) {
+      key[i] = dist3(&gx[3 * i], hpos);
+      ord[i] = i;
+    }
+    std::sort(ord.begin(), ord.end(), [&](int a, int b) {
+      return key[a] != key[b] ? key[a] < key[b] : gip[a] < gip[b];
+    });
+    /* halo radius (:385-401) */
+    const double c43 = 0.75 / pi;
+    int iis = 0;
+    for (int ii = 2; ii <= n; ++ii) {
+      const double r = key[ord[ii - 1]];
+      if (c43 * ii * mass / (r * r * r) < den_odc) { iis = ii; break; }
+    }
+    const int iodc = iis ? iis - 1 : 0;
+    if (iodc < MIN_NP) continue;
+    /* tag, halo number per PID, member PIDs (:404-405, :450-458) */
+    for (int i = 0; i < iodc; ++i) {
+      const int64_t ip = gip[ord[i]];
+      tag[ip] = 1;
+      if (use_pid) {
+        const int32_t p = o.pid[ip];
+        if (ha->hid && p >= 1 && p <= ha->hid_len) ha->hid[p - 1] = nhalo + 1;
+        if (ha->member_pid && nmem + i < ha->member_capacity) ha->member_pid[nmem + i] = p;
+      }
+    }
+    cube_halo H;
+    memset(&H, 0, sizeof(H));
+    double xm[3] = {0, 0, 0}, vm[3] = {0, 0, 0};
+    for (int i = 0; i < iodc; ++i)
+      for (int d = 0; d < 3; ++d) {
+        xm[d] += gx[3 * ord[i] + d];
+        vm[d] += gv[3 * ord[i] + d];
+      }
+    double xw[3];
+    for (int d = 0; d < 3; ++d) {
+      xm[d] /= iodc;
+      vm[d] /= iodc;
+      xw[d] = pmod(xm[d], (double)nf);
+    }
+    double sxx[3] = {0, 0, 0}, svv = 0, am[3] = {0, 0, 0}, in[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = 0; i < iodc; ++i) {
+      double dx[3], v[3];
+      for (int d = 0; d < 3; ++d) {
+        dx[d] = gx[3 * ord[i] + d] - xm[d];
+        v[d] = gv[3 * ord[i] + d];
+        sxx[d] += dx[d] * dx[d];
+        svv += (v[d] - vm[d]) * (v[d] - vm[d]);
+      }
+      am[0] += dx[1] * v[2] - dx[2] * v[1];
+      am[1] += dx[2] * v[0] - dx[0] * v[2];
+      am[2] += dx[0] * v[1] - dx[1] * v[0];
+      in[0] += dx[0] * dx[0]; in[1] += dx[1] * dx[1]; in[2] += dx[2] * dx[2];
+      in[3] += dx[0] * dx[1]; in[4] += dx[1] * dx[2]; in[5] += dx[2] * dx[0];
+    }
+    /* q-space: PID - 1 = iq_x + nf iq_y + nf^2 iq_z, qpos = iq + 1/2 (:460-500) */
+    double qm[3] = {0, 0, 0}, iq[6] = {0, 0, 0, 0, 0, 0};
+    if (use_pid) {
+      const int64_t nfl = nf;
+      double dq[3] = {0, 0, 0};
+      int64_t nq = 0;
+      auto qpos = [&](int64_t qt, double q[3]) {
+        const int64_t qz = qt / (nfl * nfl), qy = (qt - qz * nfl * nfl) / nfl, qx = qt % nfl;
+        q[0] = qx + 0.5; q[1] = qy + 0.5; q[2] = qz + 0.5;
+      };
+      for (int i = 0; i < iodc; ++i) {
+        const int64_t qt = (int64_t)o.pid[gip[ord[i]]] - 1;
+        if (qt < 0) continue;
+        double q[3];
+        qpos(qt, q);
+        for (int d = 0; d < 3; ++d) dq[d] += pmod((q[d] - xw[d]) + hnf, (double)nf) - hnf;
+        ++nq;
+      }
+      if (nq > 0) {
+        for (int d = 0; d < 3; ++d) qm[d] = pmod(xw[d] + dq[d] / (double)nq, (double)nf);
+        for (int i = 0; i < iodc; ++i) {
+          const int64_t qt = (int64_t)o.pid[gip[ord[i]]] - 1;
+          if (qt < 0) continue;
+          double q[3], e[3];
+          qpos(qt, q);
+          for (int d = 0; d < 3; ++d) e[d] = pmod(((q[d] + 0.5) - qm[d]) + hnf, (double)nf) - hnf;
+          iq[0] += e[0] * e[0]; iq[1] += e[1] * e[1]; iq[2] += e[2] * e[2];
+          iq[3] += e[0] * e[1]; iq[4] += e[1] * e[2]; iq[5] += e[2] * e[0];
+        }
+      }
+    }
+    for (int d = 0; d < 3; ++d) H.hpos[d] = (float)pmod(hpos[d], (double)nf);
+    H.mass_odc = (float)iodc;
+    {
+      const double r2 = key[ord[iis - 1]], r1 = key[ord[iis - 2]];
+      const double den2 = c43 * iis * mass / (r2 * r2 * r2), den1 = c43 * (iis - 1) * mass / (r1 * r1 * r1);
+      const double lr2 = log10(r2), lr1 = log10(r1), d2 = log10(den2), d1 = log10(den1), lo = log10(den_odc);
+      H.radius_odc = (float)pow(10.0, ((lo - d2) * lr1 + (d1 - lo) * lr2) / (d1 - d2));
+    }
+    H.v_disp = (float)sqrt(svv / (iodc - 1));
+    for (int d = 0; d < 3; ++d) {
+      H.x_mean[d] = (float)xw[d];
+      H.v_mean[d] = (float)vm[d];
+      H.var_x[d] = (float)(sxx[d] / (iodc - 1));
+      H.ang_mom[d] = (float)am[d];
+      H.q_mean[d] = (float)qm[d];
+    }
+    const int sym[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};
+    for (int k = 0; k < 9; ++k) {
+      H.inertia[k] = (float)in[sym[k]];
+      H.inertia_q[k] = (float)iq[sym[k]];
+    }
+    /* redshift-space mean position (:425-430); ng_global = nc in the main code */
+    double los[3], ln = 0.0, vlos = 0.0;
+    const double cen[3] = {30.0, 370.0, 370.0};
+    for (int d = 0; d < 3; ++d) {
+      los[d] = xw[d] - cen[d] / 500.0 * (double)nc;
+      ln += los[d] * los[d];
+    }
+    ln = sqrt(ln);
+    for (int d = 0; d < 3; ++d) {
+      los[d] /= ln;
+      vlos += vm[d] * los[d];
+    }
+    for (int d = 0; d < 3; ++d) {
+      const double sx = vlos * los[d] * (double)s->vsim2phys / (double)s->a / (100.0 * (double)o.P.h0) /
+                        ((double)o.P.h0 * (double)o.P.box / nf);
+      H.s_mean[d] = (float)pmod(xw[d] + sx, (double)nf);
+    }
+    if (nhalo < ha->capacity) ha->halos[nhalo] = H;
+    ++nhalo;
+    if (use_pid) nmem += iodc;
+  }
+  res->nhalo = nhalo;
+  res->nmember = nmem;
+  if (nhalo > ha->capacity || (ha->member_pid && nmem > ha->member_capacity)) {
+    o.err = "halofind: the output arrays are too small";
+    return CUBE_ERR_CAPACITY;
+  }
+  return CUBE_OK;
+}
+
+}  // namespace hf
+
 void setup_sizes(Orc& o, const cube_params* p) {
   o.P = *p;
   o.nc = p->nc; o.nnt = p->nnt; o.nt = p->nc / p->nnt; o.ncell = p->ncell; o.ncb = p->ncb;
@@ -1116,6 +1462,11 @@ int64_t orc_fetch(void* h, int which, void* out, int64_t cap) {
   if (n > cap) return -1;
   memcpy(out, src, es * n);
   return n;
+}
+
+/* run-time halo finder (halofind.f90:18-598), global periodic box */
+int orc_halofind(void* h, const cube_scalars* s, const cube_halo_args* a, cube_halo_result* r) {
+  return hf::halofind(*(Orc*)h, s, a, r);
 }
 
 /* dt constraints only (pm.f90:427-443) */

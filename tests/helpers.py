@@ -60,3 +60,33 @@ def kick_chain(force, a_mid, dt):
     f32 = np.float32
     pif = f32(4.0) * np.arctan(f32(1.0))
     return ((((np.asarray(force, f32) * f32(a_mid)) * f32(dt)) / f32(6.0)) / pif).astype(f32)
+
+
+def planted_clumps(nc=16, nnt=2, centres=((3.0, 4.0, 5.0), (11.0, 9.5, 3.0), (6.5, 12.0, 12.5), (14.5, 2.0, 9.0)),
+                   n_per=3000, sigma=0.3, nbg=20000, seed=5, izipx=2, izipv=2, box=100.0, vel=0.02):
+    """Uniform background plus Gaussian clumps at known centres (coarse units), packed
+    in checkpoint layout; each clump moves with its own bulk velocity."""
+    rng = np.random.Generator(np.random.Philox(seed))
+    c = np.asarray(centres, np.float64)
+    xb = rng.uniform(0, nc, (nbg, 3))
+    xc = np.repeat(c, n_per, axis=0) + rng.normal(0, sigma, (len(c) * n_per, 3))
+    x = np.mod(np.concatenate([xb, xc]), float(nc))
+    v = rng.normal(0, vel, (x.shape[0], 3))
+    v[nbg:] += np.repeat(rng.normal(0, 2 * vel, (len(c), 3)), n_per, axis=0)
+    st = ic.pack(x, v, nc, nnt, izipx=izipx, izipv=izipv, a=0.5, box=box)
+    p = make_params(nc, nnt, box=box, izipx=izipx, izipv=izipv)
+    return st, p, scalars_from_ic(st)
+
+
+def particle_positions(st, nc, nnt, ncell=4):
+    """Fine-unit positions of a checkpoint-layout state in storage order."""
+    nt = nc // nnt
+    cells = np.arange(nc ** 3)
+    l = cells % nt ** 3
+    tile = cells // nt ** 3
+    g = np.stack([(tile % nnt) * nt + l % nt, ((tile // nnt) % nnt) * nt + (l // nt) % nt,
+                  (tile // (nnt * nnt)) * nt + l // (nt * nt)], axis=1)
+    cell_of = np.repeat(cells, st.rhoc.astype(np.int64))
+    mask = 0xFF if st.izipx == 1 else 0xFFFF
+    frac = ((st.xp.astype(np.int64) & mask) + 0.5) / (256.0 if st.izipx == 1 else 65536.0)
+    return ncell * (g[cell_of] + frac)

@@ -11,7 +11,7 @@ import subprocess
 
 import numpy as np
 
-from cube_nufluid_b200.abi import CubeParams, CubeScalars
+from cube_nufluid_b200.abi import HALO_DTYPE, CubeHaloArgs, CubeHaloResult, CubeParams, CubeScalars
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
@@ -47,6 +47,7 @@ def lib():
         L.orc_fetch.restype = C.c_int64
         L.orc_fetch.argtypes = [vp, C.c_int, vp, C.c_int64]
         L.orc_dt_constraints.argtypes = [vp, S]
+        L.orc_halofind.argtypes = [vp, S, C.POINTER(CubeHaloArgs), C.POINTER(CubeHaloResult)]
         L.orc_tanf_code.restype = C.c_float
         L.orc_tanf_code.argtypes = [vp, C.c_int]
         L.orc_atan.restype = C.c_double
@@ -123,6 +124,22 @@ class Oracle:
         f = np.ascontiguousarray(fine, dtype=np.float32)
         c = np.ascontiguousarray(coarse, dtype=np.float32)
         self._check(lib().orc_particle_mesh_with_force(self.h, C.byref(s), deposit_mode, _ptr(f), _ptr(c)))
+
+    def halofind(self, s: CubeScalars, *, den_odc: float = 200.0, capacity: int = 1 << 16,
+                 member_capacity: int = 1 << 24, hid_len: int = 0):
+        """halofind.f90 restated on the global periodic box (oracle hf::halofind):
+        (halos as HALO_DTYPE, member PIDs, hid or None, number of density peaks)."""
+        halos = np.zeros(capacity, HALO_DTYPE)
+        mem = np.zeros(member_capacity, np.int32)
+        hid = np.zeros(hid_len, np.int32) if hid_len > 0 else None
+        a = CubeHaloArgs()
+        a.den_odc, a.capacity, a.halos = float(den_odc), int(capacity), halos.ctypes.data
+        a.member_pid, a.member_capacity = mem.ctypes.data, int(member_capacity)
+        a.hid = hid.ctypes.data if hid is not None else None
+        a.hid_len = int(hid_len)
+        r = CubeHaloResult()
+        self._check(lib().orc_halofind(self.h, C.byref(s), C.byref(a), C.byref(r)))
+        return halos[:r.nhalo].copy(), mem[:r.nmember].copy(), hid, int(r.npeak)
 
     def fetch(self, which: int) -> np.ndarray:
         nf, nc = self.nf, self.nc

@@ -35,6 +35,15 @@ def test_uniform_noise_word_layout():
     assert u.min() >= 0.0 and u.max() < 1.0
 
 
+def test_lattice_pid_encoding():
+    # pid = iq_x + nf iq_y + nf^2 iq_z + 1 with iq = (ncell/np_nc) * lattice index
+    pid = ic.lattice_pid(8, 2, 4)
+    nf, npd = 32, 16
+    assert pid.shape == (npd ** 3,) and pid[0] == 1 and pid[1] == 3 and pid[npd] == 2 * nf + 1
+    assert pid[-1] == 30 + 30 * nf + 30 * nf * nf + 1
+    assert np.unique(pid).size == pid.size and np.all(np.diff(pid) > 0)
+
+
 def test_gaussian_noise_moments():
     g = ic.gaussian_noise(32, 5).astype(np.float64)
     assert abs(g.mean()) < 0.01 and abs(g.std() - 1.0) < 0.01
@@ -92,8 +101,10 @@ def test_gpu_ic_matches_host_generator(tables, izip):
     s = g.make_ic(q, seed)
     xp, vp, pid, rhoc, vfield = g.store_state()
     assert xp.shape[0] == st.np and int(rhoc.sum()) == st.np
-    # PIDs are the lattice indices + 1, each once, in lattice order inside a cell
-    assert np.array_equal(np.sort(pid), np.arange(1, st.np + 1, dtype=np.int32))
+    # PIDs are 1 + the fine-mesh index of each lattice point (initial_conditions.f90:834-836),
+    # each once, in lattice order inside a cell
+    assert np.array_equal(np.sort(pid), np.sort(ic.lattice_pid(nc, 2)))
+    assert np.array_equal(np.sort(pid), np.sort(st.pid))
     same_cell = np.repeat(np.arange(nc ** 3), rhoc)
     inner = same_cell[1:] == same_cell[:-1]
     assert np.all(pid[1:][inner] > pid[:-1][inner])
@@ -134,7 +145,7 @@ def test_gpu_ic_then_steps(tables):
         g.step(s)
     assert s.nplocal == n0 and s.a > 1.0 / (1.0 + z_i)
     _, _, pid, rhoc, _ = g.store_state()
-    assert int(rhoc.sum()) == n0 and np.array_equal(np.sort(pid), np.arange(1, n0 + 1, dtype=np.int32))
+    assert int(rhoc.sum()) == n0 and np.array_equal(np.sort(pid), np.sort(ic.lattice_pid(nc, 2)))
 
 
 @pytest.mark.gpu
