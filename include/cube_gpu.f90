@@ -40,6 +40,27 @@ module cube_gpu
     real(c_double) :: a, norm_d2, n_s, h, eh_s, eh_alpha, eh_omh, eh_theta2, vf, amplitude, f_cdm
   end type
 
+  ! cube_halofind: one record is type_halo_info (halofind.f90:10-15)
+  type, bind(c) :: cube_halo_t
+    real(c_float) :: hpos(3), mass_odc, radius_odc, v_disp
+    real(c_float) :: x_mean(3), v_mean(3), ang_mom(3), var_x(3), inertia(3,3)
+    real(c_float) :: q_mean(3), inertia_q(3,3), s_mean(3)
+  end type
+
+  type, bind(c) :: cube_halo_args_t
+    real(c_float) :: den_odc
+    integer(c_int32_t) :: capacity
+    type(c_ptr) :: halos, member_pid
+    integer(c_int64_t) :: member_capacity
+    type(c_ptr) :: hid
+    integer(c_int64_t) :: hid_len
+  end type
+
+  type, bind(c) :: cube_halo_result_t
+    integer(c_int32_t) :: nhalo, npeak
+    integer(c_int64_t) :: nmember
+  end type
+
   interface
     integer(c_int32_t) function cube_create(p, cap, fk, ck, ctx) bind(c, name="cube_create")
       import :: c_int32_t, c_int64_t, c_float, c_ptr, cube_params_t
@@ -103,7 +124,7 @@ module cube_gpu
       integer(c_int32_t), value :: fluid
       real(c_float), intent(out) :: fld(*)
     end function
-    ! cicpower analysis into xip(10,nbin)
+    ! Zel'dovich state on the device in place of ic.x
     integer(c_int32_t) function cube_make_ic(ctx, ic, s) bind(c, name="cube_make_ic")
       import :: c_int32_t, c_ptr, cube_ic_params_t, cube_scalars_t
       type(c_ptr), value :: ctx
@@ -111,6 +132,7 @@ module cube_gpu
       type(cube_scalars_t), intent(inout) :: s
     end function
 
+    ! cicpower analysis into xip(10,nbin)
     integer(c_int32_t) function cube_power_spectrum(ctx, log_bins, xip, capacity, nbin) &
         bind(c, name="cube_power_spectrum")
       import :: c_int32_t, c_ptr, c_float
@@ -118,6 +140,15 @@ module cube_gpu
       integer(c_int32_t), value :: log_bins, capacity
       real(c_float), intent(out) :: xip(10, *)
       integer(c_int32_t), intent(out) :: nbin
+    end function
+
+    ! run-time halo finder (halofind.f90:18-598)
+    integer(c_int32_t) function cube_halofind(ctx, s, args, res) bind(c, name="cube_halofind")
+      import :: c_int32_t, c_ptr, cube_scalars_t, cube_halo_args_t, cube_halo_result_t
+      type(c_ptr), value :: ctx
+      type(cube_scalars_t), intent(in) :: s
+      type(cube_halo_args_t), intent(in) :: args
+      type(cube_halo_result_t), intent(out) :: res
     end function
   end interface
 
@@ -161,3 +192,22 @@ end module cube_gpu
 ! and the neutrino half steps of main.f90:51-54, 66-69:
 !
 !     call gpu_check(cube_nu_evolve(gpu_ctx, dt/2., dt_neu, 1, a_mid), 'nu evolve')
+!
+! and halofind (halofind.f90:18) as
+!
+!   subroutine halofind
+!     use variables; use cube_gpu
+!     type(cube_halo_t), allocatable, target :: h(:)
+!     integer(c_int32_t), allocatable, target :: mem(:), hid4(:)
+!     type(cube_halo_args_t) :: ha
+!     type(cube_halo_result_t) :: hr
+!     allocate(h(200000), mem(sim%nplocal), hid4(nf**3))
+!     ha%den_odc = 200; ha%capacity = size(h); ha%halos = c_loc(h)
+!     ha%member_pid = c_loc(mem); ha%member_capacity = size(mem, kind=c_int64_t)
+!     ha%hid = c_loc(hid4); ha%hid_len = size(hid4, kind=c_int64_t)
+!     gpu_s%a = a; gpu_s%sigma_vi = sigma_vi; gpu_s%mass_p_cdm = sim%mass_p_cdm
+!     gpu_s%vsim2phys = sim%vsim2phys
+!     call gpu_check(cube_halofind(gpu_ctx, gpu_s, ha, hr), 'halofind')
+!     ! then write(11) hr%nhalo, hr%nhalo, 200., h(:hr%nhalo); the halo_pid records from
+!     ! mem(1:hr%nmember) split by int(h%mass_odc); write(21) int(hid4, 2)
+!   end subroutine
