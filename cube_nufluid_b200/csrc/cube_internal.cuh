@@ -317,7 +317,15 @@ int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int nc
 int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io);
 int cube_halofind_dev(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* ha, cube_halo_result* res);
 // device table of cube_vdecode(tan_table[c], coef) for every code c (index code + nvbin/2),
-// built on first use of a coefficient; the last two coefficients stay cached
+// built on first use of a coefficient; the last two coefficients stay cached.  After
+// the nvbin doubles follow nvbin/32 words of cube_vfixed bits.
 const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc);
+
+// true if re-encoding the decoded velocity of code index c (code + nvbin/2) at the
+// table's coefficient, cube_wrap_code(cube_vencode_fast(v)), gives the code back: a
+// velocity kicked by exactly zero then keeps its code
+__device__ __forceinline__ bool cube_vfixed(const double* dec, int nvbin, int c) {
+  return (reinterpret_cast<const uint32_t*>(dec + nvbin)[c >> 5] >> (c & 31)) & 1u;
+}
 
 #endif

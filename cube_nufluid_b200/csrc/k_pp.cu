@@ -124,15 +124,14 @@ __device__ __forceinline__ void pp_target(const Sorted<OffT>& S, const Chains& H
                                           const int cc[3], const PPArgs& A, void* __restrict__ vp_, PPAcc& acc) {
   typedef typename CodeT<ZV>::T TV;
   TV* vp = reinterpret_cast<TV*>(vp_);
-  double x1[3], v[3], ft[3] = {0.0, 0.0, 0.0};
-  int g1[3];
+  double x1[3], ft[3] = {0.0, 0.0, 0.0};
+  int g1[3], vc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const double fr = cube_xfrac((int32_t)(int16_t)tc[d], ZX);
     x1[d] = cube_dadd(4.0 * (double)cc[d], cube_dmul(4.0, fr));
     g1[d] = 4 * cc[d] + (int)floor(cube_dmul(4.0, fr));
-    const int vc = (int)vp[(size_t)d * A.cap + ip];
-    v[d] = __ldg(&A.dec[vc + A.half_nvbin]);
+    vc[d] = (int)vp[(size_t)d * A.cap + ip] + A.half_nvbin;
   }
   ++acc.n1;
   const bool pow2_cut = (A.nf_cutoff & (A.nf_cutoff - 1)) == 0;
@@ -190,12 +189,14 @@ __device__ __forceinline__ void pp_target(const Sorted<OffT>& S, const Chains& H
     }
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
+    // a zero sum gives k = +-0 and v + k = v: a code that re-encodes to itself stays
+    if (ft[d] == 0.0 && cube_vfixed(A.dec, 2 * A.half_nvbin, vc[d])) continue;
     double k = cube_dmul(ft[d], A.a_mid);
     k = cube_dmul(k, A.dt);
     k = cube_ddiv(k, 6.0);
     k = cube_ddiv(k, A.pi_d);
-    v[d] = cube_dadd(v[d], k);
-    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&A.codec, v[d], A.coef, A.inv_pi), ZV);
+    const double v = cube_dadd(__ldg(&A.dec[vc[d]]), k);
+    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&A.codec, v, A.coef, A.inv_pi), ZV);
   }
   const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
   acc.f2max = fmaxf(acc.f2max, (float)f2);

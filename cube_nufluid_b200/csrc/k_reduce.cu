@@ -165,27 +165,39 @@ int cube_exclusive_scan(cube_ctx* ctx, const int32_t* in, int64_t n, int64_t* ou
 }
 
 namespace {
-__global__ void k_vdec_build(const float* __restrict__ tan_table, double coef, double* __restrict__ out, int nvbin) {
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nvbin; c += gridDim.x * blockDim.x)
-    out[c] = cube_vdecode(tan_table[c], coef);
+// decode of every code, and one bit per code: the step's encode returns the code
+// itself for its decoded velocity (nvbin is a multiple of 256, so every warp is full)
+__global__ void k_vdec_build(const float* __restrict__ tan_table, double coef, double* __restrict__ out, int nvbin,
+                             cube_codec codec, double inv_pi) {
+  uint32_t* fix = reinterpret_cast<uint32_t*>(out + nvbin);
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nvbin; c += gridDim.x * blockDim.x) {
+    const double v = cube_vdecode(tan_table[c], coef);
+    out[c] = v;
+    const int code = c - nvbin / 2;
+    const bool same = cube_wrap_code(cube_vencode_fast(&codec, v, coef, inv_pi), codec.izipv) == code;
+    const uint32_t bits = __ballot_sync(0xffffffffu, same);
+    if ((threadIdx.x & 31) == 0) fix[c >> 5] = bits;
+  }
 }
 }  // namespace
 
 // decode table for coef: the velocity decode tan(pi*code/(nvbin-1))/coef of every
 // code, computed by the same FP32 table and FP64 division as a per-particle decode,
-// so a lookup is bit-identical to it
+// so a lookup is bit-identical to it; followed by the bits of cube_vfixed
 const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc) {
   *rc = CUBE_OK;
   for (int i = 0; i < 2; ++i)
     if (ctx->vdec[i] && ctx->vdec_coef[i] == coef) return ctx->vdec[i];
   const int i = ctx->vdec_next;
   ctx->vdec_next ^= 1;
-  if (!ctx->vdec[i] && cudaMalloc((void**)&ctx->vdec[i], sizeof(double) * ctx->nvbin) != cudaSuccess) {
+  if (!ctx->vdec[i] && cudaMalloc((void**)&ctx->vdec[i], sizeof(double) * ctx->nvbin + sizeof(uint32_t) * (ctx->nvbin / 32)) !=
+                           cudaSuccess) {
     ctx->err = "cudaMalloc of the velocity decode table failed";
     *rc = CUBE_ERR_CUDA;
     return nullptr;
   }
-  k_vdec_build<<<(ctx->nvbin + 255) / 256, 256, 0, ctx->stream>>>(ctx->tan_table, coef, ctx->vdec[i], ctx->nvbin);
+  k_vdec_build<<<(ctx->nvbin + 255) / 256, 256, 0, ctx->stream>>>(ctx->tan_table, coef, ctx->vdec[i], ctx->nvbin,
+                                                                  ctx->codec, 1.0 / (double)ctx->codec.pi_f);
   ctx->launches++;
   if (cudaGetLastError() != cudaSuccess) {
     ctx->err = "velocity decode table launch failed";
