@@ -301,7 +301,7 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
   // FP32 tangent of every velocity code with the C library's tanf (decode table)
   std::vector<float> tt(ctx->nvbin);
   for (int c = -ctx->nvbin / 2; c < ctx->nvbin / 2; ++c) tt[c + ctx->nvbin / 2] = tanf(cube_varg(&ctx->codec, c));
-  if (cudaMemcpy(ctx->tan_table, tt.data(), 4 * ctx->nvbin, cudaMemcpyHostToDevice) != cudaSuccess) {
+  if (cudaMemcpyAsync(ctx->tan_table, tt.data(), 4 * ctx->nvbin, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
     ctx->err = "tan table upload failed";
     return fail(CUBE_ERR_CUDA);
   }
@@ -713,7 +713,8 @@ int64_t cube_debug_fetch(cube_ctx* ctx, int32_t which, void* host, int64_t capac
       L = which == 4 ? &ctx->fine : &ctx->coarse;
       const int64_t kp = L->n / 2 + 1, n = 3 * kp * kp * kp;
       if (n > capacity) return -1;
-      if (cudaMemcpy(host, L->kern, 4 * n, cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+      if (cudaMemcpyAsync(host, L->kern, 4 * n, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) return -1;
+      if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return -1;
       return n;
     }
     default: return -1;
@@ -759,7 +760,7 @@ int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float*
     const int64_t n = 3 * (int64_t)L.n * L.n * L.n;
     float* tmp = nullptr;
     CUBE_CUDA_TRY(ctx, cudaMalloc(&tmp, 4 * n));
-    CUBE_CUDA_TRY(ctx, cudaMemcpy(tmp, hs[l], 4 * n, cudaMemcpyHostToDevice));
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(tmp, hs[l], 4 * n, cudaMemcpyHostToDevice, ctx->stream));
     k_pitch<<<1184, 256, 0, ctx->stream>>>(tmp, L.force, L.n, L.rp, 3);
     CUBE_LAUNCH_CHECK(ctx);
     CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));

@@ -163,7 +163,7 @@ int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table
     CUBE_CUDA_TRY(ctx, cudaMalloc(&dfk, sizeof(float) * nfk));
     CUBE_CUDA_TRY(ctx, cudaMalloc(&s1, sizeof(double) * (size_t)kp * nfc * nfc));
     CUBE_CUDA_TRY(ctx, cudaMalloc(&s2, sizeof(double) * (size_t)kp * kp * nfc));
-    CUBE_CUDA_TRY(ctx, cudaMemcpy(dfk, fk_table, sizeof(float) * nfk, cudaMemcpyHostToDevice));
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(dfk, fk_table, sizeof(float) * nfk, cudaMemcpyHostToDevice, ctx->stream));
     const int ppz = ctx->P.ext_pp_force ? ctx->P.pp_range : -1;
     for (int d = 0; d < 3; ++d) {
       k_green_x<<<1184, 256, 0, ctx->stream>>>(dfk, nfc, n, d, ppz, s1);
@@ -223,7 +223,8 @@ int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table
             oct[(size_t)d * kp * kp * kp + ((size_t)ky * kp + kx) * kp + kz] = (float)(v / (double)n3);
           }
     }
-    CUBE_CUDA_TRY(ctx, cudaMemcpy(ctx->coarse.kern, oct.data(), sizeof(float) * oct.size(), cudaMemcpyHostToDevice));
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->coarse.kern, oct.data(), sizeof(float) * oct.size(), cudaMemcpyHostToDevice,
+                                       ctx->stream));
   }
   return CUBE_OK;
 }

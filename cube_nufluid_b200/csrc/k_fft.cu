@@ -321,7 +321,7 @@ int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n) {
     tw[j] = make_float2((float)cosl(ang), (float)sinl(ang));
   }
   CUBE_CUDA_TRY(ctx, cudaMalloc(&p.tw, sizeof(float2) * n));
-  CUBE_CUDA_TRY(ctx, cudaMemcpy(p.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(p.tw, tw.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, ctx->stream));
   int R, T;
   if (cube_fast_rt(n, &R, &T)) {
     // the twiddles thread t of a register transform multiplies its k1-th value by,
@@ -330,7 +330,7 @@ int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n) {
     for (int k1 = 0; k1 < R; ++k1)
       for (int t = 0; t < T; ++t) tw2[(size_t)k1 * T + t] = tw[(t * k1) & (n - 1)];
     CUBE_CUDA_TRY(ctx, cudaMalloc(&p.tw2, sizeof(float2) * R * T));
-    CUBE_CUDA_TRY(ctx, cudaMemcpy(p.tw2, tw2.data(), sizeof(float2) * R * T, cudaMemcpyHostToDevice));
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(p.tw2, tw2.data(), sizeof(float2) * R * T, cudaMemcpyHostToDevice, ctx->stream));
   }
   return CUBE_OK;
 }

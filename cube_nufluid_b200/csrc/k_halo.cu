@@ -43,9 +43,17 @@
  * the moment accumulators start from zero for every halo (the reference never
  * resets its inertia, dx_mean and q-space sums).
  *
- * The halo loop runs in one CTA of 1024 threads that parallelises each halo's
- * gather, refined grid, sort and sums; distances and centres use explicitly
- * rounded FP64 operations so that the CPU restatement reproduces them bit for bit.
+ * A candidate is processed by one CTA, which parallelises its gather, refined grid,
+ * sort and sums.  Candidates are independent when their search balls do not meet
+ * (a candidate only gathers, and tags, untagged particles within its rsearch of its
+ * peak), so the host groups them into waves: a candidate goes one wave after the
+ * latest earlier candidate whose ball meets its own, and each wave runs as one
+ * launch of many CTAs, each with its own scratch slot.  A candidate a slot cannot
+ * hold (more particles or a larger refined grid) is left untouched and runs after
+ * its wave in a single CTA with the full-size scratch.  The result is the sequential
+ * one: halo numbers, records and member lists are assembled in candidate order at
+ * the end.  Distances and centres use explicitly rounded FP64 operations so that
+ * the CPU restatement reproduces them bit for bit.
  */
 #include "cube_internal.cuh"
 
@@ -62,6 +70,9 @@ constexpr int64_t GCAP = 1 << 22;       // particles gathered per halo (max_halo
 constexpr int CAND_CAP = 1 << 21;       // density peaks
 constexpr int RMAX = 64;                // radius of the shell list in fine cells
 constexpr int MIN_NP = 100;             // min_halo_particles (:37)
+constexpr int W_THREADS = 256;          // threads of a wave CTA
+constexpr int W_GCAP = 1 << 16;         // particles a wave slot gathers
+constexpr int W_NB = 72;                // refined cells per dimension a wave slot holds
 
 struct HaloCand {
   int64_t node;             // fine node index (x fastest)
@@ -177,6 +188,14 @@ __global__ void __launch_bounds__(256) k_halo_peaks(const unsigned long long* __
   }
 }
 
+// per-candidate result, assembled into the outputs in candidate order at the end
+struct HaloRec {
+  int is_halo;
+  int iodc;              // particles in the halo
+  long long moff;        // first of its member PIDs in the unordered member buffer
+  cube_halo H;
+};
+
 struct HaloArgs {
   const void* xp; const void* vp; const int32_t* pid; const int64_t* cell_start; const float* vfield;
   const double* dec;         // decoded velocity per code at sigma_vi, index code + nvbin/2
@@ -185,17 +204,34 @@ struct HaloArgs {
   int nc, nt, nnt, nf, ncb, ncell, cmax;
   double mass, den_odc, pi;  // particle mass; threshold; the reference's FP32 pi
   double vsim2phys, a, h0, box;
-  const HaloCand* cand; int ncand;
+  const HaloCand* cand;
   uint8_t* tag;              // per particle (storage index)
-  int32_t* hid; int64_t hid_len;         // halo number per PID - 1, or null
-  int32_t* member; int64_t member_cap;   // PIDs of each halo in radius order, or null
-  double* gx; double* gv;    // gathered positions / velocities [3][GCAP]
-  int64_t* gip;              // gathered storage indices
-  double* key;               // distance of each gathered particle
-  int32_t* ord;              // sort permutation
-  unsigned long long* grid;  // refined grid, (nb+3)^3 at most
-  cube_halo* out; int out_cap;
-  int* nhalo; long long* nmember; int* err;
+  HaloRec* rec;              // per candidate
+  int32_t* mtmp;             // member PIDs, unordered by candidate
+  long long* mcount;         // next free entry of mtmp
+  long long mcap;
+  int* err;                  // 2: refined grid beyond 300, 3: gather beyond GCAP, 4: box wraps
+  int* overflow;             // candidates a slot could not hold (wave kernel): [0] count, then indices
+};
+
+// scratch of one CTA: gathered particles (capacity gcap) and the refined grid
+struct HaloSlot {
+  double* gx; double* gv;    // [3][gcap]
+  int64_t* gip;
+  double* key;
+  int32_t* ord;
+  unsigned long long* grid;  // (nbmax + 3)^3
+  int gcap, nbmax;
+};
+
+struct HaloShared {
+  double hpos[3], rp, rs;
+  int flo[3], nbx[3], mx[3], clo[3], cn[3];
+  unsigned int cnt;
+  unsigned long long best;
+  int bidx, iodc, skip;
+  long long ws[32];
+  double red[33];
 };
 
 __device__ double block_sum(double v, double* red) {
@@ -251,325 +287,379 @@ __device__ __forceinline__ void search_cell(const int clo[3], const int cn[3], i
   *c = cube_cell_of(cube_wrap(cu[0] % nc, nc), cube_wrap(cu[1] % nc, nc), cube_wrap(cu[2] % nc, nc), nt, nnt);
 }
 
+// One candidate by the whole CTA (halofind.f90:231-513).  Returns 0 when done (halo or
+// not), 1 when the slot cannot hold it (nothing written, no particle tagged), and a
+// negative error code.  Every thread returns the same value.
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(H_THREADS) k_halo_seq(HaloArgs A) {
+__device__ int halo_candidate(const HaloArgs& A, int ic, const HaloSlot& S, HaloShared& sh, long long* s_first,
+                              long long* s_pref) {
   typedef typename CodeT<ZV>::T TV;
   const TV* vp = reinterpret_cast<const TV*>(A.vp);
-  extern __shared__ long long hsm[];
-  long long* s_first = hsm;                  // first storage index of each searched cell
-  long long* s_pref = hsm + A.cmax;          // exclusive prefix of their counts
-  __shared__ double hpos[3], sh_rp, sh_rs;
-  __shared__ int flo[3], nbx[3], mx[3], clo[3], cn[3];
-  __shared__ unsigned int s_cnt;
-  __shared__ unsigned long long s_best;
-  __shared__ int s_bidx, s_iodc, s_skip, s_nhalo;
-  __shared__ long long s_nmem, s_ws[32];
-  __shared__ double red[33];
   const int nf = A.nf, nc = A.nc, ncell = A.ncell;
   const double ng = 1.0 / 3.0, half_ng = 0.5 / 3.0;
-  if (threadIdx.x == 0) { s_nhalo = 0; s_nmem = 0; }
-  for (int ic = 0; ic < A.ncand; ++ic) {
-    __syncthreads();  // the previous candidate's shared values are consumed
-    if (threadIdx.x == 0) {
-      const HaloCand& h = A.cand[ic];
-      for (int d = 0; d < 3; ++d) hpos[d] = h.pos[d];
-      const double rp = h.rp;
-      const double rs = fmin(2.0 * rp, (double)((A.ncb - 1) * ncell));
-      sh_rp = rp;
-      sh_rs = rs;
-      int bad = 0;
+  __syncthreads();  // the previous candidate's shared values are consumed
+  if (threadIdx.x == 0) {
+    const HaloCand& h = A.cand[ic];
+    for (int d = 0; d < 3; ++d) sh.hpos[d] = h.pos[d];
+    const double rp = h.rp;
+    const double rs = fmin(2.0 * rp, (double)((A.ncb - 1) * ncell));
+    sh.rp = rp;
+    sh.rs = rs;
+    int bad = 0;
+    for (int d = 0; d < 3; ++d) {
+      sh.clo[d] = (int)floor((sh.hpos[d] - rs) / ncell);
+      sh.cn[d] = (int)floor((sh.hpos[d] + rs) / ncell) - sh.clo[d] + 1;
+      const int rlo = (int)floor((sh.hpos[d] - rp) / ncell), rhi = (int)floor((sh.hpos[d] + rp) / ncell);
+      sh.flo[d] = ncell * rlo;
+      sh.nbx[d] = 3 * ncell * (rhi - rlo + 1);
+      sh.mx[d] = min(sh.nbx[d] + 1, NB_MAX);
+      if (sh.nbx[d] > NB_MAX) bad = -2;
+      else if (sh.nbx[d] > S.nbmax && !bad) bad = 1;
+      if (sh.cn[d] > nc) bad = -4;
+    }
+    if (!bad && sh.cn[0] * sh.cn[1] * sh.cn[2] > A.cmax) bad = -4;
+    sh.cnt = 0;
+    sh.best = 0ull;
+    sh.bidx = 0x7fffffff;
+    sh.iodc = 0x7fffffff;
+    sh.skip = bad;
+  }
+  __syncthreads();
+  if (sh.skip) return sh.skip;
+  const int gxn = sh.nbx[0] + 3, gyn = sh.nbx[1] + 3, gzn = sh.nbx[2] + 3;
+  const int64_t gtot = (int64_t)gxn * gyn * gzn;
+  for (int64_t i = threadIdx.x; i < gtot; i += blockDim.x) S.grid[i] = 0ull;
+  // cells of the search box: first particle and count prefix
+  const int ncl = sh.cn[0] * sh.cn[1] * sh.cn[2];
+  const int per = (ncl + blockDim.x - 1) / blockDim.x;
+  const int q0 = min(ncl, (int)threadIdx.x * per), q1 = min(ncl, q0 + per);
+  long long mine = 0;
+  for (int q = q0; q < q1; ++q) {
+    int cu[3];
+    int64_t c;
+    search_cell(sh.clo, sh.cn, q, nc, A.nt, A.nnt, cu, &c);
+    s_first[q] = A.cell_start[c];
+    mine += A.cell_start[c + 1] - A.cell_start[c];
+  }
+  long long tot;
+  long long run = block_scan(mine, sh.ws, &tot);
+  for (int q = q0; q < q1; ++q) {
+    int cu[3];
+    int64_t c;
+    search_cell(sh.clo, sh.cn, q, nc, A.nt, A.nnt, cu, &c);
+    s_pref[q] = run;
+    run += A.cell_start[c + 1] - A.cell_start[c];
+  }
+  __syncthreads();
+  // gather the untagged particles within rsearch; CIC of those within r_proxy
+  const double rs = sh.rs, rpx = sh.rp;
+  const double hp[3] = {sh.hpos[0], sh.hpos[1], sh.hpos[2]};
+  const int flo[3] = {sh.flo[0], sh.flo[1], sh.flo[2]};
+  const int gcap = S.gcap;
+  for (long long t = threadIdx.x; t < tot; t += blockDim.x) {
+    int lo = 0, hi = ncl - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (s_pref[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const int64_t ip = s_first[lo] + (t - s_pref[lo]);
+    if (A.tag[ip]) continue;
+    int cu[3];
+    int64_t c;
+    search_cell(sh.clo, sh.cn, lo, nc, A.nt, A.nnt, cu, &c);
+    double x[3];
+    for (int d = 0; d < 3; ++d) x[d] = h_pos<ZX>(A.xp, A.cap, ip, d, cu[d]);  // unwrapped next to the peak
+    const double r = dist3(x, hp);
+    if (!(r < rs)) continue;
+    const unsigned int s = atomicAdd(&sh.cnt, 1u);
+    if (s < (unsigned)gcap) {
       for (int d = 0; d < 3; ++d) {
-        clo[d] = (int)floor((hpos[d] - rs) / ncell);
-        cn[d] = (int)floor((hpos[d] + rs) / ncell) - clo[d] + 1;
-        const int rlo = (int)floor((hpos[d] - rp) / ncell), rhi = (int)floor((hpos[d] + rp) / ncell);
-        flo[d] = ncell * rlo;
-        nbx[d] = 3 * ncell * (rhi - rlo + 1);
-        mx[d] = min(nbx[d] + 1, NB_MAX);
-        if (nbx[d] > NB_MAX) bad = 2;
-        if (cn[d] > nc && !bad) bad = 4;
+        S.gx[(size_t)d * gcap + s] = x[d];
+        const int code = (int)vp[(size_t)d * A.cap + ip];
+        S.gv[(size_t)d * gcap + s] = __dadd_rn(A.dec[code + A.half_nvbin], (double)A.vfield[(size_t)d * A.ncells + c]);
       }
-      if (!bad && cn[0] * cn[1] * cn[2] > A.cmax) bad = 4;
-      s_cnt = 0;
-      s_best = 0ull;
-      s_bidx = 0x7fffffff;
-      s_iodc = 0x7fffffff;
-      s_skip = 0;
-      if (bad) atomicCAS(A.err, 0, bad);
+      S.gip[s] = ip;
     }
-    __syncthreads();
-    if (*(volatile int*)A.err) break;
-    const int gxn = nbx[0] + 3, gyn = nbx[1] + 3, gzn = nbx[2] + 3;
-    const int64_t gtot = (int64_t)gxn * gyn * gzn;
-    for (int64_t i = threadIdx.x; i < gtot; i += blockDim.x) A.grid[i] = 0ull;
-    // cells of the search box: first particle and count prefix
-    const int ncl = cn[0] * cn[1] * cn[2];
-    const int per = (ncl + H_THREADS - 1) / H_THREADS;
-    const int q0 = min(ncl, (int)threadIdx.x * per), q1 = min(ncl, q0 + per);
-    long long mine = 0;
-    for (int q = q0; q < q1; ++q) {
-      int cu[3];
-      int64_t c;
-      search_cell(clo, cn, q, nc, A.nt, A.nnt, cu, &c);
-      s_first[q] = A.cell_start[c];
-      mine += A.cell_start[c + 1] - A.cell_start[c];
-    }
-    long long tot;
-    long long run = block_scan(mine, s_ws, &tot);
-    for (int q = q0; q < q1; ++q) {
-      int cu[3];
-      int64_t c;
-      search_cell(clo, cn, q, nc, A.nt, A.nnt, cu, &c);
-      s_pref[q] = run;
-      run += A.cell_start[c + 1] - A.cell_start[c];
-    }
-    __syncthreads();
-    // gather the untagged particles within rsearch; CIC of those within r_proxy
-    const double rs = sh_rs, rpx = sh_rp;
-    const double hp[3] = {hpos[0], hpos[1], hpos[2]};
-    for (long long t = threadIdx.x; t < tot; t += blockDim.x) {
-      int lo = 0, hi = ncl - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s_pref[mid] <= t) lo = mid; else hi = mid - 1;
-      }
-      const int64_t ip = s_first[lo] + (t - s_pref[lo]);
-      if (A.tag[ip]) continue;
-      int cu[3];
-      int64_t c;
-      search_cell(clo, cn, lo, nc, A.nt, A.nnt, cu, &c);
-      double x[3];
-      for (int d = 0; d < 3; ++d) x[d] = h_pos<ZX>(A.xp, A.cap, ip, d, cu[d]);  // unwrapped next to the peak
-      const double r = dist3(x, hp);
-      if (!(r < rs)) continue;
-      const unsigned int s = atomicAdd(&s_cnt, 1u);
-      if (s < GCAP) {
-        for (int d = 0; d < 3; ++d) {
-          A.gx[(size_t)d * GCAP + s] = x[d];
-          const int code = (int)vp[(size_t)d * A.cap + ip];
-          A.gv[(size_t)d * GCAP + s] = __dadd_rn(A.dec[code + A.half_nvbin], (double)A.vfield[(size_t)d * A.ncells + c]);
-        }
-        A.gip[s] = ip;
-      }
-      if (r < rpx) {  // nodes at refined-cell centres, 1-based refined index
-        int i1[3];
-        double w1[3], w2[3];
-        for (int d = 0; d < 3; ++d) {
-          const double p = __ddiv_rn(__dsub_rn(__dsub_rn(x[d], half_ng), (double)flo[d]), ng);
-          const double f = floor(p);
-          w1[d] = (f + 1.0) - p;
-          w2[d] = 1.0 - w1[d];
-          i1[d] = (int)f + 1;
-        }
-        for (int cc = 0; cc < 8; ++cc) {
-          const int ox = cc & 1, oy = (cc >> 1) & 1, oz = cc >> 2;
-          const int ix = i1[0] + ox, iy = i1[1] + oy, iz = i1[2] + oz;
-          if (ix < 0 || iy < 0 || iz < 0 || ix >= gxn || iy >= gyn || iz >= gzn) continue;
-          const double w = __dmul_rn(__dmul_rn(ox ? w2[0] : w1[0], oy ? w2[1] : w1[1]), oz ? w2[2] : w1[2]);
-          atomicAdd(&A.grid[((size_t)iz * gyn + iy) * gxn + ix], (unsigned long long)__double2ll_rn(w * HFIX));
-        }
-      }
-    }
-    __syncthreads();
-    const unsigned int nraw = s_cnt;
-    if (nraw > (unsigned)GCAP) {
-      if (threadIdx.x == 0) atomicCAS(A.err, 0, 3);
-      break;
-    }
-    const int n = (int)nraw;
-    // refined maximum: the first one in x-fastest order over nodes 1..min(nb+1, 300)
-    unsigned long long bv = 0ull;
-    int bi = 0x7fffffff;
-    const int64_t inner = (int64_t)mx[0] * mx[1] * mx[2];
-    for (int64_t i = threadIdx.x; i < inner; i += blockDim.x) {
-      const int ix = (int)(i % mx[0]) + 1, iy = (int)((i / mx[0]) % mx[1]) + 1, iz = (int)(i / ((int64_t)mx[0] * mx[1])) + 1;
-      const unsigned long long v = A.grid[((size_t)iz * gyn + iy) * gxn + ix];
-      if (v > bv || (v == bv && (int)i < bi)) { bv = v; bi = (int)i; }
-    }
-    atomicMax(&s_best, bv);
-    __syncthreads();
-    if (bv == s_best) atomicMin(&s_bidx, bi);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const int i = s_bidx;
-      const int i0 = i % mx[0] + 1, j0 = (i / mx[0]) % mx[1] + 1, k0 = i / (mx[0] * mx[1]) + 1;
-      auto g = [&](int a, int b, int c) { return (long long)A.grid[((size_t)c * gyn + b) * gxn + a]; };
-      const long long g0 = g(i0, j0, k0);
-      const long long dxn = 2 * g0 - g(i0 - 1, j0, k0) - g(i0 + 1, j0, k0);
-      const long long dyn = 2 * g0 - g(i0, j0 - 1, k0) - g(i0, j0 + 1, k0);
-      const long long dzn = 2 * g0 - g(i0, j0, k0 - 1) - g(i0, j0, k0 - 1);  // the reference's z denominator
-      if (dxn == 0 || dyn == 0 || dzn == 0) {
-        s_skip = 1;
-      } else {
-        const double hr[3] = {(i0 - 0.5) + parab(g(i0 - 1, j0, k0), g(i0 + 1, j0, k0), dxn),
-                              (j0 - 0.5) + parab(g(i0, j0 - 1, k0), g(i0, j0 + 1, k0), dyn),
-                              (k0 - 0.5) + parab(g(i0, j0, k0 - 1), g(i0, j0, k0 + 1), dzn)};
-        for (int d = 0; d < 3; ++d) hpos[d] = __dadd_rn((double)flo[d], __dmul_rn(ng, hr[d]));
-      }
-    }
-    __syncthreads();
-    if (s_skip) continue;
-    // distances from the refined centre; sort by (distance, storage index)
-    const double hc[3] = {hpos[0], hpos[1], hpos[2]};
-    int np2 = 1;
-    while (np2 < n) np2 <<= 1;
-    for (int i = threadIdx.x; i < np2; i += blockDim.x) {
-      if (i < n) {
-        const double x[3] = {A.gx[i], A.gx[(size_t)GCAP + i], A.gx[2 * (size_t)GCAP + i]};
-        A.key[i] = dist3(x, hc);
-      }
-      A.ord[i] = i;
-    }
-    __syncthreads();
-    for (int k = 2; k <= np2; k <<= 1)
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int i = threadIdx.x; i < np2; i += blockDim.x) {
-          const int l = i ^ j;
-          if (l > i) {
-            const int a = A.ord[i], b = A.ord[l];
-            bool gt;
-            if (a >= n || b >= n) {
-              gt = a >= n && (b < n || a > b);  // padding sorts last
-            } else {
-              const double ka = A.key[a], kb = A.key[b];
-              gt = ka > kb || (ka == kb && A.gip[a] > A.gip[b]);
-            }
-            if (gt == ((i & k) == 0)) { A.ord[i] = b; A.ord[l] = a; }
-          }
-        }
-        __syncthreads();
-      }
-    // i_odc: the first ii >= 2 (1-based) whose enclosed density is below den_odc
-    const double c43 = 0.75 / A.pi;
-    for (int ii = threadIdx.x + 2; ii <= n; ii += blockDim.x) {
-      const double r = A.key[A.ord[ii - 1]];
-      if (c43 * ii * A.mass / (r * r * r) < A.den_odc) atomicMin(&s_iodc, ii);
-    }
-    __syncthreads();
-    const int iis = s_iodc;
-    const int iodc = iis == 0x7fffffff ? 0 : iis - 1;
-    if (iodc < MIN_NP) continue;
-    // a halo: tag its particles, record the PIDs
-    const int hnum = s_nhalo;
-    const long long moff = s_nmem;
-    for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
-      const int64_t ip = A.gip[A.ord[i]];
-      A.tag[ip] = 1;
-      if (A.use_pid) {
-        const int32_t p = A.pid[ip];
-        if (A.hid && p >= 1 && p <= A.hid_len) A.hid[p - 1] = hnum + 1;
-        if (A.member && moff + i < A.member_cap) A.member[moff + i] = p;
-      }
-    }
-    double xm[3], vm[3], xl[3] = {0, 0, 0}, vl[3] = {0, 0, 0};
-    for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
-      const int o = A.ord[i];
+    if (r < rpx) {  // nodes at refined-cell centres, 1-based refined index
+      int i1[3];
+      double w1[3], w2[3];
       for (int d = 0; d < 3; ++d) {
-        xl[d] += A.gx[(size_t)d * GCAP + o];
-        vl[d] += A.gv[(size_t)d * GCAP + o];
+        const double p = __ddiv_rn(__dsub_rn(__dsub_rn(x[d], half_ng), (double)flo[d]), ng);
+        const double f = floor(p);
+        w1[d] = (f + 1.0) - p;
+        w2[d] = 1.0 - w1[d];
+        i1[d] = (int)f + 1;
       }
-    }
-    for (int d = 0; d < 3; ++d) xm[d] = block_sum(xl[d], red) / iodc;
-    for (int d = 0; d < 3; ++d) vm[d] = block_sum(vl[d], red) / iodc;
-    double xw[3];
-    for (int d = 0; d < 3; ++d) xw[d] = pmod(xm[d], (double)nf);
-    // second moments about the means; Lagrangian offsets from the wrapped mean
-    double sxx[3] = {0, 0, 0}, svv = 0, am[3] = {0, 0, 0}, in[6] = {0, 0, 0, 0, 0, 0}, dq[3] = {0, 0, 0}, nq = 0;
-    const long long nfl = nf;
-    const double hnf = (double)(nf / 2);
-    for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
-      const int o = A.ord[i];
-      double dx[3], v[3];
-      for (int d = 0; d < 3; ++d) {
-        dx[d] = A.gx[(size_t)d * GCAP + o] - xm[d];
-        v[d] = A.gv[(size_t)d * GCAP + o];
-        sxx[d] += dx[d] * dx[d];
-        svv += (v[d] - vm[d]) * (v[d] - vm[d]);
+      for (int cc = 0; cc < 8; ++cc) {
+        const int ox = cc & 1, oy = (cc >> 1) & 1, oz = cc >> 2;
+        const int ix = i1[0] + ox, iy = i1[1] + oy, iz = i1[2] + oz;
+        if (ix < 0 || iy < 0 || iz < 0 || ix >= gxn || iy >= gyn || iz >= gzn) continue;
+        const double w = __dmul_rn(__dmul_rn(ox ? w2[0] : w1[0], oy ? w2[1] : w1[1]), oz ? w2[2] : w1[2]);
+        atomicAdd(&S.grid[((size_t)iz * gyn + iy) * gxn + ix], (unsigned long long)__double2ll_rn(w * HFIX));
       }
-      am[0] += dx[1] * v[2] - dx[2] * v[1];
-      am[1] += dx[2] * v[0] - dx[0] * v[2];
-      am[2] += dx[0] * v[1] - dx[1] * v[0];
-      in[0] += dx[0] * dx[0]; in[1] += dx[1] * dx[1]; in[2] += dx[2] * dx[2];
-      in[3] += dx[0] * dx[1]; in[4] += dx[1] * dx[2]; in[5] += dx[2] * dx[0];
-      if (A.use_pid) {
-        const long long qt = (long long)A.pid[A.gip[o]] - 1;
-        if (qt >= 0) {
-          const long long qz = qt / (nfl * nfl), qy = (qt - qz * nfl * nfl) / nfl, qx = qt % nfl;
-          const double qp[3] = {qx + 0.5, qy + 0.5, qz + 0.5};
-          for (int d = 0; d < 3; ++d) dq[d] += pmod(__dadd_rn(__dsub_rn(qp[d], xw[d]), hnf), (double)nf) - hnf;
-          nq += 1.0;
-        }
-      }
-    }
-    for (int d = 0; d < 3; ++d) sxx[d] = block_sum(sxx[d], red);
-    svv = block_sum(svv, red);
-    for (int d = 0; d < 3; ++d) am[d] = block_sum(am[d], red);
-    for (int q = 0; q < 6; ++q) in[q] = block_sum(in[q], red);
-    for (int d = 0; d < 3; ++d) dq[d] = block_sum(dq[d], red);
-    nq = block_sum(nq, red);
-    double qm[3] = {0, 0, 0}, iq[6] = {0, 0, 0, 0, 0, 0};
-    if (A.use_pid && nq > 0) {
-      for (int d = 0; d < 3; ++d) qm[d] = pmod(xw[d] + dq[d] / nq, (double)nf);
-      for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
-        const long long qt = (long long)A.pid[A.gip[A.ord[i]]] - 1;
-        if (qt < 0) continue;
-        const long long qz = qt / (nfl * nfl), qy = (qt - qz * nfl * nfl) / nfl, qx = qt % nfl;
-        const double qp[3] = {qx + 0.5, qy + 0.5, qz + 0.5};
-        double e[3];
-        for (int d = 0; d < 3; ++d)  // the reference adds 1/2 once more here
-          e[d] = pmod(__dadd_rn(__dsub_rn(__dadd_rn(qp[d], 0.5), qm[d]), hnf), (double)nf) - hnf;
-        iq[0] += e[0] * e[0]; iq[1] += e[1] * e[1]; iq[2] += e[2] * e[2];
-        iq[3] += e[0] * e[1]; iq[4] += e[1] * e[2]; iq[5] += e[2] * e[0];
-      }
-      for (int q = 0; q < 6; ++q) iq[q] = block_sum(iq[q], red);
-    }
-    if (threadIdx.x == 0) {
-      cube_halo H;
-      for (int d = 0; d < 3; ++d) H.hpos[d] = (float)pmod(hpos[d], (double)nf);
-      H.mass_odc = (float)iodc;
-      {
-        const double r2 = A.key[A.ord[iis - 1]], r1 = A.key[A.ord[iis - 2]];
-        const double den2 = c43 * iis * A.mass / (r2 * r2 * r2), den1 = c43 * (iis - 1) * A.mass / (r1 * r1 * r1);
-        const double lr2 = log10(r2), lr1 = log10(r1), d2 = log10(den2), d1 = log10(den1), lo = log10(A.den_odc);
-        H.radius_odc = (float)pow(10.0, ((lo - d2) * lr1 + (d1 - lo) * lr2) / (d1 - d2));
-      }
-      H.v_disp = (float)sqrt(svv / (iodc - 1));
-      for (int d = 0; d < 3; ++d) {
-        H.x_mean[d] = (float)xw[d];
-        H.v_mean[d] = (float)vm[d];
-        H.var_x[d] = (float)(sxx[d] / (iodc - 1));
-        H.ang_mom[d] = (float)am[d];
-        H.q_mean[d] = (float)qm[d];
-      }
-      const int sym[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};  // (3,3) column-major from xx,yy,zz,xy,yz,zx
-      for (int k = 0; k < 9; ++k) {
-        H.inertia[k] = (float)in[sym[k]];
-        H.inertia_q[k] = (float)iq[sym[k]];
-      }
-      // redshift-space mean position along the line of sight (:425-430)
-      double los[3], ln = 0.0, vlos = 0.0;
-      const double cen[3] = {30.0, 370.0, 370.0};
-      for (int d = 0; d < 3; ++d) {
-        los[d] = xw[d] - cen[d] / 500.0 * (double)nc;
-        ln += los[d] * los[d];
-      }
-      ln = sqrt(ln);
-      for (int d = 0; d < 3; ++d) {
-        los[d] /= ln;
-        vlos += vm[d] * los[d];
-      }
-      for (int d = 0; d < 3; ++d) {
-        const double sx = vlos * los[d] * A.vsim2phys / A.a / (100.0 * A.h0) / (A.h0 * A.box / nf);
-        H.s_mean[d] = (float)pmod(xw[d] + sx, (double)nf);
-      }
-      if (hnum < A.out_cap) A.out[hnum] = H;
-      s_nhalo = hnum + 1;
-      if (A.use_pid) s_nmem = moff + iodc;
     }
   }
   __syncthreads();
+  const unsigned int nraw = sh.cnt;
+  if (nraw > (unsigned)gcap) return gcap < GCAP ? 1 : -3;
+  const int n = (int)nraw;
+  // refined maximum: the first one in x-fastest order over nodes 1..min(nb+1, 300)
+  unsigned long long bv = 0ull;
+  int bi = 0x7fffffff;
+  const int mx0 = sh.mx[0], mx1 = sh.mx[1], mx2 = sh.mx[2];
+  const int64_t inner = (int64_t)mx0 * mx1 * mx2;
+  for (int64_t i = threadIdx.x; i < inner; i += blockDim.x) {
+    const int ix = (int)(i % mx0) + 1, iy = (int)((i / mx0) % mx1) + 1, iz = (int)(i / ((int64_t)mx0 * mx1)) + 1;
+    const unsigned long long v = S.grid[((size_t)iz * gyn + iy) * gxn + ix];
+    if (v > bv || (v == bv && (int)i < bi)) { bv = v; bi = (int)i; }
+  }
+  atomicMax(&sh.best, bv);
+  __syncthreads();
+  if (bv == sh.best) atomicMin(&sh.bidx, bi);
+  __syncthreads();
   if (threadIdx.x == 0) {
-    *A.nhalo = s_nhalo;
-    *A.nmember = s_nmem;
+    const int i = sh.bidx;
+    const int i0 = i % mx0 + 1, j0 = (i / mx0) % mx1 + 1, k0 = i / (mx0 * mx1) + 1;
+    auto g = [&](int a, int b, int c) { return (long long)S.grid[((size_t)c * gyn + b) * gxn + a]; };
+    const long long g0 = g(i0, j0, k0);
+    const long long dxn = 2 * g0 - g(i0 - 1, j0, k0) - g(i0 + 1, j0, k0);
+    const long long dyn = 2 * g0 - g(i0, j0 - 1, k0) - g(i0, j0 + 1, k0);
+    const long long dzn = 2 * g0 - g(i0, j0, k0 - 1) - g(i0, j0, k0 - 1);  // the reference's z denominator
+    if (dxn == 0 || dyn == 0 || dzn == 0) {
+      sh.skip = 2;
+    } else {
+      const double hr[3] = {(i0 - 0.5) + parab(g(i0 - 1, j0, k0), g(i0 + 1, j0, k0), dxn),
+                            (j0 - 0.5) + parab(g(i0, j0 - 1, k0), g(i0, j0 + 1, k0), dyn),
+                            (k0 - 0.5) + parab(g(i0, j0, k0 - 1), g(i0, j0, k0 + 1), dzn)};
+      for (int d = 0; d < 3; ++d) sh.hpos[d] = __dadd_rn((double)flo[d], __dmul_rn(ng, hr[d]));
+    }
+  }
+  __syncthreads();
+  if (sh.skip) return 0;  // a zero denominator: not a halo
+  // distances from the refined centre; sort by (distance, storage index)
+  const double hc[3] = {sh.hpos[0], sh.hpos[1], sh.hpos[2]};
+  int np2 = 1;
+  while (np2 < n) np2 <<= 1;
+  for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+    if (i < n) {
+      const double x[3] = {S.gx[i], S.gx[(size_t)gcap + i], S.gx[2 * (size_t)gcap + i]};
+      S.key[i] = dist3(x, hc);
+    }
+    S.ord[i] = i;
+  }
+  __syncthreads();
+  for (int k = 2; k <= np2; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < np2; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) {
+          const int a = S.ord[i], b = S.ord[l];
+          bool gt;
+          if (a >= n || b >= n) {
+            gt = a >= n && (b < n || a > b);  // padding sorts last
+          } else {
+            const double ka = S.key[a], kb = S.key[b];
+            gt = ka > kb || (ka == kb && S.gip[a] > S.gip[b]);
+          }
+          if (gt == ((i & k) == 0)) { S.ord[i] = b; S.ord[l] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  // i_odc: the first ii >= 2 (1-based) whose enclosed density is below den_odc
+  const double c43 = 0.75 / A.pi;
+  for (int ii = threadIdx.x + 2; ii <= n; ii += blockDim.x) {
+    const double r = S.key[S.ord[ii - 1]];
+    if (c43 * ii * A.mass / (r * r * r) < A.den_odc) atomicMin(&sh.iodc, ii);
+  }
+  __syncthreads();
+  const int iis = sh.iodc;
+  const int iodc = iis == 0x7fffffff ? 0 : iis - 1;
+  if (iodc < MIN_NP) return 0;
+  // a halo: tag its particles, record its PIDs
+  __shared__ long long s_moff;
+  if (threadIdx.x == 0)
+    s_moff = A.use_pid ? (long long)atomicAdd(reinterpret_cast<unsigned long long*>(A.mcount),
+                                              (unsigned long long)iodc)
+                       : 0;
+  __syncthreads();
+  const long long moff = s_moff;
+  for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
+    const int64_t ip = S.gip[S.ord[i]];
+    A.tag[ip] = 1;
+    if (A.use_pid && moff + i < A.mcap) A.mtmp[moff + i] = A.pid[ip];
+  }
+  double xm[3], vm[3], xl[3] = {0, 0, 0}, vl[3] = {0, 0, 0};
+  for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
+    const int o = S.ord[i];
+    for (int d = 0; d < 3; ++d) {
+      xl[d] += S.gx[(size_t)d * gcap + o];
+      vl[d] += S.gv[(size_t)d * gcap + o];
+    }
+  }
+  for (int d = 0; d < 3; ++d) xm[d] = block_sum(xl[d], sh.red) / iodc;
+  for (int d = 0; d < 3; ++d) vm[d] = block_sum(vl[d], sh.red) / iodc;
+  double xw[3];
+  for (int d = 0; d < 3; ++d) xw[d] = pmod(xm[d], (double)nf);
+  // second moments about the means; Lagrangian offsets from the wrapped mean
+  double sxx[3] = {0, 0, 0}, svv = 0, am[3] = {0, 0, 0}, in[6] = {0, 0, 0, 0, 0, 0}, dq[3] = {0, 0, 0}, nq = 0;
+  const long long nfl = nf;
+  const double hnf = (double)(nf / 2);
+  for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
+    const int o = S.ord[i];
+    double dx[3], v[3];
+    for (int d = 0; d < 3; ++d) {
+      dx[d] = S.gx[(size_t)d * gcap + o] - xm[d];
+      v[d] = S.gv[(size_t)d * gcap + o];
+      sxx[d] += dx[d] * dx[d];
+      svv += (v[d] - vm[d]) * (v[d] - vm[d]);
+    }
+    am[0] += dx[1] * v[2] - dx[2] * v[1];
+    am[1] += dx[2] * v[0] - dx[0] * v[2];
+    am[2] += dx[0] * v[1] - dx[1] * v[0];
+    in[0] += dx[0] * dx[0]; in[1] += dx[1] * dx[1]; in[2] += dx[2] * dx[2];
+    in[3] += dx[0] * dx[1]; in[4] += dx[1] * dx[2]; in[5] += dx[2] * dx[0];
+    if (A.use_pid) {
+      const long long qt = (long long)A.pid[S.gip[o]] - 1;
+      if (qt >= 0) {
+        const long long qz = qt / (nfl * nfl), qy = (qt - qz * nfl * nfl) / nfl, qx = qt % nfl;
+        const double qp[3] = {qx + 0.5, qy + 0.5, qz + 0.5};
+        for (int d = 0; d < 3; ++d) dq[d] += pmod(__dadd_rn(__dsub_rn(qp[d], xw[d]), hnf), (double)nf) - hnf;
+        nq += 1.0;
+      }
+    }
+  }
+  for (int d = 0; d < 3; ++d) sxx[d] = block_sum(sxx[d], sh.red);
+  svv = block_sum(svv, sh.red);
+  for (int d = 0; d < 3; ++d) am[d] = block_sum(am[d], sh.red);
+  for (int q = 0; q < 6; ++q) in[q] = block_sum(in[q], sh.red);
+  for (int d = 0; d < 3; ++d) dq[d] = block_sum(dq[d], sh.red);
+  nq = block_sum(nq, sh.red);
+  double qm[3] = {0, 0, 0}, iq[6] = {0, 0, 0, 0, 0, 0};
+  if (A.use_pid && nq > 0) {
+    for (int d = 0; d < 3; ++d) qm[d] = pmod(xw[d] + dq[d] / nq, (double)nf);
+    for (int i = threadIdx.x; i < iodc; i += blockDim.x) {
+      const long long qt = (long long)A.pid[S.gip[S.ord[i]]] - 1;
+      if (qt < 0) continue;
+      const long long qz = qt / (nfl * nfl), qy = (qt - qz * nfl * nfl) / nfl, qx = qt % nfl;
+      const double qp[3] = {qx + 0.5, qy + 0.5, qz + 0.5};
+      double e[3];
+      for (int d = 0; d < 3; ++d)  // the reference adds 1/2 once more here
+        e[d] = pmod(__dadd_rn(__dsub_rn(__dadd_rn(qp[d], 0.5), qm[d]), hnf), (double)nf) - hnf;
+      iq[0] += e[0] * e[0]; iq[1] += e[1] * e[1]; iq[2] += e[2] * e[2];
+      iq[3] += e[0] * e[1]; iq[4] += e[1] * e[2]; iq[5] += e[2] * e[0];
+    }
+    for (int q = 0; q < 6; ++q) iq[q] = block_sum(iq[q], sh.red);
+  }
+  if (threadIdx.x == 0) {
+    HaloRec& R = A.rec[ic];
+    cube_halo& H = R.H;
+    for (int d = 0; d < 3; ++d) H.hpos[d] = (float)pmod(sh.hpos[d], (double)nf);
+    H.mass_odc = (float)iodc;
+    {
+      const double r2 = S.key[S.ord[iis - 1]], r1 = S.key[S.ord[iis - 2]];
+      const double den2 = c43 * iis * A.mass / (r2 * r2 * r2), den1 = c43 * (iis - 1) * A.mass / (r1 * r1 * r1);
+      const double lr2 = log10(r2), lr1 = log10(r1), d2 = log10(den2), d1 = log10(den1), lo = log10(A.den_odc);
+      H.radius_odc = (float)pow(10.0, ((lo - d2) * lr1 + (d1 - lo) * lr2) / (d1 - d2));
+    }
+    H.v_disp = (float)sqrt(svv / (iodc - 1));
+    for (int d = 0; d < 3; ++d) {
+      H.x_mean[d] = (float)xw[d];
+      H.v_mean[d] = (float)vm[d];
+      H.var_x[d] = (float)(sxx[d] / (iodc - 1));
+      H.ang_mom[d] = (float)am[d];
+      H.q_mean[d] = (float)qm[d];
+    }
+    const int sym[9] = {0, 3, 5, 3, 1, 4, 5, 4, 2};  // (3,3) column-major from xx,yy,zz,xy,yz,zx
+    for (int k = 0; k < 9; ++k) {
+      H.inertia[k] = (float)in[sym[k]];
+      H.inertia_q[k] = (float)iq[sym[k]];
+    }
+    // redshift-space mean position along the line of sight (:425-430)
+    double los[3], ln = 0.0, vlos = 0.0;
+    const double cen[3] = {30.0, 370.0, 370.0};
+    for (int d = 0; d < 3; ++d) {
+      los[d] = xw[d] - cen[d] / 500.0 * (double)nc;
+      ln += los[d] * los[d];
+    }
+    ln = sqrt(ln);
+    for (int d = 0; d < 3; ++d) {
+      los[d] /= ln;
+      vlos += vm[d] * los[d];
+    }
+    for (int d = 0; d < 3; ++d) {
+      const double sx = vlos * los[d] * A.vsim2phys / A.a / (100.0 * A.h0) / (A.h0 * A.box / nf);
+      H.s_mean[d] = (float)pmod(xw[d] + sx, (double)nf);
+    }
+    R.iodc = iodc;
+    R.moff = moff;
+    R.is_halo = 1;
+  }
+  return 0;
+}
+
+// candidates list[0..n) one after the other in one CTA (large ones, or every one)
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(H_THREADS) k_halo_seq(HaloArgs A, const int* __restrict__ list, int n, HaloSlot S) {
+  extern __shared__ long long hsm[];
+  __shared__ HaloShared sh;
+  for (int i = 0; i < n; ++i) {
+    const int rc = halo_candidate<ZX, ZV>(A, list[i], S, sh, hsm, hsm + A.cmax);
+    if (rc < 0) {
+      if (threadIdx.x == 0) atomicCAS(A.err, 0, -rc);
+      return;
+    }
+  }
+}
+
+// one wave of mutually independent candidates: CTA b takes list[b], list[b + grid], ...
+// with its own slot; candidates a slot cannot hold go to the overflow list untouched
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(W_THREADS) k_halo_wave(HaloArgs A, const int* __restrict__ list, int n,
+                                                         HaloSlot S0, size_t gstride, size_t grid_stride) {
+  extern __shared__ long long hsm[];
+  __shared__ HaloShared sh;
+  HaloSlot S = S0;
+  S.gx += (size_t)blockIdx.x * 3 * gstride;
+  S.gv += (size_t)blockIdx.x * 3 * gstride;
+  S.gip += (size_t)blockIdx.x * gstride;
+  S.key += (size_t)blockIdx.x * gstride;
+  S.ord += (size_t)blockIdx.x * gstride;
+  S.grid += (size_t)blockIdx.x * grid_stride;
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int rc = halo_candidate<ZX, ZV>(A, list[i], S, sh, hsm, hsm + A.cmax);
+    if (rc < 0) {
+      if (threadIdx.x == 0) atomicCAS(A.err, 0, -rc);
+      return;
+    }
+    if (rc == 1 && threadIdx.x == 0) A.overflow[1 + atomicAdd(A.overflow, 1)] = list[i];
+  }
+}
+
+__global__ void k_halo_flags(const HaloRec* __restrict__ rec, int n, int2* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = make_int2(rec[i].is_halo, rec[i].iodc);
+}
+
+// the outputs in candidate order: halo number k+1 for the k-th halo, its record,
+// its member PIDs at the running offset, hid per member PID
+__global__ void k_halo_emit(const HaloRec* __restrict__ rec, const int* __restrict__ hnum,
+                            const long long* __restrict__ foff, const int* __restrict__ halo_ids, int nh,
+                            const int32_t* __restrict__ mtmp, cube_halo* __restrict__ out, int out_cap,
+                            int32_t* __restrict__ member, long long member_cap, int32_t* __restrict__ hid,
+                            long long hid_len, int use_pid) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  const int nw = (gridDim.x * blockDim.x) >> 5;
+  for (int k = warp; k < nh; k += nw) {
+    const int ic = halo_ids[k];
+    const HaloRec& R = rec[ic];
+    if (lane == 0 && k < out_cap) out[k] = R.H;
+    if (!use_pid) continue;
+    for (int i = lane; i < R.iodc; i += 32) {
+      const int32_t p = mtmp[R.moff + i];
+      if (member && foff[k] + i < member_cap) member[foff[k] + i] = p;
+      if (hid && p >= 1 && p <= hid_len) hid[p - 1] = hnum[k];
+    }
   }
 }
 
@@ -603,6 +693,54 @@ struct HaloScratch {
     return e;
   }
 };
+
+// Waves: candidate j depends on an earlier candidate i when their search balls meet
+// (i tags only particles within its rsearch of its peak, j gathers only within its
+// own), wave(j) = 1 + the largest wave of those, 0 if none.  Candidates of one wave
+// share no particle, so running them at once gives the sequential result.
+std::vector<int> halo_waves(const std::vector<HaloCand>& hc, const std::vector<double>& rs, int nf, int* nwaves) {
+  const int n = (int)hc.size();
+  std::vector<int> wave(n, 0);
+  double rmax = 0.0;
+  for (double r : rs) rmax = std::max(rmax, r);
+  const double reach = 2.0 * rmax + 1e-6;
+  const int G = std::max(1, (int)std::floor(nf / std::max(reach, 1e-9)));  // buckets per dimension
+  const double bw = (double)nf / G;
+  std::vector<std::vector<int>> bucket((size_t)G * G * G);
+  auto bidx = [&](double x) { int b = (int)std::floor(x / bw); return ((b % G) + G) % G; };
+  int w_max = -1;
+  for (int j = 0; j < n; ++j) {
+    const int bj[3] = {bidx(hc[j].pos[0]), bidx(hc[j].pos[1]), bidx(hc[j].pos[2])};
+    int w = 0;
+    const int span = G >= 3 ? 1 : 0;
+    auto visit = [&](int b) {
+      for (int i : bucket[b]) {
+        double d2 = 0.0;
+        for (int d = 0; d < 3; ++d) {
+          double dd = std::fabs(hc[i].pos[d] - hc[j].pos[d]);
+          dd = std::fmod(dd, (double)nf);
+          dd = std::min(dd, (double)nf - dd);
+          d2 += dd * dd;
+        }
+        const double lim = rs[i] + rs[j] + 1e-6;
+        if (d2 < lim * lim) w = std::max(w, wave[i] + 1);
+      }
+    };
+    if (G < 3) {
+      for (size_t b = 0; b < bucket.size(); ++b) visit((int)b);
+    } else {
+      for (int dz = -span; dz <= span; ++dz)
+        for (int dy = -span; dy <= span; ++dy)
+          for (int dx = -span; dx <= span; ++dx)
+            visit((((bj[2] + dz + G) % G) * G + (bj[1] + dy + G) % G) * G + (bj[0] + dx + G) % G);
+    }
+    wave[j] = w;
+    w_max = std::max(w_max, w);
+    bucket[((size_t)bj[2] * G + bj[1]) * G + bj[0]].push_back(j);
+  }
+  *nwaves = w_max + 1;
+  return wave;
+}
 
 template <int ZX, int ZV>
 int run_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* ha, cube_halo_result* res) {
@@ -650,13 +788,31 @@ int run_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* ha
   res->npeak = (int32_t)nc_h;
   // densest first, ties by node index; r_proxy = (3 m/(4 pi den_odc))^(1/3)
   std::vector<HaloCand> hc(nc_h);
-  if (nc_h) CUBE_CUDA_TRY(ctx, cudaMemcpy(hc.data(), cand, sizeof(HaloCand) * nc_h, cudaMemcpyDeviceToHost));
+  if (nc_h) {
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(hc.data(), cand, sizeof(HaloCand) * nc_h, cudaMemcpyDeviceToHost, ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   std::sort(hc.begin(), hc.end(), [](const HaloCand& a, const HaloCand& b) {
     return a.acc != b.acc ? a.acc > b.acc : a.node < b.node;
   });
   const double pi = (double)ctx->codec.pi_f;
-  for (HaloCand& h : hc) h.rp = std::cbrt(0.75 / pi / den_odc * h.mass);
-  if (nc_h) CUBE_CUDA_TRY(ctx, cudaMemcpy(cand, hc.data(), sizeof(HaloCand) * nc_h, cudaMemcpyHostToDevice));
+  std::vector<double> rsv(nc_h);
+  for (size_t i = 0; i < nc_h; ++i) {
+    hc[i].rp = std::cbrt(0.75 / pi / den_odc * hc[i].mass);
+    rsv[i] = std::min(2.0 * hc[i].rp, (double)((ctx->ncb - 1) * ctx->ncell));
+  }
+  if (nc_h)
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(cand, hc.data(), sizeof(HaloCand) * nc_h, cudaMemcpyHostToDevice, ctx->stream));
+  // waves of independent candidates, each wave's members in candidate order
+  int nwaves = 0;
+  const std::vector<int> wave = halo_waves(hc, rsv, nf, &nwaves);
+  std::vector<int> wstart(nwaves + 1, 0), order(nc_h);
+  for (size_t i = 0; i < nc_h; ++i) wstart[wave[i] + 1]++;
+  for (int w = 0; w < nwaves; ++w) wstart[w + 1] += wstart[w];
+  {
+    std::vector<int> fill(wstart.begin(), wstart.end() - 1);
+    for (size_t i = 0; i < nc_h; ++i) order[fill[wave[i]]++] = (int)i;
+  }
   HaloArgs A;
   A.xp = ctx->xp; A.vp = ctx->vp; A.pid = ctx->pid; A.cell_start = ctx->cell_start; A.vfield = ctx->vfield;
   int rc = 0;
@@ -669,60 +825,130 @@ int run_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* ha
   A.cmax = cmax;
   A.mass = mass; A.den_odc = den_odc; A.pi = pi;
   A.vsim2phys = io->vsim2phys; A.a = io->a; A.h0 = ctx->P.h0; A.box = ctx->P.box;
-  A.cand = cand; A.ncand = (int)nc_h;
+  A.cand = cand;
   const size_t npb = (size_t)std::max<int64_t>(ctx->np, 1);
   CUBE_CUDA_TRY(ctx, S.get(&A.tag, npb));
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(A.tag, 0, npb, ctx->stream));
-  A.hid = nullptr;
-  A.hid_len = ha->hid_len;
-  if (ha->hid && ha->hid_len > 0) {
-    CUBE_CUDA_TRY(ctx, S.get(&A.hid, 4 * (size_t)ha->hid_len));
-    CUBE_CUDA_TRY(ctx, cudaMemsetAsync(A.hid, 0, 4 * (size_t)ha->hid_len, ctx->stream));
+  CUBE_CUDA_TRY(ctx, S.get(&A.rec, sizeof(HaloRec) * std::max<size_t>(nc_h, 1)));
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(A.rec, 0, sizeof(HaloRec) * std::max<size_t>(nc_h, 1), ctx->stream));
+  A.mcap = (long long)npb;  // members are distinct particles
+  CUBE_CUDA_TRY(ctx, S.get(&A.mtmp, 4 * npb));
+  int* dlists;
+  CUBE_CUDA_TRY(ctx, S.get(&dlists, sizeof(int) * (2 * std::max<size_t>(nc_h, 1) + 8)));
+  int* dorder = dlists;
+  A.overflow = dlists + std::max<size_t>(nc_h, 1);
+  long long* dcounters;
+  CUBE_CUDA_TRY(ctx, S.get(&dcounters, 4 * sizeof(long long)));
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(dcounters, 0, 4 * sizeof(long long), ctx->stream));
+  A.mcount = dcounters;
+  A.err = reinterpret_cast<int*>(dcounters + 1);
+  if (nc_h)
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(dorder, order.data(), sizeof(int) * nc_h, cudaMemcpyHostToDevice, ctx->stream));
+  // scratch: the wave slots and one large slot for what a wave slot cannot hold
+  const int nslot = ctx->num_sms * 2;
+  const size_t wg = W_GCAP, wgrid = (size_t)(W_NB + 3) * (W_NB + 3) * (W_NB + 3);
+  HaloSlot W;
+  CUBE_CUDA_TRY(ctx, S.get(&W.gx, sizeof(double) * 3 * wg * nslot));
+  CUBE_CUDA_TRY(ctx, S.get(&W.gv, sizeof(double) * 3 * wg * nslot));
+  CUBE_CUDA_TRY(ctx, S.get(&W.gip, sizeof(int64_t) * wg * nslot));
+  CUBE_CUDA_TRY(ctx, S.get(&W.key, sizeof(double) * wg * nslot));
+  CUBE_CUDA_TRY(ctx, S.get(&W.ord, sizeof(int32_t) * wg * nslot));
+  CUBE_CUDA_TRY(ctx, S.get(&W.grid, sizeof(unsigned long long) * wgrid * nslot));
+  W.gcap = (int)wg;
+  W.nbmax = W_NB;
+  HaloSlot B;
+  CUBE_CUDA_TRY(ctx, S.get(&B.gx, sizeof(double) * 3 * GCAP));
+  CUBE_CUDA_TRY(ctx, S.get(&B.gv, sizeof(double) * 3 * GCAP));
+  CUBE_CUDA_TRY(ctx, S.get(&B.gip, sizeof(int64_t) * GCAP));
+  CUBE_CUDA_TRY(ctx, S.get(&B.key, sizeof(double) * GCAP));
+  CUBE_CUDA_TRY(ctx, S.get(&B.ord, sizeof(int32_t) * GCAP));
+  CUBE_CUDA_TRY(ctx, S.get(&B.grid, sizeof(unsigned long long) * (size_t)(NB_MAX + 3) * (NB_MAX + 3) * (NB_MAX + 3)));
+  B.gcap = (int)GCAP;
+  B.nbmax = NB_MAX;
+  auto kw = k_halo_wave<ZX, ZV>;
+  auto ks = k_halo_seq<ZX, ZV>;
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(kw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  std::vector<int> ovf;
+  for (int w = 0; w < nwaves; ++w) {
+    const int n = wstart[w + 1] - wstart[w];
+    CUBE_CUDA_TRY(ctx, cudaMemsetAsync(A.overflow, 0, sizeof(int), ctx->stream));
+    kw<<<std::min(n, nslot), W_THREADS, smem, ctx->stream>>>(A, dorder + wstart[w], n, W, wg, wgrid);
+    CUBE_LAUNCH_CHECK(ctx);
+    int no = 0;
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&no, A.overflow, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (no) {  // this wave's large candidates, one after the other in the large slot
+      ks<<<1, H_THREADS, smem, ctx->stream>>>(A, A.overflow + 1, no, B);
+      CUBE_LAUNCH_CHECK(ctx);
+    }
   }
-  A.member = nullptr;
-  A.member_cap = ha->member_capacity;
-  if (ha->member_pid && ha->member_capacity > 0)
-    CUBE_CUDA_TRY(ctx, S.get(&A.member, 4 * (size_t)ha->member_capacity));
-  CUBE_CUDA_TRY(ctx, S.get(&A.gx, sizeof(double) * 3 * GCAP));
-  CUBE_CUDA_TRY(ctx, S.get(&A.gv, sizeof(double) * 3 * GCAP));
-  CUBE_CUDA_TRY(ctx, S.get(&A.gip, sizeof(int64_t) * GCAP));
-  CUBE_CUDA_TRY(ctx, S.get(&A.key, sizeof(double) * GCAP));
-  CUBE_CUDA_TRY(ctx, S.get(&A.ord, sizeof(int32_t) * GCAP));
-  CUBE_CUDA_TRY(ctx, S.get(&A.grid, sizeof(unsigned long long) * (size_t)(NB_MAX + 3) * (NB_MAX + 3) * (NB_MAX + 3)));
-  const int cap_out = std::max(ha->capacity, 0);
-  cube_halo* dout;
-  CUBE_CUDA_TRY(ctx, S.get(&dout, sizeof(cube_halo) * (size_t)std::max(cap_out, 1)));
-  int* dcnt;
-  long long* dmem;
-  CUBE_CUDA_TRY(ctx, S.get(&dcnt, 2 * sizeof(int)));
-  CUBE_CUDA_TRY(ctx, S.get(&dmem, sizeof(long long)));
-  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(dcnt, 0, 2 * sizeof(int), ctx->stream));
-  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(dmem, 0, sizeof(long long), ctx->stream));
-  A.out = dout; A.out_cap = cap_out; A.nhalo = dcnt; A.err = dcnt + 1; A.nmember = dmem;
-  auto kern = k_halo_seq<ZX, ZV>;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<1, H_THREADS, smem, ctx->stream>>>(A);
-  CUBE_LAUNCH_CHECK(ctx);
-  int hcnt[2] = {0, 0};
-  long long nmem = 0;
-  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(hcnt, dcnt, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
-  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&nmem, dmem, sizeof(long long), cudaMemcpyDeviceToHost, ctx->stream));
+  int herr = 0;
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&herr, A.err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-  if (hcnt[1]) {
-    ctx->err = hcnt[1] == 2 ? "halofind: a refined grid exceeds 300 cells per dimension (newbox_max)"
-             : hcnt[1] == 3 ? "halofind: more particles within a search radius than the gather list holds"
-                            : "halofind: a search box wraps onto itself (nc too small for rsearch)";
-    return hcnt[1] == 4 ? CUBE_ERR_PARAM : CUBE_ERR_CAPACITY;
+  if (herr) {
+    ctx->err = herr == 2 ? "halofind: a refined grid exceeds 300 cells per dimension (newbox_max)"
+             : herr == 3 ? "halofind: more particles within a search radius than the gather list holds"
+                         : "halofind: a search box wraps onto itself (nc too small for rsearch)";
+    return herr == 4 ? CUBE_ERR_PARAM : CUBE_ERR_CAPACITY;
   }
-  res->nhalo = hcnt[0];
-  res->nmember = nmem;
-  const int nout = std::min(hcnt[0], cap_out);
-  if (nout > 0) CUBE_CUDA_TRY(ctx, cudaMemcpy(ha->halos, dout, sizeof(cube_halo) * nout, cudaMemcpyDeviceToHost));
-  if (A.hid) CUBE_CUDA_TRY(ctx, cudaMemcpy(ha->hid, A.hid, 4 * (size_t)ha->hid_len, cudaMemcpyDeviceToHost));
-  if (A.member && nmem > 0)
-    CUBE_CUDA_TRY(ctx, cudaMemcpy(ha->member_pid, A.member, 4 * (size_t)std::min<long long>(nmem, ha->member_capacity),
-                                  cudaMemcpyDeviceToHost));
-  if (hcnt[0] > cap_out || (ha->member_pid && nmem > ha->member_capacity)) {
+  // numbering and offsets in candidate order
+  std::vector<int2> flags(nc_h);
+  if (nc_h) {
+    int2* dfl;
+    CUBE_CUDA_TRY(ctx, S.get(&dfl, sizeof(int2) * nc_h));
+    k_halo_flags<<<(nc_h + 255) / 256, 256, 0, ctx->stream>>>(A.rec, (int)nc_h, dfl);
+    CUBE_LAUNCH_CHECK(ctx);
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(flags.data(), dfl, sizeof(int2) * nc_h, cudaMemcpyDeviceToHost, ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  std::vector<int> halo_ids, hnum;
+  std::vector<long long> foff;
+  long long run = 0;
+  for (size_t i = 0; i < nc_h; ++i)
+    if (flags[i].x) {
+      halo_ids.push_back((int)i);
+      hnum.push_back((int)halo_ids.size());
+      foff.push_back(run);
+      run += flags[i].y;
+    }
+  const int nh = (int)halo_ids.size();
+  res->nhalo = nh;
+  res->nmember = A.use_pid ? run : 0;
+  const int cap_out = std::max(ha->capacity, 0);
+  cube_halo* dout = nullptr;
+  int32_t* dmem = nullptr;
+  int32_t* dhid = nullptr;
+  if (nh) {
+    int* dids;
+    long long* dfoff;
+    CUBE_CUDA_TRY(ctx, S.get(&dids, sizeof(int) * 2 * nh));
+    CUBE_CUDA_TRY(ctx, S.get(&dfoff, sizeof(long long) * nh));
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(dids, halo_ids.data(), sizeof(int) * nh, cudaMemcpyHostToDevice, ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(dids + nh, hnum.data(), sizeof(int) * nh, cudaMemcpyHostToDevice, ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(dfoff, foff.data(), sizeof(long long) * nh, cudaMemcpyHostToDevice, ctx->stream));
+    CUBE_CUDA_TRY(ctx, S.get(&dout, sizeof(cube_halo) * (size_t)std::max(cap_out, 1)));
+    if (ha->member_pid && ha->member_capacity > 0) CUBE_CUDA_TRY(ctx, S.get(&dmem, 4 * (size_t)ha->member_capacity));
+    if (ha->hid && ha->hid_len > 0) {
+      CUBE_CUDA_TRY(ctx, S.get(&dhid, 4 * (size_t)ha->hid_len));
+      CUBE_CUDA_TRY(ctx, cudaMemsetAsync(dhid, 0, 4 * (size_t)ha->hid_len, ctx->stream));
+    }
+    k_halo_emit<<<ctx->num_sms * 4, 256, 0, ctx->stream>>>(A.rec, dids + nh, dfoff, dids, nh, A.mtmp, dout, cap_out,
+                                                           dmem, ha->member_capacity, dhid, ha->hid_len, A.use_pid);
+    CUBE_LAUNCH_CHECK(ctx);
+    const int nout = std::min(nh, cap_out);
+    if (nout > 0)
+      CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(ha->halos, dout, sizeof(cube_halo) * nout, cudaMemcpyDeviceToHost, ctx->stream));
+    if (dmem && run > 0)
+      CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(ha->member_pid, dmem, 4 * (size_t)std::min<long long>(run, ha->member_capacity),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
+    if (dhid)
+      CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(ha->hid, dhid, 4 * (size_t)ha->hid_len, cudaMemcpyDeviceToHost, ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  } else if (ha->hid && ha->hid_len > 0) {
+    std::fill(ha->hid, ha->hid + ha->hid_len, 0);
+  }
+  if (nh > cap_out || (ha->member_pid && A.use_pid && run > ha->member_capacity)) {
     ctx->err = "halofind: the output arrays are too small (the counts are returned)";
     return CUBE_ERR_CAPACITY;
   }
