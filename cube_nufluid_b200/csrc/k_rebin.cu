@@ -19,7 +19,8 @@
  *             the reference order -- then run the FP32 velocity sum in that
  *             order and the division by (n + weight_v); cells with more than
  *             32 particles go to a block-wide sorter
- *   emit    : per slot (fully parallel), re-encode, move and copy the PID
+ *   emit    : per particle in the old order (coalesced reads; the sort pass
+ *             records each particle's slot), re-encode, move and copy the PID
  *   stats   : per cell, the velocity statistics terms summed in slot order,
  *             for the fixed-tree sums
  * Positions move by nint(dt_mid*v/(x_resolution*ncell)) with the integer
@@ -215,6 +216,7 @@ __global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   for (int d = 0; d < 3; ++d) acc[d] = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
   for (int r = 0; r < n; ++r) {
     const int64_t ip = A.perm[s + r];
+    A.tkey[ip] = (uint32_t)(s + r);  // the particle's slot (tkey is free after the place pass)
     const int64_t sc = src_cell(A, A.pkey[s + r], tt);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -241,6 +243,7 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
     const int64_t s = A.start2[c];
     if (n > BIG_MAX) {
       if (threadIdx.x == 0) cube_dev_error(A.dscal, CUBE_ERR_CELL, n);
+      for (int i = threadIdx.x; i < n; i += blockDim.x) A.tkey[A.perm[s + i]] = 0xFFFFFFFFu;  // no slot: not emitted
       continue;
     }
     int m = 1;
@@ -265,8 +268,9 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
       const uint32_t key = (uint32_t)(sk[i] >> 32);
       const int32_t ip = (int32_t)(uint32_t)(sk[i] & 0xffffffffu);
-      A.pkey[s + i] = key;  // sorted order back to the slots for the emit pass
+      A.pkey[s + i] = key;  // sorted order back to the slots
       A.perm[s + i] = ip;
+      A.tkey[ip] = (uint32_t)(s + i);  // the particle's slot
       const int64_t sc = src_cell(A, key, tt);
       for (int d = 0; d < 3; ++d)
         sv[d * BIG_MAX + i] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
@@ -282,17 +286,27 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
   }
 }
 
-// F2: one thread per slot of the new layout: re-encode, move, copy the PID,
-// and keep the particle's two statistics terms for the in-order cell sums
+// F2: one thread per particle in its old storage order (coalesced reads of its
+// codes and PID): re-encode, move and copy it to its slot of the new layout (the
+// slots of neighbouring particles are close, so the writes gather in L2), and keep
+// its two statistics terms for the in-order cell sums
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_rebin_emit(RebinArgs A, int64_t np) {
-  for (int64_t slot = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; slot < np;
-       slot += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t ip = A.perm[slot];
+  __shared__ int64_t cs[RCELLS + 1];
+  const int64_t c0 = (int64_t)blockIdx.x * RCELLS;
+  const int ncl = (int)min((int64_t)RCELLS, A.ncells - c0);
+  for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = A.cell_start[c0 + i];
+  __syncthreads();
+  for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
+    int lo = 0, hi = ncl - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
+    }
+    const int64_t sc = c0 + lo;  // the particle's cell before the drift
     const int64_t c = A.tcell[ip];
-    int tt[3];
-    cell_tile(A, c, tt);
-    const int64_t sc = src_cell(A, A.pkey[slot], tt);
+    const int64_t slot = A.tkey[ip];
+    if (slot >= np) continue;  // its cell overflowed the sorter (error reported)
     double v[3];
     float vfn[3];
 #pragma unroll
@@ -342,7 +356,7 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
   CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rebin_big<ZX, ZV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_rebin_big<ZX, ZV><<<296, 512, smem, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
-  k_rebin_emit<ZX, ZV><<<(unsigned)std::min<int64_t>((ctx->np + 255) / 256, 148 * 64), 256, 0, ctx->stream>>>(A, ctx->np);
+  k_rebin_emit<ZX, ZV><<<(unsigned)nb, 256, 0, ctx->stream>>>(A, ctx->np);
   CUBE_LAUNCH_CHECK(ctx);
   k_rebin_stats<<<cb, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
