@@ -1,6 +1,6 @@
 """Benchmark of the B200 PM step (one JSON line on stdout).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4]
 
 Workload (default c2, the single-GPU precision configuration): 512^3 CDM
 particles in a 1000 Mpc/h box, fine mesh 1024^3, coarse mesh 256^3, 8^3 tiles,
@@ -47,6 +47,11 @@ CONFIGS = {
     "c3": dict(nc=256, nnt=8, box=500.0, izip=2, pp=True, z_i=10.0, nu=True,
                workload="512^3 CDM particles + fluid neutrinos (1 species, 3 x 0.1 eV; Gauss-Laguerre fluids "
                         "512^3, 256^3, 128^3), 500 Mpc/h, fine 1024^3, coarse 256^3, int2 x/v, PP on, from z=10"),
+    # batched ensemble: 96 independent boxes of 32^3-128^3 particles, one context and
+    # stream each, stepped by a pool of host threads (cube_nufluid_b200.ensemble)
+    "c4": dict(nc=0, nnt=1, box=0.0, izip=2, pp=False, z_i=49.0, ensemble=96,
+               workload="ensemble of 96 boxes, 32^3-128^3 particles (uniform over 32,48,64,96,128 per side), "
+                        "50-400 Mpc/h log-uniform, Om~U[0.25,0.35], s8~U[0.7,0.9], per-box seeds, int2 x/v, PP off"),
     "c3s": dict(nc=128, nnt=4, box=250.0, izip=2, pp=True, z_i=10.0, nu=True,
                 workload="256^3 CDM particles + fluid neutrinos (fluids 256^3, 128^3, 64^3), 250 Mpc/h, "
                          "fine 512^3, coarse 128^3, int2 x/v, PP on, from z=10 (profiling size)"),
@@ -334,6 +339,41 @@ def cpu_sample(threads: int):
                       f"{dt:.1f} s"}
 
 
+def run_ensemble(args, cfg):
+    """C4: box-steps/s of an ensemble of independent boxes on one GPU (per rank)."""
+    import torch
+    from cube_nufluid_b200 import build
+    from cube_nufluid_b200.ensemble import Ensemble, ensemble_specs
+    rank = int(os.environ.get("RANK", 0))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local_rank)
+    if rank == 0:
+        build.build()
+    specs = ensemble_specs(cfg["ensemble"], 2024 + rank)
+    ens = Ensemble(specs)
+    workers = 16
+    ens.run(args.warmup, workers=workers)
+    torch.cuda.synchronize()
+    l0 = sum(m.cube.launch_count() for m in ens.members)
+    with ClockSampler(local_rank) as clk:
+        r = ens.run(args.steps, workers=workers)
+        torch.cuda.synchronize()
+    launches = sum(m.cube.launch_count() for m in ens.members) - l0
+    npart = sum(sp.particles for sp in specs)
+    line = {"metric": "ensemble box-steps/s", "value": r["box_steps_per_s"], "unit": "box-steps/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["wall_s"] * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "boxes": len(specs), "particles_total": npart,
+                       "workers": r["workers"], "parallelism": "boxes on concurrent streams",
+                       "timing": "host wall clock between device synchronisations (one stream per box)"},
+            "particle_updates_per_s": r["particle_updates_per_s"], "gpu_launches": int(launches),
+            "clocks": clk.summary()}
+    ens.close()
+    if rank == 0:
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -344,6 +384,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if cfg.get("ensemble"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no ensemble mode; "
+                              "its CPU path is timed on the single-box configurations"}))
+            return
+        run_ensemble(args, cfg)
+        return
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))

@@ -166,6 +166,24 @@ __device__ __forceinline__ void cube_dev_error(DevScal* s, int code, int info) {
   if (atomicCAS(&s->err, 0, code) == 0) s->err_info = info;
 }
 
+// Raises a kernel's dynamic shared-memory limit to the most the device allows beside
+// the kernel's static shared memory.  The limit is a per-kernel global, so contexts on
+// other host threads launching the same kernel with other sizes must never see it
+// lowered under them: it is only ever set to that one value.  Fails if the launch
+// would need more.
+template <typename F>
+inline cudaError_t cube_smem_limit(F* func, size_t bytes) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  cudaFuncAttributes fa;
+  if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, func);
+  if (e != cudaSuccess) return e;
+  const size_t lim = (size_t)optin > fa.sharedSizeBytes ? (size_t)optin - fa.sharedSizeBytes : 0;
+  if (bytes > lim) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lim);
+}
+
 // device-side view of the particle codes
 template <int Z>
 struct CodeT;

@@ -179,12 +179,12 @@ int cube_deposit(cube_ctx* ctx, cube_scalars* io) {
   const int blocks = (nc / BX) * (nc / BY) * (nc / BZ);
   const size_t smem = sizeof(unsigned long long) * (FX * FY * FZ + CX * CY * CZ);
   if (ctx->izipx == 1) {
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_deposit<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUBE_CUDA_TRY(ctx, cube_smem_limit(k_deposit<1>, smem));
     k_deposit<1><<<blocks, 256, smem, ctx->stream>>>(ctx->xp, ctx->cell_start, ctx->cap, nc, ctx->nt, ctx->nnt,
                                                      io->mass_p_cdm, ctx->fine.rho, ctx->fine.rp, ctx->fine.plane,
                                                      ctx->rho_c_acc, mtot);
   } else {
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_deposit<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUBE_CUDA_TRY(ctx, cube_smem_limit(k_deposit<2>, smem));
     k_deposit<2><<<blocks, 256, smem, ctx->stream>>>(ctx->xp, ctx->cell_start, ctx->cap, nc, ctx->nt, ctx->nnt,
                                                      io->mass_p_cdm, ctx->fine.rho, ctx->fine.rp, ctx->fine.plane,
                                                      ctx->rho_c_acc, mtot);

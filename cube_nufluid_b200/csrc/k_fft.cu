@@ -346,7 +346,7 @@ int cube_fft_r2c_x(cube_ctx* ctx, MeshLevel& L, float* data, int inverse, int nc
   const size_t smem = sizeof(float2) * (size_t)ncomp * rpb * ss;
   const int thr = pick_threads(rpb * n / 2, MAXIT_X);
   const int blocks = (npairs + rpb - 1) / rpb;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fft_x<MAXIT_X>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_fft_x<MAXIT_X>, smem));
   k_fft_x<MAXIT_X><<<blocks, thr, smem, ctx->stream>>>(data, (size_t)n * L.plane, ncomp, n, L.rp, npairs, rpb,
                                                        L.plan, inverse, f2_bits);
   CUBE_LAUNCH_CHECK(ctx);
@@ -363,7 +363,7 @@ static int col_pass(cube_ctx* ctx, MeshLevel& L, float* data, int ncomp, int alo
   const long long cp = L.cp;
   const long long jstride = along_z ? (long long)n * cp : cp;
   const long long ostride = along_z ? cp : (long long)n * cp;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fft_col<MAXIT_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_fft_col<MAXIT_C>, smem));
   k_fft_col<MAXIT_C><<<grid, thr, smem, ctx->stream>>>(reinterpret_cast<float2*>(data), (size_t)n * L.plane / 2,
                                                        n, ncol, tk, jstride, ostride, L.plan, sgn);
   CUBE_LAUNCH_CHECK(ctx);
@@ -400,7 +400,7 @@ int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickSca
     const int thr = pick_threads(tk * n / 4, MAXIT_C);
     dim3 grid((ncol + tk - 1) / tk, n, 1);
     const long long cp = L.cp;
-    CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_fft_z_green<MAXIT_C>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUBE_CUDA_TRY(ctx, cube_smem_limit(k_fft_z_green<MAXIT_C>, smem));
     k_fft_z_green<MAXIT_C><<<grid, thr, smem, ctx->stream>>>(
         reinterpret_cast<const float2*>(L.rho), reinterpret_cast<float2*>(L.force), (size_t)n * L.plane / 2, n,
         ncol, tk, (long long)n * cp, cp, L.plan, L.kern, L.kern_pitch, cube_kick_scalar(ks));

@@ -396,11 +396,11 @@ int run_poisson_t(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale 
   const size_t sm1 = sizeof(float2) * 4 * cs_row<N, R, 4>();
   const size_t sm8 = sizeof(float2) * 8 * cs_row<N, R, 8>();
   const size_t sm3 = sizeof(float2) * 3 * RB3 * (N + R + 8);
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, 1, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_xr2c_t<N, R, T>, sm1));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_row_t<N, R, T, -1, 0>, sm8));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_row_t<N, R, T, 1, 1>, sm8));
 
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xc2r3_t<N, R, T, RB3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm3));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_xc2r3_t<N, R, T, RB3>, sm3));
   float2* ext = reinterpret_cast<float2*>(L.ext);
   float2* rho = reinterpret_cast<float2*>(L.rho);
   // x r2c: rho -> S1 (ext)
@@ -410,7 +410,7 @@ int run_poisson_t(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale 
   k_row_t<N, R, T, -1, 0><<<H * (N / 8), 8 * T, sm8, ctx->stream>>>(ext, rho, L.cp, tw);
   CUBE_LAUNCH_CHECK(ctx);
   // z forward, Green, z inverse: S2 -> S3 of components 0, 1, 2 in force 1, force 2, ext
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_zgreen_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_zgreen_t<N, R, T>, sm8));
   k_zgreen_t<N, R, T><<<H * (N / 8), 8 * T, sm8, ctx->stream>>>(
       rho, reinterpret_cast<float2*>(F[1]), reinterpret_cast<float2*>(F[2]), ext, tw, L.kern, L.kern_pitch,
       cube_kick_scalar(ks));
@@ -438,9 +438,9 @@ int run_forward3_t(cube_ctx* ctx, MeshLevel& L, float* data) {
   const float2* tw = L.plan.tw2;
   const size_t sm1 = sizeof(float2) * 4 * cs_row<N, R, 4>();
   const size_t sm8 = sizeof(float2) * 8 * cs_row<N, R, 8>();
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_xr2c_t<N, R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_t<N, R, T, -1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_row_inplace<N, R, T, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm8));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_xr2c_t<N, R, T>, sm1));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_row_t<N, R, T, -1, 0>, sm8));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_row_inplace<N, R, T, -1>, sm8));
   float2* ext = reinterpret_cast<float2*>(L.ext);
   float2* d2 = reinterpret_cast<float2*>(data);
   k_xr2c_t<N, R, T><<<N * (N / 8), 4 * T, sm1, ctx->stream>>>(data, L.rp, ext, tw);

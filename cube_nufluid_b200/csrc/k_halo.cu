@@ -666,16 +666,17 @@ __global__ void k_halo_emit(const HaloRec* __restrict__ rec, const int* __restri
 // cell offsets within RMAX, (dx, dy, dz, r^2), in the reference's generation order
 // (x outermost, z innermost, :68-80), stably sorted by the exact r^2
 const std::vector<int4>& shell_list() {
-  static std::vector<int4> L;
-  if (L.empty()) {
+  static const std::vector<int4> L = [] {  // built once, thread-safe
+    std::vector<int4> v;
     for (int i = -RMAX; i <= RMAX; ++i)
       for (int j = -RMAX; j <= RMAX; ++j)
         for (int k = -RMAX; k <= RMAX; ++k) {
           const int r2 = i * i + j * j + k * k;
-          if (r2 <= RMAX * RMAX) L.push_back(make_int4(i, j, k, r2));
+          if (r2 <= RMAX * RMAX) v.push_back(make_int4(i, j, k, r2));
         }
-    std::stable_sort(L.begin(), L.end(), [](const int4& a, const int4& b) { return a.w < b.w; });
-  }
+    std::stable_sort(v.begin(), v.end(), [](const int4& a, const int4& b) { return a.w < b.w; });
+    return v;
+  }();
   return L;
 }
 
@@ -867,8 +868,8 @@ int run_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* ha
   B.nbmax = NB_MAX;
   auto kw = k_halo_wave<ZX, ZV>;
   auto ks = k_halo_seq<ZX, ZV>;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(kw, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(kw, smem));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(ks, smem));
   std::vector<int> ovf;
   for (int w = 0; w < nwaves; ++w) {
     const int n = wstart[w + 1] - wstart[w];

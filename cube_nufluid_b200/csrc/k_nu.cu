@@ -622,13 +622,13 @@ int cube_nu_sweeps(cube_ctx* ctx, NuFluid& F, float dt, int dir) {
     const size_t smem = sizeof(float) * (size_t)5 * A.tx * ((A.ts + 4) + (A.ts + 1));
     dim3 grid((unsigned)((n / A.ts) * (n / A.tx)), (unsigned)n);
     if (ax == 0) {
-      CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_nu_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CUBE_CUDA_TRY(ctx, cube_smem_limit(k_nu_sweep<0>, smem));
       k_nu_sweep<0><<<grid, 256, smem, ctx->stream>>>(A);
     } else if (ax == 1) {
-      CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_nu_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CUBE_CUDA_TRY(ctx, cube_smem_limit(k_nu_sweep<1>, smem));
       k_nu_sweep<1><<<grid, 256, smem, ctx->stream>>>(A);
     } else {
-      CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_nu_sweep<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      CUBE_CUDA_TRY(ctx, cube_smem_limit(k_nu_sweep<2>, smem));
       k_nu_sweep<2><<<grid, 256, smem, ctx->stream>>>(A);
     }
     CUBE_LAUNCH_CHECK(ctx);

@@ -241,7 +241,7 @@ int cube_power_spectrum_dev(cube_ctx* ctx, int logbins, std::vector<double>& bin
   const size_t nb = (size_t)NQ * (nbin + 1);
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(gb, 0, 8 * nb, ctx->stream));
   const size_t smem = 8 * nb;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_pk_bin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_pk_bin, smem));
   const float norm = (float)(1.0 / ((double)ng * ng * ng));
   k_pk_bin<<<ctx->num_sms * 2, 256, smem, ctx->stream>>>(reinterpret_cast<const float2*>(L.rho),
                                                         reinterpret_cast<const float2*>(dnu), has2, ng, L.cp, kxm, nbin,

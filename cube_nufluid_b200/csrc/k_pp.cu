@@ -579,7 +579,7 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   const int nbricks = (ctx->nc / PB) * (ctx->nc / PB) * (ctx->nc / PB);
   const size_t smem = sizeof(uint16_t) * ((size_t)NFC + 5 * (size_t)PB_CAP);
   auto kb = k_pp_brick<ZX, ZV>;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(kb, smem));
   kb<<<nbricks, PP_THREADS, smem, ctx->stream>>>(ctx->xp, ctx->vp, ctx->cell_start, ctx->nc, ctx->nt, ctx->nnt, A,
                                                  spill, ctx->dscal);
   CUBE_LAUNCH_CHECK(ctx);

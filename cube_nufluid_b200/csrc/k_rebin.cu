@@ -353,7 +353,7 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
   k_rebin_sortsum<ZX, ZV><<<cb, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
   const size_t smem = sizeof(unsigned long long) * BIG_MAX + sizeof(double) * 3 * BIG_MAX;
-  CUBE_CUDA_TRY(ctx, cudaFuncSetAttribute(k_rebin_big<ZX, ZV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_big<ZX, ZV>, smem));
   k_rebin_big<ZX, ZV><<<296, 512, smem, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
   k_rebin_emit<ZX, ZV><<<(unsigned)nb, 256, 0, ctx->stream>>>(A, ctx->np);
