@@ -1,6 +1,6 @@
 """Benchmark of the B200 PM step (one JSON line on stdout).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5]
 
 Workload (default c2, the single-GPU precision configuration): 512^3 CDM
 particles in a 1000 Mpc/h box, fine mesh 1024^3, coarse mesh 256^3, 8^3 tiles,
@@ -52,6 +52,12 @@ CONFIGS = {
     "c4": dict(nc=0, nnt=1, box=0.0, izip=2, pp=False, z_i=49.0, ensemble=96,
                workload="ensemble of 96 boxes, 32^3-128^3 particles (uniform over 32,48,64,96,128 per side), "
                         "50-400 Mpc/h log-uniform, Om~U[0.25,0.35], s8~U[0.7,0.9], per-box seeds, int2 x/v, PP off"),
+    # serving: Poisson requests at 20/s of 32^3-256^3 particles, each evolved z=49 -> 0
+    # in 48 steps and answered with P(k) and a 1/64 subsample (cube_nufluid_b200.serving)
+    "c5": dict(nc=0, nnt=1, box=0.0, izip=2, pp=False, z_i=49.0, serving=60,
+               workload="serving: Poisson arrivals at 20/s, 32^3-256^3 particles log-uniform, 50-400 Mpc/h, "
+                        "Om~U[0.25,0.35], s8~U[0.7,0.9], 48 steps z=49->0, P(k) in 32 log bins + 1/64 "
+                        "subsample, 160 GB HBM admission budget, int2 x/v, PP off"),
     "c3s": dict(nc=128, nnt=4, box=250.0, izip=2, pp=True, z_i=10.0, nu=True,
                 workload="256^3 CDM particles + fluid neutrinos (fluids 256^3, 128^3, 64^3), 250 Mpc/h, "
                          "fine 512^3, coarse 128^3, int2 x/v, PP on, from z=10 (profiling size)"),
@@ -374,6 +380,50 @@ def run_ensemble(args, cfg):
         print(json.dumps(line))
 
 
+def run_serving(args, cfg):
+    """C5: latency percentiles of a Poisson request stream served on one GPU, and the
+    same percentiles relative to each request's plain service time (its size served
+    alone on an idle GPU)."""
+    import torch
+    from cube_nufluid_b200 import build
+    from cube_nufluid_b200.serving import SERVE_SIDES, Request, Server, request_stream
+    from cube_nufluid_b200.ensemble import BoxSpec
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local_rank)
+    build.build()
+    srv = Server(hbm_budget=160e9, workers=8)
+    # warm-up: one request per size creates the contexts; then the plain service
+    # time of each size on the idle server (contexts reused, as under load)
+    plain = {}
+    for rep in range(2):
+        for i, side in enumerate(SERVE_SIDES):
+            req = Request(-1, 0.0, BoxSpec(nc=side // 2, box=200.0, omega_m=0.3, sigma8=0.8, seed=77 + i))
+            t = time.perf_counter()
+            srv.answer(req)
+            plain[side // 2] = time.perf_counter() - t
+    reqs = request_stream(cfg["serving"], 20.0, 2025)
+    with ClockSampler(local_rank) as clk:
+        t0 = time.perf_counter()
+        ans = srv.serve(reqs, realtime=True)
+        wall = time.perf_counter() - t0
+    srv.close()
+    lat = np.array([a.latency for a in ans])
+    slow = np.array([a.latency / plain[r.spec.nc] for a, r in zip(ans, reqs)])
+    line = {"metric": "serving p99 latency", "value": float(np.percentile(lat, 99)), "unit": "s",
+            "n_gpus": 1, "steps": 48, "warmup": 2 * len(SERVE_SIDES), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "requests": len(reqs), "workers": 8,
+                       "timing": "host wall clock per request (arrival to answer)"},
+            "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+            "vs_plain": {"p50": float(np.percentile(slow, 50)), "p99": float(np.percentile(slow, 99))},
+            "plain_service_s": {str(2 * k): v for k, v in sorted(plain.items())},
+            "requests_per_s": len(reqs) / wall, "steps_mean": float(np.mean([a.steps for a in ans])),
+            "offered_gpu_s_per_s": 20.0 * float(np.mean([plain[r.spec.nc] for r in reqs])),
+            "clocks": clk.summary()}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -384,6 +434,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if cfg.get("serving"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving mode; "
+                              "its CPU path is timed on the single-box configurations"}))
+            return
+        run_serving(args, cfg)
+        return
     if cfg.get("ensemble"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no ensemble mode; "

@@ -191,6 +191,24 @@ int32_t cube_set_stream(cube_ctx* ctx, void* stream) {
   return CUBE_OK;
 }
 
+int32_t cube_set_params(cube_ctx* ctx, const cube_params* p) {
+  if (!ctx || !p) return CUBE_ERR_PARAM;
+  cube_params q = *p;  // everything but the changeable fields must match
+  q.box = ctx->P.box; q.h0 = ctx->P.h0; q.omega_m = ctx->P.omega_m; q.omega_l = ctx->P.omega_l;
+  q.wde = ctx->P.wde; q.ra_max = ctx->P.ra_max; q.dt_max = ctx->P.dt_max;
+  if (memcmp(&q, &ctx->P, sizeof(cube_params)) != 0) {
+    ctx->err = "cube_set_params: only box, h0, omega_m, omega_l, wde, ra_max and dt_max may change";
+    return CUBE_ERR_PARAM;
+  }
+  if (!(p->box > 0.f) || !(p->h0 > 0.f) || !(p->omega_m > 0.f)) {
+    ctx->err = "cube_set_params: box, h0 and omega_m must be positive";
+    return CUBE_ERR_PARAM;
+  }
+  ctx->P.box = p->box; ctx->P.h0 = p->h0; ctx->P.omega_m = p->omega_m; ctx->P.omega_l = p->omega_l;
+  ctx->P.wde = p->wde; ctx->P.ra_max = p->ra_max; ctx->P.dt_max = p->dt_max;
+  return CUBE_OK;
+}
+
 void cube_destroy(cube_ctx* ctx) {
   if (!ctx) return;
   cudaStreamSynchronize(ctx->stream);
@@ -211,6 +229,7 @@ void cube_destroy(cube_ctx* ctx) {
   }
   if (ctx->nu.partial) cudaFree(ctx->nu.partial);
   if (ctx->pp_scratch) cudaFree(ctx->pp_scratch);
+  if (ctx->rebin_scratch) cudaFree(ctx->rebin_scratch);
   for (double* t : ctx->vdec)
     if (t) cudaFree(t);
   if (ctx->hscal) cudaFreeHost(ctx->hscal);

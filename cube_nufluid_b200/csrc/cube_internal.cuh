@@ -71,6 +71,8 @@ struct DevScal {
   unsigned long long itest1, npairs;
   unsigned long long moved_far;
   unsigned int nu_dt_bits[3];  // per-fluid CFL step as float bits
+  unsigned long long n_huge;   // re-bin cells beyond the shared-memory sorter
+  unsigned long long max_huge; // the most particles in one of them
 };
 
 // one isothermal fluid of the dispersive sum (hydrogr.f90 type hydro): five FP32
@@ -126,6 +128,8 @@ struct cube_ctx {
   int vdec_next = 0;
   void* pp_scratch = nullptr;     // sorted particles of crowded PP bricks, grown on demand
   size_t pp_scratch_bytes = 0;
+  void* rebin_scratch = nullptr;  // sort slots of re-bin cells beyond 4096 particles, grown on demand
+  size_t rebin_scratch_bytes = 0;
   // meshes
   MeshLevel fine, coarse;
   unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator

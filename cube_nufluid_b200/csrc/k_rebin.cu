@@ -18,7 +18,8 @@
  *   sortsum : per target cell, sort its entries by (key, source index) --
  *             the reference order -- then run the FP32 velocity sum in that
  *             order and the division by (n + weight_v); cells with more than
- *             32 particles go to a block-wide sorter
+ *             32 particles go to a block-wide sorter in shared memory, those
+ *             beyond 4096 to one in a global scratch grown on demand
  *   emit    : per particle in the old order (coalesced reads; the sort pass
  *             records each particle's slot), re-encode, move and copy the PID
  *   stats   : per cell, the velocity statistics terms summed in slot order,
@@ -229,9 +230,55 @@ __global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   for (int d = 0; d < 3; ++d) A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc[d], den);
 }
 
-// F1 for crowded cells: one CTA per cell, bitonic sort of (key<<32|source) in
-// shared memory, per-particle velocities in parallel, the sum by one thread per
-// component in order
+// one crowded cell by the whole CTA: bitonic sort of (key<<32|source) in sk (m =
+// next power of two of n entries), the sorted order back to the slots, the
+// per-particle velocities into sv[d * vstride + i] in parallel, the FP32 sum by
+// one thread per component in order.  sk and sv may be shared or global memory.
+template <int ZX, int ZV>
+__device__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk, double* sv,
+                              int vstride) {
+  int m = 1;
+  while (m < n) m <<= 1;
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    sk[i] = i < n ? (((unsigned long long)A.pkey[s + i] << 32) | (uint32_t)A.perm[s + i]) : ~0ull;
+  __syncthreads();
+  for (int k = 2; k <= m; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = sk[i], bb = sk[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > bb) == up) { sk[i] = bb; sk[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  int tt[3];
+  cell_tile(A, c, tt);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const uint32_t key = (uint32_t)(sk[i] >> 32);
+    const int32_t ip = (int32_t)(uint32_t)(sk[i] & 0xffffffffu);
+    A.pkey[s + i] = key;  // sorted order back to the slots
+    A.perm[s + i] = ip;
+    A.tkey[ip] = (uint32_t)(s + i);  // the particle's slot
+    const int64_t sc = src_cell(A, key, tt);
+    for (int d = 0; d < 3; ++d)
+      sv[(size_t)d * vstride + i] =
+          cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int d = threadIdx.x;
+    float acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
+    for (int i = 0; i < n; ++i) acc = (float)cube_dadd((double)acc, sv[(size_t)d * vstride + i]);
+    A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
+  }
+  __syncthreads();
+}
+
+// F1 for crowded cells: one CTA per cell, sorted in shared memory; cells beyond
+// BIG_MAX entries are listed (from the end of big_list) for k_rebin_huge
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
   extern __shared__ unsigned long long sk[];
@@ -242,47 +289,30 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
     const int n = A.cnt2[c];
     const int64_t s = A.start2[c];
     if (n > BIG_MAX) {
-      if (threadIdx.x == 0) cube_dev_error(A.dscal, CUBE_ERR_CELL, n);
-      for (int i = threadIdx.x; i < n; i += blockDim.x) A.tkey[A.perm[s + i]] = 0xFFFFFFFFu;  // no slot: not emitted
+      if (threadIdx.x == 0) {
+        const unsigned long long q = atomicAdd(&A.dscal->n_huge, 1ull);
+        A.big_list[A.ncells - 1 - (int64_t)q] = (int32_t)c;
+        atomicMax(&A.dscal->max_huge, (unsigned long long)n);
+      }
       continue;
     }
-    int m = 1;
-    while (m < n) m <<= 1;
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-      sk[i] = i < n ? (((unsigned long long)A.pkey[s + i] << 32) | (uint32_t)A.perm[s + i]) : ~0ull;
-    __syncthreads();
-    for (int k = 2; k <= m; k <<= 1)
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int i = threadIdx.x; i < m; i += blockDim.x) {
-          const int ixj = i ^ j;
-          if (ixj > i) {
-            const unsigned long long a = sk[i], bb = sk[ixj];
-            const bool up = (i & k) == 0;
-            if ((a > bb) == up) { sk[i] = bb; sk[ixj] = a; }
-          }
-        }
-        __syncthreads();
-      }
-    int tt[3];
-    cell_tile(A, c, tt);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) {
-      const uint32_t key = (uint32_t)(sk[i] >> 32);
-      const int32_t ip = (int32_t)(uint32_t)(sk[i] & 0xffffffffu);
-      A.pkey[s + i] = key;  // sorted order back to the slots
-      A.perm[s + i] = ip;
-      A.tkey[ip] = (uint32_t)(s + i);  // the particle's slot
-      const int64_t sc = src_cell(A, key, tt);
-      for (int d = 0; d < 3; ++d)
-        sv[d * BIG_MAX + i] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
-    }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-      const int d = threadIdx.x;
-      float acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
-      for (int i = 0; i < n; ++i) acc = (float)cube_dadd((double)acc, sv[d * BIG_MAX + i]);
-      A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
-    }
-    __syncthreads();
+    sort_sum_cell<ZX, ZV>(A, c, n, s, sk, sv, BIG_MAX);
+  }
+}
+
+// F1 for cells beyond BIG_MAX: the same in a global scratch slot per CTA
+// (slot_u64 = keys for the largest cell padded to a power of two, then its
+// velocities)
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(1024) k_rebin_huge(RebinArgs A, unsigned long long* __restrict__ scratch,
+                                                     size_t slot_u64, int mmax) {
+  unsigned long long* sk = scratch + (size_t)blockIdx.x * slot_u64;
+  double* sv = reinterpret_cast<double*>(sk + mmax);
+  const unsigned long long nh = A.dscal->n_huge;
+  const int vstride = (int)((slot_u64 - mmax) / 3);
+  for (unsigned long long q = blockIdx.x; q < nh; q += gridDim.x) {
+    const int64_t c = A.big_list[A.ncells - 1 - (int64_t)q];
+    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, vstride);
   }
 }
 
@@ -356,6 +386,28 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
   CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_big<ZX, ZV>, smem));
   k_rebin_big<ZX, ZV><<<296, 512, smem, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
+  // cells beyond the shared-memory sorter: global scratch sized for the largest
+  unsigned long long hv[2] = {0ull, 0ull};
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(hv, &ctx->dscal->n_huge, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (hv[0]) {
+    int mmax = 1;
+    while ((unsigned long long)mmax < hv[1]) mmax <<= 1;
+    const size_t slot = (size_t)mmax + 3 * (size_t)hv[1];
+    const int grid = (int)std::min<unsigned long long>(hv[0], 148);
+    const size_t need = sizeof(unsigned long long) * slot * grid;
+    if (need > ctx->rebin_scratch_bytes) {
+      if (ctx->rebin_scratch) cudaFree(ctx->rebin_scratch);
+      ctx->rebin_scratch = nullptr;
+      ctx->rebin_scratch_bytes = 0;
+      CUBE_CUDA_TRY(ctx, cudaMalloc(&ctx->rebin_scratch, need));
+      ctx->rebin_scratch_bytes = need;
+    }
+    k_rebin_huge<ZX, ZV><<<grid, 1024, 0, ctx->stream>>>(A, reinterpret_cast<unsigned long long*>(ctx->rebin_scratch),
+                                                         slot, mmax);
+    CUBE_LAUNCH_CHECK(ctx);
+  }
   k_rebin_emit<ZX, ZV><<<(unsigned)nb, 256, 0, ctx->stream>>>(A, ctx->np);
   CUBE_LAUNCH_CHECK(ctx);
   k_rebin_stats<<<cb, 256, 0, ctx->stream>>>(A);

@@ -82,6 +82,8 @@ def load_library():
     L.cube_phase_times.restype = C.c_int32
     L.cube_launch_count.argtypes = [vp]
     L.cube_launch_count.restype = C.c_int64
+    L.cube_set_params.argtypes = [vp, P]
+    L.cube_set_params.restype = C.c_int32
     L.cube_set_stream.argtypes = [vp, vp]
     L.cube_set_stream.restype = C.c_int32
     L.cube_last_error.argtypes = [vp]
@@ -131,6 +133,12 @@ class Cube:
         self.np_capacity = int(np_capacity)
         self.nc = params.nc
         self.nf = params.nc * params.ncell
+
+    def set_params(self, params: CubeParams):
+        """cube_set_params: another box size and cosmology for this context (mesh
+        sizes and options unchanged), e.g. before make_ic for the next box."""
+        self._check(self.L.cube_set_params(self.h, C.byref(params)))
+        self.p = params
 
     def close(self):
         if getattr(self, "h", None):

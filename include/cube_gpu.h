@@ -285,6 +285,14 @@ int64_t cube_launch_count(cube_ctx* ctx);
 /* Sets the CUDA stream (cudaStream_t passed as void*) the context launches on. */
 int32_t cube_set_stream(cube_ctx* ctx, void* stream);
 
+/* Gives an existing context another box size and cosmology (box, h0, omega_m,
+ * omega_l, wde, ra_max, dt_max) without reallocating, so that a host serving many
+ * boxes of one mesh size can reuse a context (and not stall the device in cudaFree)
+ * by following this with cube_make_ic or cube_load_state.  No counterpart in the
+ * reference, whose parameters are compile-time.  Every other field must equal the
+ * context's (they size its arrays or its Green's functions): CUBE_ERR_PARAM if not. */
+int32_t cube_set_params(cube_ctx* ctx, const cube_params* params);
+
 /* Text of the last error on this context (or the last create error if ctx is NULL). */
 const char* cube_last_error(cube_ctx* ctx);
 

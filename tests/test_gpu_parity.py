@@ -204,3 +204,21 @@ def test_multi_step_run_tracks_oracle(tables):
     assert np.mean(dx == 0) > 0.99 and dx.max() <= 2
     dv = np.abs(vo[io].astype(np.int32) - vg[ig].astype(np.int32))
     assert np.mean(dv == 0) > 0.99
+
+
+@pytest.mark.gpu
+def test_update_x_bit_exact_with_cells_beyond_the_shared_sorter(tables):
+    # two dense clumps put cells of more than 4096 particles through the global-
+    # scratch sorter (and others through the shared-memory one)
+    from helpers import planted_clumps
+    st, p, s = planted_clumps(nc=16, centres=((3.5, 4.5, 5.5), (10.5, 11.5, 2.5)), n_per=12000, sigma=0.08,
+                              nbg=20000, seed=41)
+    assert st.rhoc.max() > 4096
+    s.dt_old, s.dt = 20.0, 20.0
+    o, g = pair(st, p, tables, build=False)
+    so, sg = s.copy(), s.copy()
+    o.update_x(so)
+    g.update_x(sg)
+    assert_same_state(o, g)
+    assert so.sigma_vi_new == sg.sigma_vi_new and so.std_vsim == sg.std_vsim
+    assert g.store_state()[3].max() > 4096
