@@ -42,6 +42,10 @@ inline bool cube_fast_rt(int n, int* R, int* T) {
     case 128: *R = 16; *T = 8; return true;
     case 64: *R = 8; *T = 8; return true;
     case 32: *R = 8; *T = 4; return true;
+    case 768: *R = 48; *T = 16; return true;
+    case 384: *R = 48; *T = 8; return true;
+    case 192: *R = 24; *T = 8; return true;
+    case 96: *R = 24; *T = 4; return true;
     default: return false;
   }
 }

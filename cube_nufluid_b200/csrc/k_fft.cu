@@ -328,7 +328,7 @@ int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n) {
     // laid out so that a warp's loads are contiguous
     std::vector<float2> tw2((size_t)R * T);
     for (int k1 = 0; k1 < R; ++k1)
-      for (int t = 0; t < T; ++t) tw2[(size_t)k1 * T + t] = tw[(t * k1) & (n - 1)];
+      for (int t = 0; t < T; ++t) tw2[(size_t)k1 * T + t] = tw[(t * k1) % n];
     CUBE_CUDA_TRY(ctx, cudaMalloc(&p.tw2, sizeof(float2) * R * T));
     CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(p.tw2, tw2.data(), sizeof(float2) * R * T, cudaMemcpyHostToDevice, ctx->stream));
   }

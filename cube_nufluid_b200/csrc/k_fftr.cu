@@ -1,5 +1,6 @@
 /*
- * k_fftr.cu -- register-resident FFT passes for power-of-two meshes.
+ * k_fftr.cu -- register-resident FFT passes for power-of-two meshes and three
+ * times a power of two.
  *
  * A length N = R*T transform runs on a group of T threads (T <= 32, inside
  * one warp): with n = t + T*q and k = k1 + R*k2,
@@ -10,7 +11,8 @@
  * transpose has bank conflicts), and each thread does
  * R/T T-point DFTs in registers (over t).  Only __syncwarp is needed inside a
  * transform.  Sizes: 1024 = 32*32, 512 = 32*16, 256 = 16*16, 128 = 16*8,
- * 64 = 8*8, 32 = 8*4; other sizes use the shared-memory Stockham passes of
+ * 64 = 8*8, 32 = 8*4, and with a radix-3 first stage 768 = 48*16, 384 = 48*8,
+ * 192 = 24*8, 96 = 24*4; other sizes use the shared-memory Stockham passes of
  * k_fft.cu.
  *
  * Passes of the Poisson solve (the layouts are listed above k_xr2c_t):
@@ -48,6 +50,59 @@ __device__ constexpr float cos16(int j) {  // cos(pi j / 16), any integer j
                           : kC16[32 - (j & 31)];
 }
 __device__ constexpr float sin16(int j) { return cos16(8 - j); }
+
+// cos(2 pi j/48), j = 0..47 (twiddles of the radix-3 in-register DFTs)
+__device__ constexpr float kC48[48] = {
+    1.00000000000000000000e+00f,
+    9.91444861373810382155e-01f,
+    9.65925826289068312214e-01f,
+    9.23879532511286738483e-01f,
+    8.66025403784438707611e-01f,
+    7.93353340291235165083e-01f,
+    7.07106781186547572737e-01f,
+    6.08761429008720655887e-01f,
+    5.00000000000000111022e-01f,
+    3.82683432365089837290e-01f,
+    2.58819045102520739476e-01f,
+    1.30526192220051712178e-01f,
+    6.12323399573676603587e-17f,
+    -1.30526192220051601156e-01f,
+    -2.58819045102520628454e-01f,
+    -3.82683432365089504223e-01f,
+    -4.99999999999999777955e-01f,
+    -6.08761429008720655887e-01f,
+    -7.07106781186547461715e-01f,
+    -7.93353340291235054060e-01f,
+    -8.66025403784438707611e-01f,
+    -9.23879532511286738483e-01f,
+    -9.65925826289068201191e-01f,
+    -9.91444861373810382155e-01f,
+    -1.00000000000000000000e+00f,
+    -9.91444861373810382155e-01f,
+    -9.65925826289068312214e-01f,
+    -9.23879532511286849505e-01f,
+    -8.66025403784438818633e-01f,
+    -7.93353340291235165083e-01f,
+    -7.07106781186547905804e-01f,
+    -6.08761429008720877931e-01f,
+    -5.00000000000000444089e-01f,
+    -3.82683432365089504223e-01f,
+    -2.58819045102520628454e-01f,
+    -1.30526192220051628912e-01f,
+    -1.83697019872102968750e-16f,
+    1.30526192220051268089e-01f,
+    2.58819045102520295387e-01f,
+    3.82683432365089171157e-01f,
+    5.00000000000000111022e-01f,
+    6.08761429008719878730e-01f,
+    7.07106781186547350693e-01f,
+    7.93353340291234943038e-01f,
+    8.66025403784438374544e-01f,
+    9.23879532511286849505e-01f,
+    9.65925826289068090169e-01f,
+    9.91444861373810382155e-01f};
+__device__ constexpr float cos48(int j) { return kC48[((j % 48) + 48) % 48]; }  // cos(2 pi j/48)
+__device__ constexpr float sin48(int j) { return cos48(j - 12); }                // sin(2 pi j/48)
 
 __device__ __forceinline__ float2 cmul(float2 a, float2 b) {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -98,12 +153,48 @@ __device__ __forceinline__ void dft_stage(float2* v) {
   if constexpr (LEN < L) dft_stage<L, SIGN, 2 * LEN>(v);
 }
 
-// in-register DFT of length L (power of two <= 32) on v[0..L-1], natural order out;
-// SIGN = -1 forward (exp(-2 pi i jk/L)), +1 inverse.  Decimation in time.
+template <int L, int SIGN>
+__device__ __forceinline__ void dft_reg(float2* v);
+
+// in-register DFT of length L = 3*M (M a power of two, L dividing 48): the three
+// decimated sequences v[3m + r] by M-point DFTs, twiddled by W_L^{r k} and joined
+// by a 3-point DFT, X[k + M q] = sum_r W_L^{r k} Y_r[k] W_3^{r q}
+template <int L, int SIGN>
+__device__ __forceinline__ void dft_reg3(float2* v) {
+  constexpr int M = L / 3, S = 48 / L;  // angle 2 pi j/L = 2 pi (S j)/48
+  float2 y[3][M];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+#pragma unroll
+    for (int m = 0; m < M; ++m) y[r][m] = v[3 * m + r];
+    dft_reg<M, SIGN>(y[r]);
+  }
+  const float c3 = -0.5f, s3 = SIGN * 0.86602540378443864676f;  // W_3 = exp(SIGN 2 pi i/3)
+#pragma unroll
+  for (int k = 0; k < M; ++k) {
+    const float2 z0 = y[0][k];
+    const float2 z1 = k == 0 ? y[1][k] : cmul(y[1][k], make_float2(cos48(S * k), SIGN * sin48(S * k)));
+    const float2 z2 = k == 0 ? y[2][k] : cmul(y[2][k], make_float2(cos48(2 * S * k), SIGN * sin48(2 * S * k)));
+    const float2 a = make_float2(z1.x + z2.x, z1.y + z2.y), b = make_float2(z1.x - z2.x, z1.y - z2.y);
+    v[k] = make_float2(z0.x + a.x, z0.y + a.y);
+    // z0 + W3 z1 + W3^2 z2 = z0 + c3 (z1 + z2) + i s3 (z1 - z2), and its conjugate-twiddle partner
+    const float2 m0 = make_float2(z0.x + c3 * a.x, z0.y + c3 * a.y), m1 = make_float2(-s3 * b.y, s3 * b.x);
+    v[k + M] = make_float2(m0.x + m1.x, m0.y + m1.y);
+    v[k + 2 * M] = make_float2(m0.x - m1.x, m0.y - m1.y);
+  }
+}
+
+// in-register DFT of length L on v[0..L-1], natural order out; SIGN = -1 forward
+// (exp(-2 pi i jk/L)), +1 inverse.  Powers of two <= 32 by decimation in time,
+// 24 and 48 by dft_reg3.
 template <int L, int SIGN>
 __device__ __forceinline__ void dft_reg(float2* v) {
-  bitrev_perm<L>(v, std::make_integer_sequence<int, L>{});
-  if constexpr (L > 1) dft_stage<L, SIGN, 2>(v);
+  if constexpr (L % 3 == 0) {
+    dft_reg3<L, SIGN>(v);
+  } else {
+    bitrev_perm<L>(v, std::make_integer_sequence<int, L>{});
+    if constexpr (L > 1) dft_stage<L, SIGN, 2>(v);
+  }
 }
 
 // sequence element n at s[n*ES]; ROW layout has ES = 1 and a padded exchange,
@@ -189,7 +280,7 @@ __global__ void __launch_bounds__(4 * T) k_xr2c_t(const float* __restrict__ rho,
   for (int i = threadIdx.x; i < 4 * H; i += 4 * T) {
     const int k = i >> 2, p = i & 3;
     const float2 Zk = sm[p * CS + k];
-    const float2 Zm = sm[p * CS + ((N - k) & (N - 1))];
+    const float2 Zm = sm[p * CS + (k ? N - k : 0)];
     const float2 A = make_float2(0.5f * (Zk.x + Zm.x), 0.5f * (Zk.y - Zm.y));
     const float2 B = make_float2(0.5f * (Zk.y + Zm.y), -0.5f * (Zk.x - Zm.x));
     *reinterpret_cast<float4*>(o + (size_t)k * N + 2 * p) = make_float4(A.x, A.y, B.x, B.y);
@@ -466,6 +557,10 @@ int cube_fft_forward3_fast(cube_ctx* ctx, MeshLevel& L, float* data, int* rc, in
     CUBE_F3(128, 16, 8)
     CUBE_F3(64, 8, 8)
     CUBE_F3(32, 8, 4)
+    CUBE_F3(768, 48, 16)
+    CUBE_F3(384, 48, 8)
+    CUBE_F3(192, 24, 8)
+    CUBE_F3(96, 24, 4)
 #undef CUBE_F3
     default: return 0;
   }
@@ -482,6 +577,10 @@ int cube_fft_poisson_fast(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, Ki
     CUBE_PS(128, 16, 8)
     CUBE_PS(64, 8, 8)
     CUBE_PS(32, 8, 4)
+    CUBE_PS(768, 48, 16)
+    CUBE_PS(384, 48, 8)
+    CUBE_PS(192, 24, 8)
+    CUBE_PS(96, 24, 4)
 #undef CUBE_PS
     default: return 0;
   }

@@ -166,9 +166,11 @@ def test_fine_green_octant_matches_closed_form(tables):
     assert np.max(np.abs(got - ref)) <= 1e-6 * np.max(np.abs(ref))
 
 
-def test_radix3_mesh_forces(tables):
-    # nc=24 -> nf=96 = 3*2^5 exercises the radix-3 stages of the FFT
-    st, p, s = clustered_state(nc=24, nnt=2, npart=60000, seed=61)
+@pytest.mark.parametrize("nc", [24, 48])
+def test_radix3_mesh_forces(tables, nc):
+    # nf = 96 = 24*4 and 192 = 24*8: the register FFT with a radix-3 first stage on
+    # the fine mesh; the coarse meshes (24, 48) take the Stockham passes
+    st, p, s = clustered_state(nc=nc, nnt=2, npart=60000 * (nc // 24) ** 3, seed=61)
     o, g = pair(st, p, tables)
     s.a, s.a_mid, s.dt = 0.5, 0.5, 20.0
     so, sg = s.copy(), s.copy()

@@ -47,6 +47,21 @@ def test_gpu_power_spectrum_matches_restatement(tables, log_bins):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("nc", [24, 48])
+def test_gpu_power_spectrum_radix3_meshes(tables, nc):
+    # nf = 96 and 192: the forward transform with a radix-3 first stage
+    st, p, s = small_state(nc=nc, nnt=2, box=200.0, seed=19, amplitude=4.0)
+    fk, ck = tables
+    g = Cube(p, np_capacity=st.np, fk_table=fk, ck_table=ck)
+    g.load_state(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    got = g.power_spectrum(True)
+    ref = cross_power(cic_delta(particle_positions(st), nc, 4 * nc), None, box=200.0, log_bins=True)
+    assert got.shape == ref.shape
+    ok = ref[:, 0] > 0
+    np.testing.assert_allclose(got[ok, 2], ref[ok, 2], rtol=2e-4)
+
+
+@pytest.mark.gpu
 def test_gpu_cross_power_with_neutrinos(tables):
     st, _, s = small_state(nc=16, nnt=2, box=300.0, seed=13, amplitude=2.0)
     p = nu_params(nc=16, nnt=2, box=300.0)
