@@ -83,6 +83,31 @@ def test_deposit_bit_exact(pm_pair, tables):
     assert sd.testrhof == pytest.approx(st.np * st.mass_p_cdm, rel=1e-9)
 
 
+def test_deposit_bit_exact_on_dense_clumps(tables):
+    # cells of 12,000 and 24,000 particles: thousands of weights collide on the same
+    # shared-memory nodes and the 64-bit node sums (~1e14 in fixed point) carry out of
+    # their low words many times
+    from cube_nufluid_b200 import ic
+    from cube_nufluid_b200.cube import scalars_from_ic
+    rng = np.random.Generator(np.random.Philox(43))
+    parts = [rng.uniform(0, 16, (20000, 3))]
+    for c, n, sig in (((3.5, 4.5, 5.5), 12000, 0.08), ((10.5, 11.5, 2.5), 12000, 0.08), ((8.5, 8.5, 12.5), 24000, 0.02)):
+        parts.append(np.asarray(c) + rng.normal(0, sig, (n, 3)))
+    x = np.mod(np.concatenate(parts), 16.0)
+    st = ic.pack(x, rng.normal(0, 0.02, x.shape), 16, 2, a=0.5, box=100.0)
+    p = make_params(16, 2, box=100.0)
+    s = scalars_from_ic(st)
+    assert st.rhoc.max() > 20000
+    o, g = pair(st, p, tables)
+    s.a, s.a_mid, s.dt = 0.5, 0.5, 20.0
+    so, sd = s.copy(), s.copy()
+    o.particle_mesh(so, 1)
+    g.debug_deposit(sd)
+    assert np.array_equal(o.fetch(0).view(np.int32), g.fetch(0).view(np.int32))
+    assert np.array_equal(o.fetch(1).view(np.int32), g.fetch(1).view(np.int32))
+    assert sd.testrhof == pytest.approx(st.np * st.mass_p_cdm, rel=1e-9)
+
+
 def test_forces_match_fp64_oracle(pm_pair):
     st, p, s, o, g, so, sg = pm_pair
     # the library's meshes hold force*a_mid*dt/6/pi; compare against the same chain
