@@ -304,7 +304,7 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
             A((void**)&ctx->pkey, 4 * cap) && A((void**)&ctx->cursor, 4 * nce) &&
             A((void**)&ctx->big_list, 4 * nce) && A((void**)&ctx->cell_stats, 24 * nce) &&
             A((void**)&ctx->slot_r2, 8 * cap) && A((void**)&ctx->slot_s2, 8 * cap) &&
-            A((void**)&ctx->red_tmp, 8 * (2 * (nce / 1024 + 64) + 64)) &&
+            A((void**)&ctx->red_tmp, 8 * (2 * (std::max<int64_t>(nce, cap) / 1024 + 64) + 64)) &&
             A((void**)&ctx->scan_tmp, 8 * (nce / 2048 + 64)) &&
             A((void**)&ctx->rho_c_acc, 8 * nce) && A((void**)&ctx->tan_table, 4 * ctx->nvbin) &&
             A((void**)&ctx->dscal, sizeof(DevScal)) &&
@@ -432,9 +432,11 @@ int32_t cube_update_x(cube_ctx* ctx, cube_scalars* io) {
   std::swap(ctx->rhoc, ctx->rhoc2);
   std::swap(ctx->cell_start, ctx->cell_start2);
   std::swap(ctx->vfield, ctx->vfield2);
+  // |vfield|^2 per cell, |v_res|^2 and |v|^2 per particle in the new storage order
   double sums[3];
-  for (int k = 0; k < 3; ++k)
-    if ((rc = cube_tree_sum_dev(ctx, ctx->cell_stats + k * ctx->ncells, ctx->ncells, &sums[k]))) return rc;
+  if ((rc = cube_tree_sum_dev(ctx, ctx->cell_stats, ctx->ncells, &sums[0]))) return rc;
+  if ((rc = cube_tree_sum_dev(ctx, ctx->slot_r2, ctx->np, &sums[1]))) return rc;
+  if ((rc = cube_tree_sum_dev(ctx, ctx->slot_s2, ctx->np, &sums[2]))) return rc;
   const double npg = (double)(io->npglobal > 0 ? io->npglobal : ctx->np);
   io->std_vsim_c = sqrt(sums[0] / (double)ctx->ncells);
   io->std_vsim_res = sqrt(sums[1] / npg);

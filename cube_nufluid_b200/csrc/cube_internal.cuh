@@ -71,12 +71,13 @@ struct DevScal {
   unsigned int f2_pp_bits;
   int err;                     // first error code seen on the device
   int err_info;
-  unsigned long long n_big;    // re-bin cells needing the block sorter
+  unsigned long long n_big;    // re-bin cells for the warp sorter (PP: spilled bricks)
   unsigned long long itest1, npairs;
   unsigned long long moved_far;
   unsigned int nu_dt_bits[3];  // per-fluid CFL step as float bits
   unsigned long long n_huge;   // re-bin cells beyond the shared-memory sorter
   unsigned long long max_huge; // the most particles in one of them
+  unsigned long long n_mid;    // re-bin cells for the block sorter (beyond the warp sorter)
 };
 
 // one isothermal fluid of the dispersive sum (hydrogr.f90 type hydro): five FP32

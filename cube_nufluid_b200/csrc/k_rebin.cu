@@ -18,12 +18,14 @@
  *   sortsum : per target cell, sort its entries by (key, source index) --
  *             the reference order -- then run the FP32 velocity sum in that
  *             order and the division by (n + weight_v); cells with more than
- *             32 particles go to a block-wide sorter in shared memory, those
- *             beyond 4096 to one in a global scratch grown on demand
+ *             32 particles go to a warp sorter (one warp per cell, many cells
+ *             per SM, so the serial sums of different cells overlap), those
+ *             beyond 256 to a block-wide sorter in shared memory, those beyond
+ *             4096 to one in a global scratch grown on demand
  *   emit    : per particle in the old order (coalesced reads; the sort pass
  *             records each particle's slot), re-encode, move and copy the PID
- *   stats   : per cell, the velocity statistics terms summed in slot order,
- *             for the fixed-tree sums
+ *   stats   : per cell |vfield|^2; with the per-slot terms of emit, summed
+ *             by the fixed tree
  * Positions move by nint(dt_mid*v/(x_resolution*ncell)) with the integer
  * wrap of the 1- or 2-byte store (update_particle.f90:117).
  */
@@ -35,6 +37,8 @@ namespace {
 
 constexpr int RCELLS = 64;
 constexpr int SMALL = 32;
+constexpr int WARP_MAX = 256;  // warp sorter: keys + 3 velocity columns, 8 KB per warp
+constexpr int WARP_WARPS = 8;
 constexpr int BIG_MAX = 4096;
 
 struct RebinArgs {
@@ -154,7 +158,7 @@ __device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t i
   TX* xp2 = reinterpret_cast<TX*>(A.xp2);
   TV* vp2 = reinterpret_cast<TV*>(A.vp2);
   const double xstep = cube_dmul(A.codec.x_resolution, (double)A.ncell);
-  double r2 = 0.0, s2 = 0.0;
+  double r2 = 0.0, s2 = 0.0;  // ((x0^2 + x1^2) + x2^2), the first add exact
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const int64_t mv = cube_nint(cube_ddiv(cube_dmul((double)A.dt_mid, v[d]), xstep));
@@ -181,7 +185,10 @@ __device__ __forceinline__ void cell_tile(const RebinArgs& A, int64_t c, int tt[
 
 // F1: per target cell, sort its entries into the reference order and run the
 // cell's FP32 velocity sum in that order (update_particle.f90:74,83-85).
-// Cells with more than SMALL entries go to k_rebin_big.
+// Crowded cells are listed for the sorter of their size: up to WARP_MAX entries
+// at the front of big_list (k_rebin_warp), up to BIG_MAX at its back
+// (k_rebin_big), beyond that in cursor, which is free after the place pass
+// (k_rebin_huge).
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -189,8 +196,17 @@ __global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   const int n = A.cnt2[c];
   const int64_t s = A.start2[c];
   if (n > SMALL) {
-    const unsigned long long q = atomicAdd(&A.dscal->n_big, 1ull);
-    A.big_list[q] = (int32_t)c;
+    if (n <= WARP_MAX) {
+      const unsigned long long q = atomicAdd(&A.dscal->n_big, 1ull);
+      A.big_list[q] = (int32_t)c;
+    } else if (n <= BIG_MAX) {
+      const unsigned long long q = atomicAdd(&A.dscal->n_mid, 1ull);
+      A.big_list[A.ncells - 1 - (int64_t)q] = (int32_t)c;
+    } else {
+      const unsigned long long q = atomicAdd(&A.dscal->n_huge, 1ull);
+      A.cursor[q] = (int32_t)c;
+      atomicMax(&A.dscal->max_huge, (unsigned long long)n);
+    }
     return;
   }
   // insertion sort of the cell's (key, source) entries, ascending
@@ -277,26 +293,76 @@ __device__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, u
   __syncthreads();
 }
 
-// F1 for crowded cells: one CTA per cell, sorted in shared memory; cells beyond
-// BIG_MAX entries are listed (from the end of big_list) for k_rebin_huge
+// the same for one cell of at most WARP_MAX entries by one warp, in the warp's
+// own shared-memory segment (sk: WARP_MAX keys, sv: [3][WARP_MAX] velocities)
+template <int ZX, int ZV>
+__device__ void sort_sum_cell_warp(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk,
+                                   double* sv) {
+  const int lane = threadIdx.x & 31;
+  int m = 1;
+  while (m < n) m <<= 1;
+  for (int i = lane; i < m; i += 32)
+    sk[i] = i < n ? (((unsigned long long)A.pkey[s + i] << 32) | (uint32_t)A.perm[s + i]) : ~0ull;
+  __syncwarp();
+  for (int k = 2; k <= m; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = lane; i < m; i += 32) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = sk[i], bb = sk[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > bb) == up) { sk[i] = bb; sk[ixj] = a; }
+        }
+      }
+      __syncwarp();
+    }
+  int tt[3];
+  cell_tile(A, c, tt);
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t key = (uint32_t)(sk[i] >> 32);
+    const int32_t ip = (int32_t)(uint32_t)(sk[i] & 0xffffffffu);
+    A.pkey[s + i] = key;
+    A.perm[s + i] = ip;
+    A.tkey[ip] = (uint32_t)(s + i);
+    const int64_t sc = src_cell(A, key, tt);
+    for (int d = 0; d < 3; ++d)
+      sv[d * WARP_MAX + i] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
+  }
+  __syncwarp();
+  if (lane < 3) {
+    const int d = lane;
+    float acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
+    for (int i = 0; i < n; ++i) acc = (float)cube_dadd((double)acc, sv[d * WARP_MAX + i]);
+    A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
+  }
+  __syncwarp();
+}
+
+// F1 for cells of SMALL+1..WARP_MAX entries: one warp per cell
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(32 * WARP_WARPS) k_rebin_warp(RebinArgs A) {
+  extern __shared__ unsigned long long wsm[];
+  const int w = threadIdx.x >> 5;
+  unsigned long long* sk = wsm + (size_t)w * 4 * WARP_MAX;
+  double* sv = reinterpret_cast<double*>(sk + WARP_MAX);
+  const unsigned long long nw = A.dscal->n_big;
+  const unsigned long long stride = (unsigned long long)gridDim.x * WARP_WARPS;
+  for (unsigned long long b = (unsigned long long)blockIdx.x * WARP_WARPS + w; b < nw; b += stride) {
+    const int64_t c = A.big_list[b];
+    sort_sum_cell_warp<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv);
+  }
+}
+
+// F1 for cells of WARP_MAX+1..BIG_MAX entries: one CTA per cell, sorted in shared
+// memory
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
   extern __shared__ unsigned long long sk[];
   double* sv = reinterpret_cast<double*>(sk + BIG_MAX);  // [3][BIG_MAX] velocities
-  const unsigned long long nbig = A.dscal->n_big;
-  for (unsigned long long b = blockIdx.x; b < nbig; b += gridDim.x) {
-    const int64_t c = A.big_list[b];
-    const int n = A.cnt2[c];
-    const int64_t s = A.start2[c];
-    if (n > BIG_MAX) {
-      if (threadIdx.x == 0) {
-        const unsigned long long q = atomicAdd(&A.dscal->n_huge, 1ull);
-        A.big_list[A.ncells - 1 - (int64_t)q] = (int32_t)c;
-        atomicMax(&A.dscal->max_huge, (unsigned long long)n);
-      }
-      continue;
-    }
-    sort_sum_cell<ZX, ZV>(A, c, n, s, sk, sv, BIG_MAX);
+  const unsigned long long nmid = A.dscal->n_mid;
+  for (unsigned long long b = blockIdx.x; b < nmid; b += gridDim.x) {
+    const int64_t c = A.big_list[A.ncells - 1 - (int64_t)b];
+    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, BIG_MAX);
   }
 }
 
@@ -311,7 +377,7 @@ __global__ void __launch_bounds__(1024) k_rebin_huge(RebinArgs A, unsigned long 
   const unsigned long long nh = A.dscal->n_huge;
   const int vstride = (int)((slot_u64 - mmax) / 3);
   for (unsigned long long q = blockIdx.x; q < nh; q += gridDim.x) {
-    const int64_t c = A.big_list[A.ncells - 1 - (int64_t)q];
+    const int64_t c = A.cursor[q];
     sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, vstride);
   }
 }
@@ -351,23 +417,16 @@ __global__ void __launch_bounds__(256) k_rebin_emit(RebinArgs A, int64_t np) {
   }
 }
 
-// F3: per cell, the statistics terms summed in slot order
+// F3: per cell, |vfield|^2 in FP32 (update_particle.f90:183); the per-particle
+// terms are summed from slot_r2 and slot_s2 by the fixed tree
 __global__ void k_rebin_stats(RebinArgs A) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= A.ncells) return;
-  const int64_t s0 = A.start2[c], s1 = s0 + A.cnt2[c];
-  double sr = 0.0, ss = 0.0;
-  for (int64_t q = s0; q < s1; ++q) {
-    sr = cube_dadd(sr, A.slot_r2[q]);
-    ss = cube_dadd(ss, A.slot_s2[q]);
-  }
   float vfn[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) vfn[d] = A.vfield2[(size_t)d * A.ncells + c];
   const float f2 = cube_fadd(cube_fadd(cube_fmul(vfn[0], vfn[0]), cube_fmul(vfn[1], vfn[1])), cube_fmul(vfn[2], vfn[2]));
   A.stats[c] = (double)f2;
-  A.stats[A.ncells + c] = sr;
-  A.stats[2 * A.ncells + c] = ss;
 }
 
 template <int ZX, int ZV>
@@ -381,6 +440,10 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
   CUBE_LAUNCH_CHECK(ctx);
   const unsigned cb = (unsigned)((ctx->ncells + 255) / 256);
   k_rebin_sortsum<ZX, ZV><<<cb, 256, 0, ctx->stream>>>(A);
+  CUBE_LAUNCH_CHECK(ctx);
+  const size_t wsmem = sizeof(unsigned long long) * 4 * WARP_MAX * WARP_WARPS;
+  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_warp<ZX, ZV>, wsmem));
+  k_rebin_warp<ZX, ZV><<<3 * ctx->num_sms, 32 * WARP_WARPS, wsmem, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
   const size_t smem = sizeof(unsigned long long) * BIG_MAX + sizeof(double) * 3 * BIG_MAX;
   CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_big<ZX, ZV>, smem));

@@ -25,9 +25,9 @@
  *
  * Two choices replace reference behaviour that is not deterministic:
  *   - the velocity statistics of update_xp (update_particle.f90:174-226) are an
- *     OpenMP reduction in the reference; here they are per-cell sequential sums
- *     followed by a fixed pairwise tree over cells (cube_tree_sum below), the
- *     same order the GPU uses;
+ *     OpenMP reduction in the reference; here the per-particle terms, in the new
+ *     storage order, and the per-cell terms are each summed by a fixed pairwise
+ *     tree (cube_tree_sum below), the same order the GPU uses;
  *   - the fine deposit has two modes: the reference's FP32 accumulation in its
  *     (layer,k,j,i,l) order, and a 64-bit fixed-point accumulation (weights
  *     scaled by 2^32) whose result is order-independent.
@@ -285,24 +285,24 @@ int update_xp(Orc& o, cube_scalars* s) {
   o.rhoc.swap(nrho); o.vfield.swap(nvf);
   o.np = np_prev;
   s->nplocal = np_prev;
-  // velocity statistics (update_particle.f90:171-226) in the fixed order
+  // velocity statistics (update_particle.f90:171-226) in the fixed order: the
+  // per-cell |vfield|^2 and the per-particle |v_res|^2, |v|^2 in the new storage
+  // order, each list summed by the fixed pairwise tree
   std::vector<int64_t> cs2 = compact_cell_start(o);
-  std::vector<double> sc(ncells), sr(ncells), ss(ncells);
+  std::vector<double> sc(ncells), sr(o.np), ss(o.np);
   for (int64_t c = 0; c < ncells; ++c) {
     const float* vf = &o.vfield[3 * c];
     float f2 = cube_fadd(cube_fadd(cube_fmul(vf[0], vf[0]), cube_fmul(vf[1], vf[1])), cube_fmul(vf[2], vf[2]));
     sc[c] = (double)f2;
-    double r = 0, q = 0;
     for (int64_t ip = cs2[c]; ip < cs2[c + 1]; ++ip) {
       double v[3], w[3];
       for (int d = 0; d < 3; ++d) {
         v[d] = cube_vdecode(tanf_code(o, o.vp[3 * ip + d]), coef);
         w[d] = cube_dadd(v[d], (double)vf[d]);
       }
-      r = cube_dadd(r, cube_dadd(cube_dadd(cube_dmul(v[0], v[0]), cube_dmul(v[1], v[1])), cube_dmul(v[2], v[2])));
-      q = cube_dadd(q, cube_dadd(cube_dadd(cube_dmul(w[0], w[0]), cube_dmul(w[1], w[1])), cube_dmul(w[2], w[2])));
+      sr[ip] = cube_dadd(cube_dadd(cube_dmul(v[0], v[0]), cube_dmul(v[1], v[1])), cube_dmul(v[2], v[2]));
+      ss[ip] = cube_dadd(cube_dadd(cube_dmul(w[0], w[0]), cube_dmul(w[1], w[1])), cube_dmul(w[2], w[2]));
     }
-    sr[c] = r; ss[c] = q;
   }
   const double sum_c = cube_tree_sum(sc), sum_r = cube_tree_sum(sr), sum_s = cube_tree_sum(ss);
   const double npg = (double)(s->npglobal > 0 ? s->npglobal : o.np);
