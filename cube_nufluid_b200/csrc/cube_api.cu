@@ -214,7 +214,7 @@ void cube_destroy(cube_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   void* ptrs[] = {ctx->xp, ctx->vp, ctx->pid, ctx->xp2, ctx->vp2, ctx->pid2, ctx->rhoc, ctx->rhoc2,
                   ctx->cell_start, ctx->cell_start2, ctx->vfield, ctx->vfield2, ctx->tcell, ctx->tkey,
-                  ctx->perm, ctx->pkey, ctx->cursor, ctx->big_list, ctx->cell_stats, ctx->slot_r2, ctx->slot_s2,
+                  ctx->perm, ctx->pkey, ctx->cursor, ctx->big_list, ctx->rebin_items, ctx->cell_stats, ctx->slot_r2, ctx->slot_s2,
                   ctx->red_tmp,
                   ctx->scan_tmp, ctx->fine.rho, ctx->fine.force, ctx->fine.ext, ctx->fine.kern, ctx->fine.plan.tw, ctx->fine.plan.tw2,
                   ctx->coarse.rho, ctx->coarse.force, ctx->coarse.ext, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->coarse.plan.tw2,
@@ -303,6 +303,7 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
             A((void**)&ctx->tcell, 4 * cap) && A((void**)&ctx->tkey, 4 * cap) && A((void**)&ctx->perm, 4 * cap) &&
             A((void**)&ctx->pkey, 4 * cap) && A((void**)&ctx->cursor, 4 * nce) &&
             A((void**)&ctx->big_list, 4 * nce) && A((void**)&ctx->cell_stats, 24 * nce) &&
+            A((void**)&ctx->rebin_items, 32 * cube_rebin_items_max(nce, cap)) &&
             A((void**)&ctx->slot_r2, 8 * cap) && A((void**)&ctx->slot_s2, 8 * cap) &&
             A((void**)&ctx->red_tmp, 8 * (2 * (std::max<int64_t>(nce, cap) / 1024 + 64) + 64)) &&
             A((void**)&ctx->scan_tmp, 8 * (nce / 2048 + 64)) &&

@@ -78,6 +78,8 @@ struct DevScal {
   unsigned long long n_huge;   // re-bin cells beyond the shared-memory sorter
   unsigned long long max_huge; // the most particles in one of them
   unsigned long long n_mid;    // re-bin cells for the block sorter (beyond the warp sorter)
+  unsigned long long huge_next;  // next cell for a k_rebin_huge block
+  unsigned long long n_items;    // re-bin work items beyond the one per 64-cell group
 };
 
 // one isothermal fluid of the dispersive sum (hydrogr.f90 type hydro): five FP32
@@ -122,6 +124,7 @@ struct cube_ctx {
   // re-bin scratch
   int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
   int32_t* big_list;
+  int64_t* rebin_items;  // [4] per item: first cell, cells, first and end particle
   double* cell_stats;   // [3][ncells]
   double* slot_r2; double* slot_s2;  // per-slot statistics terms of the re-bin
   double* red_tmp;      // scratch for tree sums
@@ -320,6 +323,7 @@ __device__ __forceinline__ int32_t cube_vencode_fast(const cube_codec* c, double
 
 // ---- launchers (implemented in the k_*.cu files) -----------------------------
 int cube_rebin(cube_ctx* ctx, cube_scalars* io);
+int64_t cube_rebin_items_max(int64_t ncells, int64_t cap);
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks);
 int cube_force_scale(cube_ctx* ctx, MeshLevel& L, KickScale ks);

@@ -36,6 +36,7 @@
 namespace {
 
 constexpr int RCELLS = 64;
+constexpr int PMAX = 4096;     // particles per work item of the count and emit passes
 constexpr int SMALL = 32;
 constexpr int WARP_MAX = 256;  // warp sorter: keys + 3 velocity columns, 8 KB per warp
 constexpr int WARP_WARPS = 8;
@@ -48,6 +49,7 @@ struct RebinArgs {
   int32_t* cnt2; int64_t* start2; float* vfield2;
   int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
   int32_t* big_list; double* stats; double* slot_r2; double* slot_s2;
+  const int64_t* items; int64_t items_max;
   const double* dec; int half_nvbin;  // tan(code)/coef per code (cube_vdec_table)
   cube_codec codec; double coef, inv_pi;
   int64_t cap, ncells;
@@ -66,14 +68,74 @@ __device__ __forceinline__ double decode_v(const RebinArgs& A, int64_t ip, int d
   return __ldg(&A.dec[code + A.half_nvbin]);
 }
 
+// Work items of the count and emit passes: a run of at most RCELLS cells and a
+// particle range inside it of at most PMAX particles.  Item g < ngroups is the
+// 64-cell group g (all of it when it holds at most PMAX particles); a crowded
+// group is cut greedily into runs of whole cells, a cell beyond PMAX particles
+// into ranges of PMAX, and the items after its first are appended after the
+// groups.  A group of cnt > PMAX particles makes at most 4 cnt/PMAX items.
+__device__ __forceinline__ void put_item(const RebinArgs& A, int64_t* items, int64_t g, bool& first, int64_t c0,
+                                         int64_t ncl, int64_t p0, int64_t p1) {
+  int64_t idx = g;
+  if (!first) {
+    const int64_t ngroups = (A.ncells + RCELLS - 1) / RCELLS;
+    idx = ngroups + (int64_t)atomicAdd(&A.dscal->n_items, 1ull);
+    if (idx >= A.items_max) {
+      cube_dev_error(A.dscal, CUBE_ERR_CAPACITY, (int)(g & 0x7fffffff));
+      return;
+    }
+  }
+  first = false;
+  int64_t* it = items + 4 * idx;
+  it[0] = c0; it[1] = ncl; it[2] = p0; it[3] = p1;
+}
+
+__global__ void k_rebin_items(RebinArgs A, int64_t* __restrict__ items) {
+  const int64_t ngroups = (A.ncells + RCELLS - 1) / RCELLS;
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= ngroups) return;
+  const int64_t c0 = g * RCELLS;
+  const int64_t ncl = min((int64_t)RCELLS, A.ncells - c0);
+  const int64_t* cs = A.cell_start;
+  bool first = true;
+  if (cs[c0 + ncl] - cs[c0] <= PMAX) {
+    put_item(A, items, g, first, c0, ncl, cs[c0], cs[c0 + ncl]);
+    return;
+  }
+  int64_t ic = c0;  // first cell of the open run
+  for (int64_t c = c0; c < c0 + ncl; ++c) {
+    const int64_t a = cs[c], e = cs[c + 1];
+    if (e - a > PMAX) {
+      if (c > ic) put_item(A, items, g, first, ic, c - ic, cs[ic], a);
+      for (int64_t q = a; q < e; q += PMAX) put_item(A, items, g, first, c, 1, q, min(q + PMAX, e));
+      ic = c + 1;
+    } else if (e - cs[ic] > PMAX) {  // cell c does not fit the open run (c > ic here)
+      put_item(A, items, g, first, ic, c - ic, cs[ic], a);
+      ic = c;
+    }
+  }
+  if (c0 + ncl > ic) put_item(A, items, g, first, ic, c0 + ncl - ic, cs[ic], cs[c0 + ncl]);
+}
+
+// item of this block, or false past the last
+__device__ __forceinline__ bool get_item(const RebinArgs& A, int64_t& c0, int& ncl, int64_t& p0, int64_t& p1) {
+  const int64_t ngroups = (A.ncells + RCELLS - 1) / RCELLS;
+  const int64_t b = blockIdx.x;
+  if (b >= ngroups + (int64_t)A.dscal->n_items || b >= A.items_max) return false;
+  const int64_t* it = A.items + 4 * b;
+  c0 = it[0]; ncl = (int)it[1]; p0 = it[2]; p1 = it[3];
+  return true;
+}
+
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_rebin_count(RebinArgs A) {
   typedef typename CodeT<ZX>::T TX;
   const TX* xp = reinterpret_cast<const TX*>(A.xp);
   __shared__ int64_t cs[RCELLS + 1];
   __shared__ int cl[RCELLS][3], ctt[RCELLS][3];  // per cell: local coords, tile coords
-  const int64_t c0 = (int64_t)blockIdx.x * RCELLS;
-  const int ncl = (int)min((int64_t)RCELLS, A.ncells - c0);
+  int64_t c0, p0, p1;
+  int ncl;
+  if (!get_item(A, c0, ncl, p0, p1)) return;
   const int nt = A.nt, nnt = A.nnt, ncb = A.ncb, nte = A.nte;
   for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = A.cell_start[c0 + i];
   for (int i = threadIdx.x; i < ncl; i += blockDim.x) {
@@ -84,7 +146,7 @@ __global__ void __launch_bounds__(256) k_rebin_count(RebinArgs A) {
     ctt[i][2] = tb[2] / nt;
   }
   __syncthreads();
-  for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
+  for (int64_t ip = p0 + threadIdx.x; ip < p1; ip += blockDim.x) {
     int lo = 0, hi = ncl - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -246,12 +308,28 @@ __global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   for (int d = 0; d < 3; ++d) A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc[d], den);
 }
 
+// acc + x[0] + x[1] + ... + x[n-1] left to right, each partial sum rounded to FP32
+// through FP64 (the reference's real(4) accumulation of real(8) terms); the
+// loads of eight terms are issued ahead of their adds
+__device__ __forceinline__ float ordered_sum(float acc, const double* x, int n) {
+  int i = 0;
+  for (; i + 8 <= n; i += 8) {
+    double t[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) t[u] = x[i + u];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) acc = (float)cube_dadd((double)acc, t[u]);
+  }
+  for (; i < n; ++i) acc = (float)cube_dadd((double)acc, x[i]);
+  return acc;
+}
+
 // one crowded cell by the whole CTA: bitonic sort of (key<<32|source) in sk (m =
 // next power of two of n entries), the sorted order back to the slots, the
 // per-particle velocities into sv[d * vstride + i] in parallel, the FP32 sum by
 // one thread per component in order.  sk and sv may be shared or global memory.
 template <int ZX, int ZV>
-__device__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk, double* sv,
+__device__ __forceinline__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk, double* sv,
                               int vstride) {
   int m = 1;
   while (m < n) m <<= 1;
@@ -286,8 +364,8 @@ __device__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, u
   __syncthreads();
   if (threadIdx.x < 3) {
     const int d = threadIdx.x;
-    float acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
-    for (int i = 0; i < n; ++i) acc = (float)cube_dadd((double)acc, sv[(size_t)d * vstride + i]);
+    const float acc = ordered_sum((float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1),
+                                  sv + (size_t)d * vstride, n);
     A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
   }
   __syncthreads();
@@ -296,7 +374,7 @@ __device__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, u
 // the same for one cell of at most WARP_MAX entries by one warp, in the warp's
 // own shared-memory segment (sk: WARP_MAX keys, sv: [3][WARP_MAX] velocities)
 template <int ZX, int ZV>
-__device__ void sort_sum_cell_warp(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk,
+__device__ __forceinline__ void sort_sum_cell_warp(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk,
                                    double* sv) {
   const int lane = threadIdx.x & 31;
   int m = 1;
@@ -331,8 +409,8 @@ __device__ void sort_sum_cell_warp(const RebinArgs& A, int64_t c, int n, int64_t
   __syncwarp();
   if (lane < 3) {
     const int d = lane;
-    float acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
-    for (int i = 0; i < n; ++i) acc = (float)cube_dadd((double)acc, sv[d * WARP_MAX + i]);
+    const float acc = ordered_sum((float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1),
+                                  sv + d * WARP_MAX, n);
     A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
   }
   __syncwarp();
@@ -372,14 +450,54 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(1024) k_rebin_huge(RebinArgs A, unsigned long long* __restrict__ scratch,
                                                      size_t slot_u64, int mmax) {
+  __shared__ unsigned long long qs;
   unsigned long long* sk = scratch + (size_t)blockIdx.x * slot_u64;
   double* sv = reinterpret_cast<double*>(sk + mmax);
   const unsigned long long nh = A.dscal->n_huge;
   const int vstride = (int)((slot_u64 - mmax) / 3);
-  for (unsigned long long q = blockIdx.x; q < nh; q += gridDim.x) {
+  while (true) {  // cells taken in list order (largest first) as blocks become free
+    if (threadIdx.x == 0) qs = atomicAdd(&A.dscal->huge_next, 1ull);
+    __syncthreads();
+    const unsigned long long q = qs;
+    __syncthreads();
+    if (q >= nh) break;
     const int64_t c = A.cursor[q];
     sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, vstride);
   }
+}
+
+// the huge-cell list in decreasing particle count (bitonic sort of (~n, cell) in
+// shared memory), so that the largest cells start first; lists longer than
+// HUGE_ORDER stay in arrival order
+constexpr int HUGE_ORDER = 4096;
+__global__ void __launch_bounds__(1024) k_rebin_huge_order(RebinArgs A) {
+  __shared__ unsigned long long h[HUGE_ORDER];
+  const int nh = (int)A.dscal->n_huge;
+  if (nh < 2 || nh > HUGE_ORDER) return;
+  int m = 1;
+  while (m < nh) m <<= 1;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    if (i < nh) {
+      const int32_t c = A.cursor[i];
+      h[i] = ((unsigned long long)(~(uint32_t)A.cnt2[c]) << 32) | (uint32_t)c;
+    } else {
+      h[i] = ~0ull;
+    }
+  }
+  __syncthreads();
+  for (int k = 2; k <= m; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const unsigned long long a = h[i], bb = h[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > bb) == up) { h[i] = bb; h[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  for (int i = threadIdx.x; i < nh; i += blockDim.x) A.cursor[i] = (int32_t)(uint32_t)(h[i] & 0xffffffffu);
 }
 
 // F2: one thread per particle in its old storage order (coalesced reads of its
@@ -389,11 +507,12 @@ __global__ void __launch_bounds__(1024) k_rebin_huge(RebinArgs A, unsigned long 
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_rebin_emit(RebinArgs A, int64_t np) {
   __shared__ int64_t cs[RCELLS + 1];
-  const int64_t c0 = (int64_t)blockIdx.x * RCELLS;
-  const int ncl = (int)min((int64_t)RCELLS, A.ncells - c0);
+  int64_t c0, p0, p1;
+  int ncl;
+  if (!get_item(A, c0, ncl, p0, p1)) return;
   for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = A.cell_start[c0 + i];
   __syncthreads();
-  for (int64_t ip = cs[0] + threadIdx.x; ip < cs[ncl]; ip += blockDim.x) {
+  for (int64_t ip = p0 + threadIdx.x; ip < p1; ip += blockDim.x) {
     int lo = 0, hi = ncl - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -432,7 +551,12 @@ __global__ void k_rebin_stats(RebinArgs A) {
 template <int ZX, int ZV>
 int run_rebin(cube_ctx* ctx, RebinArgs& A) {
   const int64_t nb = (ctx->ncells + RCELLS - 1) / RCELLS;
-  k_rebin_count<ZX, ZV><<<(unsigned)nb, 256, 0, ctx->stream>>>(A);
+  k_rebin_items<<<(unsigned)((nb + 255) / 256), 256, 0, ctx->stream>>>(A, ctx->rebin_items);
+  CUBE_LAUNCH_CHECK(ctx);
+  // one block per item: the groups, then at most 4 np/PMAX more (blocks past the
+  // last item return at once)
+  const int64_t ni = std::min<int64_t>(A.items_max, nb + 4 * (ctx->np / PMAX + 1));
+  k_rebin_count<ZX, ZV><<<(unsigned)ni, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
   int rc = cube_exclusive_scan(ctx, A.cnt2, ctx->ncells, A.start2);
   if (rc) return rc;
@@ -455,11 +579,13 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
                                      ctx->stream));
   CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (hv[0]) {
+    // one slot per SM of keys (mmax, a power of two) and three velocity columns
+    // of mmax: the scratch is reallocated only when mmax doubles
     int mmax = 1;
     while ((unsigned long long)mmax < hv[1]) mmax <<= 1;
-    const size_t slot = (size_t)mmax + 3 * (size_t)hv[1];
-    const int grid = (int)std::min<unsigned long long>(hv[0], 148);
-    const size_t need = sizeof(unsigned long long) * slot * grid;
+    const size_t slot = 4 * (size_t)mmax;
+    const int grid = (int)std::min<unsigned long long>(hv[0], (unsigned long long)ctx->num_sms);
+    const size_t need = sizeof(unsigned long long) * slot * ctx->num_sms;
     if (need > ctx->rebin_scratch_bytes) {
       if (ctx->rebin_scratch) cudaFree(ctx->rebin_scratch);
       ctx->rebin_scratch = nullptr;
@@ -467,11 +593,13 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
       CUBE_CUDA_TRY(ctx, cudaMalloc(&ctx->rebin_scratch, need));
       ctx->rebin_scratch_bytes = need;
     }
+    k_rebin_huge_order<<<1, 1024, 0, ctx->stream>>>(A);
+    CUBE_LAUNCH_CHECK(ctx);
     k_rebin_huge<ZX, ZV><<<grid, 1024, 0, ctx->stream>>>(A, reinterpret_cast<unsigned long long*>(ctx->rebin_scratch),
                                                          slot, mmax);
     CUBE_LAUNCH_CHECK(ctx);
   }
-  k_rebin_emit<ZX, ZV><<<(unsigned)nb, 256, 0, ctx->stream>>>(A, ctx->np);
+  k_rebin_emit<ZX, ZV><<<(unsigned)ni, 256, 0, ctx->stream>>>(A, ctx->np);
   CUBE_LAUNCH_CHECK(ctx);
   k_rebin_stats<<<cb, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
@@ -479,6 +607,10 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
 }
 
 }  // namespace
+
+int64_t cube_rebin_items_max(int64_t ncells, int64_t cap) {
+  return (ncells + RCELLS - 1) / RCELLS + 4 * (cap / PMAX + 1) + 64;
+}
 
 int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
   io->dt_mid = (io->dt_old + io->dt) / 2;
@@ -492,6 +624,7 @@ int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
   A.cnt2 = ctx->rhoc2; A.start2 = ctx->cell_start2; A.vfield2 = ctx->vfield2;
   A.tcell = ctx->tcell; A.tkey = ctx->tkey; A.perm = ctx->perm; A.pkey = ctx->pkey; A.cursor = ctx->cursor;
   A.big_list = ctx->big_list; A.stats = ctx->cell_stats;
+  A.items = ctx->rebin_items; A.items_max = cube_rebin_items_max(ctx->ncells, ctx->cap);
   A.slot_r2 = ctx->slot_r2; A.slot_s2 = ctx->slot_s2;
   A.half_nvbin = ctx->nvbin / 2;
   A.codec = ctx->codec; A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
