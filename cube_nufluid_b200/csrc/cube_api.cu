@@ -230,6 +230,7 @@ void cube_destroy(cube_ctx* ctx) {
   if (ctx->nu.partial) cudaFree(ctx->nu.partial);
   if (ctx->pp_scratch) cudaFree(ctx->pp_scratch);
   if (ctx->rebin_scratch) cudaFree(ctx->rebin_scratch);
+  if (ctx->rebin_mid_scratch) cudaFree(ctx->rebin_mid_scratch);
   for (double* t : ctx->vdec)
     if (t) cudaFree(t);
   if (ctx->hscal) cudaFreeHost(ctx->hscal);

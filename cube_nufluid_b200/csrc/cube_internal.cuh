@@ -80,6 +80,7 @@ struct DevScal {
   unsigned long long n_mid;    // re-bin cells for the block sorter (beyond the warp sorter)
   unsigned long long huge_next;  // next cell for a k_rebin_huge block
   unsigned long long n_items;    // re-bin work items beyond the one per 64-cell group
+  unsigned long long mid_next;   // next cell for a k_rebin_big block
 };
 
 // one isothermal fluid of the dispersive sum (hydrogr.f90 type hydro): five FP32
@@ -138,6 +139,7 @@ struct cube_ctx {
   size_t pp_scratch_bytes = 0;
   void* rebin_scratch = nullptr;  // sort slots of re-bin cells beyond 4096 particles, grown on demand
   size_t rebin_scratch_bytes = 0;
+  void* rebin_mid_scratch = nullptr;  // velocity columns of the block sorter, allocated on first use
   // meshes
   MeshLevel fine, coarse;
   unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator
@@ -324,6 +326,19 @@ __device__ __forceinline__ int32_t cube_vencode_fast(const cube_codec* c, double
 // ---- launchers (implemented in the k_*.cu files) -----------------------------
 int cube_rebin(cube_ctx* ctx, cube_scalars* io);
 int64_t cube_rebin_items_max(int64_t ncells, int64_t cap);
+// work items over the cells of cell_start into ctx->rebin_items (a run of at most
+// 64 cells and at most 4096 of its particles each); *blocks = launch size, one
+// block per item, blocks past the last return (cube_cell_item)
+int cube_cell_items(cube_ctx* ctx, const int64_t* cell_start, int64_t* blocks);
+__device__ __forceinline__ bool cube_cell_item(const int64_t* items, int64_t ncells, int64_t items_max,
+                                               const DevScal* dscal, int64_t& c0, int& ncl, int64_t& p0, int64_t& p1) {
+  const int64_t ngroups = (ncells + 63) / 64;
+  const int64_t b = blockIdx.x;
+  if (b >= ngroups + (int64_t)dscal->n_items || b >= items_max) return false;
+  const int64_t* it = items + 4 * b;
+  c0 = it[0]; ncl = (int)it[1]; p0 = it[2]; p1 = it[3];
+  return true;
+}
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);
 int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks);
 int cube_force_scale(cube_ctx* ctx, MeshLevel& L, KickScale ks);

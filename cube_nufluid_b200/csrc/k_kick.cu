@@ -21,7 +21,7 @@
 
 namespace {
 
-constexpr int KCELLS = 64;  // cells per CTA
+constexpr int KCELLS = 64;  // cells per work item at most (cube_cell_items)
 
 // One thread per particle: the node indices and CIC weights of a particle are
 // shared by its three components, which then run their chains (decode, eight
@@ -34,14 +34,15 @@ constexpr int KCELLS = 64;  // cells per CTA
 // shared memory first was measured twice as slow: at ~500 particles per brick
 // the copies of 17^3 x 3 nodes outweigh the gathers they replace, which hit L1/L2.)
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
+__global__ void __launch_bounds__(256, 3) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                               const int64_t* __restrict__ cell_start, const float* __restrict__ vfield,
                                               int64_t cap, int64_t ncells, int nc, int nt, int nnt,
                                               const float* __restrict__ ff, size_t fcomp, int frp, size_t fplane,
                                               const float* __restrict__ fc, size_t ccomp, int crp, size_t cplane,
                                               const double* __restrict__ dec_old, const double* __restrict__ dec_new,
                                               int half_nvbin, cube_codec codec, double coef_new, double inv_pi,
-                                              DevScal* __restrict__ dscal) {
+                                              DevScal* __restrict__ dscal, const int64_t* __restrict__ items,
+                                              int64_t items_max) {
   typedef typename CodeT<ZX>::T TX;
   typedef typename CodeT<ZV>::T TV;
   const TX* xp = reinterpret_cast<const TX*>(xp_);
@@ -49,15 +50,15 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
   __shared__ int64_t cs[KCELLS + 1];
   __shared__ int cl[KCELLS][3], ctb[KCELLS][3];  // per cell: local coords, tile base
   __shared__ unsigned int vmx_s[3];
-  const int64_t c0 = (int64_t)blockIdx.x * KCELLS;
-  const int ncl = (int)min((int64_t)KCELLS, ncells - c0);
+  int64_t c0, p0, p1;
+  int ncl;
+  if (!cube_cell_item(items, ncells, items_max, dscal, c0, ncl, p0, p1)) return;
   for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = cell_start[c0 + i];
   if (threadIdx.x < ncl) cube_cell_coords(c0 + threadIdx.x, nt, nnt, cl[threadIdx.x], ctb[threadIdx.x]);
   if (threadIdx.x < 3) vmx_s[threadIdx.x] = 0u;
   __syncthreads();
   const int nf = 4 * nc;
-  const int64_t p0 = cs[0];
-  const int npb = (int)(cs[ncl] - p0);
+  const int npb = (int)(p1 - p0);
   const float xres = ZX == 1 ? 0.00390625f : 1.52587890625e-05f;  // 2^-8, 2^-16
   // reference corner order: 111,211,121,112,122,212,221,222
   const int ox[8] = {0, 1, 0, 0, 0, 1, 1, 1}, oy[8] = {0, 0, 1, 0, 1, 0, 1, 1}, oz[8] = {0, 0, 0, 1, 1, 1, 0, 1};
@@ -145,7 +146,10 @@ __global__ void __launch_bounds__(256) k_kick(const void* __restrict__ xp_, void
 
 template <int ZX, int ZV>
 int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
-  const int64_t blocks = (ctx->ncells + KCELLS - 1) / KCELLS;
+  // work items of at most 64 cells and 4096 particles, so that the blocks over
+  // crowded cells take no longer than the others
+  int64_t blocks = 0;
+  if (int irc = cube_cell_items(ctx, ctx->cell_start, &blocks)) return irc;
   const double coef_old = cube_vcoef(&ctx->codec, io->sigma_vi);
   const double coef_new = cube_vcoef(&ctx->codec, io->sigma_vi_new);
   int rc;
@@ -158,7 +162,8 @@ int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
   k_kick<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
       ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, F.force,
       (size_t)F.n * F.plane, F.rp, F.plane, Cc.force, (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, dec_old, dec_new,
-      ctx->nvbin / 2, ctx->codec, coef_new, 1.0 / (double)ctx->codec.pi_f, ctx->dscal);
+      ctx->nvbin / 2, ctx->codec, coef_new, 1.0 / (double)ctx->codec.pi_f, ctx->dscal, ctx->rebin_items,
+      cube_rebin_items_max(ctx->ncells, ctx->cap));
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }

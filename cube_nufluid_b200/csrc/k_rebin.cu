@@ -35,7 +35,7 @@
 
 namespace {
 
-constexpr int RCELLS = 64;
+constexpr int RCELLS = 64;  // cube_cell_item assumes 64-cell groups
 constexpr int PMAX = 4096;     // particles per work item of the count and emit passes
 constexpr int SMALL = 32;
 constexpr int WARP_MAX = 256;  // warp sorter: keys + 3 velocity columns, 8 KB per warp
@@ -68,20 +68,20 @@ __device__ __forceinline__ double decode_v(const RebinArgs& A, int64_t ip, int d
   return __ldg(&A.dec[code + A.half_nvbin]);
 }
 
-// Work items of the count and emit passes: a run of at most RCELLS cells and a
-// particle range inside it of at most PMAX particles.  Item g < ngroups is the
-// 64-cell group g (all of it when it holds at most PMAX particles); a crowded
-// group is cut greedily into runs of whole cells, a cell beyond PMAX particles
-// into ranges of PMAX, and the items after its first are appended after the
-// groups.  A group of cnt > PMAX particles makes at most 4 cnt/PMAX items.
-__device__ __forceinline__ void put_item(const RebinArgs& A, int64_t* items, int64_t g, bool& first, int64_t c0,
-                                         int64_t ncl, int64_t p0, int64_t p1) {
+// Work items of the count and emit passes (and of the kick): a run of at most
+// RCELLS cells and a particle range inside it of at most PMAX particles.  Item
+// g < ngroups is the 64-cell group g (all of it when it holds at most PMAX
+// particles); a crowded group is cut greedily into runs of whole cells, a cell
+// beyond PMAX particles into ranges of PMAX, and the items after its first are
+// appended after the groups.  A group of cnt > PMAX particles makes at most
+// 4 cnt/PMAX items.
+__device__ __forceinline__ void put_item(int64_t* items, int64_t items_max, int64_t ngroups, DevScal* dscal, int64_t g,
+                                         bool& first, int64_t c0, int64_t ncl, int64_t p0, int64_t p1) {
   int64_t idx = g;
   if (!first) {
-    const int64_t ngroups = (A.ncells + RCELLS - 1) / RCELLS;
-    idx = ngroups + (int64_t)atomicAdd(&A.dscal->n_items, 1ull);
-    if (idx >= A.items_max) {
-      cube_dev_error(A.dscal, CUBE_ERR_CAPACITY, (int)(g & 0x7fffffff));
+    idx = ngroups + (int64_t)atomicAdd(&dscal->n_items, 1ull);
+    if (idx >= items_max) {
+      cube_dev_error(dscal, CUBE_ERR_CAPACITY, (int)(g & 0x7fffffff));
       return;
     }
   }
@@ -90,41 +90,37 @@ __device__ __forceinline__ void put_item(const RebinArgs& A, int64_t* items, int
   it[0] = c0; it[1] = ncl; it[2] = p0; it[3] = p1;
 }
 
-__global__ void k_rebin_items(RebinArgs A, int64_t* __restrict__ items) {
-  const int64_t ngroups = (A.ncells + RCELLS - 1) / RCELLS;
+__global__ void k_cell_items(const int64_t* __restrict__ cs, int64_t ncells, int64_t* __restrict__ items,
+                             int64_t items_max, DevScal* dscal) {
+  const int64_t ngroups = (ncells + RCELLS - 1) / RCELLS;
   const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (g >= ngroups) return;
   const int64_t c0 = g * RCELLS;
-  const int64_t ncl = min((int64_t)RCELLS, A.ncells - c0);
-  const int64_t* cs = A.cell_start;
+  const int64_t ncl = min((int64_t)RCELLS, ncells - c0);
   bool first = true;
   if (cs[c0 + ncl] - cs[c0] <= PMAX) {
-    put_item(A, items, g, first, c0, ncl, cs[c0], cs[c0 + ncl]);
+    put_item(items, items_max, ngroups, dscal, g, first, c0, ncl, cs[c0], cs[c0 + ncl]);
     return;
   }
   int64_t ic = c0;  // first cell of the open run
   for (int64_t c = c0; c < c0 + ncl; ++c) {
     const int64_t a = cs[c], e = cs[c + 1];
     if (e - a > PMAX) {
-      if (c > ic) put_item(A, items, g, first, ic, c - ic, cs[ic], a);
-      for (int64_t q = a; q < e; q += PMAX) put_item(A, items, g, first, c, 1, q, min(q + PMAX, e));
+      if (c > ic) put_item(items, items_max, ngroups, dscal, g, first, ic, c - ic, cs[ic], a);
+      for (int64_t q = a; q < e; q += PMAX)
+        put_item(items, items_max, ngroups, dscal, g, first, c, 1, q, min(q + PMAX, e));
       ic = c + 1;
     } else if (e - cs[ic] > PMAX) {  // cell c does not fit the open run (c > ic here)
-      put_item(A, items, g, first, ic, c - ic, cs[ic], a);
+      put_item(items, items_max, ngroups, dscal, g, first, ic, c - ic, cs[ic], a);
       ic = c;
     }
   }
-  if (c0 + ncl > ic) put_item(A, items, g, first, ic, c0 + ncl - ic, cs[ic], cs[c0 + ncl]);
+  if (c0 + ncl > ic) put_item(items, items_max, ngroups, dscal, g, first, ic, c0 + ncl - ic, cs[ic], cs[c0 + ncl]);
 }
 
 // item of this block, or false past the last
 __device__ __forceinline__ bool get_item(const RebinArgs& A, int64_t& c0, int& ncl, int64_t& p0, int64_t& p1) {
-  const int64_t ngroups = (A.ncells + RCELLS - 1) / RCELLS;
-  const int64_t b = blockIdx.x;
-  if (b >= ngroups + (int64_t)A.dscal->n_items || b >= A.items_max) return false;
-  const int64_t* it = A.items + 4 * b;
-  c0 = it[0]; ncl = (int)it[1]; p0 = it[2]; p1 = it[3];
-  return true;
+  return cube_cell_item(A.items, A.ncells, A.items_max, A.dscal, c0, ncl, p0, p1);
 }
 
 template <int ZX, int ZV>
@@ -324,18 +320,9 @@ __device__ __forceinline__ float ordered_sum(float acc, const double* x, int n) 
   return acc;
 }
 
-// one crowded cell by the whole CTA: bitonic sort of (key<<32|source) in sk (m =
-// next power of two of n entries), the sorted order back to the slots, the
-// per-particle velocities into sv[d * vstride + i] in parallel, the FP32 sum by
-// one thread per component in order.  sk and sv may be shared or global memory.
-template <int ZX, int ZV>
-__device__ __forceinline__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk, double* sv,
-                              int vstride) {
-  int m = 1;
-  while (m < n) m <<= 1;
-  for (int i = threadIdx.x; i < m; i += blockDim.x)
-    sk[i] = i < n ? (((unsigned long long)A.pkey[s + i] << 32) | (uint32_t)A.perm[s + i]) : ~0ull;
-  __syncthreads();
+// ascending bitonic sort of m (a power of two) keys by the whole CTA, in place
+// (shared or global memory)
+__device__ __forceinline__ void bitonic_block(unsigned long long* sk, int m) {
   for (int k = 2; k <= m; k <<= 1)
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int i = threadIdx.x; i < m; i += blockDim.x) {
@@ -348,6 +335,93 @@ __device__ __forceinline__ void sort_sum_cell(const RebinArgs& A, int64_t c, int
       }
       __syncthreads();
     }
+}
+
+// one pass (k, j < T) of the bitonic network on a tile of T keys that starts at
+// key `base` (the direction follows the key's global index)
+__device__ __forceinline__ void tile_pass(unsigned long long* t, int T, int base, int j, int k) {
+  for (int i = threadIdx.x; i < T; i += blockDim.x) {
+    const int ixj = i ^ j;
+    if (ixj > i) {
+      const unsigned long long a = t[i], bb = t[ixj];
+      const bool up = ((base + i) & k) == 0;
+      if ((a > bb) == up) { t[i] = bb; t[ixj] = a; }
+    }
+  }
+}
+
+// The same sort for m > T keys in global memory with a shared tile of T keys
+// (both powers of two): the stages up to T and, in every later stage, the passes
+// of stride below T run tile by tile in shared memory; only the passes of stride
+// T and above go through global memory, four compare-exchanges per thread in
+// flight (their pairs are disjoint, so the loads of a batch precede its stores).
+__device__ __forceinline__ void bitonic_tiled(unsigned long long* g, int m, unsigned long long* t, int T) {
+  const int nthr = blockDim.x;
+  for (int base = 0; base < m; base += T) {
+    for (int i = threadIdx.x; i < T; i += nthr) t[i] = g[base + i];
+    __syncthreads();
+    for (int k = 2; k <= T; k <<= 1)
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        tile_pass(t, T, base, j, k);
+        __syncthreads();
+      }
+    for (int i = threadIdx.x; i < T; i += nthr) g[base + i] = t[i];
+    __syncthreads();
+  }
+  const int npairs = m >> 1;
+  for (int k = 2 * T; k <= m; k <<= 1) {
+    for (int j = k >> 1; j >= T; j >>= 1) {
+      for (int p0 = threadIdx.x; p0 < npairs; p0 += 4 * nthr) {
+        unsigned long long a[4], bb[4];
+        int ii[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int p = p0 + u * nthr;
+          ii[u] = -1;
+          if (p < npairs) {
+            const int i = ((p & ~(j - 1)) << 1) | (p & (j - 1));  // bit j of i clear
+            ii[u] = i;
+            a[u] = g[i];
+            bb[u] = g[i | j];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (ii[u] >= 0) {
+            const bool up = (ii[u] & k) == 0;
+            if ((a[u] > bb[u]) == up) { g[ii[u]] = bb[u]; g[ii[u] | j] = a[u]; }
+          }
+      }
+      __syncthreads();
+    }
+    for (int base = 0; base < m; base += T) {
+      for (int i = threadIdx.x; i < T; i += nthr) t[i] = g[base + i];
+      __syncthreads();
+      for (int j = T >> 1; j > 0; j >>= 1) {
+        tile_pass(t, T, base, j, k);
+        __syncthreads();
+      }
+      for (int i = threadIdx.x; i < T; i += nthr) g[base + i] = t[i];
+      __syncthreads();
+    }
+  }
+}
+
+// one crowded cell by the whole CTA: bitonic sort of (key<<32|source) in sk (m =
+// next power of two of n entries; through the shared tile of T keys when sk is in
+// global memory and m > T), the sorted order back to the slots, the per-particle
+// velocities into sv[d * vstride + i] in parallel, the FP32 sum by one thread per
+// component in order.  sk and sv may be shared or global memory.
+template <int ZX, int ZV>
+__device__ __forceinline__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk,
+                                              double* sv, int vstride, unsigned long long* tile = nullptr, int T = 0) {
+  int m = 1;
+  while (m < n) m <<= 1;
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    sk[i] = i < n ? (((unsigned long long)A.pkey[s + i] << 32) | (uint32_t)A.perm[s + i]) : ~0ull;
+  __syncthreads();
+  if (tile && m > T) bitonic_tiled(sk, m, tile, T);
+  else bitonic_block(sk, m);
   int tt[3];
   cell_tile(A, c, tt);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -431,14 +505,22 @@ __global__ void __launch_bounds__(32 * WARP_WARPS) k_rebin_warp(RebinArgs A) {
   }
 }
 
-// F1 for cells of WARP_MAX+1..BIG_MAX entries: one CTA per cell, sorted in shared
-// memory
+// F1 for cells of WARP_MAX+1..BIG_MAX entries: one CTA per cell, keys sorted in
+// shared memory (32 KB, so four CTAs share an SM and their serial sums overlap),
+// the velocity columns in the CTA's global slot of 3 BIG_MAX doubles; cells are
+// taken as CTAs become free
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
+__global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A, double* __restrict__ scratch) {
   extern __shared__ unsigned long long sk[];
-  double* sv = reinterpret_cast<double*>(sk + BIG_MAX);  // [3][BIG_MAX] velocities
+  __shared__ unsigned long long qs;
+  double* sv = scratch + (size_t)blockIdx.x * 3 * BIG_MAX;
   const unsigned long long nmid = A.dscal->n_mid;
-  for (unsigned long long b = blockIdx.x; b < nmid; b += gridDim.x) {
+  while (true) {
+    if (threadIdx.x == 0) qs = atomicAdd(&A.dscal->mid_next, 1ull);
+    __syncthreads();
+    const unsigned long long b = qs;
+    __syncthreads();
+    if (b >= nmid) break;
     const int64_t c = A.big_list[A.ncells - 1 - (int64_t)b];
     sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, BIG_MAX);
   }
@@ -447,9 +529,11 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A) {
 // F1 for cells beyond BIG_MAX: the same in a global scratch slot per CTA
 // (slot_u64 = keys for the largest cell padded to a power of two, then its
 // velocities)
+constexpr int HUGE_TILE = 8192;  // keys per shared tile of the huge-cell sort (64 KB)
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(1024) k_rebin_huge(RebinArgs A, unsigned long long* __restrict__ scratch,
                                                      size_t slot_u64, int mmax) {
+  extern __shared__ unsigned long long tile[];
   __shared__ unsigned long long qs;
   unsigned long long* sk = scratch + (size_t)blockIdx.x * slot_u64;
   double* sv = reinterpret_cast<double*>(sk + mmax);
@@ -462,7 +546,7 @@ __global__ void __launch_bounds__(1024) k_rebin_huge(RebinArgs A, unsigned long 
     __syncthreads();
     if (q >= nh) break;
     const int64_t c = A.cursor[q];
-    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, vstride);
+    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, vstride, tile, HUGE_TILE);
   }
 }
 
@@ -550,34 +634,38 @@ __global__ void k_rebin_stats(RebinArgs A) {
 
 template <int ZX, int ZV>
 int run_rebin(cube_ctx* ctx, RebinArgs& A) {
-  const int64_t nb = (ctx->ncells + RCELLS - 1) / RCELLS;
-  k_rebin_items<<<(unsigned)((nb + 255) / 256), 256, 0, ctx->stream>>>(A, ctx->rebin_items);
-  CUBE_LAUNCH_CHECK(ctx);
-  // one block per item: the groups, then at most 4 np/PMAX more (blocks past the
-  // last item return at once)
-  const int64_t ni = std::min<int64_t>(A.items_max, nb + 4 * (ctx->np / PMAX + 1));
+  int64_t ni = 0;  // one block per item (blocks past the last item return at once)
+  int rc = cube_cell_items(ctx, ctx->cell_start, &ni);
+  if (rc) return rc;
   k_rebin_count<ZX, ZV><<<(unsigned)ni, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
-  int rc = cube_exclusive_scan(ctx, A.cnt2, ctx->ncells, A.start2);
+  rc = cube_exclusive_scan(ctx, A.cnt2, ctx->ncells, A.start2);
   if (rc) return rc;
   k_rebin_place<<<1184, 256, 0, ctx->stream>>>(A, ctx->np);
   CUBE_LAUNCH_CHECK(ctx);
   const unsigned cb = (unsigned)((ctx->ncells + 255) / 256);
   k_rebin_sortsum<ZX, ZV><<<cb, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
+  // sizes of the block and global sorters' lists (n_huge, max_huge, n_mid)
+  unsigned long long hv[3] = {0ull, 0ull, 0ull};
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(hv, &ctx->dscal->n_huge, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   const size_t wsmem = sizeof(unsigned long long) * 4 * WARP_MAX * WARP_WARPS;
   CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_warp<ZX, ZV>, wsmem));
   k_rebin_warp<ZX, ZV><<<3 * ctx->num_sms, 32 * WARP_WARPS, wsmem, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
-  const size_t smem = sizeof(unsigned long long) * BIG_MAX + sizeof(double) * 3 * BIG_MAX;
-  CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_big<ZX, ZV>, smem));
-  k_rebin_big<ZX, ZV><<<296, 512, smem, ctx->stream>>>(A);
-  CUBE_LAUNCH_CHECK(ctx);
-  // cells beyond the shared-memory sorter: global scratch sized for the largest
-  unsigned long long hv[2] = {0ull, 0ull};
-  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(hv, &ctx->dscal->n_huge, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                     ctx->stream));
-  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (hv[2]) {
+    const int nblk = 4 * ctx->num_sms;
+    if (!ctx->rebin_mid_scratch)
+      CUBE_CUDA_TRY(ctx, cudaMalloc(&ctx->rebin_mid_scratch, sizeof(double) * 3 * BIG_MAX * (size_t)nblk));
+    const size_t smem = sizeof(unsigned long long) * BIG_MAX;
+    CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_big<ZX, ZV>, smem));
+    const int grid = (int)std::min<unsigned long long>(hv[2], (unsigned long long)nblk);
+    k_rebin_big<ZX, ZV><<<grid, 512, smem, ctx->stream>>>(A, reinterpret_cast<double*>(ctx->rebin_mid_scratch));
+    CUBE_LAUNCH_CHECK(ctx);
+  }
+  // cells beyond the block sorter: global scratch sized for the largest
   if (hv[0]) {
     // one slot per SM of keys (mmax, a power of two) and three velocity columns
     // of mmax: the scratch is reallocated only when mmax doubles
@@ -595,8 +683,10 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
     }
     k_rebin_huge_order<<<1, 1024, 0, ctx->stream>>>(A);
     CUBE_LAUNCH_CHECK(ctx);
-    k_rebin_huge<ZX, ZV><<<grid, 1024, 0, ctx->stream>>>(A, reinterpret_cast<unsigned long long*>(ctx->rebin_scratch),
-                                                         slot, mmax);
+    const size_t tsmem = sizeof(unsigned long long) * HUGE_TILE;
+    CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_huge<ZX, ZV>, tsmem));
+    k_rebin_huge<ZX, ZV><<<grid, 1024, tsmem, ctx->stream>>>(
+        A, reinterpret_cast<unsigned long long*>(ctx->rebin_scratch), slot, mmax);
     CUBE_LAUNCH_CHECK(ctx);
   }
   k_rebin_emit<ZX, ZV><<<(unsigned)ni, 256, 0, ctx->stream>>>(A, ctx->np);
@@ -610,6 +700,17 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
 
 int64_t cube_rebin_items_max(int64_t ncells, int64_t cap) {
   return (ncells + RCELLS - 1) / RCELLS + 4 * (cap / PMAX + 1) + 64;
+}
+
+int cube_cell_items(cube_ctx* ctx, const int64_t* cell_start, int64_t* blocks) {
+  const int64_t ngroups = (ctx->ncells + RCELLS - 1) / RCELLS;
+  const int64_t items_max = cube_rebin_items_max(ctx->ncells, ctx->cap);
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(&ctx->dscal->n_items, 0, sizeof(unsigned long long), ctx->stream));
+  k_cell_items<<<(unsigned)((ngroups + 255) / 256), 256, 0, ctx->stream>>>(cell_start, ctx->ncells, ctx->rebin_items,
+                                                                         items_max, ctx->dscal);
+  CUBE_LAUNCH_CHECK(ctx);
+  *blocks = std::min<int64_t>(items_max, ngroups + 4 * (ctx->np / PMAX + 1));
+  return CUBE_OK;
 }
 
 int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
