@@ -231,6 +231,7 @@ void cube_destroy(cube_ctx* ctx) {
   if (ctx->pp_scratch) cudaFree(ctx->pp_scratch);
   if (ctx->rebin_scratch) cudaFree(ctx->rebin_scratch);
   if (ctx->rebin_mid_scratch) cudaFree(ctx->rebin_mid_scratch);
+  if (ctx->dep_scratch) cudaFree(ctx->dep_scratch);
   for (double* t : ctx->vdec)
     if (t) cudaFree(t);
   if (ctx->hscal) cudaFreeHost(ctx->hscal);
@@ -379,6 +380,7 @@ int32_t cube_load_state(cube_ctx* ctx, int64_t nplocal, const void* xp, const vo
   if (rc) return rc;
   CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->state_loaded = 1;
+  ctx->cells_le32 = 0;
   (void)dummy;
   return CUBE_OK;
 }

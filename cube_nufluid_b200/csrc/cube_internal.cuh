@@ -81,6 +81,8 @@ struct DevScal {
   unsigned long long huge_next;  // next cell for a k_rebin_huge block
   unsigned long long n_items;    // re-bin work items beyond the one per 64-cell group
   unsigned long long mid_next;   // next cell for a k_rebin_big block
+  unsigned long long n_dep_extra;  // deposit work items beyond one per brick
+  unsigned long long n_split;      // bricks whose particles are split over several deposit blocks
 };
 
 // one isothermal fluid of the dispersive sum (hydrogr.f90 type hydro): five FP32
@@ -115,6 +117,7 @@ struct cube_ctx {
   int own_stream;
   int64_t np, cap;
   int state_loaded;
+  int cells_le32;  // the last re-bin left no cell beyond 32 particles (no deposit brick needs splitting)
   int num_sms;
   // particles (double-buffered for the re-bin)
   void* xp;  void* vp;  int32_t* pid;
@@ -140,6 +143,8 @@ struct cube_ctx {
   void* rebin_scratch = nullptr;  // sort slots of re-bin cells beyond 4096 particles, grown on demand
   size_t rebin_scratch_bytes = 0;
   void* rebin_mid_scratch = nullptr;  // velocity columns of the block sorter, allocated on first use
+  void* dep_scratch = nullptr;   // fine nodes and block counters of split deposit bricks, grown on demand
+  size_t dep_scratch_bytes = 0;
   // meshes
   MeshLevel fine, coarse;
   unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator

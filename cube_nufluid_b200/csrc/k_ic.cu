@@ -370,6 +370,7 @@ int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io)
   }
   ctx->np = np;
   ctx->state_loaded = 1;
+  ctx->cells_le32 = 0;
   float vmax[3];
   for (int d = 0; d < 3; ++d) memcpy(&vmax[d], &hs.vmax_bits[d], 4);
   // the scalar block of a freshly read IC (particle_initialization.f90:37-39)

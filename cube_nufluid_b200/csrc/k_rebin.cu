@@ -646,11 +646,14 @@ int run_rebin(cube_ctx* ctx, RebinArgs& A) {
   const unsigned cb = (unsigned)((ctx->ncells + 255) / 256);
   k_rebin_sortsum<ZX, ZV><<<cb, 256, 0, ctx->stream>>>(A);
   CUBE_LAUNCH_CHECK(ctx);
-  // sizes of the block and global sorters' lists (n_huge, max_huge, n_mid)
-  unsigned long long hv[3] = {0ull, 0ull, 0ull};
+  // sizes of the sorters' lists: n_huge, max_huge, n_mid, and n_big
+  unsigned long long hv[4] = {0ull, 0ull, 0ull, 0ull};
   CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(hv, &ctx->dscal->n_huge, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                      ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(hv + 3, &ctx->dscal->n_big, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                     ctx->stream));
   CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  ctx->cells_le32 = (hv[0] | hv[2] | hv[3]) == 0ull;
   const size_t wsmem = sizeof(unsigned long long) * 4 * WARP_MAX * WARP_WARPS;
   CUBE_CUDA_TRY(ctx, cube_smem_limit(k_rebin_warp<ZX, ZV>, wsmem));
   k_rebin_warp<ZX, ZV><<<3 * ctx->num_sms, 32 * WARP_WARPS, wsmem, ctx->stream>>>(A);

@@ -83,6 +83,24 @@ def test_deposit_bit_exact(pm_pair, tables):
     assert sd.testrhof == pytest.approx(st.np * st.mass_p_cdm, rel=1e-9)
 
 
+def test_deposit_bit_exact_after_a_smooth_drift(tables):
+    # after a re-bin that leaves no cell beyond 32 particles the deposit launches one
+    # block per brick without work items
+    st, p, s = small_state(nc=16, nnt=2, seed=23, amplitude=8.0)
+    s.dt_old, s.dt = 2.0, 2.0
+    o, g = pair(st, p, tables)
+    so, sg = s.copy(), s.copy()
+    o.update_x(so)
+    g.update_x(sg)
+    assert g.store_state()[3].max() <= 32
+    so.a, so.a_mid, so.dt = 0.5, 0.5, 20.0
+    sg.a, sg.a_mid, sg.dt = 0.5, 0.5, 20.0
+    o.particle_mesh(so, 1)
+    g.debug_deposit(sg)
+    assert np.array_equal(o.fetch(0).view(np.int32), g.fetch(0).view(np.int32))
+    assert np.array_equal(o.fetch(1).view(np.int32), g.fetch(1).view(np.int32))
+
+
 def test_deposit_bit_exact_on_dense_clumps(tables):
     # cells of 12,000 and 24,000 particles: thousands of weights collide on the same
     # shared-memory nodes and the 64-bit node sums (~1e14 in fixed point) carry out of
