@@ -58,6 +58,12 @@ CONFIGS = {
                workload="serving: Poisson arrivals at 20/s, 32^3-256^3 particles log-uniform, 50-400 Mpc/h, "
                         "Om~U[0.25,0.35], s8~U[0.7,0.9], 48 steps z=49->0, P(k) in 32 log bins + 1/64 "
                         "subsample, 160 GB HBM admission budget, int2 x/v, PP off"),
+    # late times: a small box evolved from z=49 to z=0 (48 log-spaced targets, untimed;
+    # cached with --state-cache), then timed steps of the clustered state (cells of up
+    # to ~40,000 particles)
+    "c6": dict(nc=128, nnt=4, box=50.0, izip=2, pp=False, z_i=49.0, late=True,
+               workload="late-time clustered box: 256^3 particles, 50 Mpc/h, evolved z=49 -> 0 "
+                        "(Om=0.3, s8=0.8), fine 512^3, coarse 128^3, int2 x/v, PP off"),
     "c3s": dict(nc=128, nnt=4, box=250.0, izip=2, pp=True, z_i=10.0, nu=True,
                 workload="256^3 CDM particles + fluid neutrinos (fluids 256^3, 128^3, 64^3), 250 Mpc/h, "
                          "fine 512^3, coarse 128^3, int2 x/v, PP on, from z=10 (profiling size)"),
@@ -380,6 +386,61 @@ def run_ensemble(args, cfg):
         print(json.dumps(line))
 
 
+def run_late(args, cfg):
+    """C6: particle-updates/s of steps of a clustered late-time state; device time of
+    each step from the library's own events on its stream."""
+    import torch
+    from cube_nufluid_b200 import build, ic
+    from cube_nufluid_b200.abi import CubeScalars, make_params
+    from cube_nufluid_b200.cube import Cube
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local_rank)
+    build.build()
+    nc, box = cfg["nc"], cfg["box"]
+    cube = Cube(make_params(nc, cfg["nnt"], box=box, omega_m=0.3, omega_l=0.7, izipx=cfg["izip"], izipv=cfg["izip"],
+                            ext_pp_force=cfg["pp"]), np_capacity=(2 * nc) ** 3)
+    cache = args.state_cache
+    if cache and os.path.exists(cache):
+        d = np.load(cache)
+        cube.load_state(d["xp"], d["vp"], d["pid"], d["rhoc"], d["vfield"])
+        s = CubeScalars.from_buffer_copy(d["scal"].tobytes())
+    else:
+        cos = ic.Cosmology(omega_m=0.3, omega_l=0.7, sigma8=0.8)
+        s = cube.make_ic(ic.device_ic_params(cos, cfg["z_i"], nc, box=box), 7)
+        n = 0
+        for a_next in np.geomspace(s.a, 1.0, 49)[1:]:
+            while True:
+                n += 1
+                if cube.step(s, a_next=float(a_next)) or n > 2000:
+                    break
+        if cache:
+            xp, vp, pid, rhoc, vfield = cube.store_state()
+            np.savez(cache, xp=xp, vp=vp, pid=pid, rhoc=rhoc, vfield=vfield, scal=np.frombuffer(bytes(s), np.uint8))
+    rhoc = cube.store_state()[3]
+    for _ in range(args.warmup):
+        cube.step(s)
+    l0 = cube.launch_count()
+    ph = np.zeros(8)
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            cube.step(s)
+            ph += np.array(cube.phase_times())
+    launches = cube.launch_count() - l0
+    npart = (2 * nc) ** 3
+    ms = float(ph[7])
+    line = {"metric": "late-time PM step particle-updates/s", "value": npart * args.steps / (ms / 1e3),
+            "unit": "particle-updates/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "particles": npart, "nc": nc, "nf": 4 * nc,
+                       "largest_cell": int(rhoc.max()), "cells_over_4096": int((rhoc > 4096).sum()),
+                       "timing": "device time of each step (the library's CUDA events on its stream)"},
+            "gpu_launches": int(launches),
+            "phases_ms": {k: float(v) / args.steps for k, v in zip(PHASES, ph[:6])}, "clocks": clk.summary()}
+    cube.close()
+    print(json.dumps(line))
+
+
 def run_serving(args, cfg):
     """C5: latency percentiles of a Poisson request stream served on one GPU, and the
     same percentiles relative to each request's plain service time (its size served
@@ -432,8 +493,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--state-cache", default="", help="c6: file holding the evolved state (made if absent)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
+    if cfg.get("late"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the late-time state is made by this library's "
+                              "own evolution; the reference's CPU path is timed on the single-box configurations"}))
+            return
+        run_late(args, cfg)
+        return
     if cfg.get("serving"):
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving mode; "

@@ -414,7 +414,8 @@ __device__ __forceinline__ void bitonic_tiled(unsigned long long* g, int m, unsi
 // component in order.  sk and sv may be shared or global memory.
 template <int ZX, int ZV>
 __device__ __forceinline__ void sort_sum_cell(const RebinArgs& A, int64_t c, int n, int64_t s, unsigned long long* sk,
-                                              double* sv, int vstride, unsigned long long* tile = nullptr, int T = 0) {
+                                              double* sv, int vstride, unsigned long long* tile = nullptr, int T = 0,
+                                              double* stage = nullptr, int stage_len = 0) {
   int m = 1;
   while (m < n) m <<= 1;
   for (int i = threadIdx.x; i < m; i += blockDim.x)
@@ -436,12 +437,27 @@ __device__ __forceinline__ void sort_sum_cell(const RebinArgs& A, int64_t c, int
           cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
   }
   __syncthreads();
-  if (threadIdx.x < 3) {
-    const int d = threadIdx.x;
-    const float acc = ordered_sum((float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1),
-                                  sv + (size_t)d * vstride, n);
-    A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
+  const int d = threadIdx.x;
+  float acc = 0.f;
+  if (d < 3) acc = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
+  if (stage) {
+    // sv in global memory: the CTA copies the next chunk of the three columns into
+    // shared memory (free after the sort), the three sums read it from there
+    const int ch = stage_len / 3;
+    for (int j0 = 0; j0 < n; j0 += ch) {
+      const int len = min(ch, n - j0);
+      for (int i = threadIdx.x; i < 3 * len; i += blockDim.x) {
+        const int dd = i / len, k = i - dd * len;
+        stage[dd * ch + k] = sv[(size_t)dd * vstride + j0 + k];
+      }
+      __syncthreads();
+      if (d < 3) acc = ordered_sum(acc, stage + d * ch, len);
+      __syncthreads();
+    }
+  } else if (d < 3) {
+    acc = ordered_sum(acc, sv + (size_t)d * vstride, n);
   }
+  if (d < 3) A.vfield2[(size_t)d * A.ncells + c] = (float)cube_ddiv((double)acc, cube_dadd((double)n, 0.1));
   __syncthreads();
 }
 
@@ -522,7 +538,8 @@ __global__ void __launch_bounds__(512) k_rebin_big(RebinArgs A, double* __restri
     __syncthreads();
     if (b >= nmid) break;
     const int64_t c = A.big_list[A.ncells - 1 - (int64_t)b];
-    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, BIG_MAX);
+    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, BIG_MAX, nullptr, 0, reinterpret_cast<double*>(sk),
+                          BIG_MAX);
   }
 }
 
@@ -546,7 +563,8 @@ __global__ void __launch_bounds__(1024) k_rebin_huge(RebinArgs A, unsigned long 
     __syncthreads();
     if (q >= nh) break;
     const int64_t c = A.cursor[q];
-    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, vstride, tile, HUGE_TILE);
+    sort_sum_cell<ZX, ZV>(A, c, A.cnt2[c], A.start2[c], sk, sv, vstride, tile, HUGE_TILE,
+                          reinterpret_cast<double*>(tile), HUGE_TILE);
   }
 }
 
