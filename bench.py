@@ -1,6 +1,7 @@
 """Benchmark of the B200 PM step (one JSON line on stdout).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c3|c4|c5]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c2|c1|c3|c4|c5|c6|c2s|c3s] [--state-cache FILE]
 
 Workload (default c2, the single-GPU precision configuration): 512^3 CDM
 particles in a 1000 Mpc/h box, fine mesh 1024^3, coarse mesh 256^3, 8^3 tiles,
@@ -19,6 +20,10 @@ N > 1 : one independent box per rank (replicas, weak scaling), no collective
 --impl reference: the CPU oracle (a restatement of the reference's Fortran
         step; the Fortran reference cannot be built here) on the host cores, on
         a bounded sample of the workload.
+Other configurations: c3 (fluid neutrinos), c4 (ensemble of small boxes), c5
+(serving a Poisson request stream), c6 (steps of a clustered z=0 state of a
+256^3-particle, 50 Mpc/h box; --state-cache keeps the evolved state in a file),
+c2s/c3s (profiling sizes).
 """
 from __future__ import annotations
 
