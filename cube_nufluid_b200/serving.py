@@ -74,14 +74,20 @@ def request_stream(n: int, rate: float, master_seed: int, *, sides=SERVE_SIDES, 
 def footprint_bytes(nc: int, izip: int = 2) -> int:
     """Estimated device memory of a context of nc coarse cells per side and 8 nc^3
     particles: fine and coarse meshes (density, three force meshes, scratch, Green
-    octants), particle arrays (double-buffered codes and PIDs, re-bin scratch) and
-    per-cell arrays, with 10% margin."""
+    octants), particle arrays (double-buffered codes and PIDs, re-bin scratch, work
+    items) and per-cell arrays, plus the scratch that clustered late-time states
+    grow (the block sorter's velocity columns, 58 MB; sort slots of cells beyond 4096
+    particles, 148 x 32 B x the largest cell rounded up to a power of two, the
+    largest cell taken as 0.3% of the particles; split deposit bricks, ~12 B per
+    particle), with 10% margin."""
     nf = 4 * nc
     mesh = lambda n: 5 * n * n * (n + 32) * 4 + 3 * (n // 2 + 1) ** 3 * 4
     npart = 8 * nc ** 3
-    per_particle = 2 * (6 * izip + 4) + 4 * 4 + 16 + 1
-    per_cell = 2 * 4 + 2 * 8 + 2 * 12 + 24 + 4 + 8
-    return int(1.1 * (mesh(nf) + mesh(nc) + npart * per_particle + nc ** 3 * per_cell))
+    per_particle = 2 * (6 * izip + 4) + 4 * 4 + 16 + 1 + 1
+    per_cell = 2 * 4 + 2 * 8 + 2 * 12 + 24 + 4 + 8 + 1
+    big_cell = 1 << max(0, math.ceil(math.log2(max(1.0, 0.003 * npart))))
+    late = 58e6 + 148 * 32 * big_cell + 12 * npart
+    return int(1.1 * (mesh(nf) + mesh(nc) + npart * per_particle + nc ** 3 * per_cell + late))
 
 
 def positions(xp: np.ndarray, rhoc: np.ndarray, nc: int, nnt: int, izipx: int) -> np.ndarray:

@@ -181,6 +181,27 @@ def test_kick_bit_exact_on_identical_forces(tables, izip):
     assert list(so.vmax) == list(sg.vmax)
 
 
+def test_kick_bit_exact_on_cells_beyond_one_work_item(tables):
+    # cells of 12,000 particles: the kick's work items cut their 64-cell groups into
+    # runs of cells and the crowded cells into slices of 4096 particles
+    from helpers import planted_clumps
+    st, p, s = planted_clumps(nc=16, centres=((3.5, 4.5, 5.5), (10.5, 11.5, 2.5)), n_per=12000, sigma=0.08,
+                              nbg=20000, seed=45)
+    assert st.rhoc.max() > 2 * 4096  # three slices
+    o, g = pair(st, p, tables, build=False)
+    s.a, s.a_mid, s.dt = 0.5, 0.5, 20.0
+    s.sigma_vi_new = np.float32(s.sigma_vi * 1.01)
+    rng = np.random.default_rng(10)
+    nf, nc = 64, 16
+    fine = rng.normal(0, 2.0, 3 * nf ** 3).astype(np.float32)
+    coarse = rng.normal(0, 0.5, 3 * nc ** 3).astype(np.float32)
+    so, sg = s.copy(), s.copy()
+    o.particle_mesh_with_force(so, fine, coarse, 1)
+    g.kick_with_force(sg, fine, coarse)
+    assert_same_state(o, g)
+    assert list(so.vmax) == list(sg.vmax)
+
+
 @pytest.mark.parametrize("izip", [2, 1])
 def test_pp_bit_exact(tables, izip):
     st, p, s = clustered_state(nc=16, nnt=2, seed=51, izipx=izip, izipv=izip)
