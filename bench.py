@@ -45,8 +45,8 @@ CONFIGS = {
                workload="512^3 particles, 1000 Mpc/h, fine 1024^3, coarse 256^3, int2 x/v, PP on (pp_range=1)"),
     "c2s": dict(nc=128, nnt=4, box=500.0, izip=2, pp=True, z_i=49.0,
                 workload="256^3 particles, 500 Mpc/h, fine 512^3, coarse 128^3, int2 x/v, PP on (profiling size)"),
-    "c1": dict(nc=32, nnt=2, box=200.0, izip=2, pp=False, z_i=49.0,
-               workload="64^3 particles, 200 Mpc/h, fine 128^3, coarse 32^3, int2 x/v, PP off"),
+    "c1": dict(nc=32, nnt=2, box=200.0, izip=2, izipx=1, izipv=2, pp=False, z_i=49.0,
+               workload="64^3 particles, 200 Mpc/h, fine 128^3, coarse 32^3, int1 x / int2 v, PP off"),
     # CDM + fluid neutrinos, started at the neutrino turn-on z_i_nu = 10 (the redshift
     # neutrino_ic.f90 builds the fluids at), so every timed step evolves the fluids
     "c3": dict(nc=256, nnt=8, box=500.0, izip=2, pp=True, z_i=10.0, nu=True,
@@ -69,6 +69,14 @@ CONFIGS = {
     "c6": dict(nc=128, nnt=4, box=50.0, izip=2, pp=False, z_i=49.0, late=True,
                workload="late-time clustered box: 256^3 particles, 50 Mpc/h, evolved z=49 -> 0 "
                         "(Om=0.3, s8=0.8), fine 512^3, coarse 128^3, int2 x/v, PP off"),
+    # precision study: the same 64 steps in FP32 and in the FP64 Poisson mode from one
+    # seeded IC (force error against the FP64 run of the same step, P(k) ratio at z=0)
+    "c2p": dict(nc=256, nnt=8, box=1000.0, izip=2, pp=True, z_i=49.0, precision=64,
+                workload="precision study: 512^3 particles, 1000 Mpc/h, fine 1024^3, coarse 256^3, int2 x/v, "
+                         "PP on; 64 steps z=49 -> 0 in FP32 and in the FP64 Poisson mode from the same IC"),
+    "c2ps": dict(nc=128, nnt=4, box=500.0, izip=2, pp=True, z_i=49.0, precision=64,
+                 workload="precision study (profiling size): 256^3 particles, 500 Mpc/h, fine 512^3, coarse "
+                          "128^3, int2 x/v, PP on; 64 steps z=49 -> 0 in FP32 and in FP64 Poisson mode"),
     "c3s": dict(nc=128, nnt=4, box=250.0, izip=2, pp=True, z_i=10.0, nu=True,
                 workload="256^3 CDM particles + fluid neutrinos (fluids 256^3, 128^3, 64^3), 250 Mpc/h, "
                          "fine 512^3, coarse 128^3, int2 x/v, PP on, from z=10 (profiling size)"),
@@ -91,14 +99,23 @@ def read_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle-reason samples during the timed region."""
+    """nvidia-smi clock / throttle-reason samples during the timed region.
+
+    start() launches nvidia-smi and waits for its first row, so that its start-up
+    happens before the warm-up steps, not inside the timed region; the timed region
+    is bracketed by `with sampler:` and summary() keeps the rows that arrived inside
+    it (with the nearest row on either side when the region is shorter than the
+    200 ms sampling period)."""
 
     def __init__(self, index: int):
         self.index = index
-        self.rows = []
+        self.rows = []  # (arrival time, fields)
         self.proc = None
+        self.t0 = self.t1 = None
 
-    def __enter__(self):
+    def start(self, wait_s: float = 10.0):
+        if self.proc is not None:
+            return self
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -108,6 +125,9 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            t_end = time.time() + wait_s
+            while not self.rows and time.time() < t_end and self.proc.poll() is None:
+                time.sleep(0.05)
         except Exception:
             self.proc = None
         return self
@@ -116,9 +136,16 @@ class ClockSampler:
         for line in self.proc.stdout:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) >= 9:
-                self.rows.append(parts)
+                self.rows.append((time.time(), parts))
+
+    def __enter__(self):
+        self.start()
+        self.t0 = time.time()
+        return self
 
     def __exit__(self, *a):
+        self.t1 = time.time()
+        time.sleep(0.25)  # one more row after the region
         if self.proc:
             self.proc.terminate()
             try:
@@ -127,14 +154,21 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        t0 = self.t0 if self.t0 is not None else 0.0
+        t1 = self.t1 if self.t1 is not None else time.time()
+        inside = [r for (t, r) in self.rows if t0 <= t <= t1]
+        if not inside:
+            before = [r for (t, r) in self.rows if t < t0][-1:]
+            after = [r for (t, r) in self.rows if t > t1][:1]
+            inside = before + after
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in inside if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in inside if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in inside for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(inside)}
 
 
 def make_state(cfg, seed):
@@ -143,13 +177,14 @@ def make_state(cfg, seed):
     import tempfile
     from cube_nufluid_b200 import ic
     nu = bool(cfg.get("nu"))
-    key = f"cube_ic_{cfg['nc']}_{cfg['nnt']}_{cfg['box']}_{cfg['z_i']}_{cfg['izip']}_{seed}_{int(nu)}.pkl"
+    zx, zv = cfg.get("izipx", cfg["izip"]), cfg.get("izipv", cfg["izip"])
+    key = f"cube_ic_{cfg['nc']}_{cfg['nnt']}_{cfg['box']}_{cfg['z_i']}_{zx}{zv}_{seed}_{int(nu)}.pkl"
     path = os.path.join(tempfile.gettempdir(), key)
     if os.path.exists(path):
         with open(path, "rb") as f:
             return pickle.load(f)
     st = ic.zeldovich(cfg["nc"], cfg["nnt"], box=cfg["box"], z_i=cfg["z_i"], seed=seed,
-                      izipx=cfg["izip"], izipv=cfg["izip"], f_cdm=(1.0 - NU_F) if nu else 1.0)
+                      izipx=zx, izipv=zv, f_cdm=(1.0 - NU_F) if nu else 1.0)
     if nu:
         # fluid meshes nf/2, nf/4, nf/8 and hg_setup's cs2 = (u/beta*c * hg_dv)^2 (hydrogr.f90:66)
         f32 = np.float32
@@ -168,6 +203,12 @@ def make_state(cfg, seed):
     except OSError:
         pass
     return st
+
+
+def plain_params_for(cfg):
+    from cube_nufluid_b200 import make_params
+    return make_params(cfg["nc"], cfg["nnt"], box=cfg["box"], izipx=cfg.get("izipx", cfg["izip"]),
+                       izipv=cfg.get("izipv", cfg["izip"]), ext_pp_force=cfg["pp"])
 
 
 def nu_params_for(cfg):
@@ -230,8 +271,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     if nu:
         p = nu_params_for(cfg)
     else:
-        p = make_params(cfg["nc"], cfg["nnt"], box=cfg["box"], izipx=cfg["izip"], izipv=cfg["izip"],
-                        ext_pp_force=cfg["pp"])
+        p = plain_params_for(cfg)
     cube = Cube(p, np_capacity=st.np)
     stream = torch.cuda.Stream()
     cube.L.cube_set_stream(cube.h, stream.cuda_stream)
@@ -258,6 +298,7 @@ def run_ours(args, cfg, rank, world, local_rank):
             s.dt_neu = cube.nu_evolve(s.dt / 2.0, s.dt_neu, -1, s.a_mid)
             nu_ms[0] += cube.phase_times()[6]
 
+    clk = ClockSampler(local_rank).start()
     for _ in range(args.warmup):
         step()
     nu_ms[0] = 0.0
@@ -267,7 +308,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     torch.cuda.synchronize()
     l0 = cube.launch_count()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
+    with clk:
         with torch.cuda.stream(stream):
             ev0.record(stream)
             for _ in range(args.steps):
@@ -325,35 +366,207 @@ def run_ours(args, cfg, rank, world, local_rank):
     e2e_ms = float(t2.item())
     if nu:
         phase_sum = np.append(phase_sum, nu_timed)
-    return dict(ms=ms_max, npart=npart, launches=launches, phase_ms=phase_sum / args.steps, clocks=clk.summary(),
+    cufft = None
+    if getattr(args, "cufft", False) and world == 1:
+        cufft = cufft_comparison(cube, 4 * cfg["nc"])
+    return dict(cufft=cufft, ms=ms_max, npart=npart, launches=launches, phase_ms=phase_sum / args.steps, clocks=clk.summary(),
                 e2e_ms=e2e_ms, e2e_steps=e2e_steps, h2d=h2d, d2h=h2d, scal=s.as_dict())
 
 
-def cpu_sample(threads: int):
-    """The CPU oracle on a bounded sample: one step (update_x + PP + particle_mesh)
-    of a 64^3-particle box with the workload's method settings, OpenMP over all
-    host threads where the reference's loops are parallel (its nlayer scheme)."""
+def cufft_comparison(cube, nf: int, reps: int = 5) -> dict:
+    """The fine-mesh Poisson solve of the library (its own FFT passes with the Green
+    multiply and the kick scale fused) timed beside the same transforms done by
+    cuFFT through torch.fft (one r2c, three c2r, the Green multiply as a separate
+    elementwise pass) on a mesh of the same size.  A timed comparison only: cuFFT
+    is never on the library's path."""
+    import ctypes as C
+    import torch
+    ms = C.c_float(0.0)
+    cube._check(cube.L.cube_debug_time_poisson(cube.h, reps, C.byref(ms)))
+    ours = float(ms.value)
+    x = torch.randn(nf, nf, nf, device="cuda", dtype=torch.float32)
+    kern = torch.randn(3, nf, nf, nf // 2 + 1, device="cuda", dtype=torch.float32)
+
+    def fft_only():
+        X = torch.fft.rfftn(x)
+        return [torch.fft.irfftn(X, s=x.shape) for _ in range(3)]
+
+    def with_green():
+        X = torch.fft.rfftn(x)
+        return [torch.fft.irfftn(X * (1j * kern[d]), s=x.shape) for d in range(3)]
+
+    out = {"library_ms": ours}
+    for name, fn in (("cufft_transforms_ms", fft_only), ("cufft_with_green_ms", with_green)):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            r = fn()
+            del r
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = e0.elapsed_time(e1) / reps
+    del x, kern
+    torch.cuda.empty_cache()
+    out["mesh"] = f"{nf}^3, one r2c + three c2r (+ Green multiply), FP32"
+    return out
+
+
+def cpu_sample(threads: int, cfg=None, steps: int = 3, warmup: int = 1):
+    """The CPU oracle (a restatement of the reference's step) on a bounded sample of
+    the workload itself: the seeded state of the configuration, and per sample step
+    one of its tiles run through the oracle's per-tile loops of update_x,
+    ext_pp_force and particle_mesh (the reference's loop structure, FP32
+    reference-order deposit, OpenMP where the reference's loops are parallel) with
+    the particle state left as it was.  The global coarse Poisson solve is timed
+    once and charged to each sample in proportion to its particles.  Rate =
+    sampled particles / (their tiles' time + their share of the coarse solve)."""
     os.environ.setdefault("OMP_NUM_THREADS", str(threads))
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     from oracle_ref import Oracle
-    from cube_nufluid_b200 import ic, tables, make_params, scalars_from_ic
-
-    st = ic.zeldovich(32, 2, box=200.0, z_i=49.0, seed=7)
-    p = make_params(32, 2, box=200.0, ext_pp_force=True)
+    from cube_nufluid_b200 import tables, scalars_from_ic
+    cfg = cfg or CONFIGS["c2"]
+    t_setup = time.perf_counter()
+    st = make_state(cfg, seed=1000)
+    p = nu_params_for(cfg) if cfg.get("nu") else plain_params_for(cfg)
     o = Oracle(p, tables.read_fine_table(), tables.read_coarse_table())
     o.load(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
     s = scalars_from_ic(st)
-    s.dt_old = s.dt = 0.5
-    s.a_mid = s.a
+    import ctypes as C
+    from cube_nufluid_b200.cube import load_library
+    hit = C.c_int32(0)
+    load_library().cube_timestep(C.byref(p), C.byref(s), C.c_float(0.0), C.byref(hit))
+    nnt, nt = cfg["nnt"], cfg["nc"] // cfg["nnt"]
+    ntiles = nnt ** 3
+    tile_np = np.asarray(st.rhoc, dtype=np.int64).reshape(ntiles, nt ** 3).sum(axis=1)
     t0 = time.perf_counter()
-    o.update_x(s)
-    o.ext_pp_force(s)
-    o.particle_mesh(s, 0)
-    dt = time.perf_counter() - t0
-    return {"value": st.np / dt, "unit": "particle-updates/s", "cores": threads, "kind": "port",
-            "sample": f"1 step (update_x + ext_pp_force + particle_mesh, FP32 reference-order deposit, FP64 FFT) "
-                      f"of a {st.np}-particle box (nc=32, nf=128, 2^3 tiles) on {threads} host threads; "
-                      f"{dt:.1f} s"}
+    o.coarse_poisson()
+    t_coarse = time.perf_counter() - t0
+    t_setup = time.perf_counter() - t_setup
+    rng = np.random.default_rng(7)
+    order = rng.permutation(ntiles)
+    done_np, done_t = 0, 0.0
+    for i in range(warmup + steps):
+        tile = int(order[i % ntiles])
+        mask = np.zeros(ntiles, np.int8)
+        mask[tile] = 1
+        o.set_tile_mask(mask)
+        ss = s.copy()
+        t0 = time.perf_counter()
+        o.update_x(ss)
+        if cfg["pp"]:
+            o.ext_pp_force(ss)
+        o.particle_mesh(ss, 0)
+        dt = time.perf_counter() - t0
+        if i >= warmup:
+            done_np += int(tile_np[tile])
+            done_t += dt + t_coarse * float(tile_np[tile]) / float(st.np)
+    o.set_tile_mask(None)
+    return {"value": done_np / done_t, "unit": "particle-updates/s", "cores": threads, "kind": "port",
+            "sample": f"{steps} sample steps (after {warmup} untimed), each one tile of the {st.np}-particle "
+                      f"{cfg['nc']}^3-cell state ({nt}^3 coarse cells, about {int(tile_np.mean())} particles) "
+                      f"through the CPU oracle's update_x + ext_pp_force + particle_mesh tile loops "
+                      f"(FP32 reference-order deposit, FP64 FFT) on {threads} host threads, plus the global "
+                      f"coarse Poisson solve ({t_coarse:.2f} s, timed once) charged per particle; "
+                      f"{done_t:.1f} s timed, {t_setup:.0f} s set-up",
+            "tiles_timed": steps, "coarse_solve_s": t_coarse}
+
+
+def _rel_rms_chunked(a, b, scale_a=1.0, scale_b=1.0, chunk=1 << 26):
+    """sqrt(sum((a/sa - b/sb)^2) / sum((b/sb)^2)) over large arrays, in chunks."""
+    num = den = 0.0
+    for i in range(0, a.size, chunk):
+        x = a[i:i + chunk].astype(np.float64) / scale_a
+        y = b[i:i + chunk].astype(np.float64) / scale_b
+        num += float(np.sum((x - y) ** 2))
+        den += float(np.sum(y * y))
+    return float(np.sqrt(num / den))
+
+
+def run_precision(args, cfg):
+    """Precision study: the configuration's step run twice from the same seeded state,
+    once in FP32 and once in the library's FP64 Poisson mode (FP64 meshes, FFT, Green
+    and interpolation; the same integer deposit, codec and PP), in lockstep time steps
+    (the FP64 run takes the FP32 run's dt limits).  At checkpoint steps the FP64
+    context also computes the forces of the FP32 run's own state (the FP64 run of the
+    same step): the relative RMS difference of the fine and coarse force meshes.  At
+    z = 0 the power spectra of the two runs (the library's P(k), 4 log bins per octave)
+    give the P(k) ratio."""
+    import torch
+    from cube_nufluid_b200 import Cube, build, scalars_from_ic
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local_rank)
+    build.build()
+    st = make_state(cfg, seed=1000)
+    p32 = plain_params_for(cfg)
+    p64 = type(p32).from_buffer_copy(p32)
+    p64.poisson_fp64 = 1
+    g32, g64 = Cube(p32, st.np), Cube(p64, st.np)
+    for g in (g32, g64):
+        g.load_state(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    s32 = scalars_from_ic(st)
+    s64 = s32.copy()
+    nsteps = cfg["precision"]
+    targets = np.geomspace(float(s32.a), 1.0, nsteps + 1)[1:]
+    checks = {0, nsteps // 4, nsteps // 2, (3 * nsteps) // 4, nsteps - 1}
+    limits = ("dt_fine", "dt_coarse", "dt_pp", "dt_vmax", "dt_vmax_nu", "dt_neu")
+    rows = []
+    n = 0
+    pif = float(np.float32(4.0) * np.arctan(np.float32(1.0)))
+    for i, a_next in enumerate(targets):
+        hit = False
+        while not hit:
+            for k in limits:
+                setattr(s64, k, getattr(s32, k))
+            hit = g32.timestep(s32, float(a_next))
+            g64.timestep(s64, float(a_next))
+            for g, sc in ((g32, s32), (g64, s64)):
+                g.update_x(sc)
+                if cfg["pp"]:
+                    g.ext_pp_force(sc)
+            if hit and i in checks:
+                # FP64 forces of the FP32 run's state: the FP64 context takes that state,
+                # runs the step's particle_mesh on a copy of the scalars, and gets its own back
+                keep = g64.store_state()
+                g64.load_state(*g32.store_state())
+                probe = s32.copy()
+                g64.particle_mesh(probe)
+                f64, c64 = g64.fetch(2), g64.fetch(3)
+                g64.load_state(*keep)
+                del keep
+                g32.particle_mesh(s32)
+                f32, c32 = g32.fetch(2), g32.fetch(3)
+                # both meshes hold force * ((a_mid dt)/6)/pi: compare the forces
+                k32 = float(np.float32(np.float32(np.float32(s32.a_mid) * np.float32(s32.dt)) / np.float32(6.0))
+                            / np.float32(pif))
+                k64 = ((float(s32.a_mid) * float(s32.dt)) / 6.0) / pif
+                rows.append({"step": n, "a": float(s32.a), "fine": _rel_rms_chunked(f32, f64, k32, k64),
+                             "coarse": _rel_rms_chunked(c32, c64, k32, k64)})
+                del f64, c64, f32, c32
+            else:
+                g32.particle_mesh(s32)
+            g64.particle_mesh(s64)
+            n += 1
+    # P(k) of both runs on the FP32 context (the FP64 mode's meshes are not FP32)
+    pk32 = g32.power_spectrum(log_bins=True)
+    g32.load_state(*g64.store_state())
+    pk64 = g32.power_spectrum(log_bins=True)
+    ok = pk64[:, 0] > 0
+    ratio = pk32[ok, 2] / pk64[ok, 2]
+    k = pk32[ok, 1]
+    line = {"metric": "precision study: force RMS relative error and P(k) ratio, FP32 vs FP64 Poisson mode",
+            "value": float(np.max(np.abs(ratio - 1.0))), "unit": "max |P32/P64 - 1| at z=0",
+            "n_gpus": 1, "steps": n, "higher_is_better": False, "dtype": "f32 vs f64", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "particles": st.np, "nc": cfg["nc"], "nf": 4 * cfg["nc"]},
+            "force_rms_rel_err": rows,
+            "pk": {"k_h_per_mpc": [float(x) for x in k], "ratio": [float(x) for x in ratio],
+                   "max_abs_dev": float(np.max(np.abs(ratio - 1.0))),
+                   "max_abs_dev_k_below_half_nyquist": float(np.max(np.abs(ratio - 1.0)[k <= k.max() / 2]))},
+            "a_final": float(s32.a)}
+    g32.close()
+    g64.close()
+    print(json.dumps(line))
 
 
 def run_ensemble(args, cfg):
@@ -369,10 +582,11 @@ def run_ensemble(args, cfg):
     specs = ensemble_specs(cfg["ensemble"], 2024 + rank)
     ens = Ensemble(specs)
     workers = 16
+    clk = ClockSampler(local_rank).start()
     ens.run(args.warmup, workers=workers)
     torch.cuda.synchronize()
     l0 = sum(m.cube.launch_count() for m in ens.members)
-    with ClockSampler(local_rank) as clk:
+    with clk:
         r = ens.run(args.steps, workers=workers)
         torch.cuda.synchronize()
     launches = sum(m.cube.launch_count() for m in ens.members) - l0
@@ -422,11 +636,12 @@ def run_late(args, cfg):
             xp, vp, pid, rhoc, vfield = cube.store_state()
             np.savez(cache, xp=xp, vp=vp, pid=pid, rhoc=rhoc, vfield=vfield, scal=np.frombuffer(bytes(s), np.uint8))
     rhoc = cube.store_state()[3]
+    clk = ClockSampler(local_rank).start()
     for _ in range(args.warmup):
         cube.step(s)
     l0 = cube.launch_count()
     ph = np.zeros(8)
-    with ClockSampler(local_rank) as clk:
+    with clk:
         for _ in range(args.steps):
             cube.step(s)
             ph += np.array(cube.phase_times())
@@ -458,6 +673,7 @@ def run_serving(args, cfg):
     torch.cuda.set_device(local_rank)
     build.build()
     srv = Server(hbm_budget=160e9, workers=8)
+    clk = ClockSampler(local_rank).start()
     # warm-up: one request per size creates the contexts; then the plain service
     # time of each size on the idle server (contexts reused, as under load)
     plain = {}
@@ -468,7 +684,7 @@ def run_serving(args, cfg):
             srv.answer(req)
             plain[side // 2] = time.perf_counter() - t
     reqs = request_stream(cfg["serving"], 20.0, 2025)
-    with ClockSampler(local_rank) as clk:
+    with clk:
         t0 = time.perf_counter()
         ans = srv.serve(reqs, realtime=True)
         wall = time.perf_counter() - t0
@@ -498,6 +714,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=list(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cufft", action="store_true",
+                    help="also time the fine Poisson solve against cuFFT (torch.fft) on the same mesh size")
     ap.add_argument("--state-cache", default="", help="c6: file holding the evolved state (made if absent)")
     args = ap.parse_args()
     cfg = CONFIGS[args.config]
@@ -514,6 +732,14 @@ def main():
                               "its CPU path is timed on the single-box configurations"}))
             return
         run_serving(args, cfg)
+        return
+    if cfg.get("precision"):
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the precision study compares the library's "
+                              "FP32 and FP64 runs; the reference's CPU path is timed on the single-box "
+                              "configurations"}))
+            return
+        run_precision(args, cfg)
         return
     if cfg.get("ensemble"):
         if args.impl == "reference":
@@ -534,9 +760,10 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        base = cpu_sample(os.cpu_count() or 1)
+        base = cpu_sample(os.cpu_count() or 1, cfg, steps=args.steps, warmup=args.warmup)
         line = {"impl": "reference", "metric": metric, "value": base["value"], "unit": "particle-updates/s",
-                "n_gpus": args.gpus, "steps": 1, "warmup": 0, "higher_is_better": True, "config": config,
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                "config": config,
                 "cpu_baseline": base, "e2e": {"value": base["value"], "unit": "particle-updates/s",
                                               "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
                 "data": "synthetic", "dtype": "f32"}
@@ -576,8 +803,10 @@ def main():
                      "algorithmic_bytes": ab[dom]},
         "phases_ms": phases, "phase_gbs": phase_gbs, "clocks": r["clocks"],
     }
+    if r.get("cufft"):
+        line["cufft_comparison"] = r["cufft"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_sample(os.cpu_count() or 1)
+        line["cpu_baseline"] = cpu_sample(os.cpu_count() or 1, cfg, steps=2, warmup=1)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -19,7 +19,8 @@ class CubeParams(C.Structure):
         ("box", C.c_float), ("h0", C.c_float), ("omega_m", C.c_float), ("omega_l", C.c_float),
         ("wde", C.c_float), ("ra_max", C.c_float), ("dt_max", C.c_float),
         ("z_i_nu", C.c_float), ("f_neu", C.c_float), ("m_nu_ev", C.c_float), ("deg_nu", C.c_float),
-        ("nu_nc", C.c_int32 * 3), ("reserved", C.c_int32 * 8),
+        ("nu_nc", C.c_int32 * 3), ("stockham_only", C.c_int32), ("poisson_fp64", C.c_int32),
+        ("reserved", C.c_int32 * 6),
     ]
 
 

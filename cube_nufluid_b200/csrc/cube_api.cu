@@ -32,7 +32,8 @@ __global__ void k_soa_to_aos(const T* __restrict__ soa, T* __restrict__ aos, int
 }
 
 // fine (octant) multiplier for debug fetch: straight copy; mesh copy with pitch
-__global__ void k_unpitch(const float* __restrict__ src, float* __restrict__ dst, int n, int rp, int ncomp) {
+template <typename T>
+__global__ void k_unpitch(const T* __restrict__ src, T* __restrict__ dst, int n, int rp, int ncomp) {
   const int64_t n3 = (int64_t)n * n * n;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < n3 * ncomp; q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t c = q / n3, r = q - c * n3;
@@ -50,21 +51,25 @@ __global__ void k_pitch(const float* __restrict__ src, float* __restrict__ dst, 
   }
 }
 
-int alloc_level(cube_ctx* ctx, MeshLevel& L, int n) {
+int alloc_level(cube_ctx* ctx, MeshLevel& L, int n, int fp64) {
   L.n = n;
   L.rp = n + 32;
   L.cp = L.rp / 2;
   L.plane = (size_t)n * L.rp;
+  L.fp64 = fp64;
   const size_t vol = (size_t)n * L.plane;
-  CUBE_CUDA_TRY(ctx, cudaMalloc(&L.rho, sizeof(float) * vol));
-  CUBE_CUDA_TRY(ctx, cudaMalloc(&L.force, sizeof(float) * 3 * vol));
-  CUBE_CUDA_TRY(ctx, cudaMalloc(&L.ext, sizeof(float) * vol));
+  const size_t es = fp64 ? sizeof(double) : sizeof(float);  // the pitches count elements
+  CUBE_CUDA_TRY(ctx, cudaMalloc(&L.rho, es * vol));
+  CUBE_CUDA_TRY(ctx, cudaMalloc(&L.force, es * 3 * vol));
+  CUBE_CUDA_TRY(ctx, cudaMalloc(&L.ext, es * vol));
   const int kp = n / 2 + 1;
   L.kern_octant = 1;
   L.kern_pitch = kp;
   CUBE_CUDA_TRY(ctx, cudaMalloc(&L.kern, sizeof(float) * 3 * (size_t)kp * kp * kp));
-  CUBE_CUDA_TRY(ctx, cudaMemset(L.rho, 0, sizeof(float) * vol));
-  CUBE_CUDA_TRY(ctx, cudaMemset(L.force, 0, sizeof(float) * 3 * vol));
+  L.kernd = nullptr;
+  if (fp64) CUBE_CUDA_TRY(ctx, cudaMalloc(&L.kernd, sizeof(double) * 3 * (size_t)kp * kp * kp));
+  CUBE_CUDA_TRY(ctx, cudaMemset(L.rho, 0, es * vol));
+  CUBE_CUDA_TRY(ctx, cudaMemset(L.force, 0, es * 3 * vol));
   return cube_fft_plan(ctx, L.plan, n);
 }
 
@@ -218,6 +223,7 @@ void cube_destroy(cube_ctx* ctx) {
                   ctx->red_tmp,
                   ctx->scan_tmp, ctx->fine.rho, ctx->fine.force, ctx->fine.ext, ctx->fine.kern, ctx->fine.plan.tw, ctx->fine.plan.tw2,
                   ctx->coarse.rho, ctx->coarse.force, ctx->coarse.ext, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->coarse.plan.tw2,
+                  ctx->fine.kernd, ctx->coarse.kernd, ctx->fine.plan.twd, ctx->coarse.plan.twd,
                   ctx->rho_c_acc,
                   ctx->tan_table, ctx->dscal, ctx->pk_bins};
   for (void* p : ptrs)
@@ -229,6 +235,7 @@ void cube_destroy(cube_ctx* ctx) {
   }
   if (ctx->nu.partial) cudaFree(ctx->nu.partial);
   if (ctx->pp_scratch) cudaFree(ctx->pp_scratch);
+  if (ctx->pp_staged) cudaFree(ctx->pp_staged);
   if (ctx->rebin_scratch) cudaFree(ctx->rebin_scratch);
   if (ctx->rebin_mid_scratch) cudaFree(ctx->rebin_mid_scratch);
   if (ctx->dep_scratch) cudaFree(ctx->dep_scratch);
@@ -252,6 +259,10 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
       (P.izipv != 1 && P.izipv != 2) || P.nf_cutoff <= 0 || P.ncb <= 0 || np_capacity <= 0 ||
       np_capacity >= ((int64_t)1 << 31)) {
     g_create_error = "invalid parameters (nc % nnt == 0, ncell == 4, izip in {1,2}, capacity < 2^31)";
+    return CUBE_ERR_PARAM;
+  }
+  if (P.poisson_fp64 && P.neutrino) {
+    g_create_error = "invalid parameters: the FP64 Poisson mode runs without neutrinos";
     return CUBE_ERR_PARAM;
   }
   cube_ctx* ctx = new cube_ctx();
@@ -309,17 +320,25 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
             A((void**)&ctx->slot_r2, 8 * cap) && A((void**)&ctx->slot_s2, 8 * cap) &&
             A((void**)&ctx->red_tmp, 8 * (2 * (std::max<int64_t>(nce, cap) / 1024 + 64) + 64)) &&
             A((void**)&ctx->scan_tmp, 8 * (nce / 2048 + 64)) &&
-            A((void**)&ctx->rho_c_acc, 8 * nce) && A((void**)&ctx->tan_table, 4 * ctx->nvbin) &&
+            A((void**)&ctx->rho_c_acc, (P.neutrino ? 16 : 8) * nce) && A((void**)&ctx->tan_table, 4 * ctx->nvbin) &&
             A((void**)&ctx->dscal, sizeof(DevScal)) &&
             A((void**)&ctx->pk_bins, 8 * 7 * (size_t)(cube_pk_nbin(ctx->nf, 0) + 1));
   if (!ok) return fail(CUBE_ERR_CUDA);
   if (cudaMallocHost((void**)&ctx->hscal, sizeof(DevScal)) != cudaSuccess) { ctx->err = "cudaMallocHost failed"; return fail(CUBE_ERR_CUDA); }
-  cudaMemset(ctx->rho_c_acc, 0, 8 * nce);
+  cudaMemset(ctx->rho_c_acc, 0, (P.neutrino ? 16 : 8) * nce);
+  ctx->rho_c_nu = P.neutrino ? ctx->rho_c_acc + nce : nullptr;
   cudaMemset(ctx->dscal, 0, sizeof(DevScal));
   cudaMemset(ctx->pid, 0, 4 * cap);
   int rc;
-  if ((rc = alloc_level(ctx, ctx->fine, ctx->nf))) return fail(rc);
-  if ((rc = alloc_level(ctx, ctx->coarse, ctx->nc))) return fail(rc);
+  if (P.ext_pp_force && P.nc % 4 == 0) {
+    const size_t nbr = (size_t)(P.nc / 4) * (P.nc / 4) * (P.nc / 4);
+    if (cudaMalloc((void**)&ctx->pp_staged, nbr) != cudaSuccess || cudaMemset(ctx->pp_staged, 0, nbr) != cudaSuccess) {
+      ctx->err = "cudaMalloc of the PP brick flags failed";
+      return fail(CUBE_ERR_CUDA);
+    }
+  }
+  if ((rc = alloc_level(ctx, ctx->fine, ctx->nf, P.poisson_fp64))) return fail(rc);
+  if ((rc = alloc_level(ctx, ctx->coarse, ctx->nc, P.poisson_fp64))) return fail(rc);
   // FP32 tangent of every velocity code with the C library's tanf (decode table)
   std::vector<float> tt(ctx->nvbin);
   for (int c = -ctx->nvbin / 2; c < ctx->nvbin / 2; ++c) tt[c + ctx->nvbin / 2] = tanf(cube_varg(&ctx->codec, c));
@@ -439,8 +458,13 @@ int32_t cube_update_x(cube_ctx* ctx, cube_scalars* io) {
   // |vfield|^2 per cell, |v_res|^2 and |v|^2 per particle in the new storage order
   double sums[3];
   if ((rc = cube_tree_sum_dev(ctx, ctx->cell_stats, ctx->ncells, &sums[0]))) return rc;
-  if ((rc = cube_tree_sum_dev(ctx, ctx->slot_r2, ctx->np, &sums[1]))) return rc;
-  if ((rc = cube_tree_sum_dev(ctx, ctx->slot_s2, ctx->np, &sums[2]))) return rc;
+  {
+    int trc;
+    const double* dec = cube_vdec_table(ctx, cube_vcoef(&ctx->codec, io->sigma_vi), &trc);
+    if (trc) return trc;
+    if ((rc = cube_stats_sums(ctx, reinterpret_cast<const int32_t*>(ctx->slot_r2), dec, &sums[1], &sums[2])))
+      return rc;
+  }
   const double npg = (double)(io->npglobal > 0 ? io->npglobal : ctx->np);
   io->std_vsim_c = sqrt(sums[0] / (double)ctx->ncells);
   io->std_vsim_res = sqrt(sums[1] / npg);
@@ -470,11 +494,10 @@ int32_t cube_particle_mesh(cube_ctx* ctx, cube_scalars* io) {
     if ((rc = cube_nu_gravity(ctx, io))) return rc;
     CUBE_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[9], ctx->stream));
   }
-  unsigned long long mt[2];
-  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(mt, ctx->red_tmp, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  unsigned long long mt[3];
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(mt, ctx->red_tmp, sizeof(mt), cudaMemcpyDeviceToHost, ctx->stream));
   if ((rc = check_device_error(ctx))) return rc;
-  io->testrhof = (double)mt[0] * (1.0 / 4294967296.0);
-  io->testrhoc = (double)mt[1] * (1.0 / 4294967296.0);
+  cube_mass_sums(mt, io->mass_p_cdm, &io->testrhof, &io->testrhoc);
   if (ctx->nu.on) {
     double nus = 0.0;
     if ((rc = cube_tree_sum_dev(ctx, ctx->nu.partial, ctx->nu.nparts, &nus))) return rc;
@@ -661,6 +684,10 @@ int32_t cube_debug_time_poisson(cube_ctx* ctx, int32_t reps, float* ms) {
 
 int32_t cube_make_ic(cube_ctx* ctx, const cube_ic_params* ic, cube_scalars* io) {
   if (!ctx || !ic || !io) return CUBE_ERR_PARAM;
+  if (ctx->fine.fp64) {  // these use the FP32 meshes as scratch
+    ctx->err = "not available in the FP64 Poisson mode";
+    return CUBE_ERR_PARAM;
+  }
   const int rc = cube_make_ic_dev(ctx, ic, io);
   if (rc == CUBE_OK) io->vsim2phys = vsim2phys(ctx, io->a);
   return rc;
@@ -668,6 +695,10 @@ int32_t cube_make_ic(cube_ctx* ctx, const cube_ic_params* ic, cube_scalars* io) 
 
 int32_t cube_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_args* args, cube_halo_result* result) {
   if (!ctx || !io || !args || !result || (args->capacity > 0 && !args->halos)) return CUBE_ERR_PARAM;
+  if (ctx->fine.fp64) {  // these use the FP32 meshes as scratch
+    ctx->err = "not available in the FP64 Poisson mode";
+    return CUBE_ERR_PARAM;
+  }
   if (!ctx->state_loaded) return CUBE_ERR_STATE;
   *result = cube_halo_result{0, 0, 0};
   return cube_halofind_dev(ctx, io, args, result);
@@ -676,6 +707,10 @@ int32_t cube_halofind(cube_ctx* ctx, const cube_scalars* io, const cube_halo_arg
 int32_t cube_power_spectrum(cube_ctx* ctx, int32_t log_bins, float* xip, int32_t capacity, int32_t* nbin) {
   if (!ctx || !xip || !nbin) return CUBE_ERR_PARAM;
   if (!ctx->state_loaded) return CUBE_ERR_STATE;
+  if (ctx->fine.fp64) {  // it uses the FP32 meshes as scratch
+    ctx->err = "not available in the FP64 Poisson mode";
+    return CUBE_ERR_PARAM;
+  }
   const int need = cube_pk_nbin(ctx->nf, log_bins ? 1 : 0);
   *nbin = need;
   if (capacity < need) {
@@ -746,12 +781,17 @@ int64_t cube_debug_fetch(cube_ctx* ctx, int32_t which, void* host, int64_t capac
   }
   const int64_t n3 = (int64_t)L->n * L->n * L->n, n = n3 * ncomp;
   if (n > capacity) return -1;
-  float* tmp = nullptr;
-  if (cudaMalloc(&tmp, 4 * n) != cudaSuccess) return -1;
-  k_unpitch<<<1184, 256, 0, ctx->stream>>>(src, tmp, L->n, L->rp, ncomp);
+  const size_t es = L->fp64 ? 8 : 4;  // the FP64 Poisson mode's meshes come back as doubles
+  void* tmp = nullptr;
+  if (cudaMalloc(&tmp, es * n) != cudaSuccess) return -1;
+  if (L->fp64)
+    k_unpitch<double><<<1184, 256, 0, ctx->stream>>>(reinterpret_cast<const double*>(src),
+                                                     static_cast<double*>(tmp), L->n, L->rp, ncomp);
+  else
+    k_unpitch<float><<<1184, 256, 0, ctx->stream>>>(src, static_cast<float*>(tmp), L->n, L->rp, ncomp);
   ctx->launches++;
   cudaStreamSynchronize(ctx->stream);
-  const cudaError_t e = cudaMemcpy(host, tmp, 4 * n, cudaMemcpyDeviceToHost);
+  const cudaError_t e = cudaMemcpy(host, tmp, es * n, cudaMemcpyDeviceToHost);
   cudaFree(tmp);
   return e == cudaSuccess ? n : -1;
 }
@@ -762,11 +802,10 @@ int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io) {
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dscal, 0, sizeof(DevScal), ctx->stream));
   int rc = cube_deposit(ctx, io);
   if (rc) return rc;
-  unsigned long long mt[2];
-  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(mt, ctx->red_tmp, 16, cudaMemcpyDeviceToHost, ctx->stream));
+  unsigned long long mt[3];
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(mt, ctx->red_tmp, sizeof(mt), cudaMemcpyDeviceToHost, ctx->stream));
   if ((rc = check_device_error(ctx))) return rc;
-  io->testrhof = (double)mt[0] * (1.0 / 4294967296.0);
-  io->testrhoc = (double)mt[1] * (1.0 / 4294967296.0);
+  cube_mass_sums(mt, io->mass_p_cdm, &io->testrhof, &io->testrhoc);
   if (ctx->nu.on) {
     double nus = 0.0;
     if ((rc = cube_tree_sum_dev(ctx, ctx->nu.partial, ctx->nu.nparts, &nus))) return rc;
@@ -778,6 +817,10 @@ int32_t cube_debug_deposit(cube_ctx* ctx, cube_scalars* io) {
 int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float* fine_force,
                                    const float* coarse_force) {
   if (!ctx || !io || !fine_force || !coarse_force) return CUBE_ERR_PARAM;
+  if (ctx->fine.fp64) {
+    ctx->err = "not available in the FP64 Poisson mode";
+    return CUBE_ERR_PARAM;
+  }
   MeshLevel* Ls[2] = {&ctx->fine, &ctx->coarse};
   const float* hs[2] = {fine_force, coarse_force};
   for (int l = 0; l < 2; ++l) {

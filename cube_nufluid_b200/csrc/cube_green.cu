@@ -63,7 +63,8 @@ __global__ void k_green_y(const double* __restrict__ s1, int nfc, int n, int d, 
 }
 
 // K[ky][kx][kz] = sum_az S2[kx][ky][az] F_z(kz,az) / n^3
-__global__ void k_green_z(const double* __restrict__ s2, int nfc, int n, int d, float* __restrict__ kern) {
+__global__ void k_green_z(const double* __restrict__ s2, int nfc, int n, int d, float* __restrict__ kern,
+                          double* __restrict__ kernd) {
   const int kp = n / 2 + 1;
   const int64_t tot = (int64_t)kp * kp * kp;
   const double inv = 1.0 / ((double)n * n * n);
@@ -73,6 +74,7 @@ __global__ void k_green_z(const double* __restrict__ s2, int nfc, int n, int d, 
     double acc = 0.0;
     for (int az = 0; az < nfc; ++az) acc += s2[((size_t)kx * kp + ky) * nfc + az] * fac(kz, az, n, d == 2);
     kern[(size_t)d * tot + q] = (float)(acc * inv);
+    if (kernd) kernd[(size_t)d * tot + q] = acc * inv;  // FP64 Poisson mode
   }
 }
 
@@ -170,7 +172,7 @@ int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table
       CUBE_LAUNCH_CHECK(ctx);
       k_green_y<<<1184, 256, 0, ctx->stream>>>(s1, nfc, n, d, s2);
       CUBE_LAUNCH_CHECK(ctx);
-      k_green_z<<<4736, 256, 0, ctx->stream>>>(s2, nfc, n, d, ctx->fine.kern);
+      k_green_z<<<4736, 256, 0, ctx->stream>>>(s2, nfc, n, d, ctx->fine.kern, ctx->fine.kernd);
       CUBE_LAUNCH_CHECK(ctx);
     }
     CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -184,6 +186,7 @@ int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table
     const size_t n3 = (size_t)nc * nc * nc;
     const double pi = 3.14159265358979323846;
     std::vector<float> oct((size_t)3 * kp * kp * kp);
+    std::vector<double> octd(ctx->coarse.kernd ? oct.size() : 0);
     std::vector<cd> z(n3);
     auto off = [&](int g) { return ((g + nc / 2) % nc) - nc / 2; };  // 0-based index -> signed offset
     for (int d = 0; d < 3; ++d) {
@@ -221,10 +224,13 @@ int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table
             if (kk[d] == nc / 2) v = 0.0;  // odd in k_d: exactly zero on the Nyquist plane
             else if (!(kr > 8.0 || kk[d] == 0)) v = v * 0.25 * pi * ks[d] / ks2 / D.imag();
             oct[(size_t)d * kp * kp * kp + ((size_t)ky * kp + kx) * kp + kz] = (float)(v / (double)n3);
+            if (!octd.empty()) octd[(size_t)d * kp * kp * kp + ((size_t)ky * kp + kx) * kp + kz] = v / (double)n3;
           }
     }
     CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->coarse.kern, oct.data(), sizeof(float) * oct.size(), cudaMemcpyHostToDevice,
                                        ctx->stream));
+    if (!octd.empty())
+      CUBE_CUDA_TRY(ctx, cudaMemcpy(ctx->coarse.kernd, octd.data(), sizeof(double) * octd.size(), cudaMemcpyHostToDevice));
   }
   return CUBE_OK;
 }

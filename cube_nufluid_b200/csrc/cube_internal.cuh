@@ -30,6 +30,7 @@ struct FftPlan {
   int radix[CUBE_MAX_RADIX_STAGES];
   float2* tw;                     // device twiddles exp(-2 pi i j/n), j < n
   float2* tw2;                    // register-FFT twiddles tw[(t*k1) mod n] at [k1*T + t] (n = R*T)
+  double2* twd;                   // tw in FP64 (FP64 Poisson mode)
 };
 
 // R x T split of the register-resident transforms (T threads of one warp, R
@@ -59,6 +60,8 @@ struct MeshLevel {
   float* force;   // [3] force meshes, each n*plane floats, in place as spectra
   float* ext;     // scratch mesh (n*plane floats) for the transposed passes
   float* kern;    // Green multiplier (imaginary parts, /n^3)
+  double* kernd;  // the same in FP64 (FP64 Poisson mode, else null)
+  int fp64;       // 1: rho, force and ext hold doubles (same element pitches)
   int kern_octant;  // 1: kern is [3][(n/2+1)^3] octant; 0: [3][n][n][cp_k]
   int kern_pitch;   // inner pitch of kern (n/2+1)
   FftPlan plan;
@@ -83,6 +86,8 @@ struct DevScal {
   unsigned long long mid_next;   // next cell for a k_rebin_big block
   unsigned long long n_dep_extra;  // deposit work items beyond one per brick
   unsigned long long n_split;      // bricks whose particles are split over several deposit blocks
+  unsigned long long pp_list;      // PP targets with a neighbour, listed for the pair pass
+  unsigned long long pp_dense;     // PP bricks whose region holds a crowded cell
 };
 
 // one isothermal fluid of the dispersive sum (hydrogr.f90 type hydro): five FP32
@@ -130,7 +135,7 @@ struct cube_ctx {
   int32_t* big_list;
   int64_t* rebin_items;  // [4] per item: first cell, cells, first and end particle
   double* cell_stats;   // [3][ncells]
-  double* slot_r2; double* slot_s2;  // per-slot statistics terms of the re-bin
+  double* slot_r2; double* slot_s2;  // re-bin scratch: each slot's new cell (int32), tree block sums
   double* red_tmp;      // scratch for tree sums
   int64_t* scan_tmp;
   NuState nu;
@@ -139,6 +144,7 @@ struct cube_ctx {
   double vdec_coef[2] = {0.0, 0.0};
   int vdec_next = 0;
   void* pp_scratch = nullptr;     // sorted particles of crowded PP bricks, grown on demand
+  uint8_t* pp_staged = nullptr;   // per PP brick: staged by k_pp_brick this step (the last step's choice)
   size_t pp_scratch_bytes = 0;
   void* rebin_scratch = nullptr;  // sort slots of re-bin cells beyond 4096 particles, grown on demand
   size_t rebin_scratch_bytes = 0;
@@ -147,7 +153,8 @@ struct cube_ctx {
   size_t dep_scratch_bytes = 0;
   // meshes
   MeshLevel fine, coarse;
-  unsigned long long* rho_c_acc;  // int64 fixed-point coarse accumulator
+  unsigned long long* rho_c_acc;  // coarse particle sums, 64-bit fixed point without the mass (scale 2^38)
+  unsigned long long* rho_c_nu;   // coarse neutrino sums, 64-bit fixed point in mass units (scale 2^32)
   double* dep_partial;            // per-CTA fine mass partial sums
   int64_t dep_blocks;
   float* tan_table;               // tanf of each velocity code, index code+nvbin/2
@@ -345,6 +352,15 @@ __device__ __forceinline__ bool cube_cell_item(const int64_t* items, int64_t nce
   return true;
 }
 int cube_deposit(cube_ctx* ctx, cube_scalars* io);
+// mass sums of a deposit (pm.f90:108,280) from the three totals it leaves at the
+// start of red_tmp: fine and coarse particle sums without the mass (scale 2^32) and
+// the coarse neutrino sum (mass units, scale 2^32); the caller adds the fine
+// neutrino sum
+inline void cube_mass_sums(const unsigned long long mt[3], float mass, double* testrhof, double* testrhoc) {
+  const double m = (double)mass, s = 1.0 / 4294967296.0;
+  *testrhof = (double)mt[0] * s * m;
+  *testrhoc = (double)mt[1] * s * m + (double)mt[2] * s;
+}
 int cube_fft_poisson(cube_ctx* ctx, MeshLevel& L, unsigned int* f2_bits, KickScale ks);
 int cube_force_scale(cube_ctx* ctx, MeshLevel& L, KickScale ks);
 int cube_fft_forward3(cube_ctx* ctx, MeshLevel& L, float* data, int* kx_major);
@@ -356,6 +372,9 @@ int cube_kick(cube_ctx* ctx, cube_scalars* io);
 int cube_pp(cube_ctx* ctx, cube_scalars* io);
 int cube_build_green(cube_ctx* ctx, const float* fk_table, const float* ck_table);
 int cube_tree_sum_dev(cube_ctx* ctx, const double* in, int64_t n, double* out_host);
+// the per-particle velocity statistics of update_x, sum |v_res|^2 and sum |v|^2, in the
+// new layout from its codes, its cell means and each slot's cell (slot_cell)
+int cube_stats_sums(cube_ctx* ctx, const int32_t* slot_cell, const double* dec, double* sum_r, double* sum_s);
 int cube_exclusive_scan(cube_ctx* ctx, const int32_t* in, int64_t n, int64_t* out);
 int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n);
 int cube_nu_init(cube_ctx* ctx, NuFluid& F);

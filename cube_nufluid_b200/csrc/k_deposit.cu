@@ -4,35 +4,39 @@
  * One CTA owns a brick of BX x BY x BZ coarse cells and the 4B^3 fine nodes
  * inside it.  It reads the particles of its cells plus the one-cell layer on
  * the low side of each dimension (the only outside particles whose CIC cloud
- * reaches the brick's first node plane), accumulates every weight into
- * shared memory as a 64-bit fixed-point integer (weight * 2^32, rounded to
- * nearest), and writes each fine node once as FP32.  Integer accumulation
- * makes the density independent of particle order: the fine mesh is
+ * reaches the brick's first node plane) and accumulates every CIC weight as a
+ * 64-bit fixed-point integer q = RN(w * 2^32) in shared memory.  The weight is
+ * the reference's FP32 product of the three linear factors; the particle mass
+ * is applied once per node when the node is written, so q <= 2^32 and every
+ * node sum is exact and independent of particle order: the fine mesh is
  * bit-identical to the fixed-point mode of the CPU oracle.
  *
- * Each 64-bit accumulator is kept as two 32-bit words updated with native
- * 32-bit shared atomics: the low word's add returns the old value, and the
- * carry out of it goes into the high word with the weight's high half.  The
- * words then hold the 64-bit sum exactly (the number of low-word wraps is
- * floor(sum of low halves / 2^32) whatever the order).  A 64-bit shared
- * atomic add is a compare-and-swap loop whose colliding lanes retry: in
- * clustered states, where thousands of particles of one coarse cell add into
- * the same nodes, it took six times the atomic instructions of an unclustered
- * state of the same size.
+ * A node sum S is held as two 32-bit words, A = sum(q mod 2^16) and
+ * B = sum(q div 2^16), S = A + 2^16 B, each updated by a 32-bit shared add whose
+ * result is not needed (a no-return reduction, no round trip).  A block takes at
+ * most DMAX <= 65535 particles, so neither word can wrap.  Node slots are
+ * rotated within their 32-word row by two bits of (y, z), so the lanes of a warp,
+ * which hold neighbouring particles of a few cells, hit different banks.
  *
- * Weights follow the reference expressions in FP32, with the position formed
- * in FP64 and rounded to FP32 exactly where the reference assigns it to its
- * real tempx (tile-relative coordinates, as in pm.f90:87 and :255).
- *
- * The coarse deposit (ncell coarser, node at the cell centre) is accumulated
- * from the brick's own particles into a (B+2)^3 shared region and added to a
- * global 64-bit accumulator with atomics; the nc^3 accumulator stays in L2.
+ * The coarse density is not deposited particle by particle.  The coarse CIC
+ * kernel of a particle at fine coordinate x, seen from the coarse node whose
+ * centre is the fine node 4J+2, is the tent T(x) = 1 - |x - 4J - 2|/4; T is
+ * linear between fine nodes, and CIC interpolation reproduces linear functions,
+ * so sum_n W_fine(x - n) T(n) = T(x) exactly.  The coarse density is therefore
+ * the fine node sums restricted with the weights (4 - |d|)/4, |d| <= 3, per
+ * dimension -- the identity holds for each particle's quantised fine weights
+ * too, so the coarse sums are exact integers (scale 2^38 = 2^32 * 4^3) and
+ * order-independent.  Each brick restricts its own fine nodes (z, then y, then x
+ * passes in shared memory) into the (B+2)^3 coarse nodes they reach and adds
+ * them to a global 64-bit accumulator (nc^3, resident in L2).  This removes the
+ * per-particle coarse atomics, whose lanes (the eight particles of a cell) all
+ * hit the same coarse nodes.
  *
  * A brick whose region holds more than DMAX particles (clustered states) is
  * split over several blocks, each taking DMAX of them: a block adds its fine
- * nodes into the brick's 64-bit global slot, and the block that finishes last
- * (a fence, then a counter: no block waits for another) writes the brick's
- * nodes.  Integer sums make the split invisible in the result.
+ * node sums into the brick's 64-bit global slot, and the block that finishes
+ * last (a fence, then a counter: no block waits for another) writes the
+ * brick's fine nodes and restricts them.
  */
 #include "cube_internal.cuh"
 
@@ -44,20 +48,31 @@ constexpr int BX = 8, BY = 4, BZ = 4;
 constexpr int HX = BX + 1, HY = BY + 1, HZ = BZ + 1;
 constexpr int NHC = HX * HY * HZ;  // cells read (with the low-side layer)
 constexpr int FX = 4 * BX, FY = 4 * BY, FZ = 4 * BZ;
-constexpr int CX = BX + 2, CY = BY + 2, CZ = BZ + 2;
+constexpr int NFN = FX * FY * FZ;  // fine nodes of a brick
+constexpr int CX = BX + 2, CY = BY + 2, CZ = BZ + 2;  // coarse nodes a brick's fine nodes reach
+constexpr int DEP_THREADS = 512;
 constexpr double FIX_SCALE = 4294967296.0;  // 2^32
 constexpr int DMAX = 8192;  // region particles per deposit block
 static_assert(32 * NHC <= DMAX, "regions of cells of at most 32 particles need no split");
+static_assert(DMAX <= 65535, "the split words of a node take at most 65535 adds");
+static_assert(FX == 32, "a fine row of the brick is one bank cycle");
+static_assert(FX * FY == DEP_THREADS, "one (x, y) column of the brick per thread in the z pass");
+static_assert(CX * CY * CZ <= DEP_THREADS && CZ * FX <= DEP_THREADS, "restriction passes fit one block");
 
-// 64-bit fixed-point add into the word pair (lo[i], hi[i]); q >= 0
-__device__ __forceinline__ void fix_add(unsigned* lo, unsigned* hi, int i, unsigned long long q) {
-  const unsigned ql = (unsigned)q;
-  const unsigned old = atomicAdd(&lo[i], ql);
-  const unsigned h = (unsigned)(q >> 32) + ((unsigned)(old + ql) < old ? 1u : 0u);
-  if (h) atomicAdd(&hi[i], h);
+// shared-memory slot of fine node (nx, ny, nz) of the brick: the row is rotated
+// by 16 (ny bit 1) + (nz bit 1) words
+__device__ __forceinline__ int node_slot(int nx, int ny, int nz) {
+  return ((nz * FY + ny) << 5) + ((nx + (((ny >> 1) & 1) << 4) + ((nz >> 1) & 1)) & 31);
 }
-__device__ __forceinline__ unsigned long long fix_get(const unsigned* lo, const unsigned* hi, int i) {
-  return ((unsigned long long)hi[i] << 32) | lo[i];
+
+// restriction weight x4 of fine node n = 4m + r onto coarse nodes: node n feeds
+// local coarse index m (= J + 1 for the node J = m - 1), m + 1 and m + 2
+template <int R>
+__device__ __forceinline__ void tent_add(unsigned long long* acc, int m, unsigned long long s) {
+  if (R == 0) { acc[m] += 2ull * s; acc[m + 1] += 2ull * s; }
+  if (R == 1) { acc[m] += s; acc[m + 1] += 3ull * s; }
+  if (R == 2) { acc[m + 1] += 4ull * s; }
+  if (R == 3) { acc[m + 1] += 3ull * s; acc[m + 2] += s; }
 }
 
 // the coarse cell of region cell q of the brick at (x0, y0, z0)
@@ -112,27 +127,23 @@ __global__ void __launch_bounds__(256) k_dep_items(const int64_t* __restrict__ c
   }
 }
 
-template <int ZX>
-__global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, const int64_t* __restrict__ cell_start,
-                                                 int64_t cap, int nc, int nt, int nnt, float mass,
-                                                 float* __restrict__ rho, int rp, size_t plane,
-                                                 unsigned long long* __restrict__ rho_c_acc,
-                                                 unsigned long long* __restrict__ mass_total,
-                                                 const int64_t* __restrict__ items,
-                                                 unsigned long long* __restrict__ split_nodes,
-                                                 unsigned int* __restrict__ split_done) {
+// RT: the fine mesh's element type (float; double in the FP64 Poisson mode)
+template <int ZX, typename RT>
+__global__ void __launch_bounds__(DEP_THREADS, 3) k_deposit(
+    const void* __restrict__ xp_, const int64_t* __restrict__ cell_start, int64_t cap, int nc, int nt, int nnt,
+    double unit, RT* __restrict__ rho, int rp, size_t plane, unsigned long long* __restrict__ rho_c_acc,
+    unsigned long long* __restrict__ mass_total, const int64_t* __restrict__ items,
+    unsigned long long* __restrict__ split_nodes, unsigned int* __restrict__ split_done) {
   typedef typename CodeT<ZX>::T TX;
   const TX* xp = reinterpret_cast<const TX*>(xp_);
   extern __shared__ unsigned smem_u32[];
-  unsigned* flo = smem_u32;                  // FX*FY*FZ low words
-  unsigned* fhi = flo + FX * FY * FZ;        // high words
-  unsigned* clo = fhi + FX * FY * FZ;        // CX*CY*CZ
-  unsigned* chi = clo + CX * CY * CZ;
+  unsigned* wa = smem_u32;   // NFN words: sums of q mod 2^16
+  unsigned* wb = wa + NFN;   // NFN words: sums of q div 2^16
   __shared__ int64_t cst[NHC];
   __shared__ int cpre[NHC + 1];
-  __shared__ int lt[3][HX];  // in-tile coordinate of region cell -1..B-1 per dimension
-
+  __shared__ float ltf[3][HX];  // 4 x in-tile coordinate of region cell -1..B-1 per dimension
   __shared__ int last_block;
+  const int tid = threadIdx.x;
   int64_t brick = blockIdx.x, slot = -1;  // without items: block b = brick b, all of it
   int t0 = 0, t1 = 0x7fffffff;
   if (items) {
@@ -146,17 +157,17 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
   const int bx = (int)(brick % nbx), by = (int)((brick / nbx) % nby), bz = (int)(brick / ((int64_t)nbx * nby));
   const int x0 = bx * BX, y0 = by * BY, z0 = bz * BZ;
 
-  for (int i = threadIdx.x; i < 2 * (FX * FY * FZ + CX * CY * CZ); i += blockDim.x) smem_u32[i] = 0u;
-  if (threadIdx.x >= 32 && threadIdx.x < 32 + 3 * HX) {
-    const int d = (threadIdx.x - 32) / HX, c = (threadIdx.x - 32) % HX;
+  for (int i = tid; i < 2 * NFN; i += DEP_THREADS) smem_u32[i] = 0u;
+  if (tid >= 32 && tid < 32 + 3 * HX) {
+    const int d = (tid - 32) / HX, c = (tid - 32) % HX;
     const int base = d == 0 ? x0 : d == 1 ? y0 : z0;
-    lt[d][c] = cube_wrap(base + c - 1, nc) % nt;
+    ltf[d][c] = 4.f * (float)(cube_wrap(base + c - 1, nc) % nt);
   }
-  if (threadIdx.x < 32) {
+  if (tid < 32) {
     // cell table of the (B+1)^3 region in (z,y,x) order; warp 0 builds the prefix
     int run = 0;
     for (int base = 0; base < NHC; base += 32) {
-      const int q = base + threadIdx.x;
+      const int q = base + tid;
       int cnt = 0;
       if (q < NHC) {
         const int64_t c = region_cell(q, x0, y0, z0, nc, nt, nnt);
@@ -167,17 +178,18 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
       int inc = cnt;
       for (int o = 1; o < 32; o <<= 1) {
         const int v = __shfl_up_sync(0xffffffffu, inc, o);
-        if ((int)threadIdx.x >= o) inc += v;
+        if (tid >= o) inc += v;
       }
       if (q < NHC) cpre[q] = run + inc - cnt;
       run += __shfl_sync(0xffffffffu, inc, 31);
     }
-    if (threadIdx.x == 0) cpre[NHC] = run;
+    if (tid == 0) cpre[NHC] = run;
   }
   __syncthreads();
   const int total = cpre[NHC];
   const int tend = min(t1, total);
-  for (int t = t0 + threadIdx.x; t < tend; t += blockDim.x) {
+  const float xres = ZX == 1 ? 0.00390625f : 1.52587890625e-05f;  // 2^-8, 2^-16
+  for (int t = t0 + tid; t < tend; t += DEP_THREADS) {
     int lo = 0, hi = NHC - 1;  // last q with cpre[q] <= t
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -185,100 +197,147 @@ __global__ void __launch_bounds__(256) k_deposit(const void* __restrict__ xp_, c
     }
     const int q = lo;
     const int64_t ip = cst[q] + (t - cpre[q]);
-    const int cx = q % HX - 1, cy = (q / HX) % HY - 1, cz = q / (HX * HY) - 1;
-    const int cu[3] = {x0 + cx, y0 + cy, z0 + cz};     // unwrapped global coarse cell
-    const int cr[3] = {cx + 1, cy + 1, cz + 1};        // region index
-    const int own = (cx >= 0 && cy >= 0 && cz >= 0);
-    int o1[3], c1[3];
-    float dx1[3], dx2[3], cd1[3], cd2[3];
+    const int cr[3] = {q % HX, (q / HX) % HY, q / (HX * HY)};  // region index (cell + 1)
+    int o1[3];
+    float dx1[3], dx2[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const int l = lt[d][cr[d]];
-      const double fr = cube_xfrac((int32_t)xp[(size_t)d * cap + ip], ZX);
-      // fine: tempx = ncell*(i-1) + ncell*frac (tile-relative), FP64 -> FP32
-      const float tf = (float)cube_dadd(4.0 * (double)l, cube_dmul(4.0, fr));
-      const float f = floorf(tf) + 1.f;
-      dx1[d] = cube_fsub(f, tf);
+      const float l4 = ltf[d][cr[d]];
+      const uint32_t u = (uint32_t)(int32_t)xp[(size_t)d * cap + ip] & (ZX == 1 ? 0xFFu : 0xFFFFu);
+      const float fr = __fmul_rn((float)u + 0.5f, xres);  // exact
+      // tempx = ncell*(i-1) + ncell*frac (tile-relative) rounded once to real(4) (pm.f90:87):
+      // both terms are exact in FP32, so the FP32 add is that single rounding
+      const float tf = __fadd_rn(l4, __fmul_rn(4.f, fr));
+      const float f = floorf(tf);
+      dx1[d] = cube_fsub(f + 1.f, tf);
       dx2[d] = cube_fsub(1.f, dx1[d]);
-      o1[d] = 4 * (cu[d] - (d == 0 ? x0 : d == 1 ? y0 : z0)) + ((int)f - 1 - 4 * l);
-      // coarse: tempx = (i-1) + frac - 0.5, FP64 -> FP32
-      const float tc = (float)cube_dsub(cube_dadd((double)l, fr), 0.5);
-      const float ci = floorf(tc) + 1.f;
-      cd1[d] = cube_fsub(ci, tc);
-      cd2[d] = cube_fsub(1.f, cd1[d]);
-      c1[d] = (cu[d] - (d == 0 ? x0 : d == 1 ? y0 : z0)) + ((int)ci - 1 - l) + 1;  // +1: region starts at -1
+      o1[d] = 4 * (cr[d] - 1) + (int)(f - l4);  // brick-local fine node of the lower corner
     }
 #pragma unroll
     for (int c8 = 0; c8 < 8; ++c8) {
       const int sx = c8 & 1, sy = (c8 >> 1) & 1, sz = c8 >> 2;
       const int nx = o1[0] + sx, ny = o1[1] + sy, nz = o1[2] + sz;
       if (nx >= 0 && nx < FX && ny >= 0 && ny < FY && nz >= 0 && nz < FZ) {
-        const float w = cube_fmul(cube_fmul(cube_fmul(sx ? dx2[0] : dx1[0], sy ? dx2[1] : dx1[1]),
-                                            sz ? dx2[2] : dx1[2]), mass);
-        const unsigned long long qv = (unsigned long long)__double2ll_rn((double)w * FIX_SCALE);
-        fix_add(flo, fhi, (nz * FY + ny) * FX + nx, qv);
-      }
-      if (own) {
-        const float w = cube_fmul(cube_fmul(cube_fmul(sx ? cd2[0] : cd1[0], sy ? cd2[1] : cd1[1]),
-                                            sz ? cd2[2] : cd1[2]), mass);
-        const unsigned long long qv = (unsigned long long)__double2ll_rn((double)w * FIX_SCALE);
-        fix_add(clo, chi, ((c1[2] + sz) * CY + (c1[1] + sy)) * CX + (c1[0] + sx), qv);
+        const float w = cube_fmul(cube_fmul(sx ? dx2[0] : dx1[0], sy ? dx2[1] : dx1[1]), sz ? dx2[2] : dx1[2]);
+        // w * 2^32 is exact in FP32 (w <= 1); its nearest integer as in the FP64 form
+        const unsigned long long qv = __float2ull_rn(__fmul_rn(w, 4294967296.f));  // <= 2^32
+        const int s = node_slot(nx, ny, nz);
+        atomicAdd(&wa[s], (unsigned)(qv & 0xFFFFull));
+        atomicAdd(&wb[s], (unsigned)(qv >> 16));
       }
     }
   }
   __syncthreads();
-  unsigned long long msum = 0ull;
-  unsigned long long* sacc = slot >= 0 ? split_nodes + (size_t)slot * (FX * FY * FZ) : nullptr;
-  for (int i = threadIdx.x; i < FX * FY * FZ; i += blockDim.x) {
-    const int nx = i % FX, ny = (i / FX) % FY, nz = i / (FX * FY);
-    const unsigned long long a = fix_get(flo, fhi, i);
-    msum += a;
-    if (!sacc)
-      rho[(size_t)(4 * z0 + nz) * plane + (size_t)(4 * y0 + ny) * rp + (4 * x0 + nx)] =
-          (float)((double)a * (1.0 / FIX_SCALE));
-    else if (a)
-      atomicAdd(&sacc[i], a);
-  }
-  if (sacc) {  // the last of the brick's blocks writes its nodes
+  unsigned long long* sacc = slot >= 0 ? split_nodes + (size_t)slot * NFN : nullptr;
+  if (sacc) {  // partial sums into the brick's slot; the last of its blocks goes on
+    for (int i = tid; i < NFN; i += DEP_THREADS) {
+      const unsigned long long s = (unsigned long long)wa[i] + ((unsigned long long)wb[i] << 16);
+      if (s) atomicAdd(&sacc[i], s);
+    }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) last_block = atomicAdd(&split_done[slot], 1u) == (unsigned)((total + DMAX - 1) / DMAX - 1);
+    if (tid == 0) last_block = atomicAdd(&split_done[slot], 1u) == (unsigned)((total + DMAX - 1) / DMAX - 1);
     __syncthreads();
-    if (last_block) {
-      __threadfence();
-      for (int i = threadIdx.x; i < FX * FY * FZ; i += blockDim.x) {
-        const int nx = i % FX, ny = (i / FX) % FY, nz = i / (FX * FY);
-        rho[(size_t)(4 * z0 + nz) * plane + (size_t)(4 * y0 + ny) * rp + (4 * x0 + nx)] =
-            (float)((double)__ldcg(&sacc[i]) * (1.0 / FIX_SCALE));
-      }
+    if (!last_block) return;
+    __threadfence();
+  }
+  // z pass: one (x, y) column per thread writes its fine nodes and restricts them in z
+  const int cxl = tid & 31, cyl = tid >> 5;
+  unsigned long long rz[CZ];
+#pragma unroll
+  for (int k = 0; k < CZ; ++k) rz[k] = 0ull;
+  unsigned long long msum = 0ull;
+  RT* rrow = rho + (size_t)(4 * z0) * plane + (size_t)(4 * y0 + cyl) * rp + (4 * x0 + cxl);
+#pragma unroll
+  for (int m = 0; m < BZ; ++m) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int nz = 4 * m + r;
+      const int s = node_slot(cxl, cyl, nz);
+      const unsigned long long S =
+          sacc ? __ldcg(&sacc[s]) : (unsigned long long)wa[s] + ((unsigned long long)wb[s] << 16);
+      msum += S;
+      rrow[(size_t)nz * plane] = (RT)((double)S * unit);
+      if (r == 0) tent_add<0>(rz, m, S);
+      if (r == 1) tent_add<1>(rz, m, S);
+      if (r == 2) tent_add<2>(rz, m, S);
+      if (r == 3) tent_add<3>(rz, m, S);
     }
   }
-  for (int i = threadIdx.x; i < CX * CY * CZ; i += blockDim.x) {
-    const unsigned long long a = fix_get(clo, chi, i);
-    if (a) {
-      const int nx = i % CX - 1, ny = (i / CX) % CY - 1, nz = i / (CX * CY) - 1;
-      const int gx = cube_wrap(x0 + nx, nc), gy = cube_wrap(y0 + ny, nc), gz = cube_wrap(z0 + nz, nc);
-      atomicAdd(&rho_c_acc[((size_t)gz * nc + gy) * nc + gx], a);
+  __syncthreads();  // every node read: the words are free for the restriction
+  unsigned long long* R1 = reinterpret_cast<unsigned long long*>(smem_u32);  // [CZ][FY][FX]
+  unsigned long long* R2 = R1 + CZ * FY * FX;                                // [CZ][CY][FX]
+#pragma unroll
+  for (int k = 0; k < CZ; ++k) R1[(k * FY + cyl) * FX + cxl] = rz[k];
+  __syncthreads();
+  // y pass: one (z node, x) column per thread
+  if (tid < CZ * FX) {
+    const int k = tid >> 5, x = tid & 31;
+    unsigned long long ry[CY];
+#pragma unroll
+    for (int j = 0; j < CY; ++j) ry[j] = 0ull;
+#pragma unroll
+    for (int m = 0; m < BY; ++m) {
+      tent_add<0>(ry, m, R1[(k * FY + 4 * m) * FX + x]);
+      tent_add<1>(ry, m, R1[(k * FY + 4 * m + 1) * FX + x]);
+      tent_add<2>(ry, m, R1[(k * FY + 4 * m + 2) * FX + x]);
+      tent_add<3>(ry, m, R1[(k * FY + 4 * m + 3) * FX + x]);
+    }
+#pragma unroll
+    for (int j = 0; j < CY; ++j) R2[(k * CY + j) * FX + x] = ry[j];
+  }
+  __syncthreads();
+  // x pass: one coarse node per thread, added to the global accumulator
+  if (tid < CX * CY * CZ) {
+    const int i = tid % CX, j = (tid / CX) % CY, k = tid / (CX * CY);
+    const unsigned long long* row = R2 + (k * CY + j) * FX;
+    const int c = 4 * i - 2;  // brick-local fine node of coarse node i - 1's centre (4(i-1)+2)
+    unsigned long long s = 0ull;
+#pragma unroll
+    for (int d = -3; d <= 3; ++d) {
+      const int n = c + d;
+      if (n >= 0 && n < FX) s += (unsigned long long)(4 - (d < 0 ? -d : d)) * row[n];
+    }
+    if (s) {
+      const int gx = cube_wrap(x0 + i - 1, nc), gy = cube_wrap(y0 + j - 1, nc), gz = cube_wrap(z0 + k - 1, nc);
+      atomicAdd(&rho_c_acc[((size_t)gz * nc + gy) * nc + gx], s);
     }
   }
   for (int o = 16; o > 0; o >>= 1) msum += __shfl_xor_sync(0xffffffffu, msum, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(mass_total, msum);
+  if ((tid & 31) == 0) atomicAdd(mass_total, msum);
 }
 
-// coarse accumulator -> FP32 density (pitch rp), accumulator cleared for the next step
-__global__ void k_coarse_finalize(unsigned long long* __restrict__ acc, float* __restrict__ r3, int nc, int rp,
+// coarse accumulators -> FP32 density (pitch rp), accumulators cleared for the next
+// step: mass * (particle sum) * 2^-38 + (neutrino sum) * 2^-32; the mass totals are
+// the particle sums / 64 (scale 2^32, without the mass) and the neutrino sums
+template <typename RT>
+__global__ void k_coarse_finalize(unsigned long long* __restrict__ acc, unsigned long long* __restrict__ acc_nu,
+                                  RT* __restrict__ r3, int nc, int rp, double unit_c,
                                   unsigned long long* __restrict__ mass_total) {
   const int64_t n = (int64_t)nc * nc * nc;
-  unsigned long long msum = 0ull;
+  unsigned long long msum = 0ull, nsum = 0ull;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const unsigned long long a = acc[i];
     acc[i] = 0ull;
-    msum += a;
+    msum += a >> 6;
+    double v = (double)a * unit_c;
+    if (acc_nu) {
+      const unsigned long long b = acc_nu[i];
+      acc_nu[i] = 0ull;
+      nsum += b;
+      v = v + (double)b * (1.0 / FIX_SCALE);
+    }
     const int64_t x = i % nc, yz = i / nc;
-    r3[yz * rp + x] = (float)((double)a * (1.0 / FIX_SCALE));
+    r3[yz * rp + x] = (RT)v;
   }
-  for (int o = 16; o > 0; o >>= 1) msum += __shfl_xor_sync(0xffffffffu, msum, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(mass_total, msum);
+  for (int o = 16; o > 0; o >>= 1) {
+    msum += __shfl_xor_sync(0xffffffffu, msum, o);
+    nsum += __shfl_xor_sync(0xffffffffu, nsum, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(mass_total, msum);
+    if (nsum) atomicAdd(mass_total + 1, nsum);
+  }
 }
 
 }  // namespace
@@ -290,7 +349,7 @@ int cube_deposit(cube_ctx* ctx, cube_scalars* io) {
     return CUBE_ERR_PARAM;
   }
   unsigned long long* mtot = reinterpret_cast<unsigned long long*>(ctx->red_tmp);
-  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(mtot, 0, 2 * sizeof(unsigned long long), ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(mtot, 0, 3 * sizeof(unsigned long long), ctx->stream));
   // work items: one per brick, more for bricks beyond DMAX region particles; not
   // needed when no cell holds more than 32 particles (a region of 225 cells then
   // holds at most 7200 <= DMAX)
@@ -311,7 +370,7 @@ int cube_deposit(cube_ctx* ctx, cube_scalars* io) {
   unsigned long long* split_nodes = nullptr;
   unsigned int* split_done = nullptr;
   if (hv[1]) {
-    const size_t node_bytes = sizeof(unsigned long long) * FX * FY * FZ * hv[1];
+    const size_t node_bytes = sizeof(unsigned long long) * NFN * hv[1];
     const size_t need = node_bytes + sizeof(unsigned int) * hv[1];
     if (need > ctx->dep_scratch_bytes) {
       if (ctx->dep_scratch) cudaFree(ctx->dep_scratch);
@@ -325,24 +384,35 @@ int cube_deposit(cube_ctx* ctx, cube_scalars* io) {
     split_nodes = reinterpret_cast<unsigned long long*>(ctx->dep_scratch);
     split_done = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(ctx->dep_scratch) + node_bytes);
   }
-  const size_t smem = 2 * sizeof(unsigned) * (FX * FY * FZ + CX * CY * CZ);
-  if (ctx->izipx == 1) {
-    CUBE_CUDA_TRY(ctx, cube_smem_limit(k_deposit<1>, smem));
-    k_deposit<1><<<(unsigned)blocks, 256, smem, ctx->stream>>>(
-        ctx->xp, ctx->cell_start, ctx->cap, nc, ctx->nt, ctx->nnt, io->mass_p_cdm, ctx->fine.rho, ctx->fine.rp,
-        ctx->fine.plane, ctx->rho_c_acc, mtot, items, split_nodes, split_done);
-  } else {
-    CUBE_CUDA_TRY(ctx, cube_smem_limit(k_deposit<2>, smem));
-    k_deposit<2><<<(unsigned)blocks, 256, smem, ctx->stream>>>(
-        ctx->xp, ctx->cell_start, ctx->cap, nc, ctx->nt, ctx->nnt, io->mass_p_cdm, ctx->fine.rho, ctx->fine.rp,
-        ctx->fine.plane, ctx->rho_c_acc, mtot, items, split_nodes, split_done);
-  }
-  CUBE_LAUNCH_CHECK(ctx);
+  const size_t smem = 2 * sizeof(unsigned) * NFN;
+  const double unit = (double)io->mass_p_cdm * (1.0 / FIX_SCALE);  // exact
+  auto launch = [&](auto kern, auto* rho) -> int {
+    CUBE_CUDA_TRY(ctx, cube_smem_limit(kern, smem));
+    kern<<<(unsigned)blocks, DEP_THREADS, smem, ctx->stream>>>(ctx->xp, ctx->cell_start, ctx->cap, nc, ctx->nt,
+                                                              ctx->nnt, unit, rho, ctx->fine.rp, ctx->fine.plane,
+                                                              ctx->rho_c_acc, mtot, items, split_nodes, split_done);
+    CUBE_LAUNCH_CHECK(ctx);
+    return CUBE_OK;
+  };
+  double* rho_d = reinterpret_cast<double*>(ctx->fine.rho);
+  int lrc;
+  if (ctx->fine.fp64)
+    lrc = ctx->izipx == 1 ? launch(k_deposit<1, double>, rho_d) : launch(k_deposit<2, double>, rho_d);
+  else
+    lrc = ctx->izipx == 1 ? launch(k_deposit<1, float>, ctx->fine.rho) : launch(k_deposit<2, float>, ctx->fine.rho);
+  if (lrc) return lrc;
   if (ctx->nu.on) {  // neutrino density into both meshes (pm.f90:55-74, :198-242)
     const int rc = cube_nu_density(ctx, io);
     if (rc) return rc;
   }
-  k_coarse_finalize<<<592, 256, 0, ctx->stream>>>(ctx->rho_c_acc, ctx->coarse.rho, nc, ctx->coarse.rp, mtot + 1);
+  const double unit_c = (double)io->mass_p_cdm * (1.0 / (64.0 * FIX_SCALE));  // exact
+  if (ctx->coarse.fp64)
+    k_coarse_finalize<double><<<592, 256, 0, ctx->stream>>>(ctx->rho_c_acc, nullptr,
+                                                            reinterpret_cast<double*>(ctx->coarse.rho), nc,
+                                                            ctx->coarse.rp, unit_c, mtot + 1);
+  else
+    k_coarse_finalize<float><<<592, 256, 0, ctx->stream>>>(ctx->rho_c_acc, ctx->nu.on ? ctx->rho_c_nu : nullptr,
+                                                           ctx->coarse.rho, nc, ctx->coarse.rp, unit_c, mtot + 1);
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }

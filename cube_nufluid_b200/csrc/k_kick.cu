@@ -144,6 +144,104 @@ __global__ void __launch_bounds__(256, 3) k_kick(const void* __restrict__ xp_, v
   if (threadIdx.x < 3) atomicMax(&dscal->vmax_bits[threadIdx.x], vmx_s[threadIdx.x]);
 }
 
+// The kick of the FP64 Poisson mode: the same per-particle steps on FP64 force
+// meshes (kick increments formed in FP64 by the Green multiply), with the CIC
+// weights and the products force*dx*dy*dz in FP64 (the positions are exact in
+// FP64).  The velocity codec, its tables and the intermediate quantisation are the
+// FP32 path's, so the two runs differ only in the mesh arithmetic.
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256, 3) k_kick64(const void* __restrict__ xp_, void* __restrict__ vp_,
+                                                const int64_t* __restrict__ cell_start, const float* __restrict__ vfield,
+                                                int64_t cap, int64_t ncells, int nc, int nt, int nnt,
+                                                const double* __restrict__ ff, size_t fcomp, int frp, size_t fplane,
+                                                const double* __restrict__ fc, size_t ccomp, int crp, size_t cplane,
+                                                const double* __restrict__ dec_old, const double* __restrict__ dec_new,
+                                                int half_nvbin, cube_codec codec, double coef_new, double inv_pi,
+                                                DevScal* __restrict__ dscal, const int64_t* __restrict__ items,
+                                                int64_t items_max) {
+  typedef typename CodeT<ZX>::T TX;
+  typedef typename CodeT<ZV>::T TV;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  TV* vp = reinterpret_cast<TV*>(vp_);
+  __shared__ int64_t cs[KCELLS + 1];
+  __shared__ int cl[KCELLS][3], ctb[KCELLS][3];
+  __shared__ unsigned int vmx_s[3];
+  int64_t c0, p0, p1;
+  int ncl;
+  if (!cube_cell_item(items, ncells, items_max, dscal, c0, ncl, p0, p1)) return;
+  for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = cell_start[c0 + i];
+  if (threadIdx.x < ncl) cube_cell_coords(c0 + threadIdx.x, nt, nnt, cl[threadIdx.x], ctb[threadIdx.x]);
+  if (threadIdx.x < 3) vmx_s[threadIdx.x] = 0u;
+  __syncthreads();
+  const int nf = 4 * nc;
+  const int npb = (int)(p1 - p0);
+  const int ox[8] = {0, 1, 0, 0, 0, 1, 1, 1}, oy[8] = {0, 0, 1, 0, 1, 0, 1, 1}, oz[8] = {0, 0, 0, 1, 1, 1, 0, 1};
+  float vm[3] = {0.f, 0.f, 0.f};
+  for (int i = threadIdx.x; i < npb; i += blockDim.x) {
+    const int64_t ip = p0 + i;
+    int lo = 0, hi = ncl - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
+    }
+    const int64_t c = c0 + lo;
+    int fi[3][2], gi[3][2];
+    double dx1[3], dx2[3], cx1[3], cx2[3];
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const int l = cl[lo][e], tb = ctb[lo][e];
+      const double fr = cube_xfrac((int32_t)xp[(size_t)e * cap + ip], ZX);
+      const double tf = 4.0 * (double)l + 4.0 * fr;  // exact
+      const double f = floor(tf) + 1.0;
+      dx1[e] = f - tf;
+      dx2[e] = 1.0 - dx1[e];
+      const int n1 = 4 * tb + (int)f - 1;
+      fi[e][0] = cube_wrap(n1, nf);
+      fi[e][1] = cube_wrap(n1 + 1, nf);
+      const double tc = ((double)(tb + l) - 0.5) + fr;  // exact
+      const double ci = floor(tc) + 1.0;
+      cx1[e] = ci - tc;
+      cx2[e] = 1.0 - cx1[e];
+      const int m1 = (int)ci - 1;
+      gi[e][0] = cube_wrap(m1, nc);
+      gi[e][1] = cube_wrap(m1 + 1, nc);
+    }
+    const size_t fz[2] = {(size_t)fi[2][0] * fplane, (size_t)fi[2][1] * fplane};
+    const size_t gz[2] = {(size_t)gi[2][0] * cplane, (size_t)gi[2][1] * cplane};
+    const int fy[2] = {fi[1][0] * frp, fi[1][1] * frp}, gy[2] = {gi[1][0] * crp, gi[1][1] * crp};
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+      const double* F = ff + d * fcomp;
+      const double* G = fc + d * ccomp;
+      const int code = (int)vp[(size_t)d * cap + ip];
+      const float vf = __ldg(&vfield[(size_t)d * ncells + c]);
+      double v = __ldg(&dec_old[code + half_nvbin]);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const double q = __ldg(&F[fz[oz[k]] + (size_t)(fy[oy[k]] + fi[0][ox[k]])]);
+        v += ((q * (ox[k] ? dx2[0] : dx1[0])) * (oy[k] ? dx2[1] : dx1[1])) * (oz[k] ? dx2[2] : dx1[2]);
+      }
+      const int code1 = cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
+      v = __ldg(&dec_new[code1 + half_nvbin]);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const double q = __ldg(&G[gz[oz[k]] + (size_t)(gy[oy[k]] + gi[0][ox[k]])]);
+        v += ((q * (ox[k] ? cx2[0] : cx1[0])) * (oy[k] ? cx2[1] : cx1[1])) * (oz[k] ? cx2[2] : cx1[2]);
+      }
+      const float am = (float)fabs(v + (double)vf);
+      vm[d] = fmaxf(vm[d], am);
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
+    }
+  }
+#pragma unroll
+  for (int e = 0; e < 3; ++e) {
+    const unsigned int w = __reduce_max_sync(0xffffffffu, __float_as_uint(vm[e]));
+    if ((threadIdx.x & 31) == 0 && w) atomicMax(&vmx_s[e], w);
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) atomicMax(&dscal->vmax_bits[threadIdx.x], vmx_s[threadIdx.x]);
+}
+
 template <int ZX, int ZV>
 int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
   // work items of at most 64 cells and 4096 particles, so that the blocks over
@@ -159,6 +257,16 @@ int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
   if (rc) return rc;
   MeshLevel& F = ctx->fine;
   MeshLevel& Cc = ctx->coarse;
+  if (F.fp64) {
+    k_kick64<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+        ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt,
+        reinterpret_cast<const double*>(F.force), (size_t)F.n * F.plane, F.rp, F.plane,
+        reinterpret_cast<const double*>(Cc.force), (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, dec_old, dec_new,
+        ctx->nvbin / 2, ctx->codec, coef_new, 1.0 / (double)ctx->codec.pi_f, ctx->dscal, ctx->rebin_items,
+        cube_rebin_items_max(ctx->ncells, ctx->cap));
+    CUBE_LAUNCH_CHECK(ctx);
+    return CUBE_OK;
+  }
   k_kick<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
       ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, F.force,
       (size_t)F.n * F.plane, F.rp, F.plane, Cc.force, (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, dec_old, dec_new,

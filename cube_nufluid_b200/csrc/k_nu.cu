@@ -672,7 +672,7 @@ int cube_nu_density(cube_ctx* ctx, cube_scalars* io) {
   CUBE_LAUNCH_CHECK(ctx);
   const float hom = cube_fmul(ctx->P.f_neu, (float)(ctx->ncell * ctx->ncell * ctx->ncell));
   k_nu_coarse_deposit<<<grid_for(ctx, ctx->ncells, 256), 256, 0, ctx->stream>>>(
-      scratch, L.n, L.rp, L.plane, ctx->nc, homogeneous, hom, ctx->rho_c_acc);
+      scratch, L.n, L.rp, L.plane, ctx->nc, homogeneous, hom, ctx->rho_c_nu);
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;
 }

@@ -117,6 +117,28 @@ struct Chains {
   const uint16_t* code;
 };
 
+// kick of one target by its pair sum ft (ext_pp_force.f90:115-127): velocity codes
+// vc (index code + nvbin/2) decoded, v + ((ft*a_mid)*dt)/6/pi, re-encoded; f2 max
+template <int ZV>
+__device__ __forceinline__ void pp_apply(const double ft[3], const int vc[3], int64_t ip, const PPArgs& A,
+                                         void* __restrict__ vp_, PPAcc& acc) {
+  typedef typename CodeT<ZV>::T TV;
+  TV* vp = reinterpret_cast<TV*>(vp_);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    // a zero sum gives k = +-0 and v + k = v: a code that re-encodes to itself stays
+    if (ft[d] == 0.0 && cube_vfixed(A.dec, 2 * A.half_nvbin, vc[d])) continue;
+    double k = cube_dmul(ft[d], A.a_mid);
+    k = cube_dmul(k, A.dt);
+    k = cube_ddiv(k, 6.0);
+    k = cube_ddiv(k, A.pi_d);
+    const double v = cube_dadd(__ldg(&A.dec[vc[d]]), k);
+    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&A.codec, v, A.coef, A.inv_pi), ZV);
+  }
+  const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
+  acc.f2max = fmaxf(acc.f2max, (float)f2);
+}
+
 // one target with codes tc, global index ip, region coarse cell cc; neighbours
 // from the sorted ranges S (CHAIN = false) or the chains H (CHAIN = true)
 template <int ZX, int ZV, bool CHAIN, typename OffT>
@@ -187,19 +209,7 @@ __device__ __forceinline__ void pp_target(const Sorted<OffT>& S, const Chains& H
         }
       }
     }
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    // a zero sum gives k = +-0 and v + k = v: a code that re-encodes to itself stays
-    if (ft[d] == 0.0 && cube_vfixed(A.dec, 2 * A.half_nvbin, vc[d])) continue;
-    double k = cube_dmul(ft[d], A.a_mid);
-    k = cube_dmul(k, A.dt);
-    k = cube_ddiv(k, 6.0);
-    k = cube_ddiv(k, A.pi_d);
-    const double v = cube_dadd(__ldg(&A.dec[vc[d]]), k);
-    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&A.codec, v, A.coef, A.inv_pi), ZV);
-  }
-  const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
-  acc.f2max = fmaxf(acc.f2max, (float)f2);
+  pp_apply<ZV>(ft, vc, ip, A, vp_, acc);
 }
 
 __device__ __forceinline__ void pp_flush(PPAcc& acc, DevScal* dscal) {
@@ -384,19 +394,21 @@ template <int ZX, int ZV>
 __global__ void __launch_bounds__(PP_THREADS, 3) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                                          const int64_t* __restrict__ cell_start, int nc, int nt,
                                                          int nnt, PPArgs A, int32_t* __restrict__ spill,
-                                                         DevScal* __restrict__ dscal) {
+                                                         DevScal* __restrict__ dscal,
+                                                         const int32_t* __restrict__ bricks) {
   typedef typename CodeT<ZX>::T TX;
   const TX* xp = reinterpret_cast<const TX*>(xp_);
   extern __shared__ unsigned char pbsm[];
   __shared__ int64_t cst[PRC];
   __shared__ int cpre[PRC + 1];
   __shared__ int tpre[PB * PB * PB + 1];  // prefix of the brick's own cells (chain targets)
-  pp_region(blockIdx.x, cell_start, nc, nt, nnt, cst, cpre);
+  const int brick = bricks ? bricks[blockIdx.x] : (int)blockIdx.x;
+  pp_region(brick, cell_start, nc, nt, nnt, cst, cpre);
   const int M = cpre[PRC];
   if (M > PB_CAP) {  // crowded: sorted in global memory by k_pp_build
     if (threadIdx.x == 0) {
       const unsigned long long q = atomicAdd(&dscal->n_big, 1ull);
-      spill[2 * q] = blockIdx.x;
+      spill[2 * q] = brick;
       spill[2 * q + 1] = M;
     }
     return;
@@ -553,6 +565,303 @@ __global__ void __launch_bounds__(PP_THREADS) k_pp_crowd(void* __restrict__ vp_,
   pp_flush(acc, dscal);
 }
 
+// ---- particle-parallel path for sparse bricks -----------------------------------
+// Where most targets of a brick have no other particle in their window (early
+// times, voids), the brick is not staged: its targets are taken one per thread.
+//   k_pp_masks  one thread per coarse cell: 64-bit masks of the fine cells holding
+//               at least one and at least two particles, and each particle's fine
+//               cell; a cell of more than PP_DENSE particles instead marks every
+//               brick whose region (brick +- 1 cell) holds it as crowded;
+//   k_pp_cells  one thread per coarse cell of a brick that is not crowded: per
+//               target, isolated or not (the masks decide: no other particle in its
+//               window), counted per brick; in a brick left to the particle path an
+//               isolated target has a zero pair sum and is finished there (one window
+//               entry, the zero kick), the others are listed;
+//   k_pp_decide which bricks k_pp_brick takes: the crowded ones and those where the
+//               last step found more than a quarter of the targets with neighbours
+//               (the staged chains serve many neighbours cheaply, a listed target
+//               walks global memory); the same test on this step's counts chooses
+//               for the next step (particles move little in a step; either path gives
+//               the same bits, the choice is only about speed);
+//   k_pp_pairs  one listed target per thread walks its window in the reference's
+//               (k,j,i) order, each fine cell's particles newest-first (reverse
+//               storage order within the coarse cell), so the FP64 sums and the codes
+//               are those of the chains of ext_pp_force.f90:51-73,76-127.
+// A target in a brick that is not crowded has its window inside that brick's region,
+// which holds no crowded cell, so no window reads a crowded cell's masks (which are
+// not built) and no scan of a coarse cell takes more than PP_DENSE particles.
+constexpr int PP_DENSE = 32;
+
+struct PPPar {
+  const int64_t* cell_start;
+  int64_t ncells;
+  int nc, nt, nnt, nb;          // nb = nc / PB bricks per dimension
+  unsigned long long* occ;      // [ncells] fine cells (bit (z*4+y)*4+x) holding a particle
+  unsigned long long* multi;    // [ncells] fine cells holding two or more
+  uint8_t* pfine;               // [cap] each particle's fine cell within its coarse cell
+  unsigned int* crowded;        // [nb^3] 1: the brick's region holds a crowded cell
+  unsigned int* nonisol;        // [nb^3] non-isolated targets of the brick
+  unsigned int* ntarget;        // [nb^3] targets of the brick
+  uint8_t* staged;              // [nb^3] persistent: k_pp_brick takes the brick (last step's choice)
+  int32_t* dense_list;          // bricks for k_pp_brick, pp_dense of them
+  int32_t* list_ip;             // listed targets: particle, coarse cell
+  int32_t* list_cell;
+  DevScal* dscal;
+};
+
+// coarse cell ids of the neighbours -1, 0, +1 of (tile t, in-tile l) along one
+// dimension whose tile stride is st and in-tile stride sl (cell ids are sums of
+// the three dimensions' terms)
+__device__ __forceinline__ void pp_sep3(int l, int t, int nt, int nnt, int64_t st, int64_t sl, int64_t out[3]) {
+  out[1] = t * st + l * sl;
+  out[0] = l > 0 ? out[1] - sl : (int64_t)((t + nnt - 1) % nnt) * st + (int64_t)(nt - 1) * sl;
+  out[2] = l < nt - 1 ? out[1] + sl : (int64_t)((t + 1) % nnt) * st;
+}
+
+// the three per-dimension id terms of a cell's neighbours
+__device__ __forceinline__ void pp_neighbours(int64_t c, int nt, int nnt, int64_t X[3], int64_t Y[3], int64_t Z[3],
+                                              int g[3]) {
+  const int64_t nt3 = (int64_t)nt * nt * nt;
+  const int64_t tile = c / nt3;
+  const int rem = (int)(c - tile * nt3);
+  const int l[3] = {rem % nt, (rem / nt) % nt, rem / (nt * nt)};
+  const int t[3] = {(int)(tile % nnt), (int)((tile / nnt) % nnt), (int)(tile / ((int64_t)nnt * nnt))};
+  pp_sep3(l[0], t[0], nt, nnt, nt3, 1, X);
+  pp_sep3(l[1], t[1], nt, nnt, nt3 * nnt, nt, Y);
+  pp_sep3(l[2], t[2], nt, nnt, nt3 * nnt * nnt, (int64_t)nt * nt, Z);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) g[d] = t[d] * nt + l[d];
+}
+
+// term of coarse offset o (-1, 0, +1) from the three of pp_neighbours (no indexed
+// local array)
+__device__ __forceinline__ int64_t pp_sel(const int64_t T[3], int o) { return o < 0 ? T[0] : (o > 0 ? T[2] : T[1]); }
+
+// 4-bit mask of the fine cells [lo, hi] (coarse-cell relative) inside coarse offset o
+__device__ __forceinline__ unsigned pp_range4(int lo, int hi, int o) {
+  const int a = max(lo - 4 * o, 0), b = min(hi - 4 * o, 3);
+  return a > b ? 0u : ((2u << b) - (1u << a));
+}
+
+template <int ZX>
+__global__ void __launch_bounds__(256) k_pp_masks(const void* __restrict__ xp_, int64_t cap, PPPar Q) {
+  typedef typename CodeT<ZX>::T TX;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (c >= Q.ncells) return;
+  const int64_t s0 = Q.cell_start[c], s1 = Q.cell_start[c + 1];
+  if (s1 - s0 > PP_DENSE) {
+    int l[3], tb[3];
+    cube_cell_coords(c, Q.nt, Q.nnt, l, tb);
+    int blo[3], bhi[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int g = tb[d] + l[d];
+      blo[d] = cube_wrap(g - 1, Q.nc) / PB;
+      bhi[d] = cube_wrap(g + 1, Q.nc) / PB;
+    }
+    for (int kz = 0; kz < 2; ++kz)
+      for (int ky = 0; ky < 2; ++ky)
+        for (int kx = 0; kx < 2; ++kx) {
+          if ((kz && bhi[2] == blo[2]) || (ky && bhi[1] == blo[1]) || (kx && bhi[0] == blo[0])) continue;
+          Q.crowded[((kz ? bhi[2] : blo[2]) * Q.nb + (ky ? bhi[1] : blo[1])) * Q.nb + (kx ? bhi[0] : blo[0])] = 1u;
+        }
+    return;
+  }
+  unsigned long long occ = 0ull, multi = 0ull;
+  for (int64_t ip = s0; ip < s1; ++ip) {
+    int f = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+      f |= (int)floor(cube_dmul(4.0, cube_xfrac((int32_t)xp[(size_t)d * cap + ip], ZX))) << (2 * d);
+    Q.pfine[ip] = (uint8_t)f;
+    const unsigned long long b = 1ull << f;
+    multi |= occ & b;
+    occ |= b;
+  }
+  Q.occ[c] = occ;
+  Q.multi[c] = multi;
+}
+
+// nibble spread of a 4-bit mask (bit y -> bit 4y) and its 16-bit spread (bit z -> bit 16z)
+__device__ __forceinline__ unsigned pp_spread4(unsigned m) {
+  return (m & 1u) | ((m & 2u) << 3) | ((m & 4u) << 6) | ((m & 8u) << 9);
+}
+__device__ __forceinline__ unsigned long long pp_spread16(unsigned m) {
+  return (unsigned long long)(m & 1u) | ((unsigned long long)(m & 2u) << 15) | ((unsigned long long)(m & 4u) << 30) |
+         ((unsigned long long)(m & 8u) << 45);
+}
+
+// true if the window of +-pr fine cells around fine cell f of a coarse cell holds no
+// particle but the target: nb[9] are the ids of the coarse neighbours -1..1 per
+// dimension as separable terms (x, y, z; three each)
+__device__ __forceinline__ bool pp_isolated(const PPPar& Q, int f, int pr, const int32_t* nb) {
+  unsigned m[3][3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const int fl = (f >> (2 * d)) & 3;
+#pragma unroll
+    for (int o = 0; o < 3; ++o) m[d][o] = pp_range4(fl - pr, fl + pr, o - 1);
+  }
+  const unsigned long long own = 1ull << f;
+#pragma unroll
+  for (int oz = 0; oz < 3; ++oz)
+#pragma unroll
+    for (int oy = 0; oy < 3; ++oy)
+#pragma unroll
+      for (int ox = 0; ox < 3; ++ox) {
+        if (!(m[2][oz] && m[1][oy] && m[0][ox])) continue;
+        const int64_t C = (int64_t)nb[6 + oz] + nb[3 + oy] + nb[ox];
+        const unsigned long long w = (unsigned long long)(m[0][ox] * pp_spread4(m[1][oy])) * pp_spread16(m[2][oz]);
+        unsigned long long hit = __ldg(&Q.occ[C]) & w;
+        if (ox == 1 && oy == 1 && oz == 1) hit = (hit & ~own) | (__ldg(&Q.multi[C]) & own);
+        if (hit) return false;
+      }
+  return true;
+}
+
+template <int ZV>
+__global__ void __launch_bounds__(256, 3) k_pp_cells(PPPar Q, PPArgs A, void* __restrict__ vp_) {
+  typedef typename CodeT<ZV>::T TV;
+  const TV* vp = reinterpret_cast<const TV*>(vp_);
+  const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  PPAcc acc;
+  unsigned nonmask = 0u;  // targets of this cell with a neighbour (at most PP_DENSE = 32)
+  int64_t s0 = 0;
+  int n = 0;
+  bool apply = false;
+  if (c < Q.ncells) {
+    int64_t X[3], Y[3], Z[3];
+    int g[3];
+    pp_neighbours(c, Q.nt, Q.nnt, X, Y, Z, g);
+    const int b = ((g[2] / PB) * Q.nb + g[1] / PB) * Q.nb + g[0] / PB;
+    s0 = Q.cell_start[c];
+    n = (int)(Q.cell_start[c + 1] - s0);
+    if (!Q.crowded[b] && n > 0) {
+      const int32_t nb9[9] = {(int32_t)X[0], (int32_t)X[1], (int32_t)X[2], (int32_t)Y[0], (int32_t)Y[1],
+                              (int32_t)Y[2], (int32_t)Z[0], (int32_t)Z[1], (int32_t)Z[2]};
+      apply = !Q.staged[b];
+      for (int k = 0; k < n; ++k) {
+        const int64_t ip = s0 + k;
+        if (!pp_isolated(Q, Q.pfine[ip], A.pr, nb9)) {
+          nonmask |= 1u << k;
+        } else if (apply) {
+          // a zero pair sum: one window entry (the target), the zero kick
+          ++acc.n1;
+          ++acc.npair;
+          const double ft[3] = {0.0, 0.0, 0.0};
+          int vc[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) vc[d] = (int)vp[(size_t)d * A.cap + ip] + A.half_nvbin;
+          if (!(cube_vfixed(A.dec, 2 * A.half_nvbin, vc[0]) && cube_vfixed(A.dec, 2 * A.half_nvbin, vc[1]) &&
+                cube_vfixed(A.dec, 2 * A.half_nvbin, vc[2])))
+            pp_apply<ZV>(ft, vc, ip, A, vp_, acc);
+        }
+      }
+      atomicAdd(&Q.ntarget[b], (unsigned)n);
+      if (nonmask) atomicAdd(&Q.nonisol[b], (unsigned)__popc(nonmask));
+    }
+  }
+  // list this warp's targets with neighbours in the bricks left to the particle path
+  const unsigned cnt = apply ? (unsigned)__popc(nonmask) : 0u;
+  unsigned inc = cnt;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += v;
+  }
+  const unsigned tot = __shfl_sync(0xffffffffu, inc, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && tot) base = atomicAdd(&Q.dscal->pp_list, (unsigned long long)tot);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  if (cnt) {
+    unsigned long long k = base + inc - cnt;
+    for (unsigned m = nonmask; m; m &= m - 1, ++k) {
+      Q.list_ip[k] = (int32_t)(s0 + __ffs(m) - 1);
+      Q.list_cell[k] = (int32_t)c;
+    }
+  }
+  pp_flush(acc, Q.dscal);
+}
+
+// one thread per brick: this step's bricks for k_pp_brick (crowded, or chosen by the
+// last step's counts), and the choice for the next step from this step's counts
+__global__ void k_pp_decide(PPPar Q, int nbricks) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nbricks) return;
+  const bool crowded = Q.crowded[b] != 0u;
+  if (crowded || Q.staged[b]) Q.dense_list[atomicAdd(&Q.dscal->pp_dense, 1ull)] = b;
+  Q.staged[b] = (crowded || 4u * Q.nonisol[b] > Q.ntarget[b]) ? 1 : 0;
+}
+
+// one listed target per thread (grid-stride over the list)
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256, 3) k_pp_pairs(const void* __restrict__ xp_, const void* vp_in, void* vp_, PPPar Q,
+                                                  PPArgs A) {
+  typedef typename CodeT<ZX>::T TX;
+  typedef typename CodeT<ZV>::T TV;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  const TV* vpr = reinterpret_cast<const TV*>(vp_in);
+  const int64_t n = (int64_t)*(volatile unsigned long long*)&Q.dscal->pp_list;
+  const bool pow2_cut = (A.nf_cutoff & (A.nf_cutoff - 1)) == 0;
+  const double inv_cut = 1.0 / (double)A.nf_cutoff;
+  const int pr = A.pr;
+  PPAcc acc;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t ip = Q.list_ip[k];
+    const int64_t c = Q.list_cell[k];
+    int64_t X[3], Y[3], Z[3];
+    int g[3];
+    pp_neighbours(c, Q.nt, Q.nnt, X, Y, Z, g);
+    const int f = Q.pfine[ip];
+    const int fl[3] = {f & 3, (f >> 2) & 3, (f >> 4) & 3};
+    double x1[3], ft[3] = {0.0, 0.0, 0.0};
+    int vc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      x1[d] = cube_dmul(4.0, cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip], ZX));  // coarse-cell relative
+      vc[d] = (int)vpr[(size_t)d * A.cap + ip] + A.half_nvbin;
+    }
+    ++acc.n1;
+    for (int kk = fl[2] - pr; kk <= fl[2] + pr; ++kk) {
+      const int oz = (kk + 4) / 4 - 1;  // floor(kk / 4), kk >= -4
+      const int fz = kk - 4 * oz;
+      for (int jj = fl[1] - pr; jj <= fl[1] + pr; ++jj) {
+        const int oy = (jj + 4) / 4 - 1;
+        const int fy = jj - 4 * oy;
+        const int64_t CYZ = pp_sel(Z, oz) + pp_sel(Y, oy);
+        for (int ii = fl[0] - pr; ii <= fl[0] + pr; ++ii) {
+          const int ox = (ii + 4) / 4 - 1;
+          const int fx = ii - 4 * ox;
+          const int fb = (fz * 4 + fy) * 4 + fx;
+          const int64_t C = CYZ + pp_sel(X, ox);
+          if (!((__ldg(&Q.occ[C]) >> fb) & 1ull)) continue;
+          const double cf[3] = {4.0 * (double)ox, 4.0 * (double)oy, 4.0 * (double)oz};
+          const int64_t s0 = __ldg(&Q.cell_start[C]);
+          for (int64_t ip2 = __ldg(&Q.cell_start[C + 1]) - 1; ip2 >= s0; --ip2) {  // newest first
+            if (Q.pfine[ip2] != fb) continue;
+            ++acc.npair;
+            double x21[3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const double fr = cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip2], ZX);
+              x21[d] = cube_dsub(cube_dadd(cf[d], cube_dmul(4.0, fr)), x1[d]);
+            }
+            // a coincident particle (the target itself included) adds exactly +0
+            if (x21[0] == 0.0 && x21[1] == 0.0 && x21[2] == 0.0) continue;
+            double fp[3];
+            pp_pair(x21, A.mass, A.rsoft, A.nf_cutoff, pow2_cut, inv_cut, fp);
+#pragma unroll
+            for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], fp[d]);
+          }
+        }
+      }
+    }
+    pp_apply<ZV>(ft, vc, ip, A, vp_, acc);
+  }
+  pp_flush(acc, Q.dscal);
+}
+
 template <int ZX, int ZV>
 int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   if (ctx->nc % PB) {
@@ -575,13 +884,47 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   A.half_nvbin = ctx->nvbin / 2;
   A.codec = ctx->codec;
   A.cap = ctx->cap;
-  int32_t* spill = ctx->big_list;  // re-bin scratch, free outside update_x: (brick, M) pairs
-  const int nbricks = (ctx->nc / PB) * (ctx->nc / PB) * (ctx->nc / PB);
+  // re-bin scratch, free outside update_x: per-cell masks in cell_stats, fine cells in
+  // pkey, per-brick flags and counters in cursor, the target list in perm/tcell, and
+  // in big_list the (brick, M) pairs of crowded bricks followed by the dense-brick list
+  const int nb = ctx->nc / PB;
+  const int nbricks = nb * nb * nb;
+  int32_t* spill = ctx->big_list;
+  PPPar Q;
+  Q.cell_start = ctx->cell_start;
+  Q.ncells = ctx->ncells;
+  Q.nc = ctx->nc; Q.nt = ctx->nt; Q.nnt = ctx->nnt; Q.nb = nb;
+  Q.occ = reinterpret_cast<unsigned long long*>(ctx->cell_stats);
+  Q.multi = Q.occ + ctx->ncells;
+  Q.pfine = reinterpret_cast<uint8_t*>(ctx->pkey);
+  Q.crowded = reinterpret_cast<unsigned int*>(ctx->cursor);
+  Q.nonisol = Q.crowded + nbricks;
+  Q.ntarget = Q.crowded + 2 * (size_t)nbricks;
+  Q.staged = ctx->pp_staged;
+  Q.dense_list = ctx->big_list + 2 * (size_t)nbricks;
+  Q.list_ip = ctx->perm;
+  Q.list_cell = ctx->tcell;
+  Q.dscal = ctx->dscal;
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(Q.crowded, 0, 3 * sizeof(unsigned int) * nbricks, ctx->stream));
+  const unsigned cblocks = (unsigned)((ctx->ncells + 255) / 256);
+  k_pp_masks<ZX><<<cblocks, 256, 0, ctx->stream>>>(ctx->xp, ctx->cap, Q);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_pp_cells<ZV><<<cblocks, 256, 0, ctx->stream>>>(Q, A, ctx->vp);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_pp_decide<<<(unsigned)((nbricks + 255) / 256), 256, 0, ctx->stream>>>(Q, nbricks);
+  CUBE_LAUNCH_CHECK(ctx);
+  k_pp_pairs<ZX, ZV><<<(unsigned)(4 * ctx->num_sms), 256, 0, ctx->stream>>>(ctx->xp, ctx->vp, ctx->vp, Q, A);
+  CUBE_LAUNCH_CHECK(ctx);
+  unsigned long long ndense = 0;
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&ndense, &ctx->dscal->pp_dense, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!ndense) return CUBE_OK;
+  // bricks whose region holds a crowded cell: one CTA per brick as before
   const size_t smem = sizeof(uint16_t) * ((size_t)NFC + 5 * (size_t)PB_CAP);
   auto kb = k_pp_brick<ZX, ZV>;
   CUBE_CUDA_TRY(ctx, cube_smem_limit(kb, smem));
-  kb<<<nbricks, PP_THREADS, smem, ctx->stream>>>(ctx->xp, ctx->vp, ctx->cell_start, ctx->nc, ctx->nt, ctx->nnt, A,
-                                                 spill, ctx->dscal);
+  kb<<<(unsigned)ndense, PP_THREADS, smem, ctx->stream>>>(ctx->xp, ctx->vp, ctx->cell_start, ctx->nc, ctx->nt,
+                                                          ctx->nnt, A, spill, ctx->dscal, Q.dense_list);
   CUBE_LAUNCH_CHECK(ctx);
   unsigned long long nspill = 0;
   CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&nspill, &ctx->dscal->n_big, 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -644,6 +987,10 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
 int cube_pp(cube_ctx* ctx, cube_scalars* io) {
   if (ctx->P.pp_range < 0 || ctx->P.pp_range > 4) {
     ctx->err = "pp_range must be in 0..4";
+    return CUBE_ERR_PARAM;
+  }
+  if (!ctx->pp_staged) {
+    ctx->err = "the context was created with PP off";
     return CUBE_ERR_PARAM;
   }
   if (ctx->izipx == 1 && ctx->izipv == 1) return launch_pp<1, 1>(ctx, io);

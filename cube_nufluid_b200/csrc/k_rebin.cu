@@ -48,7 +48,7 @@ struct RebinArgs {
   void* xp2; void* vp2; int32_t* pid2;
   int32_t* cnt2; int64_t* start2; float* vfield2;
   int32_t* tcell; uint32_t* tkey; int32_t* perm; uint32_t* pkey; int32_t* cursor;
-  int32_t* big_list; double* stats; double* slot_r2; double* slot_s2;
+  int32_t* big_list; double* stats; int32_t* slot_cell;  // new cell of each slot
   const int64_t* items; int64_t items_max;
   const double* dec; int half_nvbin;  // tan(code)/coef per code (cube_vdec_table)
   cube_codec codec; double coef, inv_pi;
@@ -208,29 +208,21 @@ __device__ __forceinline__ int64_t src_cell(const RebinArgs& A, uint32_t key, co
 }
 
 template <int ZX, int ZV>
-__device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t ip, const double v[3], const float vfn[3],
-                                     double& sr, double& ss) {
+__device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t ip, const double v[3], const float vfn[3]) {
   typedef typename CodeT<ZX>::T TX;
   typedef typename CodeT<ZV>::T TV;
   const TX* xp = reinterpret_cast<const TX*>(A.xp);
   TX* xp2 = reinterpret_cast<TX*>(A.xp2);
   TV* vp2 = reinterpret_cast<TV*>(A.vp2);
   const double xstep = cube_dmul(A.codec.x_resolution, (double)A.ncell);
-  double r2 = 0.0, s2 = 0.0;  // ((x0^2 + x1^2) + x2^2), the first add exact
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
     const int64_t mv = cube_nint(cube_ddiv(cube_dmul((double)A.dt_mid, v[d]), xstep));
     xp2[(size_t)d * A.cap + slot] = (TX)cube_wrap_code((int64_t)xp[(size_t)d * A.cap + ip] + (int32_t)mv, ZX);
     const int code = cube_wrap_code(cube_vencode_fast(&A.codec, cube_dsub(v[d], (double)vfn[d]), A.coef, A.inv_pi), ZV);
     vp2[(size_t)d * A.cap + slot] = (TV)code;
-    const double vr = __ldg(&A.dec[code + A.half_nvbin]);
-    const double vs = cube_dadd(vr, (double)vfn[d]);
-    r2 = cube_dadd(r2, cube_dmul(vr, vr));
-    s2 = cube_dadd(s2, cube_dmul(vs, vs));
   }
   if (A.use_pid) A.pid2[slot] = A.pid[ip];
-  sr = cube_dadd(sr, r2);
-  ss = cube_dadd(ss, s2);
 }
 
 __device__ __forceinline__ void cell_tile(const RebinArgs& A, int64_t c, int tt[3]) {
@@ -292,6 +284,7 @@ __global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   for (int r = 0; r < n; ++r) {
     const int64_t ip = A.perm[s + r];
     A.tkey[ip] = (uint32_t)(s + r);  // the particle's slot (tkey is free after the place pass)
+    A.slot_cell[s + r] = (int32_t)c;
     const int64_t sc = src_cell(A, A.pkey[s + r], tt);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -431,6 +424,7 @@ __device__ __forceinline__ void sort_sum_cell(const RebinArgs& A, int64_t c, int
     A.pkey[s + i] = key;  // sorted order back to the slots
     A.perm[s + i] = ip;
     A.tkey[ip] = (uint32_t)(s + i);  // the particle's slot
+    A.slot_cell[s + i] = (int32_t)c;
     const int64_t sc = src_cell(A, key, tt);
     for (int d = 0; d < 3; ++d)
       sv[(size_t)d * vstride + i] =
@@ -492,6 +486,7 @@ __device__ __forceinline__ void sort_sum_cell_warp(const RebinArgs& A, int64_t c
     A.pkey[s + i] = key;
     A.perm[s + i] = ip;
     A.tkey[ip] = (uint32_t)(s + i);
+    A.slot_cell[s + i] = (int32_t)c;
     const int64_t sc = src_cell(A, key, tt);
     for (int d = 0; d < 3; ++d)
       sv[d * WARP_MAX + i] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
@@ -604,8 +599,8 @@ __global__ void __launch_bounds__(1024) k_rebin_huge_order(RebinArgs A) {
 
 // F2: one thread per particle in its old storage order (coalesced reads of its
 // codes and PID): re-encode, move and copy it to its slot of the new layout (the
-// slots of neighbouring particles are close, so the writes gather in L2), and keep
-// its two statistics terms for the in-order cell sums
+// slots of neighbouring particles are close, so the writes gather in L2); the
+// statistics terms are formed from the new codes by the tree pass (k_stats_first)
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_rebin_emit(RebinArgs A, int64_t np) {
   __shared__ int64_t cs[RCELLS + 1];
@@ -631,15 +626,12 @@ __global__ void __launch_bounds__(256) k_rebin_emit(RebinArgs A, int64_t np) {
       v[d] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
       vfn[d] = A.vfield2[(size_t)d * A.ncells + c];
     }
-    double sr = 0.0, ss = 0.0;
-    emit<ZX, ZV>(A, slot, ip, v, vfn, sr, ss);
-    A.slot_r2[slot] = sr;
-    A.slot_s2[slot] = ss;
+    emit<ZX, ZV>(A, slot, ip, v, vfn);
   }
 }
 
 // F3: per cell, |vfield|^2 in FP32 (update_particle.f90:183); the per-particle
-// terms are summed from slot_r2 and slot_s2 by the fixed tree
+// terms are formed and summed by k_stats_first and the fixed tree
 __global__ void k_rebin_stats(RebinArgs A) {
   const int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (c >= A.ncells) return;
@@ -747,7 +739,7 @@ int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
   A.tcell = ctx->tcell; A.tkey = ctx->tkey; A.perm = ctx->perm; A.pkey = ctx->pkey; A.cursor = ctx->cursor;
   A.big_list = ctx->big_list; A.stats = ctx->cell_stats;
   A.items = ctx->rebin_items; A.items_max = cube_rebin_items_max(ctx->ncells, ctx->cap);
-  A.slot_r2 = ctx->slot_r2; A.slot_s2 = ctx->slot_s2;
+  A.slot_cell = reinterpret_cast<int32_t*>(ctx->slot_r2);
   A.half_nvbin = ctx->nvbin / 2;
   A.codec = ctx->codec; A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
   A.inv_pi = 1.0 / (double)ctx->codec.pi_f;

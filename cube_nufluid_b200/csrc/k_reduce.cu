@@ -37,6 +37,66 @@ __global__ void k_tree_block(const double* __restrict__ in, int64_t n, double* _
   }
 }
 
+// The first level of the tree over the per-particle velocity statistics of update_x
+// (update_particle.f90:174-226) with the terms formed here: for slot q of the new
+// storage order, vr = tan(code)/coef of its new residual code and vs = vr + vfield of
+// its new cell, r2 = (vr_x^2 + vr_y^2) + vr_z^2 and s2 likewise from vs; the two
+// block sums follow the tree of k_tree_block exactly, so the totals are the ones a
+// stored list of terms would give.
+template <int ZV>
+__global__ void k_stats_first(const void* __restrict__ vp_, int64_t cap, const int32_t* __restrict__ slot_cell,
+                              const float* __restrict__ vfield, int64_t ncells, const double* __restrict__ dec,
+                              int half_nvbin, int64_t n, double* __restrict__ out_r, double* __restrict__ out_s) {
+  typedef typename CodeT<ZV>::T TV;
+  const TV* vp = reinterpret_cast<const TV*>(vp_);
+  __shared__ double lr[1024], ls[1024];
+  const int i = threadIdx.x;  // 512 threads
+  const int64_t b = blockIdx.x;
+  double r[2] = {0.0, 0.0}, sv[2] = {0.0, 0.0};
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int64_t q = b * 1024 + i + 512 * h;
+    if (q < n) {
+      const int64_t c = slot_cell[q];
+      double r2 = 0.0, s2 = 0.0;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double vr = __ldg(&dec[(int)vp[(size_t)d * cap + q] + half_nvbin]);
+        const double vs = __dadd_rn(vr, (double)__ldg(&vfield[(size_t)d * ncells + c]));
+        r2 = __dadd_rn(r2, __dmul_rn(vr, vr));
+        s2 = __dadd_rn(s2, __dmul_rn(vs, vs));
+      }
+      r[h] = r2;
+      sv[h] = s2;
+    }
+  }
+  lr[i] = __dadd_rn(r[0], r[1]);  // s = 512
+  ls[i] = __dadd_rn(sv[0], sv[1]);
+  __syncthreads();
+  for (int s = 256; s >= 32; s >>= 1) {
+    if (i < s) {
+      lr[i] = __dadd_rn(lr[i], lr[i + s]);
+      ls[i] = __dadd_rn(ls[i], ls[i + s]);
+    }
+    __syncthreads();
+  }
+  if (i < 32) {
+    double v = lr[i], w = ls[i];
+    for (int s = 16; s >= 1; s >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, v, s);
+      const double p = __shfl_down_sync(0xffffffffu, w, s);
+      if (i < s) {
+        v = __dadd_rn(v, o);
+        w = __dadd_rn(w, p);
+      }
+    }
+    if (i == 0) {
+      out_r[b] = v;
+      out_s[b] = w;
+    }
+  }
+}
+
 constexpr int SCAN_PER_THREAD = 8;
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_BLOCK = SCAN_PER_THREAD * SCAN_THREADS;
@@ -129,6 +189,26 @@ __global__ void k_scan_apply(const int32_t* __restrict__ in, int64_t n, const in
 }
 
 }  // namespace
+
+// the velocity statistics sums of update_x in the new layout (see k_stats_first)
+int cube_stats_sums(cube_ctx* ctx, const int32_t* slot_cell, const double* dec, double* sum_r, double* sum_s) {
+  const int64_t n = ctx->np;
+  if (n == 0) { *sum_r = *sum_s = 0.0; return CUBE_OK; }
+  const int64_t nb = (n + 1023) / 1024;
+  // block sums in the per-slot arrays, free after the re-bin
+  double* br = ctx->slot_s2;
+  double* bs = ctx->slot_s2 + nb;
+  if (ctx->izipv == 1)
+    k_stats_first<1><<<(unsigned)nb, 512, 0, ctx->stream>>>(ctx->vp, ctx->cap, slot_cell, ctx->vfield, ctx->ncells,
+                                                            dec, ctx->nvbin / 2, n, br, bs);
+  else
+    k_stats_first<2><<<(unsigned)nb, 512, 0, ctx->stream>>>(ctx->vp, ctx->cap, slot_cell, ctx->vfield, ctx->ncells,
+                                                            dec, ctx->nvbin / 2, n, br, bs);
+  CUBE_LAUNCH_CHECK(ctx);
+  int rc = cube_tree_sum_dev(ctx, br, nb, sum_r);
+  if (rc) return rc;
+  return cube_tree_sum_dev(ctx, bs, nb, sum_s);
+}
 
 int cube_tree_sum_dev(cube_ctx* ctx, const double* in, int64_t n, double* out_host) {
   double* a = ctx->red_tmp + 4;  // first slots hold the deposit mass totals

@@ -306,7 +306,8 @@ class Cube:
         nf, nc = self.nf, self.nc
         sizes = {0: nf ** 3, 1: nc ** 3, 2: 3 * nf ** 3, 3: 3 * nc ** 3,
                  4: 3 * (nf // 2 + 1) ** 3, 5: 3 * (nc // 2 + 1) ** 3}
-        out = np.zeros(sizes[which], np.float32)
+        fp64 = which <= 3 and bool(self.p.poisson_fp64)  # the FP64 Poisson mode's meshes
+        out = np.zeros(sizes[which], np.float64 if fp64 else np.float32)
         got = self.L.cube_debug_fetch(self.h, which, _ptr(out), out.size)
         if got < 0:
             raise CubeError(3, "debug fetch failed")

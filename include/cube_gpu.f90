@@ -19,7 +19,7 @@ module cube_gpu
     real(c_double) :: vrel_boost
     real(c_float) :: box, h0, omega_m, omega_l, wde, ra_max, dt_max
     real(c_float) :: z_i_nu, f_neu, m_nu_ev, deg_nu
-    integer(c_int32_t) :: nu_nc(3), reserved(8)
+    integer(c_int32_t) :: nu_nc(3), stockham_only, poisson_fp64, reserved(6)
   end type
 
   type, bind(c) :: cube_scalars_t

@@ -87,7 +87,13 @@ typedef struct cube_params {
   float m_nu_ev;         /* neutrino mass per species, eV */
   float deg_nu;          /* degeneracy */
   int32_t nu_nc[3];      /* fluid mesh sizes per Gauss-Laguerre fluid (0 = nf/2,nf/4,nf/8) */
-  int32_t reserved[8];
+  int32_t stockham_only; /* 1: every mesh FFT takes the shared-memory Stockham passes (testing) */
+  int32_t poisson_fp64;  /* 1: FP64 Poisson path (meshes, FFT, Green, interpolation in FP64);
+                            no counterpart in the reference, whose meshes are FP32: the FP64
+                            run of the same step that the FP32 results are measured against.
+                            Needs neutrino = 0; power spectrum, halo finder and device ICs
+                            need the FP32 meshes and return CUBE_ERR_PARAM. */
+  int32_t reserved[6];
 } cube_params;
 
 /* Scalar globals the step reads and writes (variables.f90:28-48 and sim_header,
@@ -306,6 +312,7 @@ void cube_destroy(cube_ctx* ctx);
  *   which=3 coarse force         [3][nc^3]
  *   which=4 fine Green multiplier octant [3][(nf/2+1)^3]
  *   which=5 coarse Green multiplier      [3][nc][nc][nc/2+1]
+ * In the FP64 Poisson mode (params.poisson_fp64) which=0..3 write doubles.
  * Returns the element count written, or -1. */
 int64_t cube_debug_fetch(cube_ctx* ctx, int32_t which, void* host, int64_t capacity);
 
@@ -333,9 +340,11 @@ int32_t cube_debug_time_poisson(cube_ctx* ctx, int32_t reps, float* ms);
 /* ---- allocation-free coarse density ------------------------------------------
  * No counterpart in the reference.  For hosts that may not allocate device memory
  * during a run (their HBM is owned by another allocator, or a fixed budget per box
- * was handed out at start-up): computes the coarse CIC density of pm.f90:192-278,
- * bit-identical to the coarse density of cube_particle_mesh, from caller-owned
- * device buffers, and allocates nothing.
+ * was handed out at start-up): computes the particle (CDM) coarse CIC density of
+ * pm.f90:192-278 from caller-owned device buffers and allocates nothing.  It is
+ * bit-identical to the coarse density of cube_particle_mesh when neutrinos are
+ * off (with params.neutrino = 1 the context's coarse density also holds the
+ * neutrino mass, which this call does not add).
  *   xp         device, int8|int16 [3][np_capacity] position codes (structure of arrays)
  *   cell_start device, int64 [nc^3+1] first particle of each cell, tile-major order
  *   rho        device, float [nc^3] output (x fastest), overwritten
@@ -344,7 +353,10 @@ int32_t cube_debug_time_poisson(cube_ctx* ctx, int32_t reps, float* ms);
  * by every GPU that loads the library until exit); larger nc returns
  * CUBE_ERR_CAPACITY.  Every call shares that array and clears it first, so calls
  * that overlap on the GPU race.  The first call on a device looks up the array's
- * address and should come before any stream capture. */
+ * address and should come before any stream capture.  Errors come back as the
+ * status only (no context, so cube_last_error has no text for them); a CUDA
+ * error already pending when the call starts is returned as CUBE_ERR_CUDA and
+ * nothing is launched. */
 int32_t cube_coarse_density_noalloc(int32_t nc, int32_t nnt, int32_t izipx, int64_t np_capacity, const void* xp,
                                     const int64_t* cell_start, float mass_p_cdm, float* rho, void* stream);
 

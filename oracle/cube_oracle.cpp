@@ -55,6 +55,12 @@ struct Orc {
   int izipx, izipv;
   cube_codec codec;
   std::vector<float> tan_table;  // tanf of each velocity code, index code+nvbin/2
+  int libm_codec = 0;            // 1: velocity codec on the C library's atan (orc_enc)
+  // timing sample (CPU-baseline leg): when set, the step routines run the tile
+  // loops of the marked tiles only, leave the particle state as it was, skip the
+  // global coarse Poisson solve (timed apart by orc_coarse_poisson) and the
+  // whole-mesh diagnostic copies
+  std::vector<char> tmask;
   int nvbin;
   // compact physical state (checkpoint layout)
   int64_t np;
@@ -68,6 +74,7 @@ struct Orc {
   std::vector<float> fk_table, ck_table;
   // diagnostics of the last particle_mesh
   std::vector<float> rho_f_global;    // [nf^3] central regions of the tile meshes
+  std::vector<uint64_t> rho_q_global; // [nf^3] fixed-point mode: node sums without the mass (scale 2^32)
   std::vector<float> force_f_global;  // [3][nf^3]
   std::vector<float> r3;              // [nc^3]
   std::vector<float> force_c;         // [3][nc^3]
@@ -77,12 +84,28 @@ struct Orc {
   std::string err;
 };
 
+inline bool tile_on(const Orc& o, int tx, int ty, int tz) {
+  return o.tmask.empty() || o.tmask[((size_t)tz * o.nnt + ty) * o.nnt + tx];
+}
+
 inline int64_t cell_id(const Orc& o, int tx, int ty, int tz, int lx, int ly, int lz) {
   return ((((int64_t)tz * o.nnt + ty) * o.nnt + tx) * o.nt + lz) * (int64_t)o.nt * o.nt +
          (int64_t)ly * o.nt + lx;
 }
 
 inline float tanf_code(const Orc& o, int code) { return o.tan_table[code + o.nvbin / 2]; }
+
+/* Velocity encode nint(real(nvbin-1)*atan(sqrt(pi/2)/(sigma*vrel_boost)*vreal)/pi)
+ * (pm.f90:154, update_particle.f90:119).  By default the library's own codec
+ * (cube_codec.h: the project arctangent).  With libm_codec the oracle evaluates it
+ * by itself with the C library's atan (what gfortran's atan(real(8)) calls) and
+ * Fortran NINT (halfway cases away from zero), so the library's codec is checked
+ * against an evaluation that shares none of its code. */
+inline int32_t orc_enc(const Orc& o, double v, double coef) {
+  if (!o.libm_codec) return cube_vencode(&o.codec, v, coef);
+  const double q = ((double)o.codec.nvbin_m1_f * atan(coef * v)) / (double)o.codec.pi_f;
+  return (int32_t)llround(q);
+}
 
 /* ------------------------------------------------------------------------- */
 /* Extended tile view: the reference's rhoc/vfield/xp after buffer_grid +    */
@@ -178,6 +201,7 @@ int update_xp(Orc& o, cube_scalars* s) {
   for (int tz = 0; tz < o.nnt; ++tz)
     for (int ty = 0; ty < o.nnt; ++ty)
       for (int tx = 0; tx < o.nnt; ++tx) {
+        if (!tile_on(o, tx, ty, tz)) continue;
         build_ext(o, cs, tx, ty, tz, e);
         const int nte = o.nte, lo = 1 - ncb;
         std::vector<int32_t> rhoce((size_t)n2 * n2 * n2, 0), rholocal((size_t)n2 * n2 * n2, 0);
@@ -254,7 +278,7 @@ int update_xp(Orc& o, cube_scalars* s) {
                     const int64_t nv_ = cube_nint(step);
                     xn[3 * (idx - 1) + d] = cube_wrap_code((int64_t)o.xp[3 * ip + d] + (int32_t)nv_, o.izipx);
                     const double vr = cube_dsub(h.v[d], (double)vfn[3 * q + d]);
-                    vn[3 * (idx - 1) + d] = cube_wrap_code(cube_vencode(&o.codec, vr, coef), o.izipv);
+                    vn[3 * (idx - 1) + d] = cube_wrap_code(orc_enc(o, vr, coef), o.izipv);
                   }
                   pn[idx - 1] = o.pid.empty() ? 0 : o.pid[ip];
                 }
@@ -280,6 +304,7 @@ int update_xp(Orc& o, cube_scalars* s) {
               np_prev += rhoce[q];
             }
       }
+  if (!o.tmask.empty()) return rc;  // timing sample: the state stays as it was
   o.xp.swap(nx); o.vp.swap(nv);
   if (!o.pid.empty()) o.pid.swap(npid);
   o.rhoc.swap(nrho); o.vfield.swap(nvf);
@@ -449,8 +474,11 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
   float f2_max_fine = 0.f;
   double testrhof = 0, testrhoc = 0;
   const std::vector<int64_t> cs = compact_cell_start(o);
-  o.rho_f_global.assign((size_t)nf * nf * nf, 0.f);
-  o.force_f_global.assign((size_t)3 * nf * nf * nf, 0.f);
+  const bool sample = !o.tmask.empty();
+  if (!sample) o.rho_f_global.assign((size_t)nf * nf * nf, 0.f);
+  if (deposit_mode == 1) o.rho_q_global.assign((size_t)nf * nf * nf, 0);
+  const double unit_f = (double)mass * (1.0 / 4294967296.0);  // exact
+  if (!sample) o.force_f_global.assign((size_t)3 * nf * nf * nf, 0.f);
   const double coef_old = cube_vcoef(&o.codec, s->sigma_vi);
   const double coef_new = cube_vcoef(&o.codec, s->sigma_vi_new);
   std::vector<float> rho_f((size_t)nfe * nfe * nfe);
@@ -466,6 +494,7 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
   for (int tz = 0; tz < o.nnt; ++tz)
     for (int ty = 0; ty < o.nnt; ++ty)
       for (int tx = 0; tx < o.nnt; ++tx) {
+        if (!tile_on(o, tx, ty, tz)) continue;
         build_ext(o, cs, tx, ty, tz, e);
         auto eq = [&](int i, int j, int k) { return ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo); };
         std::fill(rho_f.begin(), rho_f.end(), 0.f);
@@ -514,16 +543,18 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                     const float wx = cx[c8][0] ? dx2[0] : dx1[0];
                     const float wy = cx[c8][1] ? dx2[1] : dx1[1];
                     const float wz = cx[c8][2] ? dx2[2] : dx1[2];
-                    const float w = cube_fmul(cube_fmul(cube_fmul(wx, wy), wz), mass);
                     const size_t q = fat(cx[c8][0] ? i2[0] : i1[0], cx[c8][1] ? i2[1] : i1[1], cx[c8][2] ? i2[2] : i1[2]);
-                    if (deposit_mode == 1) rho_q[q] += (int64_t)llrint((double)w * 4294967296.0);
-                    else rho_f[q] = cube_fadd(rho_f[q], w);
+                    // fixed point: the weight without the mass, q = RN(w 2^32); the
+                    // mass is applied once per node
+                    if (deposit_mode == 1)
+                      rho_q[q] += (int64_t)llrint((double)cube_fmul(cube_fmul(wx, wy), wz) * 4294967296.0);
+                    else rho_f[q] = cube_fadd(rho_f[q], cube_fmul(cube_fmul(cube_fmul(wx, wy), wz), mass));
                   }
                 }
               }
         if (deposit_mode == 1)
           for (size_t q = 0; q < rho_f.size(); ++q) {
-            rho_f[q] = (float)((double)rho_q[q] * (1.0 / 4294967296.0));
+            rho_f[q] = (float)((double)rho_q[q] * unit_f);
             if (o.nu_on) rho_f[q] = cube_fadd(rho_f[q], nu_t[q]);
           }
         for (int k = nfb + 1; k <= nft + nfb; ++k)
@@ -531,7 +562,8 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
             for (int i = nfb + 1; i <= nft + nfb; ++i) {
               testrhof += (double)rho_f[fat(i, j, k)];
               const size_t g = ((size_t)(tz * nft + k - nfb - 1) * nf + (ty * nft + j - nfb - 1)) * nf + (tx * nft + i - nfb - 1);
-              o.rho_f_global[g] = rho_f[fat(i, j, k)];
+              if (!sample) o.rho_f_global[g] = rho_f[fat(i, j, k)];
+              if (deposit_mode == 1) o.rho_q_global[g] = (uint64_t)rho_q[fat(i, j, k)];
             }
         // fine force (pm.f90:112-126)
         const int nfo = nft + 2;  // force_f(3, nfb:nfe-nfb+1)
@@ -570,7 +602,7 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
               const float* f = &force_f[(((size_t)k * nfo + j) * nfo + i) * 3];
               const float f2 = cube_fadd(cube_fadd(cube_fmul(f[0], f[0]), cube_fmul(f[1], f[1])), cube_fmul(f[2], f[2]));
               f2_max_fine = std::max(f2_max_fine, f2);
-              if (i >= 1 && i <= nft && j >= 1 && j <= nft && k >= 1 && k <= nft) {
+              if (!sample && i >= 1 && i <= nft && j >= 1 && j <= nft && k >= 1 && k <= nft) {
                 const size_t g = ((size_t)(tz * nft + k - 1) * nf + (ty * nft + j - 1)) * nf + (tx * nft + i - 1);
                 for (int d = 0; d < 3; ++d) o.force_f_global[(size_t)d * nf * nf * nf + g] = f[d];
               }
@@ -609,7 +641,7 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                     t = cube_fmul(t, cx[c8][2] ? dx2[2] : dx1[2]);
                     v = cube_dadd(v, (double)t);
                   }
-                  o.vp[3 * ip + d] = cube_wrap_code(cube_vencode(&o.codec, v, coef_new), o.izipv);
+                  o.vp[3 * ip + d] = cube_wrap_code(orc_enc(o, v, coef_new), o.izipv);
                 }
               }
             }
@@ -638,9 +670,12 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
   s->sigma_vi = s->sigma_vi_new;
   // coarse_cic_mass (pm.f90:192-278)
   o.r3.assign((size_t)nc * nc * nc, 0.f);
+  std::vector<uint64_t> r3nu;  // fixed-point mode: coarse neutrino sums (mass units, 2^32)
+  if (deposit_mode == 1) r3nu.assign((size_t)nc * nc * nc, 0);
   for (int tz = 0; tz < o.nnt; ++tz)
     for (int ty = 0; ty < o.nnt; ++ty)
       for (int tx = 0; tx < o.nnt; ++tx) {
+        if (!tile_on(o, tx, ty, tz)) continue;
         build_ext(o, cs, tx, ty, tz, e);
         auto eq = [&](int i, int j, int k) { return ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo); };
         const int n3 = nt + 4;  // r3t(-1:nt+2)
@@ -686,7 +721,8 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                       }
           }
         }
-        for (int il = 0; il < 3; ++il)
+        // reference order (mode 0) only: the fixed-point mode restricts the fine sums below
+        for (int il = 0; il < 3 && deposit_mode == 0; ++il)
 #pragma omp parallel for schedule(static, 2)
           for (int k = 0 + il; k <= nt + 1; k += 3)
             for (int j = 0; j <= nt + 1; ++j)
@@ -710,24 +746,50 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                     const float wz = cx[c8][2] ? dx2[2] : dx1[2];
                     const float w = cube_fmul(cube_fmul(cube_fmul(wx, wy), wz), mass);
                     const size_t q = tat(i1[0] + cx[c8][0], i1[1] + cx[c8][1], i1[2] + cx[c8][2]);
-                    if (deposit_mode == 1) r3q[q] += (int64_t)llrint((double)w * 4294967296.0);
-                    else r3t[q] = cube_fadd(r3t[q], w);
+                    r3t[q] = cube_fadd(r3t[q], w);
                   }
                 }
               }
-        if (deposit_mode == 1)
-          for (size_t q = 0; q < r3t.size(); ++q) r3t[q] = (float)((double)r3q[q] * (1.0 / 4294967296.0));
         for (int k = 1; k <= nt; ++k)
           for (int j = 1; j <= nt; ++j)
-            for (int i = 1; i <= nt; ++i)
-              o.r3[((size_t)(tz * nt + k - 1) * nc + (ty * nt + j - 1)) * nc + (tx * nt + i - 1)] = r3t[tat(i, j, k)];
+            for (int i = 1; i <= nt; ++i) {
+              const size_t g = ((size_t)(tz * nt + k - 1) * nc + (ty * nt + j - 1)) * nc + (tx * nt + i - 1);
+              if (deposit_mode == 1) r3nu[g] = (uint64_t)r3q[tat(i, j, k)];  // neutrinos only
+              else o.r3[g] = r3t[tat(i, j, k)];
+            }
       }
+  if (deposit_mode == 1) {
+    // the coarse CIC of the particles is the fine node sums restricted with the
+    // weights (4 - |d|)/4, |d| <= 3, per dimension (coarse node J is centred on fine
+    // node 4J+2), exact in 64-bit integers at scale 2^38; the neutrinos' coarse
+    // sums (mass units, scale 2^32) are added when the node is written
+    const double unit_c = (double)mass * (1.0 / (64.0 * 4294967296.0));  // exact
+#pragma omp parallel for schedule(static)
+    for (int J2 = 0; J2 < nc; ++J2)
+      for (int J1 = 0; J1 < nc; ++J1)
+        for (int J0 = 0; J0 < nc; ++J0) {
+          uint64_t acc = 0;
+          for (int d2 = -3; d2 <= 3; ++d2) {
+            const int n2 = ((4 * J2 + 2 + d2) % nf + nf) % nf;
+            for (int d1 = -3; d1 <= 3; ++d1) {
+              const int n1 = ((4 * J1 + 2 + d1) % nf + nf) % nf;
+              for (int d0 = -3; d0 <= 3; ++d0) {
+                const int n0 = ((4 * J0 + 2 + d0) % nf + nf) % nf;
+                const uint64_t t = (uint64_t)((4 - std::abs(d0)) * (4 - std::abs(d1)) * (4 - std::abs(d2)));
+                acc += t * o.rho_q_global[((size_t)n2 * nf + n1) * nf + n0];
+              }
+            }
+          }
+          const size_t g = ((size_t)J2 * nc + J1) * nc + J0;
+          o.r3[g] = (float)((double)acc * unit_c + (double)r3nu[g] * (1.0 / 4294967296.0));
+        }
+  }
   for (size_t q = 0; q < o.r3.size(); ++q) testrhoc += (double)o.r3[q];
   // coarse force (pm.f90:288-300), pencil_fft on one image = 3-D r2c/c2r
   o.force_c.assign((size_t)3 * nc * nc * nc, 0.f);
   if (ext && ext->coarse_force) {
     o.force_c = *ext->coarse_force;
-  } else {
+  } else if (!sample) {
     std::vector<double> r((size_t)nc * nc * nc);
     for (size_t q = 0; q < r.size(); ++q) r[q] = (double)o.r3[q];
     std::vector<cd> sp, pr;
@@ -755,6 +817,7 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
   for (int tz = 0; tz < o.nnt; ++tz)
     for (int ty = 0; ty < o.nnt; ++ty)
       for (int tx = 0; tx < o.nnt; ++tx)
+        if (tile_on(o, tx, ty, tz))
 #pragma omp parallel for schedule(static, 2) reduction(max : vmx0, vmx1, vmx2)
         for (int k = 1; k <= nt; ++k)
           for (int j = 1; j <= nt; ++j)
@@ -793,7 +856,7 @@ int particle_mesh(Orc& o, cube_scalars* s, int deposit_mode, const KickIn* ext) 
                   if (d == 0) vmx0 = std::max(vmx0, am);
                   else if (d == 1) vmx1 = std::max(vmx1, am);
                   else vmx2 = std::max(vmx2, am);
-                  o.vp[3 * ip + d] = cube_wrap_code(cube_vencode(&o.codec, v, coef), o.izipv);
+                  o.vp[3 * ip + d] = cube_wrap_code(orc_enc(o, v, coef), o.izipv);
                 }
               }
             }
@@ -860,6 +923,7 @@ int ext_pp_force(Orc& o, cube_scalars* s) {
   for (int tz = 0; tz < o.nnt; ++tz)
     for (int ty = 0; ty < o.nnt; ++ty)
       for (int tx = 0; tx < o.nnt; ++tx) {
+        if (!tile_on(o, tx, ty, tz)) continue;
         build_ext(o, cs, tx, ty, tz, e);
         auto eq = [&](int i, int j, int k) { return ((size_t)(k - lo) * nte + (j - lo)) * nte + (i - lo); };
         auto hq = [&](int i, int j, int k) { return ((size_t)(k + ncell - 1) * nfl + (j + ncell - 1)) * nfl + (i + ncell - 1); };
@@ -937,7 +1001,7 @@ int ext_pp_force(Orc& o, cube_scalars* s) {
                 }
                 // vp(:,ip1) is written at the physical slot; buffer copies are refreshed by buffer_v
                 for (int d = 0; d < 3; ++d)
-                  o.vp[3 * ip1 + d] = cube_wrap_code(cube_vencode(&o.codec, v[d], coef), o.izipv);
+                  o.vp[3 * ip1 + d] = cube_wrap_code(orc_enc(o, v[d], coef), o.izipv);
                 const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
                 ftemp = std::max(ftemp, (double)(float)f2);
                 s1 = ll[s1];
@@ -950,7 +1014,7 @@ int ext_pp_force(Orc& o, cube_scalars* s) {
   s->dt_pp = cube_fdiv(cube_fmul(1.0f, sqrtf(1.0f)), cube_fmul(cube_fmul(sqrtf(s->f2_max_pp), s->a_mid), GG));
   s->itest1 = itest1;
   s->npairs = npairs;
-  if (itest1 != o.np) { o.err = "PP did not touch every particle once"; return CUBE_ERR_STATE; }
+  if (o.tmask.empty() && itest1 != o.np) { o.err = "PP did not touch every particle once"; return CUBE_ERR_STATE; }
   return CUBE_OK;
 }
 
@@ -1313,7 +1377,9 @@ void setup_sizes(Orc& o, const cube_params* p) {
   o.codec.vrel_boost = p->vrel_boost;
   o.codec.x_resolution = (p->izipx == 1) ? 1.0 / 256.0 : 1.0 / 65536.0;
   o.tan_table.resize(o.nvbin);
-  for (int c = -o.nvbin / 2; c < o.nvbin / 2; ++c) o.tan_table[c + o.nvbin / 2] = tanf(cube_varg(&o.codec, c));
+  // the FP32 argument (pi*real(vp))/real(nvbin-1) and tan(real) of pm.f90:145
+  for (int c = -o.nvbin / 2; c < o.nvbin / 2; ++c)
+    o.tan_table[c + o.nvbin / 2] = tanf((o.codec.pi_f * (float)c) / o.codec.nvbin_m1_f);
 }
 
 }  // namespace
@@ -1474,6 +1540,38 @@ void orc_dt_constraints(void* h, cube_scalars* s) { dt_constraints(*(Orc*)h, s);
 
 /* codec helpers for the tests */
 float orc_tanf_code(void* h, int code) { return tanf_code(*(Orc*)h, code); }
+/* Timing sample: mask[nnt^3] (tile-major, x fastest) marks the tiles the step
+ * routines run; NULL runs every tile again.  See Orc::tmask. */
+void orc_set_tile_mask(void* h, const char* mask) {
+  Orc& o = *(Orc*)h;
+  if (mask) o.tmask.assign(mask, mask + (size_t)o.nnt * o.nnt * o.nnt);
+  else o.tmask.clear();
+}
+
+/* The global coarse Poisson solve of particle_mesh (pm.f90:288-300: forward FFT of
+ * r3, three Green multiplies and inverse FFTs), on whatever r3 holds. */
+void orc_coarse_poisson(void* h) {
+  Orc& o = *(Orc*)h;
+  const int nc = o.nc;
+  std::vector<double> r((size_t)nc * nc * nc);
+  for (size_t q = 0; q < r.size() && q < o.r3.size(); ++q) r[q] = (double)o.r3[q];
+  std::vector<cd> sp, pr;
+  orc::rfft3_forward(r.data(), sp, nc);
+  pr.resize(sp.size());
+  o.force_c.assign((size_t)3 * nc * nc * nc, 0.f);
+  for (int d = 0; d < 3; ++d) {
+    for (size_t q = 0; q < sp.size(); ++q) {
+      const double kv = o.kern_c[(size_t)d * sp.size() + q];
+      pr[q] = cd(-sp[q].imag() * kv, sp[q].real() * kv);
+    }
+    orc::rfft3_backward(pr, r.data(), nc);
+    const double norm = (double)nc * nc * nc;
+    for (size_t q = 0; q < r.size(); ++q) o.force_c[(size_t)d * r.size() + q] = (float)(r[q] / norm);
+  }
+}
+
+/* 1: the step's velocity encodes use the C library's atan (orc_enc) */
+void orc_set_libm_codec(void* h, int on) { ((Orc*)h)->libm_codec = on ? 1 : 0; }
 double orc_atan(double x) { return cube_atan(x); }
 int orc_vencode(void* h, double v, float sigma) {
   Orc& o = *(Orc*)h;

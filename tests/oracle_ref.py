@@ -48,6 +48,12 @@ def lib():
         L.orc_fetch.argtypes = [vp, C.c_int, vp, C.c_int64]
         L.orc_dt_constraints.argtypes = [vp, S]
         L.orc_halofind.argtypes = [vp, S, C.POINTER(CubeHaloArgs), C.POINTER(CubeHaloResult)]
+        L.orc_set_tile_mask.argtypes = [vp, vp]
+        L.orc_set_tile_mask.restype = None
+        L.orc_coarse_poisson.argtypes = [vp]
+        L.orc_coarse_poisson.restype = None
+        L.orc_set_libm_codec.argtypes = [vp, C.c_int]
+        L.orc_set_libm_codec.restype = None
         L.orc_tanf_code.restype = C.c_float
         L.orc_tanf_code.argtypes = [vp, C.c_int]
         L.orc_atan.restype = C.c_double
@@ -96,6 +102,24 @@ class Oracle:
                       np.ascontiguousarray(rhoc, dtype=np.int32), np.ascontiguousarray(vfield, dtype=np.float32))
         x, v, p, r, f = self._keep
         self._check(lib().orc_load_state(self.h, x.shape[0], _ptr(x), _ptr(v), _ptr(p), _ptr(r), _ptr(f)))
+
+    def set_libm_codec(self, on: bool = True):
+        """Velocity encodes on the C library's atan, evaluated by the oracle itself
+        (none of the library's codec code), instead of the shared project arctangent."""
+        lib().orc_set_libm_codec(self.h, int(bool(on)))
+
+    def set_tile_mask(self, mask):
+        """Timing sample: the step routines run only the tiles marked in mask
+        (nnt^3 entries, tile-major) and leave the state as it was; None clears it."""
+        if mask is None:
+            lib().orc_set_tile_mask(self.h, None)
+        else:
+            self._mask = np.ascontiguousarray(mask, dtype=np.int8)
+            lib().orc_set_tile_mask(self.h, _ptr(self._mask))
+
+    def coarse_poisson(self):
+        """The global coarse Poisson solve of particle_mesh on the current r3."""
+        lib().orc_coarse_poisson(self.h)
 
     def store(self):
         n = C.c_int64(0)

@@ -27,12 +27,17 @@ def test_reference_arm_unavailable_for_device_only_configs(config):
 
 
 def test_reference_arm_line_on_the_single_box_workload():
-    line = run_bench("--impl", "reference", "--steps", "1", "--warmup", "0")
+    # configuration 1 (64^3 particles) keeps the CPU suite short; configuration 2 takes
+    # the same path with its own state
+    line = run_bench("--config", "c1", "--impl", "reference", "--steps", "2", "--warmup", "1")
     assert line["impl"] == "reference"
     assert line["metric"] == "PM step particle-updates/s" and line["unit"] == "particle-updates/s"
     assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["steps"] == 2 and line["warmup"] == 1
     base = line["cpu_baseline"]
     assert base["kind"] == "port" and base["cores"] >= 1 and base["value"] == line["value"]
+    assert base["tiles_timed"] == 2 and "tile" in base["sample"]
     assert line["e2e"] == {"value": line["value"], "unit": "particle-updates/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
-    assert line["config"]["particles"] == 512 ** 3
+    assert line["config"]["particles"] == 64 ** 3
+    assert "int1 x / int2 v" in line["config"]["workload"]

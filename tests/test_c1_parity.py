@@ -1,0 +1,91 @@
+"""Configuration 1 of the workload end to end on both arms, and the velocity codec
+against an oracle that shares none of the library's codec code.
+
+C1 (64^3 particles, nf = 128, nc = 32, int1 positions / int2 velocities, PP off)
+runs 100 steps from z = 49 to z = 0 on the GPU and on the CPU oracle from the same
+seeded Zel'dovich state, in lockstep (same time steps).  The oracle's forces come
+from FP64 FFTs, the library's from FP32 FFTs; the deposit is the same 64-bit fixed
+point on both.  The FP32-vs-FP64 force difference (about 1e-7 relative per step)
+moves a velocity code now and then, and over 100 steps those moves grow where the
+flow is nonlinear, i.e. at high k.  Stated tolerances after the full run:
+  * P(k) in 32 log bins (fundamental to Nyquist): relative difference <= 1e-4 in
+    every bin up to k_Nyquist / 2, <= 3e-4 in the bins above it;
+  * P(k) in the reference's log bins (4 per octave to sqrt(3) k_Nyquist): <= 5e-4;
+  * final positions by PID: 99% within 1/64 of a fine cell (one int1 position code
+    is 1/64 fine cell), all within 2 fine cells, RMS below 0.05 fine cells.
+(Measured on one B200: 99.4% within one code, max 0.23 fine cells, RMS 3e-3; P(k)
+1.0e-4 at most below k_Nyquist / 2, 1.4e-4 in the Nyquist bin, 2.3e-4 in the
+reference bins.)
+"""
+import numpy as np
+import pytest
+
+import c1_run as R
+
+pytestmark = pytest.mark.gpu
+
+
+def test_c1_update_x_and_kick_codes_match_a_libm_codec_oracle(tables):
+    """One C1 drift and one kick on identical forces: every velocity code the library
+    writes equals the code of an oracle encoding with the C library's atan."""
+    from cube_nufluid_b200 import Cube
+    from oracle_ref import Oracle
+    fk, ck = tables
+    st, p = R.c1_state(seed=77)
+    g = Cube(p, st.np, fk, ck)
+    g.load_state(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    o = Oracle(p, fk, ck)
+    o.load(st.xp, st.vp, st.pid, st.rhoc, st.vfield)
+    o.set_libm_codec(True)
+    s = R.scalars_from_ic(st)
+    R._timestep(p, s, 0.0)
+    sg, so = s.copy(), s.copy()
+    g.update_x(sg)
+    o.update_x(so)
+    a, b = g.store_state(), o.store()
+    flips = int(np.count_nonzero(a[1] != b[1]))
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[2], b[2])
+    assert flips == 0, f"{flips} velocity codes differ from the libm codec after update_x"
+    rng = np.random.default_rng(3)
+    nf, nc = 128, 32
+    fine = rng.normal(0, 30.0, 3 * nf ** 3).astype(np.float32)
+    coarse = rng.normal(0, 5.0, 3 * nc ** 3).astype(np.float32)
+    sg.sigma_vi_new = np.float32(sg.sigma_vi * 1.02)
+    so.sigma_vi_new = sg.sigma_vi_new
+    o.particle_mesh_with_force(so, fine, coarse, 1)
+    g.kick_with_force(sg, fine, coarse)
+    a, b = g.store_state(), o.store()
+    flips = int(np.count_nonzero(a[1] != b[1]))
+    assert flips == 0, f"{flips} velocity codes differ from the libm codec after the kick"
+    g.close()
+
+
+def test_c1_full_run_tracks_the_oracle():
+    st, p = R.c1_state()
+    gs, os_, sg, so, n = R.run_lockstep(st, p, steps=R.C1["steps"])
+    assert n >= R.C1["steps"]
+    assert abs(sg.a - 1.0) < 1e-5
+    nc, nnt = R.C1["nc"], R.C1["nnt"]
+    pg, idg = R.positions_by_pid(gs, nc, nnt, 1)
+    po, ido = R.positions_by_pid(os_, nc, nnt, 1)
+    assert np.array_equal(idg, ido)
+    d = np.abs(R.periodic_diff(pg, po, float(nc))) * 4.0  # fine cells
+    dmax = d.max(axis=1)
+    frac_close = float(np.mean(dmax <= 1.0 / 64.0 + 1e-12))
+    rms = float(np.sqrt(np.mean(d ** 2)))
+    xg, pg32, m = R.power(pg, nc, R.C1["box"], 4 * nc)
+    xo, po32, _ = R.power(po, nc, R.C1["box"], 4 * nc)
+    ok = m > 0
+    rel32 = np.abs(pg32[ok] / po32[ok] - 1.0)
+    ng = 4 * nc
+    low = (np.geomspace(1.0, ng / 2, 33)[1:] <= ng / 4)[ok]  # bins wholly below k_Nyquist / 2
+    relref = np.abs(xg[:, 2] / xo[:, 2] - 1.0)
+    print(f"C1 lockstep: {n} steps; positions: {frac_close:.5f} within 1/64 fine cell, max {dmax.max():.4f}, "
+          f"RMS {rms:.2e} fine cells; P(k) 32 log bins max rel {rel32.max():.2e}, reference bins max rel "
+          f"{np.nanmax(relref):.2e}; velocity codes differing {int(np.count_nonzero(gs[1] != os_[1]))}")
+    assert frac_close >= 0.99
+    assert dmax.max() <= 2.0
+    assert rms < 0.05
+    assert rel32[low].max() <= 1e-4
+    assert rel32.max() <= 3e-4
+    assert np.nanmax(relref) <= 5e-4

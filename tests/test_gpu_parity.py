@@ -218,6 +218,26 @@ def test_pp_bit_exact(tables, izip):
     assert_same_state(o, g)
 
 
+@pytest.mark.parametrize("z_i,izip", [(30.0, 2), (15.0, 2), (15.0, 1)])
+def test_pp_bit_exact_on_a_smooth_state(tables, z_i, izip):
+    # Zel'dovich states with no cell beyond 32 particles: at z = 30 almost every
+    # brick takes the listed path (most targets alone in their window), at z = 15
+    # about a third of the bricks do and the rest go to the staged brick kernel
+    st, p, s = small_state(nc=32, nnt=2, z_i=z_i, seed=17, izipx=izip, izipv=izip)
+    assert st.rhoc.max() <= 32
+    p.ext_pp_force = 1
+    o, g = pair(st, p, tables, build=False)
+    s.a_mid, s.dt = s.a, 2.0
+    so, sg = s.copy(), s.copy()
+    o.ext_pp_force(so)
+    g.ext_pp_force(sg)
+    assert so.itest1 == sg.itest1 == st.np
+    assert so.npairs == sg.npairs > 1.02 * st.np   # window entries beyond the targets themselves
+    assert so.f2_max_pp == sg.f2_max_pp
+    assert so.dt_pp == sg.dt_pp
+    assert_same_state(o, g)
+
+
 def test_fine_green_octant_matches_closed_form(tables):
     from test_oracle import separable_green
     fk, ck = tables
