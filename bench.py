@@ -342,7 +342,14 @@ def run_ours(args, cfg, rank, world, local_rank):
     def ptr(a):
         return a.ctypes.data_as(C.c_void_p)
 
-    e2e_steps = max(1, min(args.steps, 3))
+    # the end-to-end leg continues the evolved state: it starts from the state the timed
+    # steps left (stored untimed), and every step loads the state from and stores it to
+    # pinned host memory around the step, for as many steps as the timed region
+    n0 = C.c_int64(0)
+    cube._check(cube.L.cube_store_state(cube.h, C.byref(n0), ptr(xp_h), ptr(vp_h), ptr(pid_h), ptr(rhoc_h),
+                                        ptr(vf_h)))
+    torch.cuda.synchronize()
+    e2e_steps = max(1, args.steps)
     h2d = xp_h.nbytes + vp_h.nbytes + pid_h.nbytes + rhoc_h.nbytes + vf_h.nbytes
     if world > 1:
         dist.barrier()
@@ -591,6 +598,11 @@ def run_ensemble(args, cfg):
         torch.cuda.synchronize()
     launches = sum(m.cube.launch_count() for m in ens.members) - l0
     npart = sum(sp.particles for sp in specs)
+    # the same boxes one at a time (one host thread, each step returns before the next
+    # box starts): the sequential rate the concurrent ensemble is compared with
+    seq_steps = max(1, min(args.steps, 2))
+    seq = ens.run(seq_steps, workers=1)
+    torch.cuda.synchronize()
     line = {"metric": "ensemble box-steps/s", "value": r["box_steps_per_s"], "unit": "box-steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": r["wall_s"] * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -599,6 +611,8 @@ def run_ensemble(args, cfg):
                        "workers": r["workers"], "parallelism": "boxes on concurrent streams",
                        "timing": "host wall clock between device synchronisations (one stream per box)"},
             "particle_updates_per_s": r["particle_updates_per_s"], "gpu_launches": int(launches),
+            "sequential": {"box_steps_per_s": seq["box_steps_per_s"], "steps": seq_steps, "workers": 1},
+            "vs_sequential": r["box_steps_per_s"] / seq["box_steps_per_s"],
             "clocks": clk.summary()}
     ens.close()
     if rank == 0:

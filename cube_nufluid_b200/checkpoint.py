@@ -103,21 +103,41 @@ def write(opath: str, z: float, ck: Checkpoint, image: int = 1) -> list[str]:
     return files
 
 
+def _checked_file(fn: str, nbytes: int, what: str) -> str:
+    size = os.path.getsize(fn)
+    if size != nbytes:
+        raise ValueError(f"corrupted checkpoint: {what} file {fn} holds {size} bytes, the header implies {nbytes}")
+    return fn
+
+
 def read(opath: str, z: float, image: int = 1, *, with_pid: bool = True) -> Checkpoint:
-    """particle_initialization.f90:34-56."""
-    h = np.fromfile(file_name(opath, z, "info", image), dtype=SIM_HEADER, count=1)[0]
+    """particle_initialization.f90:34-56.  The header is checked against itself and
+    against the sizes of the array files before anything is read: a truncated or
+    corrupted checkpoint raises ValueError (the reference would read garbage)."""
+    info = file_name(opath, z, "info", image)
+    _checked_file(info, SIM_HEADER.itemsize, "info")
+    h = np.fromfile(info, dtype=SIM_HEADER, count=1)[0]
     n = int(h["nplocal"])
-    xdt = np.int8 if int(h["izipx"]) == 1 else np.int16
-    vdt = np.int8 if int(h["izipv"]) == 1 else np.int16
-    ncells = int(h["nnt"]) ** 3 * int(h["nt"]) ** 3
-    xp = np.fromfile(file_name(opath, z, "xp", image), dtype=xdt, count=3 * n).reshape(n, 3)
-    vp = np.fromfile(file_name(opath, z, "vp", image), dtype=vdt, count=3 * n).reshape(n, 3)
-    rhoc = np.fromfile(file_name(opath, z, "np", image), dtype=np.int32, count=ncells)
-    vf = np.fromfile(file_name(opath, z, "vc", image), dtype=np.float32, count=3 * ncells).reshape(ncells, 3)
+    izx, izv, nnt, nt = int(h["izipx"]), int(h["izipv"]), int(h["nnt"]), int(h["nt"])
+    if izx not in (1, 2) or izv not in (1, 2) or nnt <= 0 or nt <= 0 or n < 0:
+        raise ValueError(f"corrupted checkpoint header: izipx={izx} izipv={izv} nnt={nnt} nt={nt} nplocal={n}")
+    xdt = np.int8 if izx == 1 else np.int16
+    vdt = np.int8 if izv == 1 else np.int16
+    ncells = nnt ** 3 * nt ** 3
+    xp = np.fromfile(_checked_file(file_name(opath, z, "xp", image), 3 * n * izx, "xp"), dtype=xdt,
+                     count=3 * n).reshape(n, 3)
+    vp = np.fromfile(_checked_file(file_name(opath, z, "vp", image), 3 * n * izv, "vp"), dtype=vdt,
+                     count=3 * n).reshape(n, 3)
+    rhoc = np.fromfile(_checked_file(file_name(opath, z, "np", image), 4 * ncells, "np"), dtype=np.int32,
+                       count=ncells)
+    if int(rhoc.astype(np.int64).sum()) != n or (rhoc < 0).any():
+        raise ValueError("corrupted checkpoint: the cell counts do not add up to nplocal")
+    vf = np.fromfile(_checked_file(file_name(opath, z, "vc", image), 12 * ncells, "vc"), dtype=np.float32,
+                     count=3 * ncells).reshape(ncells, 3)
     pid = None
     fid = file_name(opath, z, "id", image)
     if with_pid and os.path.exists(fid):
-        pid = np.fromfile(fid, dtype=np.int32, count=n)
+        pid = np.fromfile(_checked_file(fid, 4 * n, "id"), dtype=np.int32, count=n)
     return Checkpoint(h, xp, vp, rhoc, vf, pid)
 
 

@@ -225,7 +225,7 @@ void cube_destroy(cube_ctx* ctx) {
                   ctx->coarse.rho, ctx->coarse.force, ctx->coarse.ext, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->coarse.plan.tw2,
                   ctx->fine.kernd, ctx->coarse.kernd, ctx->fine.plan.twd, ctx->coarse.plan.twd,
                   ctx->rho_c_acc,
-                  ctx->tan_table, ctx->dscal, ctx->pk_bins};
+                  ctx->tan_table, ctx->venc_band, ctx->dscal, ctx->pk_bins};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 3; ++k) {
@@ -321,6 +321,7 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
             A((void**)&ctx->red_tmp, 8 * (2 * (std::max<int64_t>(nce, cap) / 1024 + 64) + 64)) &&
             A((void**)&ctx->scan_tmp, 8 * (nce / 2048 + 64)) &&
             A((void**)&ctx->rho_c_acc, (P.neutrino ? 16 : 8) * nce) && A((void**)&ctx->tan_table, 4 * ctx->nvbin) &&
+            A((void**)&ctx->venc_band, 16 * (ctx->nvbin / 2 + 1)) &&
             A((void**)&ctx->dscal, sizeof(DevScal)) &&
             A((void**)&ctx->pk_bins, 8 * 7 * (size_t)(cube_pk_nbin(ctx->nf, 0) + 1));
   if (!ok) return fail(CUBE_ERR_CUDA);
@@ -344,6 +345,21 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
   for (int c = -ctx->nvbin / 2; c < ctx->nvbin / 2; ++c) tt[c + ctx->nvbin / 2] = tanf(cube_varg(&ctx->codec, c));
   if (cudaMemcpyAsync(ctx->tan_table, tt.data(), 4 * ctx->nvbin, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) {
     ctx->err = "tan table upload failed";
+    return fail(CUBE_ERR_CUDA);
+  }
+  // code boundaries of the encode, x_n = tan((n - 1/2)*pi_f/nvbin_m1), in x87 extended
+  // precision, widened by a relative 1e-9 either side (cube_vencode_tab)
+  const int nmax = ctx->nvbin / 2 - 1;
+  std::vector<double> vb(2 * (nmax + 2));
+  vb[0] = vb[1] = -INFINITY;
+  vb[2 * (nmax + 1)] = vb[2 * (nmax + 1) + 1] = INFINITY;
+  for (int n = 1; n <= nmax; ++n) {
+    const long double xn = tanl(((long double)n - 0.5L) * (long double)ctx->codec.pi_f / (long double)ctx->codec.nvbin_m1_f);
+    vb[2 * n] = (double)(xn * (1.0L - 1e-9L));
+    vb[2 * n + 1] = (double)(xn * (1.0L + 1e-9L));
+  }
+  if (cudaMemcpy(ctx->venc_band, vb.data(), 8 * vb.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    ctx->err = "encode boundary table upload failed";
     return fail(CUBE_ERR_CUDA);
   }
   if ((rc = cube_build_green(ctx, fk_table, ck_table))) return fail(rc);

@@ -60,8 +60,8 @@ struct MeshLevel {
   float* force;   // [3] force meshes, each n*plane floats, in place as spectra
   float* ext;     // scratch mesh (n*plane floats) for the transposed passes
   float* kern;    // Green multiplier (imaginary parts, /n^3)
-  double* kernd;  // the same in FP64 (FP64 Poisson mode, else null)
-  int fp64;       // 1: rho, force and ext hold doubles (same element pitches)
+  double* kernd = nullptr;  // the same in FP64 (FP64 Poisson mode, else null)
+  int fp64 = 0;             // 1: rho, force and ext hold doubles (same element pitches)
   int kern_octant;  // 1: kern is [3][(n/2+1)^3] octant; 0: [3][n][n][cp_k]
   int kern_pitch;   // inner pitch of kern (n/2+1)
   FftPlan plan;
@@ -158,6 +158,7 @@ struct cube_ctx {
   double* dep_partial;            // per-CTA fine mass partial sums
   int64_t dep_blocks;
   float* tan_table;               // tanf of each velocity code, index code+nvbin/2
+  double2* venc_band;             // code-boundary bands of cube_vencode_tab (nvbin/2 + 1 entries)
   DevScal* dscal;                 // device scalars
   DevScal* hscal;                 // pinned host mirror
   float2* sbuf;                   // spare spectrum buffer for the forward z pass
@@ -270,6 +271,21 @@ __device__ __forceinline__ float cube_div_const(float x, float y, float z) {
   return __fmaf_rn(r, z, q0);
 }
 
+// RN(a/b) from y = RN(1/b) for b > 0 (normal) and finite a, by two FMA corrections
+// of q0 = RN(a y): the first gives a quotient within one ulp of a/b, and then, y being
+// within half an ulp of 1/b, RN(q + (a - b q) y) with the exact FMA residual is the
+// correctly rounded quotient (Markstein's theorem; Markstein, IBM J. Res. Dev. 34(1),
+// 1990; Muller et al., Handbook of Floating-Point Arithmetic, sec. 4.7).  It replaces
+// IEEE divisions by one b shared by several a; cube_debug_division_check compares it
+// with the IEEE division on the GPU.
+__device__ __forceinline__ double cube_div_rcp(double a, double b, double y) {
+  double q = __dmul_rn(a, y);
+  double r = __fma_rn(-b, q, a);
+  q = __fma_rn(r, y, q);
+  r = __fma_rn(-b, q, a);
+  return __fma_rn(r, y, q);
+}
+
 inline float cube_kick_scalar(const KickScale& k) {
   return k.on ? cube_fdiv(cube_fdiv(cube_fmul(k.a_mid, k.dt), 6.f), k.pi_f) : 1.f;
 }
@@ -332,6 +348,52 @@ __device__ __forceinline__ int32_t cube_vencode_fast(const cube_codec* c, double
   const double fr = q - fl;  // exact
   if (fabs(fr - 0.5) < 1e-9) return cube_vencode(c, v, coef);
   const int32_t n = (int32_t)fl + (fr > 0.5 ? 1 : 0);
+  return x < 0.0 ? -n : n;
+}
+
+// Velocity encode by the code boundaries.  The encode is a function of x = RN(coef*v)
+// alone, odd in x, and its code changes from n-1 to n where the reference's
+// q(x) = nvbin_m1*atan(x)/pi_f crosses n - 1/2, i.e. at x_n = tan((n - 1/2)*pi_f/nvbin_m1)
+// (computed once per context in extended precision).  band[n] = (x_n(1 - eta), x_n(1 + eta)),
+// eta = 1e-9, for n = 1 .. nmax, band[0] = (-inf, -inf), band[nmax + 1] = (+inf, +inf).
+// cube_vencode's q differs from q(x) by less than 3e-11 (cube_atan within about 4 ulp of
+// pi/2, two roundings of |q| < 2^15), while across a band edge q(x) moves by at least
+// eta*nvbin_m1/(pi_f*max((1+x^2)/x)) > 4e-10 for both code widths (the outermost
+// boundaries have (1+x^2)/x below 41722 at nvbin_m1 = 65535), so outside every band the
+// exact encode is decided by which boundaries lie below |x|.  A first guess n0 comes from
+// an FP32 arctangent (least-squares polynomial in t^2 on [0,1], |error| < 1.8e-6 over
+// every float t, reciprocal above 1); its q is within 0.05 of the exact one, so the code is
+// n0 - 1, n0 or n0 + 1 and only the two boundaries n0 and n0 + 1 are read.  Inside a band
+// the exact encode decides.
+struct VencTab {
+  const double2* band;  // nmax + 2 entries
+  int nmax;             // largest code, nvbin/2 - 1
+  float qscale;         // nvbin_m1 / pi_f
+};
+
+inline VencTab cube_venc_tab(const cube_ctx* ctx) {
+  return VencTab{ctx->venc_band, ctx->nvbin / 2 - 1, ctx->codec.nvbin_m1_f / ctx->codec.pi_f};
+}
+__device__ __forceinline__ int32_t cube_vencode_tab(const cube_codec* c, const VencTab& T, double v, double coef) {
+  const double x = cube_dmul(coef, v);
+  const double ax = fabs(x);
+  if (!(ax < 1e30)) return cube_vencode(c, v, coef);  // beyond the FP32 guess's range, or NaN
+  const float af = __double2float_rn(ax);
+  const bool big = af > 1.f;
+  const float t = big ? __fdividef(1.f, af) : af;
+  const float s = __fmul_rn(t, t);
+  float p = -0.011719122529029846f;
+  p = __fmaf_rn(p, s, 0.052647314965724945f);
+  p = __fmaf_rn(p, s, -0.11642644554376602f);
+  p = __fmaf_rn(p, s, 0.19354036450386047f);
+  p = __fmaf_rn(p, s, -0.33262282609939575f);
+  p = __fmaf_rn(p, s, 0.9999772310256958f);
+  const float a = __fmul_rn(t, p);
+  const float r = big ? __fsub_rn(1.5707963267948966f, a) : a;
+  const int n0 = min(__float2int_rn(__fmul_rn(r, T.qscale)), T.nmax);
+  const double2 lo = __ldg(&T.band[n0]), hi = __ldg(&T.band[n0 + 1]);
+  if ((ax >= lo.x && ax < lo.y) || (ax >= hi.x && ax < hi.y)) return cube_vencode(c, v, coef);
+  const int32_t n = n0 + (ax >= hi.y ? 1 : 0) - (ax < lo.x ? 1 : 0);
   return x < 0.0 ? -n : n;
 }
 

@@ -213,6 +213,9 @@ __global__ void __launch_bounds__(DEP_THREADS, 3) k_deposit(
       dx2[d] = cube_fsub(1.f, dx1[d]);
       o1[d] = 4 * (cr[d] - 1) + (int)(f - l4);  // brick-local fine node of the lower corner
     }
+    // a particle of the low-side layer reaches the brick only from the last fine cell
+    // of its coarse cell (o1 = -1); the other three quarters touch no node here
+    if (o1[0] < -1 || o1[1] < -1 || o1[2] < -1) continue;
 #pragma unroll
     for (int c8 = 0; c8 < 8; ++c8) {
       const int sx = c8 & 1, sy = (c8 >> 1) & 1, sz = c8 >> 2;

@@ -330,6 +330,7 @@ int cube_fft_plan(cube_ctx* ctx, FftPlan& p, int n) {
   p.n = n;
   p.nst = 0;
   p.tw = p.tw2 = nullptr;
+  p.twd = nullptr;
   int m = n;
   while (m % 4 == 0) { p.radix[p.nst++] = 4; m /= 4; }
   while (m % 2 == 0) { p.radix[p.nst++] = 2; m /= 2; }

@@ -273,10 +273,12 @@ struct IcScratch {
   float* kern = nullptr;
   float2* tw = nullptr;
   float2* tw2 = nullptr;
+  double2* twd = nullptr;
   ~IcScratch() {
     if (kern) cudaFree(kern);
     if (tw) cudaFree(tw);
     if (tw2) cudaFree(tw2);
+    if (twd) cudaFree(twd);
   }
 };
 
@@ -298,7 +300,7 @@ int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io)
   }
   // the particle grid borrows the fine mesh's arrays (free outside particle_mesh);
   // npd <= nf, so it fits with its own pitch
-  MeshLevel M;
+  MeshLevel M{};  // an FP32 level (fp64 = 0, no FP64 Green table)
   M.n = npd;
   M.rp = npd + 32;
   M.cp = M.rp / 2;
@@ -312,6 +314,7 @@ int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io)
   int rc = cube_fft_plan(ctx, M.plan, npd);
   tmp.tw = M.plan.tw;
   tmp.tw2 = M.plan.tw2;
+  tmp.twd = M.plan.twd;
   if (rc) return rc;
   const size_t ksz = (size_t)M.kern_pitch * M.kern_pitch * M.kern_pitch;
   CUBE_CUDA_TRY(ctx, cudaMalloc((void**)&tmp.kern, sizeof(float) * 3 * ksz));

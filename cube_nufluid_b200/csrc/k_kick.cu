@@ -34,13 +34,13 @@ constexpr int KCELLS = 64;  // cells per work item at most (cube_cell_items)
 // shared memory first was measured twice as slow: at ~500 particles per brick
 // the copies of 17^3 x 3 nodes outweigh the gathers they replace, which hit L1/L2.)
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(256, 3) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
+__global__ void __launch_bounds__(256, 2) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                               const int64_t* __restrict__ cell_start, const float* __restrict__ vfield,
                                               int64_t cap, int64_t ncells, int nc, int nt, int nnt,
                                               const float* __restrict__ ff, size_t fcomp, int frp, size_t fplane,
                                               const float* __restrict__ fc, size_t ccomp, int crp, size_t cplane,
                                               const double* __restrict__ dec_old, const double* __restrict__ dec_new,
-                                              int half_nvbin, cube_codec codec, double coef_new, double inv_pi,
+                                              int half_nvbin, cube_codec codec, double coef_new, VencTab tab,
                                               DevScal* __restrict__ dscal, const int64_t* __restrict__ items,
                                               int64_t items_max) {
   typedef typename CodeT<ZX>::T TX;
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(256, 3) k_kick(const void* __restrict__ xp_, v
     const size_t fz[2] = {(size_t)fi[2][0] * fplane, (size_t)fi[2][1] * fplane};
     const size_t gz[2] = {(size_t)gi[2][0] * cplane, (size_t)gi[2][1] * cplane};
     const int fy[2] = {fi[1][0] * frp, fi[1][1] * frp}, gy[2] = {gi[1][0] * crp, gi[1][1] * crp};
-#pragma unroll 1
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
       const float* F = ff + d * fcomp;
       const float* G = fc + d * ccomp;
@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(256, 3) k_kick(const void* __restrict__ xp_, v
         q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
         v = cube_dadd(v, (double)q);
       }
-      const int code1 = cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
+      const int code1 = cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
       v = __ldg(&dec_new[code1 + half_nvbin]);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -131,7 +131,7 @@ __global__ void __launch_bounds__(256, 3) k_kick(const void* __restrict__ xp_, v
       vm[0] = (d == 0) ? fmaxf(vm[0], am) : vm[0];
       vm[1] = (d == 1) ? fmaxf(vm[1], am) : vm[1];
       vm[2] = (d == 2) ? fmaxf(vm[2], am) : vm[2];
-      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
     }
   }
   // every thread reaches here: warp maxima, then one shared atomic per warp and component
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(256, 3) k_kick64(const void* __restrict__ xp_,
                                                 const double* __restrict__ ff, size_t fcomp, int frp, size_t fplane,
                                                 const double* __restrict__ fc, size_t ccomp, int crp, size_t cplane,
                                                 const double* __restrict__ dec_old, const double* __restrict__ dec_new,
-                                                int half_nvbin, cube_codec codec, double coef_new, double inv_pi,
+                                                int half_nvbin, cube_codec codec, double coef_new, VencTab tab,
                                                 DevScal* __restrict__ dscal, const int64_t* __restrict__ items,
                                                 int64_t items_max) {
   typedef typename CodeT<ZX>::T TX;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(256, 3) k_kick64(const void* __restrict__ xp_,
         const double q = __ldg(&F[fz[oz[k]] + (size_t)(fy[oy[k]] + fi[0][ox[k]])]);
         v += ((q * (ox[k] ? dx2[0] : dx1[0])) * (oy[k] ? dx2[1] : dx1[1])) * (oz[k] ? dx2[2] : dx1[2]);
       }
-      const int code1 = cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
+      const int code1 = cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
       v = __ldg(&dec_new[code1 + half_nvbin]);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__(256, 3) k_kick64(const void* __restrict__ xp_,
       }
       const float am = (float)fabs(v + (double)vf);
       vm[d] = fmaxf(vm[d], am);
-      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&codec, v, coef_new, inv_pi), ZV);
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
     }
   }
 #pragma unroll
@@ -262,7 +262,7 @@ int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
         ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt,
         reinterpret_cast<const double*>(F.force), (size_t)F.n * F.plane, F.rp, F.plane,
         reinterpret_cast<const double*>(Cc.force), (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, dec_old, dec_new,
-        ctx->nvbin / 2, ctx->codec, coef_new, 1.0 / (double)ctx->codec.pi_f, ctx->dscal, ctx->rebin_items,
+        ctx->nvbin / 2, ctx->codec, coef_new, cube_venc_tab(ctx), ctx->dscal, ctx->rebin_items,
         cube_rebin_items_max(ctx->ncells, ctx->cap));
     CUBE_LAUNCH_CHECK(ctx);
     return CUBE_OK;
@@ -270,7 +270,7 @@ int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
   k_kick<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
       ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, F.force,
       (size_t)F.n * F.plane, F.rp, F.plane, Cc.force, (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, dec_old, dec_new,
-      ctx->nvbin / 2, ctx->codec, coef_new, 1.0 / (double)ctx->codec.pi_f, ctx->dscal, ctx->rebin_items,
+      ctx->nvbin / 2, ctx->codec, coef_new, cube_venc_tab(ctx), ctx->dscal, ctx->rebin_items,
       cube_rebin_items_max(ctx->ncells, ctx->cap));
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;

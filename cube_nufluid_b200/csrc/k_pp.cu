@@ -46,6 +46,8 @@ constexpr int NOWN = 16 * 16 * 16;        // the brick's own fine cells, numbere
 constexpr int PB_CAP = 4096;              // particles staged per brick in shared memory
 constexpr int PB_SPARSE = 2560;           // up to this many: the chains; above: the fine-cell sort
 constexpr int PP_THREADS = 256;
+constexpr int PP_PMAX = 4096;             // window entries of a group of PP_THREADS targets, evaluated pair-parallel
+constexpr int PP_CH = 256;                // pair terms per shared-memory chunk
 
 // fine cell (region coordinates, 0..23) -> sort index: own cells (4..19 in every
 // dimension) first in (z,y,x) order, then the halo cells in raster order
@@ -75,9 +77,10 @@ __device__ __forceinline__ void pp_pair(const double x21[3], double mass, double
   const double pcut = cube_dadd(cube_dsub(1.0, cube_dmul(1.75, rc3)), cube_dmul(0.75, rc5));
   const double r3 = cube_dmul(cube_dmul(rmag, rmag), rmag);
   const bool keep = rmag > rsoft;
+  const double y = __drcp_rn(r3);  // the three IEEE quotients x21/r3 through one reciprocal
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    double f = cube_dmul(cube_dmul(mass, cube_ddiv(x21[d], r3)), pcut);
+    double f = cube_dmul(cube_dmul(mass, cube_div_rcp(x21[d], r3, y)), pcut);
     if (!keep) f = cube_dmul(f, 0.0);
     fp[d] = f;
   }
@@ -85,7 +88,8 @@ __device__ __forceinline__ void pp_pair(const double x21[3], double mass, double
 
 struct PPArgs {
   int pr, nf_cutoff;
-  double rsoft, mass, a_mid, dt, pi_d, coef, inv_pi;
+  double rsoft, mass, a_mid, dt, pi_d, coef;
+  VencTab tab;
   const double* dec;  // tan(code)/coef per code (cube_vdec_table)
   int half_nvbin;
   cube_codec codec;
@@ -133,7 +137,7 @@ __device__ __forceinline__ void pp_apply(const double ft[3], const int vc[3], in
     k = cube_ddiv(k, 6.0);
     k = cube_ddiv(k, A.pi_d);
     const double v = cube_dadd(__ldg(&A.dec[vc[d]]), k);
-    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_fast(&A.codec, v, A.coef, A.inv_pi), ZV);
+    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_tab(&A.codec, A.tab, v, A.coef), ZV);
   }
   const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
   acc.f2max = fmaxf(acc.f2max, (float)f2);
@@ -391,7 +395,7 @@ __device__ void pp_sort_par(const void* __restrict__ xp_, int64_t cap, const int
 }
 
 template <int ZX, int ZV>
-__global__ void __launch_bounds__(PP_THREADS, 3) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
+__global__ void __launch_bounds__(PP_THREADS, 2) k_pp_brick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                                          const int64_t* __restrict__ cell_start, int nc, int nt,
                                                          int nnt, PPArgs A, int32_t* __restrict__ spill,
                                                          DevScal* __restrict__ dscal,
@@ -483,17 +487,130 @@ __global__ void __launch_bounds__(PP_THREADS, 3) k_pp_brick(const void* __restri
     const Sorted<uint16_t> S = {nullptr, nullptr, nullptr, nullptr};
     const Chains H = {head, nxt, code};
     const int T = tpre[PB * PB * PB];
-    for (int t = threadIdx.x; t < T; t += blockDim.x) {
-      int lo = 0, hi = PB * PB * PB - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (tpre[mid] <= t) lo = mid; else hi = mid - 1;
+    // Targets in groups of PP_THREADS, one per thread: each counts the entries of its
+    // window (the chains it walks), a scan places them, each writes its entries in
+    // window order, and then all lanes evaluate the FP64 pair terms of the group chunk
+    // by chunk while each thread adds its own terms in that order.  A coincident pair
+    // gives +0, which leaves the running sum unchanged (it is never -0), so the sums
+    // are those of the per-target walk; only the divergent walks stay per target.
+    uint16_t* plist = code + 3 * PB_CAP;                           // PP_PMAX staged indices
+    double* term = reinterpret_cast<double*>(plist + PP_PMAX);     // [3][PP_CH]
+    __shared__ int offs[PP_THREADS + 1];
+    __shared__ double tx1[3][PP_THREADS];
+    const bool pow2_cut = (A.nf_cutoff & (A.nf_cutoff - 1)) == 0;
+    const double inv_cut = 1.0 / (double)A.nf_cutoff;
+    const int pr = A.pr;
+    for (int g0 = 0; g0 < T; g0 += PP_THREADS) {
+      const int t = g0 + (int)threadIdx.x;
+      const bool valid = t < T;
+      int cc[3] = {0, 0, 0}, g1[3] = {0, 0, 0}, q = 0, m = 0, nt = 0;
+      int64_t ip = 0;
+      double x1[3] = {0.0, 0.0, 0.0};
+      if (valid) {
+        int lo = 0, hi = PB * PB * PB - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (tpre[mid] <= t) lo = mid; else hi = mid - 1;
+        }
+        cc[0] = (lo & 3) + 1; cc[1] = ((lo >> 2) & 3) + 1; cc[2] = (lo >> 4) + 1;
+        q = (cc[2] * PR + cc[1]) * PR + cc[0];
+        m = cpre[q] + (t - tpre[lo]);
+        ip = cst[q] + (t - tpre[lo]);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+          const double fr = cube_xfrac((int32_t)(int16_t)code[3 * m + d], ZX);
+          x1[d] = cube_dadd(4.0 * (double)cc[d], cube_dmul(4.0, fr));
+          g1[d] = 4 * cc[d] + (int)floor(cube_dmul(4.0, fr));
+        }
+        for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
+          for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj) {
+            const int rbase = (kk * PF + jj) * PF;
+            for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii)
+              for (int m2 = head[rbase + ii]; m2 != 0xFFFF; m2 = nxt[m2]) ++nt;
+          }
       }
-      const int cc[3] = {(lo & 3) + 1, ((lo >> 2) & 3) + 1, (lo >> 4) + 1};
-      const int q = (cc[2] * PR + cc[1]) * PR + cc[0];
-      const int m = cpre[q] + (t - tpre[lo]);
-      const uint16_t tc[3] = {code[3 * m], code[3 * m + 1], code[3 * m + 2]};
-      pp_target<ZX, ZV, true>(S, H, tc, cst[q] + (t - tpre[lo]), cc, A, vp_, acc);
+      // exclusive scan of the entry counts over the block
+      {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        int inc = nt;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += v;
+        }
+        __shared__ int wsum[PP_THREADS / 32];
+        if (lane == 31) wsum[warp] = inc;
+        __syncthreads();
+        int before = 0;
+        for (int w = 0; w < warp; ++w) before += wsum[w];
+        offs[threadIdx.x] = before + inc - nt;
+        if (threadIdx.x == PP_THREADS - 1) offs[PP_THREADS] = before + inc;
+        __syncthreads();
+      }
+      const int P = offs[PP_THREADS];
+      if (P > PP_PMAX) {  // too many entries for the shared list: the per-target walk
+        if (valid) {
+          const uint16_t tc[3] = {code[3 * m], code[3 * m + 1], code[3 * m + 2]};
+          pp_target<ZX, ZV, true>(S, H, tc, ip, cc, A, vp_, acc);
+        }
+        __syncthreads();
+        continue;
+      }
+      if (valid) {
+        int k = offs[threadIdx.x];
+        for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
+          for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj) {
+            const int rbase = (kk * PF + jj) * PF;
+            for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii)
+              for (int m2 = head[rbase + ii]; m2 != 0xFFFF; m2 = nxt[m2]) plist[k++] = (uint16_t)m2;
+          }
+#pragma unroll
+        for (int d = 0; d < 3; ++d) tx1[d][threadIdx.x] = x1[d];
+      }
+      __syncthreads();
+      double ft[3] = {0.0, 0.0, 0.0};
+      for (int cb = 0; cb < P; cb += PP_CH) {
+        const int ce = min(cb + PP_CH, P);
+        for (int p = cb + (int)threadIdx.x; p < ce; p += PP_THREADS) {
+          int lo = 0, hi = PP_THREADS - 1;  // the target whose entries hold p
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (offs[mid] <= p) lo = mid; else hi = mid - 1;
+          }
+          const int m2 = plist[p];
+          const int f2 = fr[m2];
+          const int fi[3] = {f2 % PF, (f2 / PF) % PF, f2 / (PF * PF)};
+          double x21[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) {
+            const double cf = 4.0 * (double)(fi[d] >> 2);
+            const double frn = cube_xfrac((int32_t)(int16_t)code[3 * m2 + d], ZX);
+            x21[d] = cube_dsub(cube_dadd(cf, cube_dmul(4.0, frn)), tx1[d][lo]);
+          }
+          double fp[3] = {0.0, 0.0, 0.0};
+          if (!(x21[0] == 0.0 && x21[1] == 0.0 && x21[2] == 0.0))
+            pp_pair(x21, A.mass, A.rsoft, A.nf_cutoff, pow2_cut, inv_cut, fp);
+#pragma unroll
+          for (int d = 0; d < 3; ++d) term[d * PP_CH + (p - cb)] = fp[d];
+        }
+        __syncthreads();
+        if (valid) {
+          const int e0 = max(offs[threadIdx.x], cb), e1 = min(offs[threadIdx.x + 1], ce);
+          for (int p = e0; p < e1; ++p)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], term[d * PP_CH + (p - cb)]);
+        }
+        __syncthreads();
+      }
+      if (valid) {
+        ++acc.n1;
+        acc.npair += (unsigned long long)nt;
+        typedef typename CodeT<ZV>::T TV;
+        const TV* vpr = reinterpret_cast<const TV*>(vp_);
+        int vc[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) vc[d] = (int)vpr[(size_t)d * A.cap + ip] + A.half_nvbin;
+        pp_apply<ZV>(ft, vc, ip, A, vp_, acc);
+      }
     }
   }
   pp_flush(acc, dscal);
@@ -876,7 +993,7 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   A.a_mid = (double)io->a_mid;
   A.dt = (double)io->dt;
   A.pi_d = (double)ctx->codec.pi_f;
-  A.inv_pi = 1.0 / A.pi_d;
+  A.tab = cube_venc_tab(ctx);
   A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
   int rc;
   A.dec = cube_vdec_table(ctx, A.coef, &rc);
@@ -920,7 +1037,8 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
   if (!ndense) return CUBE_OK;
   // bricks whose region holds a crowded cell: one CTA per brick as before
-  const size_t smem = sizeof(uint16_t) * ((size_t)NFC + 5 * (size_t)PB_CAP);
+  const size_t smem =
+      sizeof(uint16_t) * ((size_t)NFC + 5 * (size_t)PB_CAP + PP_PMAX) + sizeof(double) * 3 * (size_t)PP_CH;
   auto kb = k_pp_brick<ZX, ZV>;
   CUBE_CUDA_TRY(ctx, cube_smem_limit(kb, smem));
   kb<<<(unsigned)ndense, PP_THREADS, smem, ctx->stream>>>(ctx->xp, ctx->vp, ctx->cell_start, ctx->nc, ctx->nt,

@@ -51,7 +51,7 @@ struct RebinArgs {
   int32_t* big_list; double* stats; int32_t* slot_cell;  // new cell of each slot
   const int64_t* items; int64_t items_max;
   const double* dec; int half_nvbin;  // tan(code)/coef per code (cube_vdec_table)
-  cube_codec codec; double coef, inv_pi;
+  cube_codec codec; double coef; VencTab tab;
   int64_t cap, ncells;
   int nc, nt, nnt, ncb, nte, ncell, nlayer, use_pid;
   float dt_mid;
@@ -219,7 +219,7 @@ __device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t i
   for (int d = 0; d < 3; ++d) {
     const int64_t mv = cube_nint(cube_ddiv(cube_dmul((double)A.dt_mid, v[d]), xstep));
     xp2[(size_t)d * A.cap + slot] = (TX)cube_wrap_code((int64_t)xp[(size_t)d * A.cap + ip] + (int32_t)mv, ZX);
-    const int code = cube_wrap_code(cube_vencode_fast(&A.codec, cube_dsub(v[d], (double)vfn[d]), A.coef, A.inv_pi), ZV);
+    const int code = cube_wrap_code(cube_vencode_tab(&A.codec, A.tab, cube_dsub(v[d], (double)vfn[d]), A.coef), ZV);
     vp2[(size_t)d * A.cap + slot] = (TV)code;
   }
   if (A.use_pid) A.pid2[slot] = A.pid[ip];
@@ -742,7 +742,7 @@ int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
   A.slot_cell = reinterpret_cast<int32_t*>(ctx->slot_r2);
   A.half_nvbin = ctx->nvbin / 2;
   A.codec = ctx->codec; A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
-  A.inv_pi = 1.0 / (double)ctx->codec.pi_f;
+  A.tab = cube_venc_tab(ctx);
   {
     int trc;
     A.dec = cube_vdec_table(ctx, A.coef, &trc);

@@ -248,13 +248,13 @@ namespace {
 // decode of every code, and one bit per code: the step's encode returns the code
 // itself for its decoded velocity (nvbin is a multiple of 256, so every warp is full)
 __global__ void k_vdec_build(const float* __restrict__ tan_table, double coef, double* __restrict__ out, int nvbin,
-                             cube_codec codec, double inv_pi) {
+                             cube_codec codec, VencTab tab) {
   uint32_t* fix = reinterpret_cast<uint32_t*>(out + nvbin);
   for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nvbin; c += gridDim.x * blockDim.x) {
     const double v = cube_vdecode(tan_table[c], coef);
     out[c] = v;
     const int code = c - nvbin / 2;
-    const bool same = cube_wrap_code(cube_vencode_fast(&codec, v, coef, inv_pi), codec.izipv) == code;
+    const bool same = cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef), codec.izipv) == code;
     const uint32_t bits = __ballot_sync(0xffffffffu, same);
     if ((threadIdx.x & 31) == 0) fix[c >> 5] = bits;
   }
@@ -277,7 +277,7 @@ const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc) {
     return nullptr;
   }
   k_vdec_build<<<(ctx->nvbin + 255) / 256, 256, 0, ctx->stream>>>(ctx->tan_table, coef, ctx->vdec[i], ctx->nvbin,
-                                                                  ctx->codec, 1.0 / (double)ctx->codec.pi_f);
+                                                                  ctx->codec, cube_venc_tab(ctx));
   ctx->launches++;
   if (cudaGetLastError() != cudaSuccess) {
     ctx->err = "velocity decode table launch failed";
@@ -291,8 +291,9 @@ const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc) {
 namespace {
 // velocities spread over the code range: v = tan(pi*(code + off)/(nvbin-1))/coef with
 // off in (-1, 1) drawn from a hash of the index, so that many land near the
-// rounding boundaries code +- 1/2
-__global__ void k_encode_check(cube_codec codec, double coef, double inv_pi, int64_t n, uint64_t seed,
+// rounding boundaries code +- 1/2 (within 1.3e-8 of a code, and within 3.3e-5, where
+// the edges of cube_vencode_tab's bands lie); both fast encoders against cube_vencode
+__global__ void k_encode_check(cube_codec codec, VencTab tab, double coef, double inv_pi, int64_t n, uint64_t seed,
                                unsigned long long* __restrict__ bad) {
   unsigned long long nb = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -301,23 +302,87 @@ __global__ void k_encode_check(cube_codec codec, double coef, double inv_pi, int
     const double u = (double)(h >> 11) * 0x1p-53;                        // [0,1)
     const double half = 0.5 * (double)codec.nvbin_m1_f;
     const double code = floor(u * (double)codec.nvbin_m1_f) - half;       // whole code range
-    const double off = ((h & 7) < 4) ? ((double)((h >> 3) & 0xFF) - 128.0) * 1e-10 + 0.5  // near x.5
-                                     : ((double)((h >> 3) & 0xFFFF) / 65536.0 - 0.5);      // anywhere
+    const int cls = (int)(h & 7);
+    const double off = cls < 3 ? ((double)((h >> 3) & 0xFF) - 128.0) * 1e-10 + 0.5       // near x.5
+                     : cls < 5 ? ((double)((h >> 3) & 0xFFFF) - 32768.0) * 1e-9 + 0.5     // across the
+                                                                                          // table's bands
+                               : ((double)((h >> 3) & 0xFFFF) / 65536.0 - 0.5);          // anywhere
     const double ang = 3.141592653589793 * (code + off) / (double)codec.nvbin_m1_f;
     if (fabs(ang) >= 1.5707963) continue;
     const double v = tan(ang) / coef;
-    nb += cube_vencode_fast(&codec, v, coef, inv_pi) != cube_vencode(&codec, v, coef);
+    const int32_t ex = cube_vencode(&codec, v, coef);
+    nb += (cube_vencode_fast(&codec, v, coef, inv_pi) != ex) + (cube_vencode_tab(&codec, tab, v, coef) != ex);
   }
   if (nb) atomicAdd(bad, nb);
 }
 }  // namespace
+
+namespace {
+// splitmix64 stream for the division check
+__device__ __forceinline__ uint64_t smix(uint64_t& s) {
+  uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// quotients of the PP pair term x/r^3 (x a separation component on the 2^-14 or 2^-6
+// grid of int2/int1 positions within +-8 fine cells, r^3 from three such components,
+// r > 0.3) and of random doubles over wide ranges: cube_div_rcp against __ddiv_rn
+__global__ void k_division_check(int64_t n, uint64_t seed, unsigned long long* bad) {
+  unsigned long long nb = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    uint64_t st = seed ^ (0xD1B54A32D192ED03ull * (uint64_t)(i + 1));
+    const int kind = (int)(i & 3);
+    double a[3], b;
+    if (kind < 3) {
+      const double res = kind == 2 ? 0.015625 : 6.103515625e-05;  // 2^-6 or 2^-14
+      const int span = kind == 2 ? 1024 : 262144;                // +-8 fine cells
+      double r2 = 0.0;
+      for (int d = 0; d < 3; ++d) {
+        a[d] = res * (double)((int64_t)(smix(st) % (uint64_t)(2 * span + 1)) - span);
+        r2 = __dadd_rn(r2, __dmul_rn(a[d], a[d]));
+      }
+      const double rm = sqrt(r2);
+      if (!(rm > 0.3)) continue;
+      b = __dmul_rn(__dmul_rn(rm, rm), rm);
+    } else {
+      const uint64_t u = smix(st);
+      b = ldexp(1.0 + (double)(u >> 12) * 0x1p-52, (int)(smix(st) % 50) - 10);
+      for (int d = 0; d < 3; ++d) {
+        const uint64_t v = smix(st);
+        a[d] = ldexp(1.0 + (double)(v >> 12) * 0x1p-52, (int)(smix(st) % 60) - 30) * ((v & 1) ? -1.0 : 1.0);
+      }
+    }
+    const double y = __drcp_rn(b);
+    for (int d = 0; d < 3; ++d) {
+      const double q1 = cube_div_rcp(a[d], b, y), q2 = __ddiv_rn(a[d], b);
+      if (__double_as_longlong(q1) != __double_as_longlong(q2)) ++nb;
+    }
+  }
+  if (nb) atomicAdd(bad, nb);
+}
+}  // namespace
+
+int32_t cube_debug_division_check(cube_ctx* ctx, int64_t n, uint64_t seed, int64_t* mismatches) {
+  if (!ctx || !mismatches || n < 0) return CUBE_ERR_PARAM;
+  unsigned long long* bad = reinterpret_cast<unsigned long long*>(ctx->red_tmp);
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, 8, ctx->stream));
+  k_division_check<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(n, seed, bad);
+  CUBE_LAUNCH_CHECK(ctx);
+  unsigned long long h = 0;
+  CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&h, bad, 8, cudaMemcpyDeviceToHost, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+  *mismatches = (int64_t)h;
+  return CUBE_OK;
+}
 
 int32_t cube_debug_encode_check(cube_ctx* ctx, int64_t n, uint64_t seed, float sigma, int64_t* mismatches) {
   if (!ctx || !mismatches || n < 0) return CUBE_ERR_PARAM;
   unsigned long long* bad = reinterpret_cast<unsigned long long*>(ctx->red_tmp);
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, 8, ctx->stream));
   const double coef = cube_vcoef(&ctx->codec, sigma);
-  k_encode_check<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->codec, coef, 1.0 / (double)ctx->codec.pi_f, n,
+  k_encode_check<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->codec, cube_venc_tab(ctx), coef, 1.0 / (double)ctx->codec.pi_f, n,
                                                             seed, bad);
   CUBE_LAUNCH_CHECK(ctx);
   unsigned long long h = 0;

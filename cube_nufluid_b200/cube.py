@@ -72,6 +72,8 @@ def load_library():
     L.cube_nu_info.restype = C.c_int32
     L.cube_debug_encode_check.argtypes = [vp, C.c_int64, C.c_uint64, C.c_float, C.POINTER(C.c_int64)]
     L.cube_debug_encode_check.restype = C.c_int32
+    L.cube_debug_division_check.argtypes = [vp, C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]
+    L.cube_debug_division_check.restype = C.c_int32
     L.cube_make_ic.argtypes = [vp, C.POINTER(CubeIcParams), S]
     L.cube_make_ic.restype = C.c_int32
     L.cube_halofind.argtypes = [vp, S, C.POINTER(CubeHaloArgs), C.POINTER(CubeHaloResult)]
@@ -219,6 +221,12 @@ class Cube:
         bad = C.c_int64(0)
         self._check(self.L.cube_debug_encode_check(self.h, int(n), int(seed), float(sigma), C.byref(bad)))
         return bad.value
+
+    def debug_division_check(self, n: int, seed: int) -> int:
+        """Quotients where the shared-reciprocal division differs from IEEE division."""
+        bad = C.c_int64(0)
+        self._check(self.L.cube_debug_division_check(self.h, int(n), int(seed), C.byref(bad)))
+        return int(bad.value)
 
     def make_ic(self, ic: dict, seed: int, *, f_cdm: float = 1.0) -> CubeScalars:
         """Zel'dovich state made on the device (cube_make_ic) from the scalars of

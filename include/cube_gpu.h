@@ -328,10 +328,18 @@ int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float*
                                    const float* coarse_force);
 
 /* Compares, for n velocities spread over every code and concentrated at the
- * rounding boundaries, the step's fast velocity encode (reciprocal-based, with an
- * exact fallback near ties) with the exact FP64 encode under sigma; *mismatches
- * counts the disagreements (0 expected). */
+ * rounding boundaries, the two fast velocity encodes (reciprocal-based, and the
+ * code-boundary table with an FP32 first guess that the step uses; both fall back
+ * to the exact encode near ties) with the exact FP64 encode under sigma;
+ * *mismatches counts the disagreements of either (0 expected). */
 int32_t cube_debug_encode_check(cube_ctx* ctx, int64_t n, uint64_t seed, float sigma, int64_t* mismatches);
+
+/* Compares, for n quotients shaped like the PP pair term (separation components on
+ * the int1/int2 position grids over +-8 fine cells divided by r^3, r > 0.3) and
+ * random doubles over wide ranges, the library's division through one shared
+ * reciprocal (two FMA corrections) with the IEEE division; *mismatches counts the
+ * quotients that differ in any bit (0 expected). */
+int32_t cube_debug_division_check(cube_ctx* ctx, int64_t n, uint64_t seed, int64_t* mismatches);
 
 /* Device time of the fine-mesh Poisson solve (FFT passes + Green multiply) on
  * whatever the fine density array holds, averaged over reps runs, in *ms. */

@@ -75,3 +75,35 @@ def test_gpu_checkpoint_resume_is_exact(tables, tmp_path):
     for k in range(3):
         assert np.array_equal(g.nu_store(k), h.nu_store(k))
     assert s2.sigma_vi == np.float32(s.sigma_vi) and s2.mass_p_cdm == np.float32(s.mass_p_cdm)
+
+
+def test_corrupted_checkpoints_are_refused(tmp_path):
+    st, p, s = small_state(nc=16, nnt=2, seed=12)
+    h = ck.make_header(p, s)
+    files = ck.write(str(tmp_path), 5.0, ck.Checkpoint(h, st.xp, st.vp, st.rhoc, st.vfield, st.pid))
+    info, xpf = files[0], files[1]
+    good = open(info, "rb").read()
+    # a truncated header
+    open(info, "wb").write(good[:200])
+    with pytest.raises(ValueError, match="info"):
+        ck.read(str(tmp_path), 5.0)
+    # a header whose particle count does not match the array files
+    bad = np.frombuffer(good, dtype=ck.SIM_HEADER).copy()
+    bad["nplocal"] += 1
+    open(info, "wb").write(bad.tobytes())
+    with pytest.raises(ValueError, match="xp"):
+        ck.read(str(tmp_path), 5.0)
+    # an impossible code width
+    bad = np.frombuffer(good, dtype=ck.SIM_HEADER).copy()
+    bad["izipx"] = 3
+    open(info, "wb").write(bad.tobytes())
+    with pytest.raises(ValueError, match="header"):
+        ck.read(str(tmp_path), 5.0)
+    # a truncated position file
+    open(info, "wb").write(good)
+    data = open(xpf, "rb").read()
+    open(xpf, "wb").write(data[:-6])
+    with pytest.raises(ValueError, match="xp"):
+        ck.read(str(tmp_path), 5.0)
+    open(xpf, "wb").write(data)
+    assert ck.read(str(tmp_path), 5.0).xp.shape == st.xp.shape

@@ -218,6 +218,16 @@ def test_pp_bit_exact(tables, izip):
     assert_same_state(o, g)
 
 
+def test_pp_division_through_a_shared_reciprocal_is_ieee(tables):
+    # the pair term divides three components by one r^3: through RN(1/r^3) and two
+    # FMA corrections, which must give the IEEE quotient in every bit
+    fk, ck = tables
+    st, p, s = small_state(nc=16, nnt=2, seed=5)
+    g = Cube(p, np_capacity=st.np, fk_table=fk, ck_table=ck)
+    assert g.debug_division_check(1 << 30, 12345) == 0
+    g.close()
+
+
 @pytest.mark.parametrize("z_i,izip", [(30.0, 2), (15.0, 2), (15.0, 1)])
 def test_pp_bit_exact_on_a_smooth_state(tables, z_i, izip):
     # Zel'dovich states with no cell beyond 32 particles: at z = 30 almost every
