@@ -225,7 +225,7 @@ void cube_destroy(cube_ctx* ctx) {
                   ctx->coarse.rho, ctx->coarse.force, ctx->coarse.ext, ctx->coarse.kern, ctx->coarse.plan.tw, ctx->coarse.plan.tw2,
                   ctx->fine.kernd, ctx->coarse.kernd, ctx->fine.plan.twd, ctx->coarse.plan.twd,
                   ctx->rho_c_acc,
-                  ctx->tan_table, ctx->venc_band, ctx->dscal, ctx->pk_bins};
+                  ctx->tan_table, ctx->venc_brk, ctx->dscal, ctx->pk_bins};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (int k = 0; k < 3; ++k) {
@@ -321,7 +321,7 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
             A((void**)&ctx->red_tmp, 8 * (2 * (std::max<int64_t>(nce, cap) / 1024 + 64) + 64)) &&
             A((void**)&ctx->scan_tmp, 8 * (nce / 2048 + 64)) &&
             A((void**)&ctx->rho_c_acc, (P.neutrino ? 16 : 8) * nce) && A((void**)&ctx->tan_table, 4 * ctx->nvbin) &&
-            A((void**)&ctx->venc_band, 16 * (ctx->nvbin / 2 + 1)) &&
+            A((void**)&ctx->venc_brk, sizeof(VencBrk) * 64) &&
             A((void**)&ctx->dscal, sizeof(DevScal)) &&
             A((void**)&ctx->pk_bins, 8 * 7 * (size_t)(cube_pk_nbin(ctx->nf, 0) + 1));
   if (!ok) return fail(CUBE_ERR_CUDA);
@@ -347,19 +347,18 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
     ctx->err = "tan table upload failed";
     return fail(CUBE_ERR_CUDA);
   }
-  // code boundaries of the encode, x_n = tan((n - 1/2)*pi_f/nvbin_m1), in x87 extended
-  // precision, widened by a relative 1e-9 either side (cube_vencode_tab)
-  const int nmax = ctx->nvbin / 2 - 1;
-  std::vector<double> vb(2 * (nmax + 2));
-  vb[0] = vb[1] = -INFINITY;
-  vb[2 * (nmax + 1)] = vb[2 * (nmax + 1) + 1] = INFINITY;
-  for (int n = 1; n <= nmax; ++n) {
-    const long double xn = tanl(((long double)n - 0.5L) * (long double)ctx->codec.pi_f / (long double)ctx->codec.nvbin_m1_f);
-    vb[2 * n] = (double)(xn * (1.0L - 1e-9L));
-    vb[2 * n + 1] = (double)(xn * (1.0L + 1e-9L));
+  // angle breakpoints theta_j = (j + 1/2) pi/128 and their tangents (cube_vencode_brk)
+  VencBrk br[64];
+  const long double pil = acosl(-1.0L);
+  for (int j = 0; j < 64; ++j) {
+    const long double th = ((long double)j + 0.5L) * pil / 128.0L;
+    br[j].c = (double)tanl(th);
+    br[j].hi = (double)th;
+    br[j].lo = (double)(th - (long double)br[j].hi);
+    br[j].pad = 0.0;
   }
-  if (cudaMemcpy(ctx->venc_band, vb.data(), 8 * vb.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
-    ctx->err = "encode boundary table upload failed";
+  if (cudaMemcpy(ctx->venc_brk, br, sizeof(br), cudaMemcpyHostToDevice) != cudaSuccess) {
+    ctx->err = "encode breakpoint table upload failed";
     return fail(CUBE_ERR_CUDA);
   }
   if ((rc = cube_build_green(ctx, fk_table, ck_table))) return fail(rc);

@@ -158,7 +158,7 @@ struct cube_ctx {
   double* dep_partial;            // per-CTA fine mass partial sums
   int64_t dep_blocks;
   float* tan_table;               // tanf of each velocity code, index code+nvbin/2
-  double2* venc_band;             // code-boundary bands of cube_vencode_tab (nvbin/2 + 1 entries)
+  struct VencBrk* venc_brk;       // angle breakpoints of cube_vencode_brk (64 entries)
   DevScal* dscal;                 // device scalars
   DevScal* hscal;                 // pinned host mirror
   float2* sbuf;                   // spare spectrum buffer for the forward z pass
@@ -295,14 +295,7 @@ __device__ __forceinline__ float cube_kick_scale(float f, const KickScale& k) {
   return cube_div_const(cube_div_const(t, 6.f, k.inv6), k.pi_f, k.inv_pi);
 }
 
-// Velocity encode nint(nvbin_m1*atan(coef*v)/pi) (cube_vencode) with a cheaper
-// first attempt.  The attempt follows cube_atan step by step but forms its two
-// quotients with a reciprocal from an FP32 seed and two Newton steps (relative
-// error below 2^-49) and multiplies by 1/pi instead of dividing.  Propagated
-// through the reduction and the series (Lipschitz 1) that changes atan by less
-// than 2^-48, hence q = nvbin_m1*atan/pi (|q| < 2^15) by less than 1e-10 including
-// the final roundings.  Unless q lies within 1e-9 of a rounding boundary (k + 1/2),
-// both evaluations give the same integer; otherwise the exact evaluation decides.
+// FP64 reciprocal from an FP32 seed and two Newton steps (relative error below 2^-49)
 __device__ __forceinline__ double cube_rcp_fast(double b) {
   double y = (double)__fdividef(1.0f, (float)b);
   double e = fma(-b, y, 1.0);
@@ -311,70 +304,34 @@ __device__ __forceinline__ double cube_rcp_fast(double b) {
   return fma(y, e, y);
 }
 
-__device__ __forceinline__ int32_t cube_vencode_fast(const cube_codec* c, double v, double coef, double inv_pi) {
-  const double x = cube_dmul(coef, v);
-  const double ax = fabs(x);
-  if (!(ax < 1e30)) return cube_vencode(c, v, coef);  // beyond the FP32 seed's range, or NaN
-  double t = ax;
-  const int recip = ax > 1.0;
-  if (recip) t = cube_rcp_fast(ax);
-  const int shift = t > CUBE_TANPIO12;
-  if (shift) {
-    const double num = cube_dfma(CUBE_SQRT3, t, -1.0);
-    const double den = cube_dadd(t, CUBE_SQRT3);
-    t = cube_dmul(num, cube_rcp_fast(den));
-  }
-  const double t2 = cube_dmul(t, t);
-  double p = -1.0 / 29.0;
-  p = cube_dfma(p, t2, 1.0 / 27.0);
-  p = cube_dfma(p, t2, -1.0 / 25.0);
-  p = cube_dfma(p, t2, 1.0 / 23.0);
-  p = cube_dfma(p, t2, -1.0 / 21.0);
-  p = cube_dfma(p, t2, 1.0 / 19.0);
-  p = cube_dfma(p, t2, -1.0 / 17.0);
-  p = cube_dfma(p, t2, 1.0 / 15.0);
-  p = cube_dfma(p, t2, -1.0 / 13.0);
-  p = cube_dfma(p, t2, 1.0 / 11.0);
-  p = cube_dfma(p, t2, -1.0 / 9.0);
-  p = cube_dfma(p, t2, 1.0 / 7.0);
-  p = cube_dfma(p, t2, -1.0 / 5.0);
-  p = cube_dfma(p, t2, 1.0 / 3.0);
-  p = cube_dmul(p, t2);
-  const double sr = cube_dfma(-t, p, t);
-  const double r = shift ? cube_dadd(CUBE_PIO6_HI, cube_dadd(sr, CUBE_PIO6_LO)) : sr;
-  const double res = recip ? cube_dadd(cube_dsub(CUBE_PIO2_HI, r), CUBE_PIO2_LO) : r;
-  const double q = cube_dmul(cube_dmul((double)c->nvbin_m1_f, res), inv_pi);  // |q|, atan >= 0 here
-  const double fl = floor(q);
-  const double fr = q - fl;  // exact
-  if (fabs(fr - 0.5) < 1e-9) return cube_vencode(c, v, coef);
-  const int32_t n = (int32_t)fl + (fr > 0.5 ? 1 : 0);
-  return x < 0.0 ? -n : n;
+struct VencBrk;
+struct VencTab {
+  const VencBrk* brk;   // 64 angle breakpoints (cube_vencode_brk)
+  double qscale_d;      // nvbin_m1 * (1/pi_f)
+};
+inline VencTab cube_venc_tab(const cube_ctx* ctx) {
+  return VencTab{ctx->venc_brk, (double)ctx->codec.nvbin_m1_f * (1.0 / (double)ctx->codec.pi_f)};
 }
 
-// Velocity encode by the code boundaries.  The encode is a function of x = RN(coef*v)
-// alone, odd in x, and its code changes from n-1 to n where the reference's
-// q(x) = nvbin_m1*atan(x)/pi_f crosses n - 1/2, i.e. at x_n = tan((n - 1/2)*pi_f/nvbin_m1)
-// (computed once per context in extended precision).  band[n] = (x_n(1 - eta), x_n(1 + eta)),
-// eta = 1e-9, for n = 1 .. nmax, band[0] = (-inf, -inf), band[nmax + 1] = (+inf, +inf).
-// cube_vencode's q differs from q(x) by less than 3e-11 (cube_atan within about 4 ulp of
-// pi/2, two roundings of |q| < 2^15), while across a band edge q(x) moves by at least
-// eta*nvbin_m1/(pi_f*max((1+x^2)/x)) > 4e-10 for both code widths (the outermost
-// boundaries have (1+x^2)/x below 41722 at nvbin_m1 = 65535), so outside every band the
-// exact encode is decided by which boundaries lie below |x|.  A first guess n0 comes from
-// an FP32 arctangent (least-squares polynomial in t^2 on [0,1], |error| < 1.8e-6 over
-// every float t, reciprocal above 1); its q is within 0.05 of the exact one, so the code is
-// n0 - 1, n0 or n0 + 1 and only the two boundaries n0 and n0 + 1 are read.  Inside a band
-// the exact encode decides.
-struct VencTab {
-  const double2* band;  // nmax + 2 entries
-  int nmax;             // largest code, nvbin/2 - 1
-  float qscale;         // nvbin_m1 / pi_f
+// Velocity encode by angle breakpoints, with no reciprocal reduction and no table
+// read on the dependent chain beyond 32 bytes that stay in L1.  With theta_j =
+// (j + 1/2)*pi/128, c_j = tan(theta_j), j = 0..63 (extended-precision values, theta_j
+// split hi + lo), atan(x) = theta_j + atan(u), u = (x - c_j)/(1 + x c_j).  j comes
+// from an FP32 arctangent guess (least-squares polynomial in t^2 on [0,1], |error|
+// < 1.8e-6 over every float t, reciprocal above 1; with its roundings < 2e-6), so |u| <=
+// tan(pi/256 + 2e-6) < 0.0123 for every x >= 0 (c_63 = 81.6 bounds u by 1/c_63 as
+// x grows), and atan(u) = u - u^3/3 + u^5/5 - u^7/7 leaves out less than 1e-18.  The
+// quotient takes the FP32-seeded Newton reciprocal (relative error < 2^-49, which
+// moves atan by < 3e-17 at this |u|); with the roundings of the sum and of
+// q = nvbin_m1*atan*(1/pi_f), q is within 3e-11 of the exact evaluation's, so as in
+// the exact evaluation's own error (< 3e-11) the integer is accepted unless q lies
+// within 1e-9 of k + 1/2; there the exact FP64 evaluation decides.
+struct VencBrk {
+  double c, hi, lo, pad;  // tan(theta_j), theta_j = hi + lo
 };
 
-inline VencTab cube_venc_tab(const cube_ctx* ctx) {
-  return VencTab{ctx->venc_band, ctx->nvbin / 2 - 1, ctx->codec.nvbin_m1_f / ctx->codec.pi_f};
-}
-__device__ __forceinline__ int32_t cube_vencode_tab(const cube_codec* c, const VencTab& T, double v, double coef) {
+__device__ __forceinline__ int32_t cube_vencode_brk(const cube_codec* c, const VencBrk* __restrict__ brk, double v,
+                                                    double coef, double qscale) {
   const double x = cube_dmul(coef, v);
   const double ax = fabs(x);
   if (!(ax < 1e30)) return cube_vencode(c, v, coef);  // beyond the FP32 guess's range, or NaN
@@ -389,12 +346,28 @@ __device__ __forceinline__ int32_t cube_vencode_tab(const cube_codec* c, const V
   p = __fmaf_rn(p, s, -0.33262282609939575f);
   p = __fmaf_rn(p, s, 0.9999772310256958f);
   const float a = __fmul_rn(t, p);
-  const float r = big ? __fsub_rn(1.5707963267948966f, a) : a;
-  const int n0 = min(__float2int_rn(__fmul_rn(r, T.qscale)), T.nmax);
-  const double2 lo = __ldg(&T.band[n0]), hi = __ldg(&T.band[n0 + 1]);
-  if ((ax >= lo.x && ax < lo.y) || (ax >= hi.x && ax < hi.y)) return cube_vencode(c, v, coef);
-  const int32_t n = n0 + (ax >= hi.y ? 1 : 0) - (ax < lo.x ? 1 : 0);
+  const float th = big ? __fsub_rn(1.5707963267948966f, a) : a;
+  const int j = min(max(__float2int_rd(__fmul_rn(th, 40.743665431525205f)), 0), 63);  // 128/pi
+  const double2 ch = __ldg(reinterpret_cast<const double2*>(brk + j));
+  const double lo = __ldg(&brk[j].lo);
+  const double num = cube_dsub(ax, ch.x);
+  const double den = cube_dfma(ax, ch.x, 1.0);
+  const double u = cube_dmul(num, cube_rcp_fast(den));
+  const double u2 = cube_dmul(u, u);
+  double q7 = cube_dfma(-1.0 / 7.0, u2, 1.0 / 5.0);
+  q7 = cube_dfma(q7, u2, -1.0 / 3.0);
+  const double at = cube_dadd(ch.y, cube_dadd(cube_dfma(cube_dmul(u, u2), q7, u), lo));
+  const double q = cube_dmul(at, qscale);  // |q|, atan >= 0 here
+  const double fl = floor(q);
+  const double fr = q - fl;  // exact
+  if (fabs(fr - 0.5) < 1e-9) return cube_vencode(c, v, coef);
+  const int32_t n = (int32_t)fl + (fr > 0.5 ? 1 : 0);
   return x < 0.0 ? -n : n;
+}
+
+// the encode of the step's kernels (kick, PP, re-bin, decode-table fixed points)
+__device__ __forceinline__ int32_t cube_vencode_step(const cube_codec* c, const VencTab& T, double v, double coef) {
+  return cube_vencode_brk(c, T.brk, v, coef, T.qscale_d);
 }
 
 // ---- launchers (implemented in the k_*.cu files) -----------------------------
@@ -454,7 +427,7 @@ int cube_halofind_dev(cube_ctx* ctx, const cube_scalars* io, const cube_halo_arg
 const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc);
 
 // true if re-encoding the decoded velocity of code index c (code + nvbin/2) at the
-// table's coefficient, cube_wrap_code(cube_vencode_fast(v)), gives the code back: a
+// table's coefficient, cube_wrap_code(cube_vencode_step(v)), gives the code back: a
 // velocity kicked by exactly zero then keeps its code
 __device__ __forceinline__ bool cube_vfixed(const double* dec, int nvbin, int c) {
   return (reinterpret_cast<const uint32_t*>(dec + nvbin)[c >> 5] >> (c & 31)) & 1u;

@@ -163,27 +163,31 @@ __global__ void __launch_bounds__(DEP_THREADS, 3) k_deposit(
     const int base = d == 0 ? x0 : d == 1 ? y0 : z0;
     ltf[d][c] = 4.f * (float)(cube_wrap(base + c - 1, nc) % nt);
   }
-  if (tid < 32) {
-    // cell table of the (B+1)^3 region in (z,y,x) order; warp 0 builds the prefix
-    int run = 0;
-    for (int base = 0; base < NHC; base += 32) {
-      const int q = base + tid;
-      int cnt = 0;
-      if (q < NHC) {
-        const int64_t c = region_cell(q, x0, y0, z0, nc, nt, nnt);
-        const int64_t s0 = cell_start[c];
-        cst[q] = s0;
-        cnt = (int)(cell_start[c + 1] - s0);
-      }
-      int inc = cnt;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, inc, o);
-        if (tid >= o) inc += v;
-      }
-      if (q < NHC) cpre[q] = run + inc - cnt;
-      run += __shfl_sync(0xffffffffu, inc, 31);
+  {
+    // cell table of the (B+1)^3 region in (z,y,x) order: one region cell per thread,
+    // then a block-wide exclusive prefix of the counts (warp scans + warp totals)
+    __shared__ int wtot[(NHC + 31) / 32];
+    int cnt = 0;
+    if (tid < NHC) {
+      const int64_t c = region_cell(tid, x0, y0, z0, nc, nt, nnt);
+      const int64_t s0 = cell_start[c];
+      cst[tid] = s0;
+      cnt = (int)(cell_start[c + 1] - s0);
     }
-    if (tid == 0) cpre[NHC] = run;
+    const int lane = tid & 31, warp = tid >> 5;
+    int inc = cnt;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += v;
+    }
+    if (tid < NHC && (lane == 31 || tid == NHC - 1)) wtot[warp] = inc;
+    __syncthreads();
+    if (tid < NHC) {
+      int before = 0;
+      for (int w = 0; w < warp; ++w) before += wtot[w];
+      cpre[tid] = before + inc - cnt;
+      if (tid == NHC - 1) cpre[NHC] = before + inc;
+    }
   }
   __syncthreads();
   const int total = cpre[NHC];

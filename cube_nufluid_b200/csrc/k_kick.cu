@@ -33,8 +33,10 @@ constexpr int KCELLS = 64;  // cells per work item at most (cube_cell_items)
 // per-particle FP64 division).  (Staging each 4^3-cell brick's force nodes in
 // shared memory first was measured twice as slow: at ~500 particles per brick
 // the copies of 17^3 x 3 nodes outweigh the gathers they replace, which hit L1/L2.)
-template <int ZX, int ZV>
-__global__ void __launch_bounds__(256, 2) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
+// IT: the index type of a node within one force component, uint32_t when every
+// component has fewer than 2^32 elements (one wide multiply-add per gather), else size_t
+template <int ZX, int ZV, typename IT>
+__global__ void __launch_bounds__(256, 4) k_kick(const void* __restrict__ xp_, void* __restrict__ vp_,
                                               const int64_t* __restrict__ cell_start, const float* __restrict__ vfield,
                                               int64_t cap, int64_t ncells, int nc, int nt, int nnt,
                                               const float* __restrict__ ff, size_t fcomp, int frp, size_t fplane,
@@ -93,10 +95,19 @@ __global__ void __launch_bounds__(256, 2) k_kick(const void* __restrict__ xp_, v
       gi[e][0] = cube_wrap(m1, nc);
       gi[e][1] = cube_wrap(m1 + 1, nc);
     }
-    const size_t fz[2] = {(size_t)fi[2][0] * fplane, (size_t)fi[2][1] * fplane};
-    const size_t gz[2] = {(size_t)gi[2][0] * cplane, (size_t)gi[2][1] * cplane};
-    const int fy[2] = {fi[1][0] * frp, fi[1][1] * frp}, gy[2] = {gi[1][0] * crp, gi[1][1] * crp};
+    // the eight fine and eight coarse node indices, shared by the three components
+    IT fo[8], go[8];
+    {
+      const IT fz[2] = {(IT)fi[2][0] * (IT)fplane, (IT)fi[2][1] * (IT)fplane};
+      const IT gz[2] = {(IT)gi[2][0] * (IT)cplane, (IT)gi[2][1] * (IT)cplane};
+      const int fy[2] = {fi[1][0] * frp, fi[1][1] * frp}, gy[2] = {gi[1][0] * crp, gi[1][1] * crp};
 #pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        fo[k] = fz[oz[k]] + (IT)(fy[oy[k]] + fi[0][ox[k]]);
+        go[k] = gz[oz[k]] + (IT)(gy[oy[k]] + gi[0][ox[k]]);
+      }
+    }
+#pragma unroll 1
     for (int d = 0; d < 3; ++d) {
       const float* F = ff + d * fcomp;
       const float* G = fc + d * ccomp;
@@ -104,8 +115,8 @@ __global__ void __launch_bounds__(256, 2) k_kick(const void* __restrict__ xp_, v
       float fv[8], gv[8];
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
-        fv[k] = __ldg(&F[fz[oz[k]] + (size_t)(fy[oy[k]] + fi[0][ox[k]])]);
-        gv[k] = __ldg(&G[gz[oz[k]] + (size_t)(gy[oy[k]] + gi[0][ox[k]])]);
+        fv[k] = __ldg(&F[fo[k]]);
+        gv[k] = __ldg(&G[go[k]]);
       }
       const float vf = __ldg(&vfield[(size_t)d * ncells + c]);
       double v = __ldg(&dec_old[code + half_nvbin]);
@@ -117,7 +128,7 @@ __global__ void __launch_bounds__(256, 2) k_kick(const void* __restrict__ xp_, v
         q = cube_fmul(q, oz[k] ? dx2[2] : dx1[2]);
         v = cube_dadd(v, (double)q);
       }
-      const int code1 = cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
+      const int code1 = cube_wrap_code(cube_vencode_step(&codec, tab, v, coef_new), ZV);
       v = __ldg(&dec_new[code1 + half_nvbin]);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -131,7 +142,7 @@ __global__ void __launch_bounds__(256, 2) k_kick(const void* __restrict__ xp_, v
       vm[0] = (d == 0) ? fmaxf(vm[0], am) : vm[0];
       vm[1] = (d == 1) ? fmaxf(vm[1], am) : vm[1];
       vm[2] = (d == 2) ? fmaxf(vm[2], am) : vm[2];
-      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_step(&codec, tab, v, coef_new), ZV);
     }
   }
   // every thread reaches here: warp maxima, then one shared atomic per warp and component
@@ -221,7 +232,7 @@ __global__ void __launch_bounds__(256, 3) k_kick64(const void* __restrict__ xp_,
         const double q = __ldg(&F[fz[oz[k]] + (size_t)(fy[oy[k]] + fi[0][ox[k]])]);
         v += ((q * (ox[k] ? dx2[0] : dx1[0])) * (oy[k] ? dx2[1] : dx1[1])) * (oz[k] ? dx2[2] : dx1[2]);
       }
-      const int code1 = cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
+      const int code1 = cube_wrap_code(cube_vencode_step(&codec, tab, v, coef_new), ZV);
       v = __ldg(&dec_new[code1 + half_nvbin]);
 #pragma unroll
       for (int k = 0; k < 8; ++k) {
@@ -230,7 +241,7 @@ __global__ void __launch_bounds__(256, 3) k_kick64(const void* __restrict__ xp_,
       }
       const float am = (float)fabs(v + (double)vf);
       vm[d] = fmaxf(vm[d], am);
-      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef_new), ZV);
+      vp[(size_t)d * cap + ip] = (TV)cube_wrap_code(cube_vencode_step(&codec, tab, v, coef_new), ZV);
     }
   }
 #pragma unroll
@@ -267,7 +278,8 @@ int launch_kick(cube_ctx* ctx, const cube_scalars* io) {
     CUBE_LAUNCH_CHECK(ctx);
     return CUBE_OK;
   }
-  k_kick<ZX, ZV><<<(unsigned)blocks, 256, 0, ctx->stream>>>(
+  auto kk = (size_t)F.n * F.plane < (size_t(1) << 32) ? k_kick<ZX, ZV, uint32_t> : k_kick<ZX, ZV, size_t>;
+  kk<<<(unsigned)blocks, 256, 0, ctx->stream>>>(
       ctx->xp, ctx->vp, ctx->cell_start, ctx->vfield, ctx->cap, ctx->ncells, ctx->nc, ctx->nt, ctx->nnt, F.force,
       (size_t)F.n * F.plane, F.rp, F.plane, Cc.force, (size_t)Cc.n * Cc.plane, Cc.rp, Cc.plane, dec_old, dec_new,
       ctx->nvbin / 2, ctx->codec, coef_new, cube_venc_tab(ctx), ctx->dscal, ctx->rebin_items,

@@ -46,8 +46,8 @@ constexpr int NOWN = 16 * 16 * 16;        // the brick's own fine cells, numbere
 constexpr int PB_CAP = 4096;              // particles staged per brick in shared memory
 constexpr int PB_SPARSE = 2560;           // up to this many: the chains; above: the fine-cell sort
 constexpr int PP_THREADS = 256;
-constexpr int PP_PMAX = 4096;             // window entries of a group of PP_THREADS targets, evaluated pair-parallel
-constexpr int PP_CH = 256;                // pair terms per shared-memory chunk
+constexpr int PP_PMAX = 4096;             // staged window entries of the block's warps, evaluated pair-parallel
+constexpr int PPW_MAX = PP_PMAX / (PP_THREADS / 32);  // per warp (32 targets)
 
 // fine cell (region coordinates, 0..23) -> sort index: own cells (4..19 in every
 // dimension) first in (z,y,x) order, then the halo cells in raster order
@@ -137,7 +137,7 @@ __device__ __forceinline__ void pp_apply(const double ft[3], const int vc[3], in
     k = cube_ddiv(k, 6.0);
     k = cube_ddiv(k, A.pi_d);
     const double v = cube_dadd(__ldg(&A.dec[vc[d]]), k);
-    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_tab(&A.codec, A.tab, v, A.coef), ZV);
+    vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_step(&A.codec, A.tab, v, A.coef), ZV);
   }
   const double f2 = cube_dadd(cube_dadd(cube_dmul(ft[0], ft[0]), cube_dmul(ft[1], ft[1])), cube_dmul(ft[2], ft[2]));
   acc.f2max = fmaxf(acc.f2max, (float)f2);
@@ -487,21 +487,24 @@ __global__ void __launch_bounds__(PP_THREADS, 2) k_pp_brick(const void* __restri
     const Sorted<uint16_t> S = {nullptr, nullptr, nullptr, nullptr};
     const Chains H = {head, nxt, code};
     const int T = tpre[PB * PB * PB];
-    // Targets in groups of PP_THREADS, one per thread: each counts the entries of its
-    // window (the chains it walks), a scan places them, each writes its entries in
-    // window order, and then all lanes evaluate the FP64 pair terms of the group chunk
-    // by chunk while each thread adds its own terms in that order.  A coincident pair
-    // gives +0, which leaves the running sum unchanged (it is never -0), so the sums
-    // are those of the per-target walk; only the divergent walks stay per target.
-    uint16_t* plist = code + 3 * PB_CAP;                           // PP_PMAX staged indices
-    double* term = reinterpret_cast<double*>(plist + PP_PMAX);     // [3][PP_CH]
-    __shared__ int offs[PP_THREADS + 1];
-    __shared__ double tx1[3][PP_THREADS];
+    // Targets in groups of 32, one group per warp and one target per lane: each lane
+    // counts the entries of its window (the chains it walks), a warp scan places them,
+    // each lane writes its entries in window order (with its lane number beside each),
+    // and then the warp evaluates the FP64 pair terms of its list 32 at a time while
+    // every lane adds its own terms in that order.  A coincident pair gives +0, which
+    // leaves the running sum unchanged (it is never -0), so the sums are those of the
+    // per-target walk.  Warps only meet at __syncwarp; a group whose windows hold more
+    // than PPW_MAX entries walks per target.
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint16_t* plist = code + 3 * PB_CAP + warp * PPW_MAX;                            // staged indices
+    double* term = reinterpret_cast<double*>(code + 3 * PB_CAP + PP_PMAX) + warp * 3 * 32;  // [3][32]
+    uint8_t* ptgt = reinterpret_cast<uint8_t*>(reinterpret_cast<double*>(code + 3 * PB_CAP + PP_PMAX) +
+                                               (PP_THREADS / 32) * 3 * 32) + warp * PPW_MAX;  // lane of each entry
     const bool pow2_cut = (A.nf_cutoff & (A.nf_cutoff - 1)) == 0;
     const double inv_cut = 1.0 / (double)A.nf_cutoff;
     const int pr = A.pr;
-    for (int g0 = 0; g0 < T; g0 += PP_THREADS) {
-      const int t = g0 + (int)threadIdx.x;
+    for (int g0 = warp * 32; g0 < T; g0 += PP_THREADS) {
+      const int t = g0 + lane;
       const bool valid = t < T;
       int cc[3] = {0, 0, 0}, g1[3] = {0, 0, 0}, q = 0, m = 0, nt = 0;
       int64_t ip = 0;
@@ -529,53 +532,42 @@ __global__ void __launch_bounds__(PP_THREADS, 2) k_pp_brick(const void* __restri
               for (int m2 = head[rbase + ii]; m2 != 0xFFFF; m2 = nxt[m2]) ++nt;
           }
       }
-      // exclusive scan of the entry counts over the block
-      {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-        int inc = nt;
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(0xffffffffu, inc, o);
-          if (lane >= o) inc += v;
-        }
-        __shared__ int wsum[PP_THREADS / 32];
-        if (lane == 31) wsum[warp] = inc;
-        __syncthreads();
-        int before = 0;
-        for (int w = 0; w < warp; ++w) before += wsum[w];
-        offs[threadIdx.x] = before + inc - nt;
-        if (threadIdx.x == PP_THREADS - 1) offs[PP_THREADS] = before + inc;
-        __syncthreads();
+      int inc = nt;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
       }
-      const int P = offs[PP_THREADS];
-      if (P > PP_PMAX) {  // too many entries for the shared list: the per-target walk
+      const int off = inc - nt;
+      const int P = __shfl_sync(0xffffffffu, inc, 31);
+      if (P > PPW_MAX) {  // too many entries for the warp's list: the per-target walk
         if (valid) {
           const uint16_t tc[3] = {code[3 * m], code[3 * m + 1], code[3 * m + 2]};
           pp_target<ZX, ZV, true>(S, H, tc, ip, cc, A, vp_, acc);
         }
-        __syncthreads();
         continue;
       }
       if (valid) {
-        int k = offs[threadIdx.x];
+        int k = off;
         for (int kk = g1[2] - pr; kk <= g1[2] + pr; ++kk)
           for (int jj = g1[1] - pr; jj <= g1[1] + pr; ++jj) {
             const int rbase = (kk * PF + jj) * PF;
             for (int ii = g1[0] - pr; ii <= g1[0] + pr; ++ii)
-              for (int m2 = head[rbase + ii]; m2 != 0xFFFF; m2 = nxt[m2]) plist[k++] = (uint16_t)m2;
+              for (int m2 = head[rbase + ii]; m2 != 0xFFFF; m2 = nxt[m2]) {
+                plist[k] = (uint16_t)m2;
+                ptgt[k] = (uint8_t)lane;
+                ++k;
+              }
           }
-#pragma unroll
-        for (int d = 0; d < 3; ++d) tx1[d][threadIdx.x] = x1[d];
       }
-      __syncthreads();
+      __syncwarp();
       double ft[3] = {0.0, 0.0, 0.0};
-      for (int cb = 0; cb < P; cb += PP_CH) {
-        const int ce = min(cb + PP_CH, P);
-        for (int p = cb + (int)threadIdx.x; p < ce; p += PP_THREADS) {
-          int lo = 0, hi = PP_THREADS - 1;  // the target whose entries hold p
-          while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (offs[mid] <= p) lo = mid; else hi = mid - 1;
-          }
+      for (int cb = 0; cb < P; cb += 32) {
+        const int p = cb + lane;
+        const int tg = p < P ? ptgt[p] : lane;
+        double tx[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) tx[d] = __shfl_sync(0xffffffffu, x1[d], tg);
+        if (p < P) {
           const int m2 = plist[p];
           const int f2 = fr[m2];
           const int fi[3] = {f2 % PF, (f2 / PF) % PF, f2 / (PF * PF)};
@@ -584,22 +576,22 @@ __global__ void __launch_bounds__(PP_THREADS, 2) k_pp_brick(const void* __restri
           for (int d = 0; d < 3; ++d) {
             const double cf = 4.0 * (double)(fi[d] >> 2);
             const double frn = cube_xfrac((int32_t)(int16_t)code[3 * m2 + d], ZX);
-            x21[d] = cube_dsub(cube_dadd(cf, cube_dmul(4.0, frn)), tx1[d][lo]);
+            x21[d] = cube_dsub(cube_dadd(cf, cube_dmul(4.0, frn)), tx[d]);
           }
           double fp[3] = {0.0, 0.0, 0.0};
           if (!(x21[0] == 0.0 && x21[1] == 0.0 && x21[2] == 0.0))
             pp_pair(x21, A.mass, A.rsoft, A.nf_cutoff, pow2_cut, inv_cut, fp);
 #pragma unroll
-          for (int d = 0; d < 3; ++d) term[d * PP_CH + (p - cb)] = fp[d];
+          for (int d = 0; d < 3; ++d) term[d * 32 + lane] = fp[d];
         }
-        __syncthreads();
+        __syncwarp();
         if (valid) {
-          const int e0 = max(offs[threadIdx.x], cb), e1 = min(offs[threadIdx.x + 1], ce);
-          for (int p = e0; p < e1; ++p)
+          const int e0 = max(off, cb), e1 = min(off + nt, cb + 32);
+          for (int e = e0; e < e1; ++e)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], term[d * PP_CH + (p - cb)]);
+            for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], term[d * 32 + (e - cb)]);
         }
-        __syncthreads();
+        __syncwarp();
       }
       if (valid) {
         ++acc.n1;
@@ -1038,7 +1030,8 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   if (!ndense) return CUBE_OK;
   // bricks whose region holds a crowded cell: one CTA per brick as before
   const size_t smem =
-      sizeof(uint16_t) * ((size_t)NFC + 5 * (size_t)PB_CAP + PP_PMAX) + sizeof(double) * 3 * (size_t)PP_CH;
+      sizeof(uint16_t) * ((size_t)NFC + 5 * (size_t)PB_CAP + PP_PMAX) + sizeof(double) * 3 * 32 * (PP_THREADS / 32) +
+      (size_t)PP_PMAX;
   auto kb = k_pp_brick<ZX, ZV>;
   CUBE_CUDA_TRY(ctx, cube_smem_limit(kb, smem));
   kb<<<(unsigned)ndense, PP_THREADS, smem, ctx->stream>>>(ctx->xp, ctx->vp, ctx->cell_start, ctx->nc, ctx->nt,

@@ -32,6 +32,7 @@
 #include "cube_internal.cuh"
 
 #include <algorithm>
+#include <cmath>
 
 namespace {
 
@@ -52,6 +53,7 @@ struct RebinArgs {
   const int64_t* items; int64_t items_max;
   const double* dec; int half_nvbin;  // tan(code)/coef per code (cube_vdec_table)
   cube_codec codec; double coef; VencTab tab;
+  double inv_ncell, inv_xstep;  // 1/ncell and 1/(x_resolution*ncell), exact powers of two
   int64_t cap, ncells;
   int nc, nt, nnt, ncb, nte, ncell, nlayer, use_pid;
   float dt_mid;
@@ -157,7 +159,9 @@ __global__ void __launch_bounds__(256) k_rebin_count(RebinArgs A) {
     for (int d = 0; d < 3; ++d) {
       const double fr = cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip], ZX);
       const double v = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + c]));
-      const double dx = cube_ddiv(cube_dmul((double)A.dt_mid, v), (double)A.ncell);
+      // /ncell: ncell = 4 (cube_create), and a quotient by a power of two is the product by
+      // its reciprocal, bit for bit
+      const double dx = cube_dmul(cube_dmul((double)A.dt_mid, v), A.inv_ncell);
       // ig = ceiling(xq + deltax), xq = (i-1) + frac in the coordinates of the tile that keeps it
       int ig = (int)ceil(cube_dadd(cube_dadd((double)l[d], fr), dx));
       int ls = l[d], tt = t[d];
@@ -214,12 +218,12 @@ __device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t i
   const TX* xp = reinterpret_cast<const TX*>(A.xp);
   TX* xp2 = reinterpret_cast<TX*>(A.xp2);
   TV* vp2 = reinterpret_cast<TV*>(A.vp2);
-  const double xstep = cube_dmul(A.codec.x_resolution, (double)A.ncell);
 #pragma unroll
   for (int d = 0; d < 3; ++d) {
-    const int64_t mv = cube_nint(cube_ddiv(cube_dmul((double)A.dt_mid, v[d]), xstep));
+    // /(x_resolution*ncell), a power of two: the product by its reciprocal, bit for bit
+    const int64_t mv = cube_nint(cube_dmul(cube_dmul((double)A.dt_mid, v[d]), A.inv_xstep));
     xp2[(size_t)d * A.cap + slot] = (TX)cube_wrap_code((int64_t)xp[(size_t)d * A.cap + ip] + (int32_t)mv, ZX);
-    const int code = cube_wrap_code(cube_vencode_tab(&A.codec, A.tab, cube_dsub(v[d], (double)vfn[d]), A.coef), ZV);
+    const int code = cube_wrap_code(cube_vencode_step(&A.codec, A.tab, cube_dsub(v[d], (double)vfn[d]), A.coef), ZV);
     vp2[(size_t)d * A.cap + slot] = (TV)code;
   }
   if (A.use_pid) A.pid2[slot] = A.pid[ip];
@@ -751,6 +755,15 @@ int cube_rebin(cube_ctx* ctx, cube_scalars* io) {
   A.cap = ctx->cap; A.ncells = ctx->ncells;
   A.nc = ctx->nc; A.nt = ctx->nt; A.nnt = ctx->nnt; A.ncb = ctx->ncb; A.nte = ctx->nte; A.ncell = ctx->ncell;
   A.nlayer = nlayer; A.use_pid = ctx->P.use_pid; A.dt_mid = io->dt_mid; A.dscal = ctx->dscal;
+  A.inv_ncell = 1.0 / (double)ctx->ncell;
+  A.inv_xstep = 1.0 / (ctx->codec.x_resolution * (double)ctx->ncell);
+  {
+    int e1, e2;  // both divisors must be powers of two for the products to equal the quotients
+    if (std::frexp((double)ctx->ncell, &e1) != 0.5 || std::frexp(ctx->codec.x_resolution * ctx->ncell, &e2) != 0.5) {
+      ctx->err = "re-bin: ncell and x_resolution*ncell must be powers of two";
+      return CUBE_ERR_PARAM;
+    }
+  }
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->rhoc2, 0, sizeof(int32_t) * ctx->ncells, ctx->stream));
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->cursor, 0, sizeof(int32_t) * ctx->ncells, ctx->stream));
   int rc;

@@ -254,7 +254,7 @@ __global__ void k_vdec_build(const float* __restrict__ tan_table, double coef, d
     const double v = cube_vdecode(tan_table[c], coef);
     out[c] = v;
     const int code = c - nvbin / 2;
-    const bool same = cube_wrap_code(cube_vencode_tab(&codec, tab, v, coef), codec.izipv) == code;
+    const bool same = cube_wrap_code(cube_vencode_step(&codec, tab, v, coef), codec.izipv) == code;
     const uint32_t bits = __ballot_sync(0xffffffffu, same);
     if ((threadIdx.x & 31) == 0) fix[c >> 5] = bits;
   }
@@ -291,9 +291,9 @@ const double* cube_vdec_table(cube_ctx* ctx, double coef, int* rc) {
 namespace {
 // velocities spread over the code range: v = tan(pi*(code + off)/(nvbin-1))/coef with
 // off in (-1, 1) drawn from a hash of the index, so that many land near the
-// rounding boundaries code +- 1/2 (within 1.3e-8 of a code, and within 3.3e-5, where
-// the edges of cube_vencode_tab's bands lie); both fast encoders against cube_vencode
-__global__ void k_encode_check(cube_codec codec, VencTab tab, double coef, double inv_pi, int64_t n, uint64_t seed,
+// rounding boundaries code +- 1/2 (within 1.3e-8 of a boundary, the fallback's 1e-9
+// band in q included, and within 3.3e-5); the step's encode against cube_vencode
+__global__ void k_encode_check(cube_codec codec, VencTab tab, double coef, int64_t n, uint64_t seed,
                                unsigned long long* __restrict__ bad) {
   unsigned long long nb = 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -311,7 +311,7 @@ __global__ void k_encode_check(cube_codec codec, VencTab tab, double coef, doubl
     if (fabs(ang) >= 1.5707963) continue;
     const double v = tan(ang) / coef;
     const int32_t ex = cube_vencode(&codec, v, coef);
-    nb += (cube_vencode_fast(&codec, v, coef, inv_pi) != ex) + (cube_vencode_tab(&codec, tab, v, coef) != ex);
+    nb += cube_vencode_step(&codec, tab, v, coef) != ex;
   }
   if (nb) atomicAdd(bad, nb);
 }
@@ -382,7 +382,7 @@ int32_t cube_debug_encode_check(cube_ctx* ctx, int64_t n, uint64_t seed, float s
   unsigned long long* bad = reinterpret_cast<unsigned long long*>(ctx->red_tmp);
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(bad, 0, 8, ctx->stream));
   const double coef = cube_vcoef(&ctx->codec, sigma);
-  k_encode_check<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->codec, cube_venc_tab(ctx), coef, 1.0 / (double)ctx->codec.pi_f, n,
+  k_encode_check<<<ctx->num_sms * 8, 256, 0, ctx->stream>>>(ctx->codec, cube_venc_tab(ctx), coef, n,
                                                             seed, bad);
   CUBE_LAUNCH_CHECK(ctx);
   unsigned long long h = 0;

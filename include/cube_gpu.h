@@ -328,10 +328,9 @@ int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float*
                                    const float* coarse_force);
 
 /* Compares, for n velocities spread over every code and concentrated at the
- * rounding boundaries, the two fast velocity encodes (reciprocal-based, and the
- * code-boundary table with an FP32 first guess that the step uses; both fall back
- * to the exact encode near ties) with the exact FP64 encode under sigma;
- * *mismatches counts the disagreements of either (0 expected). */
+ * rounding boundaries, the step's velocity encode (angle breakpoints from an FP32
+ * first guess, falling back to the exact encode near ties) with the exact FP64
+ * encode under sigma; *mismatches counts the disagreements (0 expected). */
 int32_t cube_debug_encode_check(cube_ctx* ctx, int64_t n, uint64_t seed, float sigma, int64_t* mismatches);
 
 /* Compares, for n quotients shaped like the PP pair term (separation components on
