@@ -235,7 +235,6 @@ void cube_destroy(cube_ctx* ctx) {
   }
   if (ctx->nu.partial) cudaFree(ctx->nu.partial);
   if (ctx->pp_scratch) cudaFree(ctx->pp_scratch);
-  if (ctx->pp_staged) cudaFree(ctx->pp_staged);
   if (ctx->rebin_scratch) cudaFree(ctx->rebin_scratch);
   if (ctx->rebin_mid_scratch) cudaFree(ctx->rebin_mid_scratch);
   if (ctx->dep_scratch) cudaFree(ctx->dep_scratch);
@@ -331,13 +330,6 @@ int32_t cube_create(const cube_params* params, int64_t np_capacity, const float*
   cudaMemset(ctx->dscal, 0, sizeof(DevScal));
   cudaMemset(ctx->pid, 0, 4 * cap);
   int rc;
-  if (P.ext_pp_force && P.nc % 4 == 0) {
-    const size_t nbr = (size_t)(P.nc / 4) * (P.nc / 4) * (P.nc / 4);
-    if (cudaMalloc((void**)&ctx->pp_staged, nbr) != cudaSuccess || cudaMemset(ctx->pp_staged, 0, nbr) != cudaSuccess) {
-      ctx->err = "cudaMalloc of the PP brick flags failed";
-      return fail(CUBE_ERR_CUDA);
-    }
-  }
   if ((rc = alloc_level(ctx, ctx->fine, ctx->nf, P.poisson_fp64))) return fail(rc);
   if ((rc = alloc_level(ctx, ctx->coarse, ctx->nc, P.poisson_fp64))) return fail(rc);
   // FP32 tangent of every velocity code with the C library's tanf (decode table)

@@ -144,7 +144,6 @@ struct cube_ctx {
   double vdec_coef[2] = {0.0, 0.0};
   int vdec_next = 0;
   void* pp_scratch = nullptr;     // sorted particles of crowded PP bricks, grown on demand
-  uint8_t* pp_staged = nullptr;   // per PP brick: staged by k_pp_brick this step (the last step's choice)
   size_t pp_scratch_bytes = 0;
   void* rebin_scratch = nullptr;  // sort slots of re-bin cells beyond 4096 particles, grown on demand
   size_t rebin_scratch_bytes = 0;

@@ -10,14 +10,18 @@
  * is that coarse cell's particles in reverse storage order, filtered by fine
  * cell.
  *
- * Here one CTA takes a brick of 4^3 coarse cells and stages the particles of
- * the brick and of its one-cell halo (6^3 coarse cells, 24^3 fine cells) in
- * shared memory.  A thread takes one target (a particle of the brick) and adds
- * the pair terms of the 27 (or (2 pp_range+1)^3) window cells in the
- * reference's (k,j,i) order, each cell's particles newest-first:
+ * Targets in bricks of 4^3 coarse cells whose region (the brick and a one-cell
+ * halo) holds no cell of more than PP_DENSE particles walk their windows over
+ * per-cell fine-occupancy masks in global memory (k_pp_masks, k_pp_walk below),
+ * 32 targets per warp with the pair terms evaluated pair-parallel.  Crowded
+ * bricks go to k_pp_brick: one CTA stages the particles of the brick and of its
+ * halo (6^3 coarse cells, 24^3 fine cells) in shared memory, and the targets add
+ * the pair terms of the 27 (or (2 pp_range+1)^3) window cells in the reference's
+ * (k,j,i) order, each cell's particles newest-first:
  *   - sparse bricks (up to PB_SPARSE staged) keep the reference's chains: one
  *     thread per region coarse cell threads its particles into per-fine-cell
- *     lists in storage order, and targets go in storage order;
+ *     lists in storage order, and each warp evaluates its 32 targets' entries
+ *     pair-parallel;
  *   - dense bricks sort the staged particles by fine cell (counting sort, each
  *     fine cell's particles newest-first, the brick's own fine cells numbered
  *     first so that the targets are the first T slots), so each window cell is
@@ -27,9 +31,7 @@
  * The pair arithmetic is FP64 as in the reference (xvec* are real(8)), so the
  * kicked codes are bit-identical to the oracle.  Bricks with more than PB_CAP
  * staged particles build the sorted arrays in global memory (one CTA per brick)
- * and spread their targets over many CTAs.  Measured on a 256^3-particle box
- * evolved to z = 0.2 (561M pairs per step): 22 ms per step, against 108 ms with
- * chains alone, where the crowded bricks ran one CTA each.
+ * and spread their targets over many CTAs.
  */
 #include "cube_internal.cuh"
 
@@ -89,6 +91,7 @@ __device__ __forceinline__ void pp_pair(const double x21[3], double mass, double
 struct PPArgs {
   int pr, nf_cutoff;
   double rsoft, mass, a_mid, dt, pi_d, coef;
+  double rcp6, rcp_pi;  // RN(1/6), RN(1/pi_d)
   VencTab tab;
   const double* dec;  // tan(code)/coef per code (cube_vdec_table)
   int half_nvbin;
@@ -134,8 +137,8 @@ __device__ __forceinline__ void pp_apply(const double ft[3], const int vc[3], in
     if (ft[d] == 0.0 && cube_vfixed(A.dec, 2 * A.half_nvbin, vc[d])) continue;
     double k = cube_dmul(ft[d], A.a_mid);
     k = cube_dmul(k, A.dt);
-    k = cube_ddiv(k, 6.0);
-    k = cube_ddiv(k, A.pi_d);
+    k = cube_div_rcp(k, 6.0, A.rcp6);   // the IEEE quotients /6 and /pi (Markstein, one
+    k = cube_div_rcp(k, A.pi_d, A.rcp_pi);  // correctly rounded reciprocal each)
     const double v = cube_dadd(__ldg(&A.dec[vc[d]]), k);
     vp[(size_t)d * A.cap + ip] = (TV)cube_wrap_code(cube_vencode_step(&A.codec, A.tab, v, A.coef), ZV);
   }
@@ -674,28 +677,19 @@ __global__ void __launch_bounds__(PP_THREADS) k_pp_crowd(void* __restrict__ vp_,
   pp_flush(acc, dscal);
 }
 
-// ---- particle-parallel path for sparse bricks -----------------------------------
-// Where most targets of a brick have no other particle in their window (early
-// times, voids), the brick is not staged: its targets are taken one per thread.
+// ---- particle-parallel path (every brick whose region holds no crowded cell) ----
 //   k_pp_masks  one thread per coarse cell: 64-bit masks of the fine cells holding
 //               at least one and at least two particles, and each particle's fine
 //               cell; a cell of more than PP_DENSE particles instead marks every
 //               brick whose region (brick +- 1 cell) holds it as crowded;
-//   k_pp_cells  one thread per coarse cell of a brick that is not crowded: per
-//               target, isolated or not (the masks decide: no other particle in its
-//               window), counted per brick; in a brick left to the particle path an
-//               isolated target has a zero pair sum and is finished there (one window
-//               entry, the zero kick), the others are listed;
-//   k_pp_decide which bricks k_pp_brick takes: the crowded ones and those where the
-//               last step found more than a quarter of the targets with neighbours
-//               (the staged chains serve many neighbours cheaply, a listed target
-//               walks global memory); the same test on this step's counts chooses
-//               for the next step (particles move little in a step; either path gives
-//               the same bits, the choice is only about speed);
-//   k_pp_pairs  one listed target per thread walks its window in the reference's
-//               (k,j,i) order, each fine cell's particles newest-first (reverse
-//               storage order within the coarse cell), so the FP64 sums and the codes
-//               are those of the chains of ext_pp_force.f90:51-73,76-127.
+//   k_pp_walk   the targets of the other bricks over the re-bin's work items, 32 per
+//               warp: each lane walks its window in the reference's (k,j,i) order,
+//               each fine cell's particles newest-first (reverse storage order within
+//               the coarse cell), and records the partners; the warp then evaluates
+//               the FP64 pair terms of all its lanes 32 at a time and every lane adds
+//               its own in walk order, so the sums and the codes are those of the
+//               chains of ext_pp_force.f90:51-73,76-127;
+//   k_pp_crowd_list  the crowded bricks, for k_pp_brick.
 // A target in a brick that is not crowded has its window inside that brick's region,
 // which holds no crowded cell, so no window reads a crowded cell's masks (which are
 // not built) and no scan of a coarse cell takes more than PP_DENSE particles.
@@ -709,11 +703,8 @@ struct PPPar {
   unsigned long long* multi;    // [ncells] fine cells holding two or more
   uint8_t* pfine;               // [cap] each particle's fine cell within its coarse cell
   unsigned int* crowded;        // [nb^3] 1: the brick's region holds a crowded cell
-  unsigned int* nonisol;        // [nb^3] non-isolated targets of the brick
-  unsigned int* ntarget;        // [nb^3] targets of the brick
-  uint8_t* staged;              // [nb^3] persistent: k_pp_brick takes the brick (last step's choice)
-  int32_t* dense_list;          // bricks for k_pp_brick, pp_dense of them
-  int32_t* list_ip;             // listed targets: particle, coarse cell
+  int32_t* dense_list;          // crowded bricks for k_pp_brick, pp_dense of them
+  int32_t* list_ip;             // listed targets (a neighbour in the window): particle, coarse cell
   int32_t* list_cell;
   DevScal* dscal;
 };
@@ -741,10 +732,6 @@ __device__ __forceinline__ void pp_neighbours(int64_t c, int nt, int nnt, int64_
 #pragma unroll
   for (int d = 0; d < 3; ++d) g[d] = t[d] * nt + l[d];
 }
-
-// term of coarse offset o (-1, 0, +1) from the three of pp_neighbours (no indexed
-// local array)
-__device__ __forceinline__ int64_t pp_sel(const int64_t T[3], int o) { return o < 0 ? T[0] : (o > 0 ? T[2] : T[1]); }
 
 // 4-bit mask of the fine cells [lo, hi] (coarse-cell relative) inside coarse offset o
 __device__ __forceinline__ unsigned pp_range4(int lo, int hi, int o) {
@@ -829,6 +816,9 @@ __device__ __forceinline__ bool pp_isolated(const PPPar& Q, int f, int pr, const
   return true;
 }
 
+// one thread per coarse cell of a brick that is not crowded: a target alone in its
+// window (the masks decide) has a zero pair sum and is finished here (one window
+// entry, the zero kick); the others are listed for k_pp_walk
 template <int ZV>
 __global__ void __launch_bounds__(256, 3) k_pp_cells(PPPar Q, PPArgs A, void* __restrict__ vp_) {
   typedef typename CodeT<ZV>::T TV;
@@ -838,25 +828,21 @@ __global__ void __launch_bounds__(256, 3) k_pp_cells(PPPar Q, PPArgs A, void* __
   PPAcc acc;
   unsigned nonmask = 0u;  // targets of this cell with a neighbour (at most PP_DENSE = 32)
   int64_t s0 = 0;
-  int n = 0;
-  bool apply = false;
   if (c < Q.ncells) {
     int64_t X[3], Y[3], Z[3];
     int g[3];
     pp_neighbours(c, Q.nt, Q.nnt, X, Y, Z, g);
     const int b = ((g[2] / PB) * Q.nb + g[1] / PB) * Q.nb + g[0] / PB;
     s0 = Q.cell_start[c];
-    n = (int)(Q.cell_start[c + 1] - s0);
+    const int n = (int)(Q.cell_start[c + 1] - s0);
     if (!Q.crowded[b] && n > 0) {
       const int32_t nb9[9] = {(int32_t)X[0], (int32_t)X[1], (int32_t)X[2], (int32_t)Y[0], (int32_t)Y[1],
                               (int32_t)Y[2], (int32_t)Z[0], (int32_t)Z[1], (int32_t)Z[2]};
-      apply = !Q.staged[b];
       for (int k = 0; k < n; ++k) {
         const int64_t ip = s0 + k;
         if (!pp_isolated(Q, Q.pfine[ip], A.pr, nb9)) {
           nonmask |= 1u << k;
-        } else if (apply) {
-          // a zero pair sum: one window entry (the target), the zero kick
+        } else {
           ++acc.n1;
           ++acc.npair;
           const double ft[3] = {0.0, 0.0, 0.0};
@@ -868,12 +854,9 @@ __global__ void __launch_bounds__(256, 3) k_pp_cells(PPPar Q, PPArgs A, void* __
             pp_apply<ZV>(ft, vc, ip, A, vp_, acc);
         }
       }
-      atomicAdd(&Q.ntarget[b], (unsigned)n);
-      if (nonmask) atomicAdd(&Q.nonisol[b], (unsigned)__popc(nonmask));
     }
   }
-  // list this warp's targets with neighbours in the bricks left to the particle path
-  const unsigned cnt = apply ? (unsigned)__popc(nonmask) : 0u;
+  const unsigned cnt = (unsigned)__popc(nonmask);
   unsigned inc = cnt;
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned v = __shfl_up_sync(0xffffffffu, inc, o);
@@ -893,80 +876,191 @@ __global__ void __launch_bounds__(256, 3) k_pp_cells(PPPar Q, PPArgs A, void* __
   pp_flush(acc, Q.dscal);
 }
 
-// one thread per brick: this step's bricks for k_pp_brick (crowded, or chosen by the
-// last step's counts), and the choice for the next step from this step's counts
-__global__ void k_pp_decide(PPPar Q, int nbricks) {
+// the crowded bricks, for k_pp_brick (one thread per brick)
+__global__ void k_pp_crowd_list(PPPar Q, int nbricks) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbricks) return;
-  const bool crowded = Q.crowded[b] != 0u;
-  if (crowded || Q.staged[b]) Q.dense_list[atomicAdd(&Q.dscal->pp_dense, 1ull)] = b;
-  Q.staged[b] = (crowded || 4u * Q.nonisol[b] > Q.ntarget[b]) ? 1 : 0;
+  if (Q.crowded[b]) Q.dense_list[atomicAdd(&Q.dscal->pp_dense, 1ull)] = b;
 }
 
-// one listed target per thread (grid-stride over the list)
-template <int ZX, int ZV>
-__global__ void __launch_bounds__(256, 3) k_pp_pairs(const void* __restrict__ xp_, const void* vp_in, void* vp_, PPPar Q,
-                                                  PPArgs A) {
-  typedef typename CodeT<ZX>::T TX;
-  typedef typename CodeT<ZV>::T TV;
-  const TX* xp = reinterpret_cast<const TX*>(xp_);
-  const TV* vpr = reinterpret_cast<const TV*>(vp_in);
-  const int64_t n = (int64_t)*(volatile unsigned long long*)&Q.dscal->pp_list;
-  const bool pow2_cut = (A.nf_cutoff & (A.nf_cutoff - 1)) == 0;
-  const double inv_cut = 1.0 / (double)A.nf_cutoff;
-  const int pr = A.pr;
-  PPAcc acc;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t ip = Q.list_ip[k];
-    const int64_t c = Q.list_cell[k];
-    int64_t X[3], Y[3], Z[3];
-    int g[3];
-    pp_neighbours(c, Q.nt, Q.nnt, X, Y, Z, g);
-    const int f = Q.pfine[ip];
-    const int fl[3] = {f & 3, (f >> 2) & 3, (f >> 4) & 3};
-    double x1[3], ft[3] = {0.0, 0.0, 0.0};
-    int vc[3];
+constexpr int PPL = 16;        // window entries per lane for the warp's pair pass
+
+// one target's window walk in the reference's order: calls put(k, ip2, o) for each
+// particle of each window fine cell, newest first; o = (oz+1)*9 + (oy+1)*3 + (ox+1) is
+// the partner's coarse cell offset; returns the number of entries.  A window row
+// (kk, jj) is read as the 4-bit nibble of each coarse cell it crosses (occupancy
+// bits of fine cells x = 0..3), and the particles of an occupied fine cell are found
+// four at a time by a byte compare of the coarse cell's fine-cell bytes, from the top
+template <typename Put>
+__device__ __forceinline__ int pp_walk_window(const PPPar& Q, const int32_t* nb9, int f, int pr, Put put) {
+  const int fl[3] = {f & 3, (f >> 2) & 3, (f >> 4) & 3};
+  unsigned m0[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      x1[d] = cube_dmul(4.0, cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip], ZX));  // coarse-cell relative
-      vc[d] = (int)vpr[(size_t)d * A.cap + ip] + A.half_nvbin;
-    }
-    ++acc.n1;
-    for (int kk = fl[2] - pr; kk <= fl[2] + pr; ++kk) {
-      const int oz = (kk + 4) / 4 - 1;  // floor(kk / 4), kk >= -4
-      const int fz = kk - 4 * oz;
-      for (int jj = fl[1] - pr; jj <= fl[1] + pr; ++jj) {
-        const int oy = (jj + 4) / 4 - 1;
-        const int fy = jj - 4 * oy;
-        const int64_t CYZ = pp_sel(Z, oz) + pp_sel(Y, oy);
-        for (int ii = fl[0] - pr; ii <= fl[0] + pr; ++ii) {
-          const int ox = (ii + 4) / 4 - 1;
-          const int fx = ii - 4 * ox;
-          const int fb = (fz * 4 + fy) * 4 + fx;
-          const int64_t C = CYZ + pp_sel(X, ox);
-          if (!((__ldg(&Q.occ[C]) >> fb) & 1ull)) continue;
-          const double cf[3] = {4.0 * (double)ox, 4.0 * (double)oy, 4.0 * (double)oz};
-          const int64_t s0 = __ldg(&Q.cell_start[C]);
-          for (int64_t ip2 = __ldg(&Q.cell_start[C + 1]) - 1; ip2 >= s0; --ip2) {  // newest first
-            if (Q.pfine[ip2] != fb) continue;
-            ++acc.npair;
-            double x21[3];
+  for (int o = 0; o < 3; ++o) m0[o] = pp_range4(fl[0] - pr, fl[0] + pr, o - 1);
+  const uint32_t* pw = reinterpret_cast<const uint32_t*>(Q.pfine);
+  int n = 0;
+  for (int kk = fl[2] - pr; kk <= fl[2] + pr; ++kk) {
+    const int oz = (kk + 4) / 4 - 1;  // floor(kk / 4), kk >= -4
+    const int fz = kk - 4 * oz;
+    for (int jj = fl[1] - pr; jj <= fl[1] + pr; ++jj) {
+      const int oy = (jj + 4) / 4 - 1;
+      const int fy = jj - 4 * oy;
+      const int64_t CYZ = (int64_t)nb9[6 + oz + 1] + nb9[3 + oy + 1];
+      const int rs = (fz * 4 + fy) * 4;  // bit of fine cell (0, fy, fz)
 #pragma unroll
-            for (int d = 0; d < 3; ++d) {
-              const double fr = cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip2], ZX);
-              x21[d] = cube_dsub(cube_dadd(cf[d], cube_dmul(4.0, fr)), x1[d]);
+      for (int ox = -1; ox <= 1; ++ox) {
+        if (!m0[ox + 1]) continue;
+        const int64_t C = CYZ + nb9[ox + 1];
+        unsigned nib = (unsigned)(__ldg(&Q.occ[C]) >> rs) & m0[ox + 1];
+        if (!nib) continue;
+        const unsigned mnib = (unsigned)(__ldg(&Q.multi[C]) >> rs);
+        const int o = (oz + 1) * 9 + (oy + 1) * 3 + (ox + 1);
+        const int64_t s0 = __ldg(&Q.cell_start[C]), s1 = __ldg(&Q.cell_start[C + 1]);
+        for (; nib; nib &= nib - 1) {
+          const int fx = __ffs(nib) - 1;
+          const uint32_t key = (uint32_t)(rs + fx) * 0x01010101u;
+          const bool one = !((mnib >> fx) & 1u);
+          for (int64_t w = (s1 - 1) >> 2; w >= (s0 >> 2); --w) {  // newest first
+            uint32_t eq = __vcmpeq4(__ldg(&pw[w]), key);
+            const int64_t b0 = w << 2;
+            if (b0 < s0) eq &= 0xFFFFFFFFu << (8 * (int)(s0 - b0));
+            if (b0 + 4 > s1) eq &= 0xFFFFFFFFu >> (8 * (int)(b0 + 4 - s1));
+            bool done = false;
+            while (eq) {
+              const int byte = (31 - __clz(eq)) >> 3;
+              put(n, b0 + byte, o);
+              ++n;
+              eq &= ~(0xFFu << (8 * byte));
+              if (one) { done = true; break; }
             }
-            // a coincident particle (the target itself included) adds exactly +0
-            if (x21[0] == 0.0 && x21[1] == 0.0 && x21[2] == 0.0) continue;
-            double fp[3];
-            pp_pair(x21, A.mass, A.rsoft, A.nf_cutoff, pow2_cut, inv_cut, fp);
-#pragma unroll
-            for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], fp[d]);
+            if (done) break;
           }
         }
       }
     }
-    pp_apply<ZV>(ft, vc, ip, A, vp_, acc);
+  }
+  return n;
+}
+
+// pair term of target position x1 (coarse-cell relative, FP64 exact) and partner ip2 in
+// the coarse cell at offset o; +0 for a coincident particle (the target itself included)
+template <int ZX>
+__device__ __forceinline__ void pp_term(const void* __restrict__ xp_, const PPArgs& A, bool pow2_cut, double inv_cut,
+                                        const double x1[3], int64_t ip2, int o, double fp[3]) {
+  typedef typename CodeT<ZX>::T TX;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  const int od[3] = {o % 3 - 1, (o / 3) % 3 - 1, o / 9 - 1};
+  double x21[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double fr = cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip2], ZX);
+    x21[d] = cube_dsub(cube_dadd(4.0 * (double)od[d], cube_dmul(4.0, fr)), x1[d]);
+  }
+  fp[0] = fp[1] = fp[2] = 0.0;
+  if (!(x21[0] == 0.0 && x21[1] == 0.0 && x21[2] == 0.0))
+    pp_pair(x21, A.mass, A.rsoft, A.nf_cutoff, pow2_cut, inv_cut, fp);
+}
+
+// the listed targets (grid-stride), 32 per warp
+template <int ZX, int ZV>
+__global__ void __launch_bounds__(256, 2) k_pp_walk(const void* __restrict__ xp_, void* __restrict__ vp_, PPPar Q,
+                                                 PPArgs A) {
+  typedef typename CodeT<ZX>::T TX;
+  typedef typename CodeT<ZV>::T TV;
+  const TX* xp = reinterpret_cast<const TX*>(xp_);
+  const TV* vpr = reinterpret_cast<const TV*>(vp_);
+  __shared__ uint32_t rip[8][32 * PPL];   // partners per lane (lane-major)
+  __shared__ uint8_t ro[8][32 * PPL];     // their coarse offsets
+  __shared__ uint8_t ptg[8][32 * PPL];    // lane of each entry of the warp's list
+  __shared__ double term[8][3][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t nlist = (int64_t)*(volatile unsigned long long*)&Q.dscal->pp_list;
+  const bool pow2_cut = (A.nf_cutoff & (A.nf_cutoff - 1)) == 0;
+  const double inv_cut = 1.0 / (double)A.nf_cutoff;
+  const int pr = A.pr;
+  uint32_t* wrip = rip[warp];
+  uint8_t* wro = ro[warp];
+  uint8_t* wtg = ptg[warp];
+  PPAcc acc;
+  for (int64_t base = ((int64_t)blockIdx.x * 8 + warp) * 32; base < nlist; base += (int64_t)gridDim.x * 256) {
+    const int64_t k = base + lane;
+    const bool valid = k < nlist;
+    int64_t ip = 0;
+    int32_t nb9[9];
+    double x1[3] = {0.0, 0.0, 0.0};
+    int n = 0, f = 0;
+    if (valid) {
+      ip = Q.list_ip[k];
+      int64_t X[3], Y[3], Z[3];
+      int g[3];
+      pp_neighbours(Q.list_cell[k], Q.nt, Q.nnt, X, Y, Z, g);
+#pragma unroll
+      for (int t = 0; t < 3; ++t) {
+        nb9[t] = (int32_t)X[t];
+        nb9[3 + t] = (int32_t)Y[t];
+        nb9[6 + t] = (int32_t)Z[t];
+      }
+#pragma unroll
+      for (int d = 0; d < 3; ++d) x1[d] = cube_dmul(4.0, cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip], ZX));
+      f = Q.pfine[ip];
+      n = pp_walk_window(Q, nb9, f, pr, [&](int e, int64_t ip2, int o) {
+        if (e < PPL) {
+          wrip[lane * PPL + e] = (uint32_t)ip2;
+          wro[lane * PPL + e] = (uint8_t)o;
+        }
+      });
+    }
+    const bool over = n > PPL;  // this lane evaluates its walk again on its own
+    const int nl = over ? 0 : n;
+    int inc = nl;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += v;
+    }
+    const int off = inc - nl;
+    const int P = __shfl_sync(0xffffffffu, inc, 31);
+    for (int e = 0; e < nl; ++e) wtg[off + e] = (uint8_t)lane;
+    __syncwarp();
+    double ft[3] = {0.0, 0.0, 0.0};
+    for (int cb = 0; cb < P; cb += 32) {
+      const int p = cb + lane;
+      const int tg = p < P ? wtg[p] : lane;
+      const int toff = __shfl_sync(0xffffffffu, off, tg);
+      double tx[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) tx[d] = __shfl_sync(0xffffffffu, x1[d], tg);
+      if (p < P) {
+        const int e = p - toff;
+        double fp[3];
+        pp_term<ZX>(xp_, A, pow2_cut, inv_cut, tx, (int64_t)wrip[tg * PPL + e], wro[tg * PPL + e], fp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) term[warp][d][lane] = fp[d];
+      }
+      __syncwarp();
+      if (nl) {
+        const int e0 = max(off, cb), e1 = min(off + nl, cb + 32);
+        for (int e = e0; e < e1; ++e)
+#pragma unroll
+          for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], term[warp][d][e - cb]);
+      }
+      __syncwarp();
+    }
+    if (over) {
+      pp_walk_window(Q, nb9, f, pr, [&](int, int64_t ip2, int o) {
+        double fp[3];
+        pp_term<ZX>(xp_, A, pow2_cut, inv_cut, x1, ip2, o, fp);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) ft[d] = cube_dadd(ft[d], fp[d]);
+      });
+    }
+    if (valid) {
+      ++acc.n1;
+      acc.npair += (unsigned long long)n;
+      int vc[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) vc[d] = (int)vpr[(size_t)d * A.cap + ip] + A.half_nvbin;
+      pp_apply<ZV>(ft, vc, ip, A, vp_, acc);
+    }
   }
   pp_flush(acc, Q.dscal);
 }
@@ -985,6 +1079,8 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   A.a_mid = (double)io->a_mid;
   A.dt = (double)io->dt;
   A.pi_d = (double)ctx->codec.pi_f;
+  A.rcp6 = 1.0 / 6.0;
+  A.rcp_pi = 1.0 / A.pi_d;
   A.tab = cube_venc_tab(ctx);
   A.coef = cube_vcoef(&ctx->codec, io->sigma_vi);
   int rc;
@@ -994,8 +1090,8 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   A.codec = ctx->codec;
   A.cap = ctx->cap;
   // re-bin scratch, free outside update_x: per-cell masks in cell_stats, fine cells in
-  // pkey, per-brick flags and counters in cursor, the target list in perm/tcell, and
-  // in big_list the (brick, M) pairs of crowded bricks followed by the dense-brick list
+  // pkey, per-brick flags in cursor, and in big_list the (brick, M) pairs of crowded
+  // bricks followed by the crowded-brick list
   const int nb = ctx->nc / PB;
   const int nbricks = nb * nb * nb;
   int32_t* spill = ctx->big_list;
@@ -1007,22 +1103,19 @@ int launch_pp(cube_ctx* ctx, const cube_scalars* io) {
   Q.multi = Q.occ + ctx->ncells;
   Q.pfine = reinterpret_cast<uint8_t*>(ctx->pkey);
   Q.crowded = reinterpret_cast<unsigned int*>(ctx->cursor);
-  Q.nonisol = Q.crowded + nbricks;
-  Q.ntarget = Q.crowded + 2 * (size_t)nbricks;
-  Q.staged = ctx->pp_staged;
   Q.dense_list = ctx->big_list + 2 * (size_t)nbricks;
   Q.list_ip = ctx->perm;
   Q.list_cell = ctx->tcell;
   Q.dscal = ctx->dscal;
-  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(Q.crowded, 0, 3 * sizeof(unsigned int) * nbricks, ctx->stream));
+  CUBE_CUDA_TRY(ctx, cudaMemsetAsync(Q.crowded, 0, sizeof(unsigned int) * nbricks, ctx->stream));
   const unsigned cblocks = (unsigned)((ctx->ncells + 255) / 256);
   k_pp_masks<ZX><<<cblocks, 256, 0, ctx->stream>>>(ctx->xp, ctx->cap, Q);
   CUBE_LAUNCH_CHECK(ctx);
   k_pp_cells<ZV><<<cblocks, 256, 0, ctx->stream>>>(Q, A, ctx->vp);
   CUBE_LAUNCH_CHECK(ctx);
-  k_pp_decide<<<(unsigned)((nbricks + 255) / 256), 256, 0, ctx->stream>>>(Q, nbricks);
+  k_pp_walk<ZX, ZV><<<(unsigned)(4 * ctx->num_sms), 256, 0, ctx->stream>>>(ctx->xp, ctx->vp, Q, A);
   CUBE_LAUNCH_CHECK(ctx);
-  k_pp_pairs<ZX, ZV><<<(unsigned)(4 * ctx->num_sms), 256, 0, ctx->stream>>>(ctx->xp, ctx->vp, ctx->vp, Q, A);
+  k_pp_crowd_list<<<(unsigned)((nbricks + 255) / 256), 256, 0, ctx->stream>>>(Q, nbricks);
   CUBE_LAUNCH_CHECK(ctx);
   unsigned long long ndense = 0;
   CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(&ndense, &ctx->dscal->pp_dense, 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1100,7 +1193,7 @@ int cube_pp(cube_ctx* ctx, cube_scalars* io) {
     ctx->err = "pp_range must be in 0..4";
     return CUBE_ERR_PARAM;
   }
-  if (!ctx->pp_staged) {
+  if (!ctx->P.ext_pp_force) {
     ctx->err = "the context was created with PP off";
     return CUBE_ERR_PARAM;
   }
