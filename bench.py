@@ -318,6 +318,7 @@ def run_ours(args, cfg, rank, world, local_rank):
             ev1.record(stream)
         torch.cuda.synchronize()
     nu_timed = nu_ms[0]  # the end-to-end leg below runs step() again
+    npairs_timed = int(getattr(s, "npairs", 0))  # PP window entries of the last timed step
     ms = ev0.elapsed_time(ev1)
     launches = cube.launch_count() - l0
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
@@ -377,7 +378,7 @@ def run_ours(args, cfg, rank, world, local_rank):
     if getattr(args, "cufft", False) and world == 1:
         cufft = cufft_comparison(cube, 4 * cfg["nc"])
     return dict(cufft=cufft, ms=ms_max, npart=npart, launches=launches, phase_ms=phase_sum / args.steps, clocks=clk.summary(),
-                e2e_ms=e2e_ms, e2e_steps=e2e_steps, h2d=h2d, d2h=h2d, scal=s.as_dict())
+                e2e_ms=e2e_ms, e2e_steps=e2e_steps, h2d=h2d, d2h=h2d, scal=s.as_dict(), npairs=npairs_timed)
 
 
 def cufft_comparison(cube, nf: int, reps: int = 5) -> dict:
@@ -817,6 +818,12 @@ def main():
                      "algorithmic_bytes": ab[dom]},
         "phases_ms": phases, "phase_gbs": phase_gbs, "clocks": r["clocks"],
     }
+    if cfg["pp"]:
+        # window entries the PP walks in the last timed step (ext_pp_force.f90's npairs: every
+        # particle of every window fine cell, the target included) and their rate in the PP phase
+        npairs = r["npairs"]
+        line["pp"] = {"pairs_per_step": npairs, "pairs_per_particle": npairs / r["npart"],
+                      "pairs_per_s": npairs / (phases["ext_pp_force"] / 1e3) if phases["ext_pp_force"] > 0 else None}
     if r.get("cufft"):
         line["cufft_comparison"] = r["cufft"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

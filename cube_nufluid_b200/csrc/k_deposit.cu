@@ -321,22 +321,23 @@ template <typename RT>
 __global__ void k_coarse_finalize(unsigned long long* __restrict__ acc, unsigned long long* __restrict__ acc_nu,
                                   RT* __restrict__ r3, int nc, int rp, double unit_c,
                                   unsigned long long* __restrict__ mass_total) {
-  const int64_t n = (int64_t)nc * nc * nc;
+  const int64_t rows = (int64_t)nc * nc;  // (y, z) rows of nc nodes, one row per block at a time
   unsigned long long msum = 0ull, nsum = 0ull;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const unsigned long long a = acc[i];
-    acc[i] = 0ull;
-    msum += a >> 6;
-    double v = (double)a * unit_c;
-    if (acc_nu) {
-      const unsigned long long b = acc_nu[i];
-      acc_nu[i] = 0ull;
-      nsum += b;
-      v = v + (double)b * (1.0 / FIX_SCALE);
+  for (int64_t yz = blockIdx.x; yz < rows; yz += gridDim.x)
+    for (int x = threadIdx.x; x < nc; x += blockDim.x) {
+      const int64_t i = yz * nc + x;
+      const unsigned long long a = acc[i];
+      acc[i] = 0ull;
+      msum += a >> 6;
+      double v = (double)a * unit_c;
+      if (acc_nu) {
+        const unsigned long long b = acc_nu[i];
+        acc_nu[i] = 0ull;
+        nsum += b;
+        v = v + (double)b * (1.0 / FIX_SCALE);
+      }
+      r3[yz * rp + x] = (RT)v;
     }
-    const int64_t x = i % nc, yz = i / nc;
-    r3[yz * rp + x] = (RT)v;
-  }
   for (int o = 16; o > 0; o >>= 1) {
     msum += __shfl_xor_sync(0xffffffffu, msum, o);
     nsum += __shfl_xor_sync(0xffffffffu, nsum, o);
@@ -414,11 +415,11 @@ int cube_deposit(cube_ctx* ctx, cube_scalars* io) {
   }
   const double unit_c = (double)io->mass_p_cdm * (1.0 / (64.0 * FIX_SCALE));  // exact
   if (ctx->coarse.fp64)
-    k_coarse_finalize<double><<<592, 256, 0, ctx->stream>>>(ctx->rho_c_acc, nullptr,
+    k_coarse_finalize<double><<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(ctx->rho_c_acc, nullptr,
                                                             reinterpret_cast<double*>(ctx->coarse.rho), nc,
                                                             ctx->coarse.rp, unit_c, mtot + 1);
   else
-    k_coarse_finalize<float><<<592, 256, 0, ctx->stream>>>(ctx->rho_c_acc, ctx->nu.on ? ctx->rho_c_nu : nullptr,
+    k_coarse_finalize<float><<<8 * ctx->num_sms, 256, 0, ctx->stream>>>(ctx->rho_c_acc, ctx->nu.on ? ctx->rho_c_nu : nullptr,
                                                            ctx->coarse.rho, nc, ctx->coarse.rp, unit_c, mtot + 1);
   CUBE_LAUNCH_CHECK(ctx);
   return CUBE_OK;

@@ -883,7 +883,7 @@ __global__ void k_pp_crowd_list(PPPar Q, int nbricks) {
   if (Q.crowded[b]) Q.dense_list[atomicAdd(&Q.dscal->pp_dense, 1ull)] = b;
 }
 
-constexpr int PPL = 16;        // window entries per lane for the warp's pair pass
+constexpr int PPL = 24;        // window entries per lane for the warp's pair pass
 
 // one target's window walk in the reference's order: calls put(k, ip2, o) for each
 // particle of each window fine cell, newest first; o = (oz+1)*9 + (oy+1)*3 + (ox+1) is
