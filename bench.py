@@ -218,17 +218,24 @@ def nu_params_for(cfg):
                        z_i_nu=10.0, omega_m=0.3, omega_l=0.7, h0=NU_H)
 
 
-# DRAM bytes per step and phase (dram__bytes_read.sum + dram__bytes_write.sum summed
-# over the phase's kernels), measured with
-#   ncu --metrics gpu__time_duration.sum,dram__bytes_read.sum,dram__bytes_write.sum \
-#       --clock-control none -c 400 --csv python bench.py --config <c> --steps 1 --warmup 3
-# over the five steps that command runs; the roofline's "traffic" field.
-MEASURED_DRAM_BYTES = {
-    "c2": {"update_x": 21.063e9, "ext_pp_force": 2.530e9, "deposit": 5.916e9, "fine_fft_green": 87.852e9,
-           "coarse_fft_green": 1.055e9, "kick": 15.925e9},
-    "c3": {"update_x": 21.271e9, "ext_pp_force": 2.534e9, "deposit": 28.351e9, "fine_fft_green": 87.852e9,
-           "coarse_fft_green": 1.055e9, "kick": 16.283e9, "nu_fluid": 80.798e9},
-}
+# DRAM bytes per step and phase (dram__bytes_read.sum + dram__bytes_write.sum of the
+# phase's kernels) from single-kernel ncu captures of the 256^3-particle case (c2s),
+# summarised with their commands in profiles/: the fine solve is x r2c, four y passes
+# (forward and three inverse, each as the forward one), z + Green and the c2r of the
+# three components; the kick is one launch.  Particle counts and mesh sizes both grow
+# by 8 from c2s to c2 (and the fine mesh is the same in c3), so these scale with the
+# particle count; phases without a capture of every kernel have none.
+TRAFFIC_C2S = {"fine_fft_green": (0.537 + 0.492) + 4 * (0.539 + 0.492) + (0.743 + 1.568) + (1.711 + 1.554),
+               "kick": 1.894 + 0.100, "deposit": 0.135 + 0.498}  # GB per step at 256^3 particles
+
+
+def phase_traffic(config, phase, npart):
+    """DRAM bytes per step of a phase, scaled from the c2s captures (None if not captured)."""
+    if config not in ("c2", "c2s", "c3", "c3s") or phase not in TRAFFIC_C2S:
+        return None
+    if config in ("c3", "c3s") and phase != "fine_fft_green":
+        return None  # the neutrino densities and sources change the other phases
+    return TRAFFIC_C2S[phase] * 1e9 * npart / 256 ** 3
 
 
 def algorithmic_bytes(cfg, npart):
@@ -814,7 +821,9 @@ def main():
         "gpu_launches": int(r["launches"]),
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
                      "frac": ach / peak, "peak_kind": peak_kind,
-                     "traffic": MEASURED_DRAM_BYTES.get(args.config, {}).get(dom),
+                     "traffic": phase_traffic(args.config, dom, r["npart"]),
+                     "traffic_source": "ncu DRAM bytes of the phase's kernels at 256^3 particles, scaled by the "
+                                       "particle count (profiles/)",
                      "algorithmic_bytes": ab[dom]},
         "phases_ms": phases, "phase_gbs": phase_gbs, "clocks": r["clocks"],
     }
