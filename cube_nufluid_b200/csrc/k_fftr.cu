@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(8 * T) k_row_inplace(float2* __restrict__ data
 // x c2r of the three force components (S4 rows of RB row pairs, in place) with
 // max f^2, as k_xc2r3 but loading the half spectra straight into registers
 template <int N, int R, int T, int RB>
-__global__ void __launch_bounds__(3 * T * RB) k_xc2r3_t(float* __restrict__ data, size_t comp_stride, int rp,
+__global__ void __launch_bounds__(3 * T * RB, 4) k_xc2r3_t(float* __restrict__ data, size_t comp_stride, int rp,
                                                         int npairs, const float2* __restrict__ tw,
                                                         unsigned int* __restrict__ f2_bits) {
   extern __shared__ float2 sm[];

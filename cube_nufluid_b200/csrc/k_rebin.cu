@@ -144,51 +144,74 @@ __global__ void __launch_bounds__(256) k_rebin_count(RebinArgs A) {
     ctt[i][2] = tb[2] / nt;
   }
   __syncthreads();
-  for (int64_t ip = p0 + threadIdx.x; ip < p1; ip += blockDim.x) {
-    int lo = 0, hi = ncl - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
-    }
-    const int64_t c = c0 + lo;
-    const int l[3] = {cl[lo][0], cl[lo][1], cl[lo][2]};
-    const int t[3] = {ctt[lo][0], ctt[lo][1], ctt[lo][2]};
-    int tg[3], src[3];
-    bool bad = false;
+  typedef typename CodeT<ZV>::T TV;
+  const TV* vp = reinterpret_cast<const TV*>(A.vp);
+  // two particles per thread, their code and cell-mean reads issued together
+  for (int64_t ib = p0 + threadIdx.x; ib < p1; ib += 2 * blockDim.x) {
+    int lov[2];
+    int xcv[2][3];
+    double vv[2][3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const double fr = cube_xfrac((int32_t)xp[(size_t)d * A.cap + ip], ZX);
-      const double v = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + c]));
-      // /ncell: ncell = 4 (cube_create), and a quotient by a power of two is the product by
-      // its reciprocal, bit for bit
-      const double dx = cube_dmul(cube_dmul((double)A.dt_mid, v), A.inv_ncell);
-      // ig = ceiling(xq + deltax), xq = (i-1) + frac in the coordinates of the tile that keeps it
-      int ig = (int)ceil(cube_dadd(cube_dadd((double)l[d], fr), dx));
-      int ls = l[d], tt = t[d];
-      if (ig < 1 || ig > nt) {
-        const int sh = floordiv(ig - 1, nt);
-        ls = l[d] - sh * nt;
-        tt = ((t[d] + sh) % nnt + nnt) % nnt;
-        const int ig2 = (int)ceil(cube_dadd(cube_dadd((double)ls, fr), dx));
-        if (ig2 >= 1 && ig2 <= nt) ig = ig2;
-        else { ig = ig - sh * nt; atomicAdd(&A.dscal->moved_far, 1ull); }
+    for (int u = 0; u < 2; ++u) {
+      const int64_t q = ib + u * (int64_t)blockDim.x < p1 ? ib + u * (int64_t)blockDim.x : ib;
+      int lo = 0, hi = ncl - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cs[mid] <= q) lo = mid; else hi = mid - 1;
       }
-      if (ls + 1 < 1 - ncb || ls + 1 > nt + ncb) bad = true;
-      tg[d] = tt * nt + ig - 1;
-      src[d] = ls + ncb;  // 0-based index in the target tile's extended range
+      lov[u] = lo;
+      const int64_t c = c0 + lo;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        xcv[u][d] = (int32_t)xp[(size_t)d * A.cap + q];
+        vv[u][d] = cube_dadd(__ldg(&A.dec[(int)vp[(size_t)d * A.cap + q] + A.half_nvbin]),
+                             (double)__ldg(&A.vfield[(size_t)d * A.ncells + c]));
+      }
     }
-    if (bad) {
-      cube_dev_error(A.dscal, CUBE_ERR_MOVE, (int)(ip & 0x7fffffff));
-      src[0] = min(max(src[0], 0), nte - 1);
-      src[1] = min(max(src[1], 0), nte - 1);
-      src[2] = min(max(src[2], 0), nte - 1);
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int64_t ip = ib + u * (int64_t)blockDim.x;
+      if (ip >= p1) continue;
+      const int lo = lov[u];
+      const int l[3] = {cl[lo][0], cl[lo][1], cl[lo][2]};
+      const int t[3] = {ctt[lo][0], ctt[lo][1], ctt[lo][2]};
+      int tg[3], src[3];
+      bool bad = false;
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const double fr = cube_xfrac(xcv[u][d], ZX);
+        const double v = vv[u][d];
+        // /ncell: ncell = 4 (cube_create), and a quotient by a power of two is the product by
+        // its reciprocal, bit for bit
+        const double dx = cube_dmul(cube_dmul((double)A.dt_mid, v), A.inv_ncell);
+        // ig = ceiling(xq + deltax), xq = (i-1) + frac in the coordinates of the tile that keeps it
+        int ig = (int)ceil(cube_dadd(cube_dadd((double)l[d], fr), dx));
+        int ls = l[d], tt = t[d];
+        if (ig < 1 || ig > nt) {
+          const int sh = floordiv(ig - 1, nt);
+          ls = l[d] - sh * nt;
+          tt = ((t[d] + sh) % nnt + nnt) % nnt;
+          const int ig2 = (int)ceil(cube_dadd(cube_dadd((double)ls, fr), dx));
+          if (ig2 >= 1 && ig2 <= nt) ig = ig2;
+          else { ig = ig - sh * nt; atomicAdd(&A.dscal->moved_far, 1ull); }
+        }
+        if (ls + 1 < 1 - ncb || ls + 1 > nt + ncb) bad = true;
+        tg[d] = tt * nt + ig - 1;
+        src[d] = ls + ncb;  // 0-based index in the target tile's extended range
+      }
+      if (bad) {
+        cube_dev_error(A.dscal, CUBE_ERR_MOVE, (int)(ip & 0x7fffffff));
+        src[0] = min(max(src[0], 0), nte - 1);
+        src[1] = min(max(src[1], 0), nte - 1);
+        src[2] = min(max(src[2], 0), nte - 1);
+      }
+      const int64_t tc = cube_cell_of(tg[0], tg[1], tg[2], nt, nnt);
+      const uint32_t layer = (uint32_t)(src[2] % A.nlayer);
+      const uint32_t key = ((layer * nte + src[2]) * nte + src[1]) * nte + src[0];
+      A.tcell[ip] = (int32_t)tc;
+      A.tkey[ip] = key;
+      atomicAdd(&A.cnt2[tc], 1);
     }
-    const int64_t tc = cube_cell_of(tg[0], tg[1], tg[2], nt, nnt);
-    const uint32_t layer = (uint32_t)(src[2] % A.nlayer);
-    const uint32_t key = ((layer * nte + src[2]) * nte + src[1]) * nte + src[0];
-    A.tcell[ip] = (int32_t)tc;
-    A.tkey[ip] = key;
-    atomicAdd(&A.cnt2[tc], 1);
   }
 }
 
@@ -209,24 +232,6 @@ __device__ __forceinline__ int64_t src_cell(const RebinArgs& A, uint32_t key, co
   const int gy = cube_wrap(tt[1] * nt + j - ncb, nc);
   const int gz = cube_wrap(tt[2] * nt + k - ncb, nc);
   return cube_cell_of(gx, gy, gz, nt, A.nnt);
-}
-
-template <int ZX, int ZV>
-__device__ __forceinline__ void emit(const RebinArgs& A, int64_t slot, int64_t ip, const double v[3], const float vfn[3]) {
-  typedef typename CodeT<ZX>::T TX;
-  typedef typename CodeT<ZV>::T TV;
-  const TX* xp = reinterpret_cast<const TX*>(A.xp);
-  TX* xp2 = reinterpret_cast<TX*>(A.xp2);
-  TV* vp2 = reinterpret_cast<TV*>(A.vp2);
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    // /(x_resolution*ncell), a power of two: the product by its reciprocal, bit for bit
-    const int64_t mv = cube_nint(cube_dmul(cube_dmul((double)A.dt_mid, v[d]), A.inv_xstep));
-    xp2[(size_t)d * A.cap + slot] = (TX)cube_wrap_code((int64_t)xp[(size_t)d * A.cap + ip] + (int32_t)mv, ZX);
-    const int code = cube_wrap_code(cube_vencode_step(&A.codec, A.tab, cube_dsub(v[d], (double)vfn[d]), A.coef), ZV);
-    vp2[(size_t)d * A.cap + slot] = (TV)code;
-  }
-  if (A.use_pid) A.pid2[slot] = A.pid[ip];
 }
 
 __device__ __forceinline__ void cell_tile(const RebinArgs& A, int64_t c, int tt[3]) {
@@ -607,30 +612,66 @@ __global__ void __launch_bounds__(1024) k_rebin_huge_order(RebinArgs A) {
 // statistics terms are formed from the new codes by the tree pass (k_stats_first)
 template <int ZX, int ZV>
 __global__ void __launch_bounds__(256) k_rebin_emit(RebinArgs A, int64_t np) {
+  typedef typename CodeT<ZX>::T TX;
+  typedef typename CodeT<ZV>::T TV;
+  const TX* xp = reinterpret_cast<const TX*>(A.xp);
+  const TV* vp = reinterpret_cast<const TV*>(A.vp);
+  TX* xp2 = reinterpret_cast<TX*>(A.xp2);
+  TV* vp2 = reinterpret_cast<TV*>(A.vp2);
   __shared__ int64_t cs[RCELLS + 1];
   int64_t c0, p0, p1;
   int ncl;
   if (!get_item(A, c0, ncl, p0, p1)) return;
   for (int i = threadIdx.x; i <= ncl; i += blockDim.x) cs[i] = A.cell_start[c0 + i];
   __syncthreads();
-  for (int64_t ip = p0 + threadIdx.x; ip < p1; ip += blockDim.x) {
-    int lo = 0, hi = ncl - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (cs[mid] <= ip) lo = mid; else hi = mid - 1;
-    }
-    const int64_t sc = c0 + lo;  // the particle's cell before the drift
-    const int64_t c = A.tcell[ip];
-    const int64_t slot = A.tkey[ip];
-    if (slot >= np) continue;  // its cell overflowed the sorter (error reported)
-    double v[3];
-    float vfn[3];
+  // two particles per thread, their reads issued together (each read depends on one
+  // before it at most: slot and new cell, codes, then the decode table and cell means)
+  for (int64_t ib = p0 + threadIdx.x; ib < p1; ib += 2 * blockDim.x) {
+    int64_t ip[2], sc[2], c[2], slot[2];
+    int vc[2][3], xc[2][3];
+    int32_t pv[2];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      v[d] = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
-      vfn[d] = A.vfield2[(size_t)d * A.ncells + c];
+    for (int u = 0; u < 2; ++u) {
+      ip[u] = ib + u * (int64_t)blockDim.x;
+      const int64_t q = ip[u] < p1 ? ip[u] : ib;
+      int lo = 0, hi = ncl - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cs[mid] <= q) lo = mid; else hi = mid - 1;
+      }
+      sc[u] = c0 + lo;  // the particle's cell before the drift
+      c[u] = A.tcell[q];
+      slot[u] = A.tkey[q];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        vc[u][d] = (int)vp[(size_t)d * A.cap + q];
+        xc[u][d] = (int)xp[(size_t)d * A.cap + q];
+      }
+      pv[u] = A.use_pid ? A.pid[q] : 0;
     }
-    emit<ZX, ZV>(A, slot, ip, v, vfn);
+    double v[2][3];
+    float vfn[2][3];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        v[u][d] = cube_dadd(__ldg(&A.dec[vc[u][d] + A.half_nvbin]), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc[u]]));
+        vfn[u][d] = A.vfield2[(size_t)d * A.ncells + c[u]];
+      }
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      if (ip[u] >= p1 || slot[u] >= np) continue;  // past the item, or its cell overflowed the sorter (error reported)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        // /(x_resolution*ncell), a power of two: the product by its reciprocal, bit for bit
+        const int64_t mv = cube_nint(cube_dmul(cube_dmul((double)A.dt_mid, v[u][d]), A.inv_xstep));
+        xp2[(size_t)d * A.cap + slot[u]] = (TX)cube_wrap_code((int64_t)xc[u][d] + (int32_t)mv, ZX);
+        const int code =
+            cube_wrap_code(cube_vencode_step(&A.codec, A.tab, cube_dsub(v[u][d], (double)vfn[u][d]), A.coef), ZV);
+        vp2[(size_t)d * A.cap + slot[u]] = (TV)code;
+      }
+      if (A.use_pid) A.pid2[slot[u]] = pv[u];
+    }
   }
 }
 
