@@ -598,29 +598,34 @@ def run_ensemble(args, cfg):
     ens = Ensemble(specs)
     workers = 16
     clk = ClockSampler(local_rank).start()
-    ens.run(args.warmup, workers=workers)
+    ens.run_native(args.warmup, workers=workers)
     torch.cuda.synchronize()
     l0 = sum(m.cube.launch_count() for m in ens.members)
     with clk:
-        r = ens.run(args.steps, workers=workers)
+        r = ens.run_native(args.steps, workers=workers)
         torch.cuda.synchronize()
     launches = sum(m.cube.launch_count() for m in ens.members) - l0
     npart = sum(sp.particles for sp in specs)
-    # the same boxes one at a time (one host thread, each step returns before the next
-    # box starts): the sequential rate the concurrent ensemble is compared with
+    # the same boxes one at a time (one thread, each box-step returns before the next
+    # starts): the sequential rate the concurrent ensemble is compared with; and the
+    # boxes stepped from Python threads instead of the library's pool
     seq_steps = max(1, min(args.steps, 2))
-    seq = ens.run(seq_steps, workers=1)
+    seq = ens.run_native(seq_steps, workers=1)
+    pyt = ens.run(seq_steps, workers=workers)
     torch.cuda.synchronize()
     line = {"metric": "ensemble box-steps/s", "value": r["box_steps_per_s"], "unit": "box-steps/s",
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": r["wall_s"] * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": cfg["workload"], "boxes": len(specs), "particles_total": npart,
-                       "workers": r["workers"], "parallelism": "boxes on concurrent streams",
+                       "workers": r["workers"], "parallelism": "boxes on concurrent streams, stepped by the "
+                                                          "library's thread pool (cube_run_steps)",
                        "timing": "host wall clock between device synchronisations (one stream per box)"},
             "particle_updates_per_s": r["particle_updates_per_s"], "gpu_launches": int(launches),
             "sequential": {"box_steps_per_s": seq["box_steps_per_s"], "steps": seq_steps, "workers": 1},
             "vs_sequential": r["box_steps_per_s"] / seq["box_steps_per_s"],
+            "python_threads": {"box_steps_per_s": pyt["box_steps_per_s"], "steps": seq_steps,
+                               "workers": pyt["workers"]},
             "clocks": clk.summary()}
     ens.close()
     if rank == 0:

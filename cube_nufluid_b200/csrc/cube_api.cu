@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 static std::string g_create_error;
 
@@ -852,6 +853,55 @@ int32_t cube_debug_kick_with_force(cube_ctx* ctx, cube_scalars* io, const float*
   for (int d = 0; d < 3; ++d) io->vmax[d] = uint_as_float(ctx->hscal->vmax_bits[d]);
   io->sigma_vi = io->sigma_vi_new;
   return CUBE_OK;
+}
+
+// One box-step of main.f90:49-64 on one context (the order of Cube.step): timestep,
+// neutrino half step, drift, PP, particle mesh, neutrino half step.
+static int32_t run_one_step(cube_ctx* ctx, cube_scalars* io) {
+  int32_t hit = 0;
+  int32_t rc = cube_timestep(&ctx->P, io, 0.0f, &hit);
+  if (!rc && ctx->nu.on) rc = cube_nu_evolve(ctx, io->dt / 2.0f, &io->dt_neu, 1, io->a_mid);
+  if (!rc) rc = cube_update_x(ctx, io);
+  if (!rc && ctx->P.ext_pp_force) rc = cube_ext_pp_force(ctx, io);
+  if (!rc) rc = cube_particle_mesh(ctx, io);
+  if (!rc && ctx->nu.on) rc = cube_nu_evolve(ctx, io->dt / 2.0f, &io->dt_neu, -1, io->a_mid);
+  return rc;
+}
+
+int32_t cube_run_steps(cube_ctx* const* ctxs, cube_scalars* ios, int32_t n, int32_t steps, int32_t threads,
+                       int32_t* failed) {
+  if (failed) *failed = -1;
+  if (!ctxs || !ios || n < 0 || steps < 0 || threads < 1) return CUBE_ERR_PARAM;
+  for (int32_t i = 0; i < n; ++i)
+    if (!ctxs[i] || !ctxs[i]->state_loaded) {
+      if (failed) *failed = i;
+      return ctxs[i] ? CUBE_ERR_STATE : CUBE_ERR_PARAM;
+    }
+  const int32_t nt = std::min(threads, std::max(n, 1));
+  std::vector<int32_t> st(nt, CUBE_OK), at(nt, -1);
+  auto work = [&](int32_t t) {
+    for (int32_t k = 0; k < steps; ++k)
+      for (int32_t i = t; i < n; i += nt) {
+        const int32_t rc = run_one_step(ctxs[i], &ios[i]);
+        if (rc) {
+          st[t] = rc;
+          at[t] = i;
+          return;
+        }
+      }
+  };
+  std::vector<std::thread> pool;
+  for (int32_t t = 1; t < nt; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto& th : pool) th.join();
+  int32_t rc = CUBE_OK, first = -1;
+  for (int32_t t = 0; t < nt; ++t)
+    if (st[t] && (first < 0 || at[t] < first)) {
+      first = at[t];
+      rc = st[t];
+    }
+  if (failed) *failed = first;
+  return rc;
 }
 
 }  // extern "C"

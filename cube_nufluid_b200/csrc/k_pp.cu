@@ -818,7 +818,10 @@ __device__ __forceinline__ bool pp_isolated(const PPPar& Q, int f, int pr, const
 
 // one thread per coarse cell of a brick that is not crowded: a target alone in its
 // window (the masks decide) has a zero pair sum and is finished here (one window
-// entry, the zero kick); the others are listed for k_pp_walk
+// entry, the zero kick); the others are listed for k_pp_walk.  (One thread per
+// target over the re-bin's work items left 7 of 32 lanes active in the branching
+// window test; one CTA per brick with the 6^3 masks of brick and halo staged in
+// shared memory read the halo 3.4 times over: both slower at 512^3.)
 template <int ZV>
 __global__ void __launch_bounds__(256, 3) k_pp_cells(PPPar Q, PPArgs A, void* __restrict__ vp_) {
   typedef typename CodeT<ZV>::T TV;

@@ -54,6 +54,8 @@ def load_library():
     L.cube_create.restype = C.c_int32
     L.cube_load_state.argtypes = [vp, C.c_int64, vp, vp, vp, vp, vp]
     L.cube_load_state.restype = C.c_int32
+    L.cube_run_steps.argtypes = [C.POINTER(vp), S, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_int32)]
+    L.cube_run_steps.restype = C.c_int32
     L.cube_store_state.argtypes = [vp, C.POINTER(C.c_int64), vp, vp, vp, vp, vp]
     L.cube_store_state.restype = C.c_int32
     for name in ("cube_update_x", "cube_ext_pp_force", "cube_particle_mesh"):

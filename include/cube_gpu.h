@@ -163,6 +163,18 @@ int32_t cube_particle_mesh(cube_ctx* ctx, cube_scalars* io);
  * which is also the prescribed-step mode.  Returns 1 in *hit if a_next was hit. */
 int32_t cube_timestep(const cube_params* params, cube_scalars* io, float a_next, int32_t* hit);
 
+/* Steps n independent contexts (an ensemble of boxes) `steps` times each on a pool
+ * of `threads` host threads, boxes dealt round-robin: every box-step is the order
+ * of main.f90:49-64 (cube_timestep in its adaptive form, the neutrino half steps if
+ * the context has fluid neutrinos, cube_update_x, cube_ext_pp_force if enabled,
+ * cube_particle_mesh) on that context's stream and ios[i].  No counterpart in the
+ * reference, which runs one box per job; it lets a host step many small boxes
+ * without a thread of its own per box.  A thread stops at its box's first error;
+ * the call returns the error of the lowest-numbered failing box and its index in
+ * *failed (-1 if none).  Each context must have a state loaded. */
+int32_t cube_run_steps(cube_ctx* const* ctxs, cube_scalars* ios, int32_t n, int32_t steps, int32_t threads,
+                       int32_t* failed);
+
 /* Friedmann expansion of timestep.f90:136-180 (real(4) interface, FP64 inside). */
 void cube_expansion(const cube_params* params, float a0, float dt0, float* da1, float* da2);
 

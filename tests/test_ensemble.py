@@ -53,3 +53,44 @@ def test_gpu_concurrent_boxes_match_sequential(tables):
     for a, b in zip(s1, s6):
         for x, y in zip(a, b):
             assert np.array_equal(x, y)
+    # the library's own thread pool (cube_run_steps) gives the same states and scalars
+    nat = Ensemble(specs, fk, ck)
+    rn = nat.run_native(3, workers=4)
+    sn = nat.states()
+    assert all(m.steps == 3 for m in nat.members)
+    nat.close()
+    assert rn["boxes"] == 6 and rn["workers"] == 4
+    for a, b in zip(s1, sn):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+def test_gpu_native_runner_matches_python_steps_and_reports_errors(tables):
+    from cube_nufluid_b200.cube import CubeError
+    fk, ck = tables
+    specs = [BoxSpec(nc=16, box=60.0, omega_m=0.3, sigma8=0.8, seed=21),
+             BoxSpec(nc=32, box=250.0, omega_m=0.28, sigma8=0.82, seed=22, pp=True)]
+    py = Ensemble(specs, fk, ck)
+    py.run(2, workers=1)
+    nat = Ensemble(specs, fk, ck)
+    nat.run_native(2, workers=2)
+    for a, b in zip(py.members, nat.members):
+        assert a.s.as_dict() == b.s.as_dict()
+    for a, b in zip(py.states(), nat.states()):
+        for x, y in zip(a, b):
+            assert np.array_equal(x, y)
+    py.close()
+    # a context without a loaded state is refused with its index
+    import ctypes as C
+    from cube_nufluid_b200 import Cube
+    from cube_nufluid_b200.abi import CubeScalars
+    fresh = Cube(nat.members[0].cube.p, np_capacity=4096, fk_table=fk, ck_table=ck)
+    L = fresh.L
+    handles = (C.c_void_p * 2)(nat.members[0].cube.h, fresh.h)
+    ios = (CubeScalars * 2)()
+    failed = C.c_int32(-5)
+    rc = L.cube_run_steps(handles, ios, 2, 1, 2, C.byref(failed))
+    assert rc == 6 and failed.value == 1  # CUBE_ERR_STATE, the second context
+    fresh.close()
+    nat.close()
