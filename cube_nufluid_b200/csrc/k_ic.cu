@@ -8,20 +8,31 @@
  *              (w >> 8) * 2^-24, through the reference's Box-Muller pairing along x
  *              (initial_conditions.f90:320-336); the host generator in ic.py draws
  *              the same uniforms;
- *   displacement psi_d = IFFT( i k_d / k^2 * amp(k) * FFT(noise) ) on the particle
- *              grid (npd = np_nc*nc per side), amp^2 = Delta^2(k)/(4 pi) (npd/k)^3 with
- *              the Eisenstein-Hu no-wiggle transfer, sigma8 normalisation and growth
- *              passed in by the host; evaluated with the library's Poisson passes and
- *              a "Green" octant K_d = amp k_d / k^2 (odd in k_d, zero on its Nyquist
- *              plane);
- *   particles  lattice q = i/np_nc + 1/(2 ncell) (coarse units), x = q + psi/np_nc,
- *              v = psi/np_nc * ncell * vf; sorted by tile-major cell, in lattice
+ *   potential  the reference's method (initial_conditions.f90:449-523,776-836): on the
+ *              fine mesh (nf = ncell*nc per side) phi = K' * delta_L, K = -4 pi/khat^2
+ *              with the discrete Laplacian khat^2 = sum (2 sin(pi m/nf))^2, corrected
+ *              in real space to the exact -1/r within 8 cells (-2.5 at r = 0) and
+ *              shifted by -(phi8 + 1/8) beyond; the correction is the transform of a
+ *              stencil of 8-cell radius, built from the kernel's own transform (two
+ *              forward FFTs of the library); delta_L = amp(k) FFT(noise), amp^2 =
+ *              Delta^2(k)/(4 pi) (nf/k)^3 with the Eisenstein-Hu no-wiggle transfer,
+ *              sigma8 normalisation and growth passed in by the host;
+ *   displacement psi_d = -(phi(i+1) - phi(i-1))/(8 pi) along d at each particle's fine
+ *              node: in k space the multiplier -i sin(2 pi m_d/nf) K'/(4 pi), odd in its
+ *              own wavenumber, so the library's Poisson passes evaluate it as a "Green"
+ *              octant (zero on the own-dimension Nyquist plane);
+ *   particles  lattice q = i/np_nc + 1/(2 ncell) (coarse units), the centre of fine cell
+ *              (ncell/np_nc) i, x = q + psi/ncell, v = psi * vf; sorted by tile-major cell, in lattice
  *              order inside a cell; PID = 1 + the fine-mesh index of the lattice
  *              point, iq = (ncell/np_nc)*lattice index per dimension (:834-836); per cell the mean
  *              velocity (vfield), the residuals' dispersion sigma_vi, and the codes
  *              (initial_conditions.f90:797-838).
  */
 #include "cube_internal.cuh"
+
+#include <cmath>
+#include <cstdlib>
+#include <vector>
 
 namespace {
 
@@ -61,8 +72,55 @@ __global__ void k_ic_noise(float* __restrict__ rho, int n, int rp, uint32_t k0, 
 struct IcSpec {
   double norm_d2, n_s, h, eh_s, eh_alpha, eh_omh, eh_theta2;
   double box, amplitude;
-  int npd;
+  int n;              // the fine mesh per side
+  double psi_scale;   // np_nc / ncell: the packer's lattice units per fine cell
+  const float2* W;    // transform of the kernel correction stencil (null: none)
+  int kx_major, cp;   // its layout: [kx][ky][kz] dense, or [kz][ky][kx] at row pitch cp
 };
+
+constexpr int EWALD_R = 8;  // radius (cells) of the exact -1/r near field
+
+// the discrete-Laplacian potential kernel -4 pi/khat^2 at integer wavenumbers (0 at k = 0)
+__device__ __forceinline__ double ic_laplace_kernel(int mx, int my, int mz, int n) {
+  const double pin = 3.14159265358979323846 / (double)n;
+  const double sx = 2.0 * sin(pin * mx), sy = 2.0 * sin(pin * my), sz = 2.0 * sin(pin * mz);
+  const double kr = sx * sx + sy * sy + sz * sz;
+  return kr > 0.0 ? -4.0 * 3.14159265358979323846 / kr : 0.0;
+}
+
+// the kernel at every wavenumber of the mesh (index = wavenumber mod n), as a real field
+__global__ void k_ic_kfill(float* __restrict__ mesh, int n, int rp) {
+  const int64_t tot = (int64_t)n * n * n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((int64_t)n * n));
+    mesh[((size_t)z * n + y) * rp + x] = (float)ic_laplace_kernel(x, y, z, n);
+  }
+}
+
+// element (kx, ky, kz) of a forward 3-D transform left by cube_fft_forward3
+__device__ __forceinline__ float2 ic_spec(const float2* S, int kx, int ky, int kz, int n, int kx_major, int cp) {
+  return kx_major ? S[((size_t)kx * n + ky) * n + kz] : S[((size_t)kz * n + ky) * cp + kx];
+}
+
+// the real-space kernel K_r(r) = Re FFT(K)(r) / n^3 (K is real and even) for r in [0, 8]^3
+__global__ void k_ic_kreal(const float2* __restrict__ S, int n, int kx_major, int cp, double* __restrict__ out) {
+  constexpr int R1 = EWALD_R + 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= R1 * R1 * R1) return;
+  const int rx = i % R1, ry = (i / R1) % R1, rz = i / (R1 * R1);
+  out[i] = (double)ic_spec(S, rx, ry, rz, n, kx_major, cp).x / ((double)n * n * n);
+}
+
+// the correction stencil w(r) (2R+1)^3 into the zeroed mesh at r mod n
+__global__ void k_ic_wfill(float* __restrict__ mesh, int n, int rp, const float* __restrict__ w) {
+  constexpr int D = 2 * EWALD_R + 1;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= D * D * D) return;
+  const float v = w[i];
+  if (v == 0.f) return;
+  const int x = (i % D - EWALD_R + n) % n, y = ((i / D) % D - EWALD_R + n) % n, z = (i / (D * D) - EWALD_R + n) % n;
+  mesh[((size_t)z * n + y) * rp + x] = v;
+}
 
 __device__ double eh_nowiggle(double k_hmpc, const IcSpec& S) {
   const double k_mpc = k_hmpc * S.h;
@@ -74,38 +132,42 @@ __device__ double eh_nowiggle(double k_hmpc, const IcSpec& S) {
   return l0 / (l0 + c0 * q * q);
 }
 
-// Zel'dovich "Green" octant [d][ky][kx][kz] (kz fastest), (n/2+1)^3 per component,
-// with 1/n^3 folded in like the force kernels
+// the displacement "Green" octant [d][ky][kx][kz] (kz fastest), (n/2+1)^3 per
+// component: -sin(2 pi k_d/n)/(4 pi) K'(k) amp(k) (np_nc/ncell) / n^3, K' = K + Re W,
+// zero on the own-dimension Nyquist plane
 __global__ void k_ic_kernel(float* __restrict__ kern, IcSpec S) {
-  const int n = S.npd, nh = n / 2, kp = nh + 1;
+  const int n = S.n, nh = n / 2, kp = nh + 1;
   const int64_t tot = (int64_t)kp * kp * kp;
-  const float kgrid = (float)(2.0 * 3.14159265358979323846 / n);
+  const double twopi = 2.0 * 3.14159265358979323846;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int kz = (int)(i % kp);
     const int64_t r = i / kp;
     const int kx = (int)(r % kp), ky = (int)(r / kp);
     const float kr2 = (float)kx * kx + (float)ky * ky + (float)kz * kz;
     const float kr = sqrtf(fmaxf(kr2, 1.f));
-    const double kphys = 2.0 * 3.14159265358979323846 * (double)kr / S.box;
+    const double kphys = twopi * (double)kr / S.box;
     const double t = eh_nowiggle(kphys, S);
     const float d2 = (float)(S.norm_d2 * t * t * pow(kphys, 3.0 + S.n_s));
     const float nk = (float)n / kr;
     const float amp = sqrtf(d2 / (float)(4.0 * 3.14159265358979323846) * nk) * nk * (float)S.amplitude;
-    const float inv = kr2 > 0.f ? 1.f / (kgrid * kgrid * kr2) : 0.f;
+    double kc = ic_laplace_kernel(kx, ky, kz, n);
+    if (S.W && (kx | ky | kz)) kc += (double)ic_spec(S.W, kx, ky, kz, n, S.kx_major, S.cp).x;
+    const float kcf = (float)kc;
     const float norm = 1.f / ((float)n * (float)n * (float)n);
     const int kd[3] = {kx, ky, kz};
     for (int d = 0; d < 3; ++d) {
-      float v = (kd[d] == nh) ? 0.f : kgrid * (float)kd[d] * inv * amp * norm;
-      kern[(size_t)d * tot + ((size_t)ky * kp + kx) * kp + kz] = v;
+      const float g = (kd[d] == nh) ? 0.f : (float)(-sin(twopi * kd[d] / n) / (4.0 * 3.14159265358979323846));
+      kern[(size_t)d * tot + ((size_t)ky * kp + kx) * kp + kz] = g * kcf * amp * (float)S.psi_scale * norm;
     }
   }
 }
 
 struct PartArgs {
-  const float* psi;   // three displacement meshes, component stride cstride, pitch rp
+  const float* psi;   // three displacement meshes (fine mesh nf^3), component stride cstride, pitch rp
   size_t cstride;
   int rp, npd, np_nc, ncell, nc, nt, nnt;
   double vf;
+  int nf, st;         // fine mesh per side; fine cells between lattice points (ncell/np_nc)
 };
 
 // lattice point -> cell (tile-major) and counts
@@ -114,7 +176,7 @@ __global__ void k_ic_cells(PartArgs A, int32_t* __restrict__ cell, int32_t* __re
   const int64_t tot = (int64_t)n * n * n;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
     const int q[3] = {(int)(i % n), (int)((i / n) % n), (int)(i / ((int64_t)n * n))};
-    const size_t o = ((size_t)q[2] * n + q[1]) * A.rp + q[0];
+    const size_t o = ((size_t)(A.st * q[2]) * A.nf + A.st * q[1]) * A.rp + A.st * q[0];
     int g[3];
     for (int d = 0; d < 3; ++d) {
       const double psi = (double)A.psi[d * A.cstride + o];
@@ -142,7 +204,7 @@ __global__ void k_ic_place(const int32_t* __restrict__ cell, const int64_t* __re
 __device__ __forceinline__ void lattice_state(const PartArgs& A, int64_t i, double x[3], double v[3]) {
   const int n = A.npd;
   const int q[3] = {(int)(i % n), (int)((i / n) % n), (int)(i / ((int64_t)n * n))};
-  const size_t o = ((size_t)q[2] * n + q[1]) * A.rp + q[0];
+  const size_t o = ((size_t)(A.st * q[2]) * A.nf + A.st * q[1]) * A.rp + A.st * q[0];
   for (int d = 0; d < 3; ++d) {
     const double dsp = (double)A.psi[d * A.cstride + o] / A.np_nc;
     double xx = (double)q[d] / A.np_nc + 0.5 / A.ncell + dsp;
@@ -271,14 +333,12 @@ __global__ void k_ic_counts(const int64_t* __restrict__ start, int32_t* __restri
 // temporaries of one cube_make_ic call, freed on every return path
 struct IcScratch {
   float* kern = nullptr;
-  float2* tw = nullptr;
-  float2* tw2 = nullptr;
-  double2* twd = nullptr;
+  double* kr = nullptr;
+  float* w = nullptr;
   ~IcScratch() {
     if (kern) cudaFree(kern);
-    if (tw) cudaFree(tw);
-    if (tw2) cudaFree(tw2);
-    if (twd) cudaFree(twd);
+    if (kr) cudaFree(kr);
+    if (w) cudaFree(w);
   }
 };
 
@@ -286,8 +346,8 @@ int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io)
   const int np_nc = icp->np_nc;
   const int npd = np_nc * ctx->nc;
   const int64_t np = (int64_t)npd * npd * npd;
-  if (np_nc < 1 || np_nc > ctx->ncell || npd % 2) {
-    ctx->err = "initial conditions: need 1 <= np_nc <= ncell and np_nc*nc even";
+  if (np_nc < 1 || np_nc > ctx->ncell || ctx->ncell % np_nc) {
+    ctx->err = "initial conditions: need np_nc to divide ncell";
     return CUBE_ERR_PARAM;
   }
   if (np > ctx->cap || np >= (1ll << 31)) {
@@ -298,40 +358,71 @@ int cube_make_ic_dev(cube_ctx* ctx, const cube_ic_params* icp, cube_scalars* io)
     ctx->err = "initial conditions: PIDs are fine-mesh indices + 1 and need nf^3 < 2^31";
     return CUBE_ERR_PARAM;
   }
-  // the particle grid borrows the fine mesh's arrays (free outside particle_mesh);
-  // npd <= nf, so it fits with its own pitch
-  MeshLevel M{};  // an FP32 level (fp64 = 0, no FP64 Green table)
-  M.n = npd;
-  M.rp = npd + 32;
-  M.cp = M.rp / 2;
-  M.plane = (size_t)npd * M.rp;
-  M.rho = ctx->fine.rho;
-  M.force = ctx->fine.force;
-  M.ext = ctx->fine.ext;
+  // everything runs on the fine mesh's arrays (free outside particle_mesh), with its
+  // own Green table set aside for a displacement table of the same octant layout
+  MeshLevel& F = ctx->fine;
+  const int n = F.n;
+  MeshLevel M = F;
   M.kern_octant = 1;
-  M.kern_pitch = npd / 2 + 1;
+  M.kern_pitch = n / 2 + 1;
+  M.kernd = nullptr;
   IcScratch tmp;
-  int rc = cube_fft_plan(ctx, M.plan, npd);
-  tmp.tw = M.plan.tw;
-  tmp.tw2 = M.plan.tw2;
-  tmp.twd = M.plan.twd;
-  if (rc) return rc;
   const size_t ksz = (size_t)M.kern_pitch * M.kern_pitch * M.kern_pitch;
   CUBE_CUDA_TRY(ctx, cudaMalloc((void**)&tmp.kern, sizeof(float) * 3 * ksz));
   M.kern = tmp.kern;
   const int g = ctx->num_sms * 8;
-  const uint64_t seed = (uint64_t)icp->seed;
-  k_ic_noise<<<g, 256, 0, ctx->stream>>>(M.rho, npd, M.rp, (uint32_t)seed, (uint32_t)(seed >> 32), ctx->codec.pi_f);
-  CUBE_LAUNCH_CHECK(ctx);
-  IcSpec S = {icp->norm_d2, icp->n_s,      icp->h,          icp->eh_s, icp->eh_alpha, icp->eh_omh,
-              icp->eh_theta2, (double)ctx->P.box, icp->amplitude, npd};
+  int rc;
+  IcSpec S = {icp->norm_d2, icp->n_s, icp->h, icp->eh_s, icp->eh_alpha, icp->eh_omh, icp->eh_theta2,
+              (double)ctx->P.box, icp->amplitude, n, (double)np_nc / (double)ctx->ncell, nullptr, 0, F.cp};
+  if (n >= 2 * EWALD_R + 2) {
+    // the kernel correction: K_r(r) for r in [0, 8]^3 from the forward transform of K,
+    // the stencil w(r) = exact(r) - K_r(r) + phi8 + 1/8 within r <= 8, its transform W
+    constexpr int R1 = EWALD_R + 1, D = 2 * EWALD_R + 1;
+    int kxm = 0;
+    k_ic_kfill<<<g, 256, 0, ctx->stream>>>(F.rho, n, F.rp);
+    CUBE_LAUNCH_CHECK(ctx);
+    if ((rc = cube_fft_forward3(ctx, F, F.rho, &kxm))) return rc;
+    CUBE_CUDA_TRY(ctx, cudaMalloc((void**)&tmp.kr, sizeof(double) * R1 * R1 * R1));
+    CUBE_CUDA_TRY(ctx, cudaMalloc((void**)&tmp.w, sizeof(float) * D * D * D));
+    k_ic_kreal<<<(R1 * R1 * R1 + 255) / 256, 256, 0, ctx->stream>>>(reinterpret_cast<const float2*>(F.rho), n, kxm,
+                                                                    F.cp, tmp.kr);
+    CUBE_LAUNCH_CHECK(ctx);
+    std::vector<double> kr(R1 * R1 * R1);
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(kr.data(), tmp.kr, sizeof(double) * kr.size(), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    auto K_r = [&](int x, int y, int z) { return kr[((size_t)std::abs(z) * R1 + std::abs(y)) * R1 + std::abs(x)]; };
+    const double phi8 = (K_r(EWALD_R, 0, 0) + K_r(0, EWALD_R, 0) + K_r(0, 0, EWALD_R)) / 3.0;
+    std::vector<float> w((size_t)D * D * D, 0.f);
+    for (int z = -EWALD_R; z <= EWALD_R; ++z)
+      for (int y = -EWALD_R; y <= EWALD_R; ++y)
+        for (int x = -EWALD_R; x <= EWALD_R; ++x) {
+          const double d = std::sqrt((double)(x * x + y * y + z * z));
+          if (d > EWALD_R) continue;
+          const double exact = d > 0.0 ? -1.0 / d : -2.5;
+          w[((size_t)(z + EWALD_R) * D + (y + EWALD_R)) * D + (x + EWALD_R)] =
+              (float)(exact - K_r(x, y, z) + phi8 + 1.0 / EWALD_R);
+        }
+    CUBE_CUDA_TRY(ctx, cudaMemcpyAsync(tmp.w, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice, ctx->stream));
+    CUBE_CUDA_TRY(ctx, cudaMemsetAsync(F.rho, 0, sizeof(float) * (size_t)n * F.plane, ctx->stream));
+    k_ic_wfill<<<(D * D * D + 255) / 256, 256, 0, ctx->stream>>>(F.rho, n, F.rp, tmp.w);
+    CUBE_LAUNCH_CHECK(ctx);
+    if ((rc = cube_fft_forward3(ctx, F, F.rho, &kxm))) return rc;
+    S.W = reinterpret_cast<const float2*>(F.rho);
+    S.kx_major = kxm;
+    CUBE_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));  // the host stencil buffer stays alive until here
+  }
   k_ic_kernel<<<g, 256, 0, ctx->stream>>>(M.kern, S);
+  CUBE_LAUNCH_CHECK(ctx);
+  const uint64_t seed = (uint64_t)icp->seed;
+  k_ic_noise<<<g, 256, 0, ctx->stream>>>(M.rho, n, M.rp, (uint32_t)seed, (uint32_t)(seed >> 32), ctx->codec.pi_f);
   CUBE_LAUNCH_CHECK(ctx);
   CUBE_CUDA_TRY(ctx, cudaMemsetAsync(ctx->dscal, 0, sizeof(DevScal), ctx->stream));
   const KickScale none = {0.f, 0.f, 1.f, 0, 1.f, 1.f};
   if ((rc = cube_fft_poisson(ctx, M, &ctx->dscal->f2_coarse_bits, none))) return rc;
   // cells, counting sort, lattice order inside each cell, per-cell sums
-  PartArgs A = {M.force, (size_t)npd * M.plane, M.rp, npd, np_nc, ctx->ncell, ctx->nc, ctx->nt, ctx->nnt, icp->vf};
+  PartArgs A = {M.force, (size_t)n * M.plane, M.rp, npd,     np_nc, ctx->ncell, ctx->nc, ctx->nt,
+                ctx->nnt, icp->vf, n,           ctx->ncell / np_nc};
   int32_t* cell = ctx->tcell;  // cell of each lattice point
   int32_t* perm = ctx->perm;   // slot -> lattice index
   const int64_t nce = ctx->ncells;

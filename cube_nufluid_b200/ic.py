@@ -220,30 +220,81 @@ def _linear_delta_k(npd: int, box: float, a: float, seed: int, c: Cosmology, amp
     return dk, kx, ky, kz, kr2
 
 
+# radius (in mesh cells) inside which the potential kernel is the exact -1/r
+EWALD_R = 8
+
+
+def potential_kernel(n: int) -> np.ndarray:
+    """The reference's potential kernel on a periodic n^3 mesh, in k space, full
+    [z][y][x] (initial_conditions.f90:449-523): -4 pi/khat^2 with the discrete
+    Laplacian khat^2 = sum_d (2 sin(pi m_d/n))^2, zero at k = 0; with its kernel
+    correction (correct_kernel): its real-space form K_r (the inverse transform, 1/n^3
+    normalised) is replaced within r <= 8 cells by the exact -1/r (-2.5 at r = 0) and
+    shifted beyond by -(phi8 + 1/8), phi8 = the mean of K_r at distance 8 on the six
+    axes, and transformed back.  As a correction in k space: K + FFT(w), w(r) =
+    exact(r) - K_r(r) + phi8 + 1/8 on the cells within r <= 8 (the constant shift of
+    every other cell only moves k = 0, which stays zero).  K is real and even, so its
+    inverse transform is its forward one over n^3.  Meshes of fewer than 2*8+2 cells
+    per side take the kernel without the correction."""
+    m = np.fft.fftfreq(n, d=1.0 / n)
+    s2 = (2.0 * np.sin(np.pi * m / n)) ** 2
+    kr = s2[:, None, None] + s2[None, :, None] + s2[None, None, :]
+    K = np.zeros_like(kr)
+    nz = kr > 0
+    K[nz] = -4.0 * np.pi / kr[nz]
+    if n < 2 * EWALD_R + 2:
+        return K
+    Kr = np.fft.fftn(K).real / float(n) ** 3
+    R = EWALD_R
+    phi8 = (Kr[R, 0, 0] + Kr[n - R, 0, 0] + Kr[0, R, 0] + Kr[0, n - R, 0] + Kr[0, 0, R] + Kr[0, 0, n - R]) / 6.0
+    r = np.arange(-R, R + 1)
+    rz, ry, rx = np.meshgrid(r, r, r, indexing="ij")
+    d = np.sqrt(rx * rx + ry * ry + rz * rz)
+    sel = d <= R
+    exact = np.where(d > 0, -1.0 / np.where(d > 0, d, 1.0), -2.5)
+    iz, iy, ix = rz[sel] % n, ry[sel] % n, rx[sel] % n
+    w = np.zeros((n, n, n))
+    w[iz, iy, ix] = exact[sel] - Kr[iz, iy, ix] + (phi8 + 1.0 / R)
+    K = K + np.fft.fftn(w).real
+    K[0, 0, 0] = 0.0
+    return K
+
+
 def zeldovich(nc: int, nnt: int, box: float, z_i: float, seed: int, *, np_nc: int = 2,
               ncell: int = 4, izipx: int = 2, izipv: int = 2, cosmo: Cosmology | None = None,
               f_cdm: float = 1.0, amplitude: float = 1.0) -> ICState:
-    """Build a seeded Zel'dovich state at z_i in checkpoint layout."""
+    """Build a seeded Zel'dovich state at z_i in checkpoint layout, by the reference's
+    method (initial_conditions.f90:449-836): the linear density on the fine mesh, the
+    potential phi = K * delta with the corrected discrete-Laplacian kernel of
+    potential_kernel, and each particle (lattice spacing ncell/np_nc fine cells, at
+    the centre of its fine cell) displaced by -(phi(i+1) - phi(i-1))/(8 pi) fine cells
+    along each axis, with velocity that displacement times the growth factor vf.  The
+    central difference is applied in k space, where it is the multiplier
+    2 i sin(2 pi m_d/nf)."""
     c = cosmo or Cosmology()
+    nf = nc * ncell
     npd = nc * np_nc
+    st = ncell // np_nc
+    if ncell % np_nc:
+        raise ValueError("np_nc must divide ncell")
     a = 1.0 / (1.0 + z_i)
     import scipy.fft as sfft
-    dk, kx, ky, kz, kr2 = _linear_delta_k(npd, box, a, seed, c, amplitude)
-    kgrid = 2 * math.pi / npd
-    inv = np.where(kr2 > 0, 1.0 / (kgrid * kgrid * np.maximum(kr2, 1e-30)), 0.0).astype(np.float32)
+    dk, kx, ky, kz, kr2 = _linear_delta_k(nf, box, a, seed, c, amplitude)
+    Kc = potential_kernel(nf)[:, :, : nf // 2 + 1].astype(np.float32)
     disp = np.empty((3, npd, npd, npd), dtype=np.float32)
     for d, kk in enumerate((kx[None, None, :], ky[None, :, None], kz[:, None, None])):
-        # odd in its own wavenumber: zero on that dimension's Nyquist plane
-        psi_k = 1j * (kgrid * kk) * inv * dk * (np.abs(kk) != npd // 2)
-        disp[d] = sfft.irfftn(psi_k, s=(npd, npd, npd), workers=-1)
+        g = (-np.sin(2.0 * np.pi * kk.astype(np.float64) / nf) / (4.0 * np.pi)).astype(np.float32)
+        g = np.where(np.abs(kk) == nf // 2, np.float32(0), g)  # zero on the own-dimension Nyquist plane
+        psi_k = 1j * g * Kc * dk
+        disp[d] = sfft.irfftn(psi_k, s=(nf, nf, nf), workers=-1)[::st, ::st, ::st]  # fine cells
         del psi_k
-    del dk, inv
+    del dk, Kc
     # lattice positions in coarse units: q = i/np_nc + 0.5/ncell (initial_conditions.f90:793)
     ii = np.arange(npd, dtype=np.float64) / np_nc + 0.5 / ncell
     zz, yy, xx = np.meshgrid(ii, ii, ii, indexing="ij")
     pos = np.stack([xx, yy, zz], axis=-1).reshape(-1, 3)
     del xx, yy, zz
-    dsp = np.stack([disp[0], disp[1], disp[2]], axis=-1).reshape(-1, 3).astype(np.float64) / np_nc
+    dsp = np.stack([disp[0], disp[1], disp[2]], axis=-1).reshape(-1, 3).astype(np.float64) / ncell
     del disp
     x = np.mod(pos + dsp, float(nc))
     vf = vfactor(a, c.omega_m, c.omega_l)

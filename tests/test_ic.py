@@ -49,6 +49,60 @@ def test_gaussian_noise_moments():
     assert abs(g.mean()) < 0.01 and abs(g.std() - 1.0) < 0.01
 
 
+def test_potential_kernel_has_the_exact_near_field():
+    """initial_conditions.f90:478-523 (correct_kernel): in real space the corrected
+    kernel is -1/r within 8 cells and -2.5 at r = 0, up to the constant that the zeroed
+    k = 0 mode removes; beyond 8 cells it is the discrete-Laplacian kernel shifted."""
+    n = 40
+    K = ic.potential_kernel(n)
+    Kr = np.fft.ifftn(K).real
+    c = Kr[1, 0, 0] + 1.0
+    for r in [(0, 0, 0), (1, 0, 0), (0, 2, 0), (3, 4, 0), (0, 0, 8), (2, 3, 6), (5, 5, 5)]:
+        d = math.sqrt(sum(x * x for x in r))
+        exact = -2.5 if d == 0 else -1.0 / d
+        if d <= 8:
+            assert abs((Kr[r] - c) - exact) < 1e-12, (r, Kr[r] - c, exact)
+    # far field: the uncorrected lattice Green function plus the shift, close to -1/r
+    m = np.fft.fftfreq(n, d=1.0 / n)
+    s2 = (2 * np.sin(np.pi * m / n)) ** 2
+    kr = s2[:, None, None] + s2[None, :, None] + s2[None, None, :]
+    K0 = np.where(kr > 0, -4 * np.pi / np.where(kr > 0, kr, 1.0), 0.0)
+    K0r = np.fft.ifftn(K0).real
+    phi8 = (K0r[8, 0, 0] + K0r[n - 8, 0, 0] + K0r[0, 8, 0] + K0r[0, n - 8, 0] + K0r[0, 0, 8] + K0r[0, 0, n - 8]) / 6
+    for r in [(9, 0, 0), (6, 6, 3), (12, 5, 0)]:
+        assert abs((Kr[r] - c) - (K0r[r] - (phi8 + 1 / 8))) < 1e-9
+    # meshes too small for the 8-cell near field keep the plain kernel
+    m16 = np.fft.fftfreq(16, d=1.0 / 16)
+    s16 = (2 * np.sin(np.pi * m16 / 16)) ** 2
+    k16 = s16[:, None, None] + s16[None, :, None] + s16[None, None, :]
+    plain = np.where(k16 > 0, -4 * np.pi / np.where(k16 > 0, k16, 1.0), 0.0)
+    assert np.array_equal(ic.potential_kernel(16), plain)
+
+
+def test_zeldovich_displacement_is_the_central_difference_of_phi():
+    """The generator's displacement at a lattice point equals -(phi(i+1) - phi(i-1))/(8 pi)
+    of phi = IFFT(K' delta) on the fine mesh (initial_conditions.f90:794-796, 828)."""
+    import scipy.fft as sfft
+    nc, ncell, np_nc, box, z_i, seed = 8, 4, 2, 100.0, 49.0, 5
+    nf = nc * ncell
+    c = ic.Cosmology()
+    a = 1.0 / (1.0 + z_i)
+    dk, kx, ky, kz, _ = ic._linear_delta_k(nf, box, a, seed, c, 1.0)
+    Kc = ic.potential_kernel(nf)[:, :, : nf // 2 + 1]
+    phi = sfft.irfftn(Kc * dk, s=(nf, nf, nf))  # [z][y][x]
+    gx = -(np.roll(phi, -1, axis=2) - np.roll(phi, 1, axis=2)) / (8 * np.pi)
+    # the same from the generator's own k-space multiplier
+    g = -np.sin(2 * np.pi * kx / nf) / (4 * np.pi)
+    g = np.where(np.abs(kx) == nf // 2, 0.0, g)
+    psi = sfft.irfftn(1j * g[None, None, :] * Kc * dk, s=(nf, nf, nf))
+    # they differ only by the Nyquist-plane term that the generator drops
+    dkn = dk.copy()
+    dkn[:, :, : nf // 2] = 0
+    nyq = -(np.roll(sfft.irfftn(Kc * dkn, s=(nf, nf, nf)), -1, axis=2)
+            - np.roll(sfft.irfftn(Kc * dkn, s=(nf, nf, nf)), 1, axis=2)) / (8 * np.pi)
+    assert np.allclose(psi, gx - nyq, atol=1e-6 * np.abs(gx).max())
+
+
 def test_device_ic_params_reproduce_delta2():
     c = ic.Cosmology()
     z_i, box = 49.0, 200.0
