@@ -42,58 +42,72 @@ __global__ void k_tree_block(const double* __restrict__ in, int64_t n, double* _
 // storage order, vr = tan(code)/coef of its new residual code and vs = vr + vfield of
 // its new cell, r2 = (vr_x^2 + vr_y^2) + vr_z^2 and s2 likewise from vs; the two
 // block sums follow the tree of k_tree_block exactly, so the totals are the ones a
-// stored list of terms would give.
+// stored list of terms would give.  One element's terms: (vr_x^2 + vr_y^2) + vr_z^2 and
+// the same from vs (0 past the end)
 template <int ZV>
-__global__ void k_stats_first(const void* __restrict__ vp_, int64_t cap, const int32_t* __restrict__ slot_cell,
-                              const float* __restrict__ vfield, int64_t ncells, const double* __restrict__ dec,
-                              int half_nvbin, int64_t n, double* __restrict__ out_r, double* __restrict__ out_s) {
+__device__ __forceinline__ void stats_terms(const typename CodeT<ZV>::T* __restrict__ vp, int64_t cap,
+                                            const int32_t* __restrict__ slot_cell, const float* __restrict__ vfield,
+                                            int64_t ncells, const double* __restrict__ dec, int half_nvbin, int64_t n,
+                                            int64_t q, double& r2, double& s2) {
+  r2 = 0.0;
+  s2 = 0.0;
+  if (q >= n) return;
+  const int64_t c = slot_cell[q];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    const double vr = __ldg(&dec[(int)vp[(size_t)d * cap + q] + half_nvbin]);
+    const double vs = __dadd_rn(vr, (double)__ldg(&vfield[(size_t)d * ncells + c]));
+    r2 = __dadd_rn(r2, __dmul_rn(vr, vr));
+    s2 = __dadd_rn(s2, __dmul_rn(vs, vs));
+  }
+}
+
+// One warp per 1024-block of the tree, the same additions in the same order as
+// k_tree_block: lane l holds elements l + 32k, so the shared-memory stages of stride
+// 512 .. 32 (loc[i] += loc[i + s] for i < s) are register pairs (k, k + s/32), and the
+// last five stages are the same shuffles.  Elements k and k + 16 are formed together
+// and added at once (the stride-512 stage), so 16 partial sums per quantity are held.
+template <int ZV>
+__global__ void __launch_bounds__(256) k_stats_first(const void* __restrict__ vp_, int64_t cap,
+                                                     const int32_t* __restrict__ slot_cell,
+                                                     const float* __restrict__ vfield, int64_t ncells,
+                                                     const double* __restrict__ dec, int half_nvbin, int64_t n,
+                                                     int64_t nblocks, double* __restrict__ out_r,
+                                                     double* __restrict__ out_s) {
   typedef typename CodeT<ZV>::T TV;
   const TV* vp = reinterpret_cast<const TV*>(vp_);
-  __shared__ double lr[1024], ls[1024];
-  const int i = threadIdx.x;  // 512 threads
-  const int64_t b = blockIdx.x;
-  double r[2] = {0.0, 0.0}, sv[2] = {0.0, 0.0};
+  const int lane = threadIdx.x & 31;
+  const int64_t b = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (b >= nblocks) return;  // the whole warp
+  const int64_t base = b * 1024 + lane;
+  double R[16], S[16];
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int64_t q = b * 1024 + i + 512 * h;
-    if (q < n) {
-      const int64_t c = slot_cell[q];
-      double r2 = 0.0, s2 = 0.0;
+  for (int k = 0; k < 16; ++k) {
+    double r0, s0, r1, s1;
+    stats_terms<ZV>(vp, cap, slot_cell, vfield, ncells, dec, half_nvbin, n, base + 32 * k, r0, s0);
+    stats_terms<ZV>(vp, cap, slot_cell, vfield, ncells, dec, half_nvbin, n, base + 32 * (k + 16), r1, s1);
+    R[k] = __dadd_rn(r0, r1);  // stride 512
+    S[k] = __dadd_rn(s0, s1);
+  }
 #pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const double vr = __ldg(&dec[(int)vp[(size_t)d * cap + q] + half_nvbin]);
-        const double vs = __dadd_rn(vr, (double)__ldg(&vfield[(size_t)d * ncells + c]));
-        r2 = __dadd_rn(r2, __dmul_rn(vr, vr));
-        s2 = __dadd_rn(s2, __dmul_rn(vs, vs));
-      }
-      r[h] = r2;
-      sv[h] = s2;
+  for (int h = 8; h >= 1; h >>= 1)  // strides 256, 128, 64, 32
+#pragma unroll
+    for (int k = 0; k < h; ++k) {
+      R[k] = __dadd_rn(R[k], R[k + h]);
+      S[k] = __dadd_rn(S[k], S[k + h]);
+    }
+  double v = R[0], w = S[0];
+  for (int s = 16; s >= 1; s >>= 1) {
+    const double o = __shfl_down_sync(0xffffffffu, v, s);
+    const double p = __shfl_down_sync(0xffffffffu, w, s);
+    if (lane < s) {
+      v = __dadd_rn(v, o);
+      w = __dadd_rn(w, p);
     }
   }
-  lr[i] = __dadd_rn(r[0], r[1]);  // s = 512
-  ls[i] = __dadd_rn(sv[0], sv[1]);
-  __syncthreads();
-  for (int s = 256; s >= 32; s >>= 1) {
-    if (i < s) {
-      lr[i] = __dadd_rn(lr[i], lr[i + s]);
-      ls[i] = __dadd_rn(ls[i], ls[i + s]);
-    }
-    __syncthreads();
-  }
-  if (i < 32) {
-    double v = lr[i], w = ls[i];
-    for (int s = 16; s >= 1; s >>= 1) {
-      const double o = __shfl_down_sync(0xffffffffu, v, s);
-      const double p = __shfl_down_sync(0xffffffffu, w, s);
-      if (i < s) {
-        v = __dadd_rn(v, o);
-        w = __dadd_rn(w, p);
-      }
-    }
-    if (i == 0) {
-      out_r[b] = v;
-      out_s[b] = w;
-    }
+  if (lane == 0) {
+    out_r[b] = v;
+    out_s[b] = w;
   }
 }
 
@@ -198,12 +212,13 @@ int cube_stats_sums(cube_ctx* ctx, const int32_t* slot_cell, const double* dec, 
   // block sums in the per-slot arrays, free after the re-bin
   double* br = ctx->slot_s2;
   double* bs = ctx->slot_s2 + nb;
+  const unsigned grid = (unsigned)((nb + 7) / 8);  // a warp per 1024-block
   if (ctx->izipv == 1)
-    k_stats_first<1><<<(unsigned)nb, 512, 0, ctx->stream>>>(ctx->vp, ctx->cap, slot_cell, ctx->vfield, ctx->ncells,
-                                                            dec, ctx->nvbin / 2, n, br, bs);
+    k_stats_first<1><<<grid, 256, 0, ctx->stream>>>(ctx->vp, ctx->cap, slot_cell, ctx->vfield, ctx->ncells, dec,
+                                                    ctx->nvbin / 2, n, nb, br, bs);
   else
-    k_stats_first<2><<<(unsigned)nb, 512, 0, ctx->stream>>>(ctx->vp, ctx->cap, slot_cell, ctx->vfield, ctx->ncells,
-                                                            dec, ctx->nvbin / 2, n, br, bs);
+    k_stats_first<2><<<grid, 256, 0, ctx->stream>>>(ctx->vp, ctx->cap, slot_cell, ctx->vfield, ctx->ncells, dec,
+                                                    ctx->nvbin / 2, n, nb, br, bs);
   CUBE_LAUNCH_CHECK(ctx);
   int rc = cube_tree_sum_dev(ctx, br, nb, sum_r);
   if (rc) return rc;
