@@ -290,14 +290,32 @@ __global__ void __launch_bounds__(256) k_rebin_sortsum(RebinArgs A) {
   float acc[3];
 #pragma unroll
   for (int d = 0; d < 3; ++d) acc[d] = (float)cube_dmul((double)A.vfield[(size_t)d * A.ncells + c], 0.1);
+  // one entry ahead: the next entry's particle, key and codes are read while this
+  // entry is decoded and added (the adds keep their order)
+  typedef typename CodeT<ZV>::T TV;
+  const TV* vpr = reinterpret_cast<const TV*>(A.vp);
+  int64_t ipn = n > 0 ? A.perm[s] : 0;
+  uint32_t keyn = n > 0 ? A.pkey[s] : 0u;
+  int coden[3] = {0, 0, 0};
+  if (n > 0)
+#pragma unroll
+    for (int d = 0; d < 3; ++d) coden[d] = (int)vpr[(size_t)d * A.cap + ipn];
   for (int r = 0; r < n; ++r) {
-    const int64_t ip = A.perm[s + r];
+    const int64_t ip = ipn;
+    const uint32_t key = keyn;
+    const int code[3] = {coden[0], coden[1], coden[2]};
+    if (r + 1 < n) {
+      ipn = A.perm[s + r + 1];
+      keyn = A.pkey[s + r + 1];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) coden[d] = (int)vpr[(size_t)d * A.cap + ipn];
+    }
     A.tkey[ip] = (uint32_t)(s + r);  // the particle's slot (tkey is free after the place pass)
     A.slot_cell[s + r] = (int32_t)c;
-    const int64_t sc = src_cell(A, A.pkey[s + r], tt);
+    const int64_t sc = src_cell(A, key, tt);
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      const double v = cube_dadd(decode_v<ZX, ZV>(A, ip, d), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
+      const double v = cube_dadd(__ldg(&A.dec[code[d] + A.half_nvbin]), (double)__ldg(&A.vfield[(size_t)d * A.ncells + sc]));
       acc[d] = (float)cube_dadd((double)acc[d], v);
     }
   }
