@@ -10,19 +10,20 @@ on a host with numpy:
 * growth to z_i with the reference's Dgrow (initial_conditions.f90:1028-1041);
 * unit Gaussian white noise from a counter-based generator (numpy's Philox4x32-10,
   Salmon et al. 2011) seeded explicitly, scaled as at initial_conditions.f90:373;
-* Zel'dovich displacement psi_k = i k delta_k / k^2 on the particle lattice and
-  velocity v = psi * vfactor(a) (initial_conditions.f90:705,799, vfactor :1068-1079);
+* the potential on the fine mesh with the reference's corrected discrete-Laplacian
+  kernel (potential_kernel; initial_conditions.f90:449-523) and the Zel'dovich
+  displacement -(phi(i+1) - phi(i-1))/(8 pi) at each lattice particle's fine cell,
+  velocity v = psi * vfactor(a) (initial_conditions.f90:794-799, vfactor :1068-1079);
 * zip packing as at initial_conditions.f90:797-838: cell g = ceiling(x),
   xp = floor(x/x_resolution) wrapped to the code width, vfield = mean particle
   velocity of the cell, vp = arctan code of v - vfield, pid = 1 + the fine-mesh
   index of the lattice point, iq = (ncell/np_nc)*lattice index per dimension,
   pid = iq_x + nf*iq_y + nf^2*iq_z + 1 (initial_conditions.f90:834-836).
 
-The reference computes the potential on the fine mesh with a discrete
-Laplacian and central differences; this harness uses the continuous-k
-displacement on the particle lattice (np_nc particles per coarse cell per
-dimension).  Particles are ordered tile-major by coarse cell, lattice order
-inside a cell.
+Particles sit on a lattice of np_nc per coarse cell per dimension and are
+ordered tile-major by coarse cell, lattice order inside a cell.  The linear power
+comes from the Eisenstein-Hu formula where the reference reads a CAMB table, and
+the noise from Philox where it calls the compiler's random_number.
 """
 from __future__ import annotations
 
@@ -202,8 +203,9 @@ def tile_major_cell_id(g: np.ndarray, nc: int, nnt: int) -> np.ndarray:
 
 
 def _linear_delta_k(npd: int, box: float, a: float, seed: int, c: Cosmology, amplitude: float):
-    """Linear density contrast in Fourier space on an npd^3 grid from the seeded
-    noise (initial_conditions.f90:320-420): noise * sqrt(P(k)) at scale factor a."""
+    """Linear density contrast in Fourier space on an npd^3 grid (the fine mesh for
+    the particles, the particle grid for the neutrino fluids) from the seeded noise
+    (initial_conditions.f90:320-420): noise * sqrt(P(k)) at scale factor a."""
     import scipy.fft as sfft
     noise = gaussian_noise(npd, seed)  # [z][y][x]
     wk = sfft.rfftn(noise, workers=-1)
