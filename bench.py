@@ -267,6 +267,24 @@ def algorithmic_bytes(cfg, npart):
 PHASES = ["update_x", "ext_pp_force", "deposit", "fine_fft_green", "coarse_fft_green", "kick"]
 
 
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The largest of a per-rank figure (a device time) over the ranks; every rank
+    calls it at the same point.  One rank: the figure itself."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(npart_per_rank: int, world: int, steps: int, ms_max: float) -> float:
+    """Whole-job particle-updates/s: every rank advances its own box of npart_per_rank
+    particles (replicas, weak scaling), over the slowest rank's time."""
+    return npart_per_rank * world * steps / (ms_max / 1e3)
+
+
 def run_ours(args, cfg, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -328,11 +346,9 @@ def run_ours(args, cfg, rank, world, local_rank):
     npairs_timed = int(getattr(s, "npairs", 0))  # PP window entries of the last timed step
     ms = ev0.elapsed_time(ev1)
     launches = cube.launch_count() - l0
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    ms_max = max_over_ranks(ms, world)
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    ms_max = float(t.item())
 
     # end to end through the C-ABI with host-resident arrays (pinned)
     pin = {}
@@ -374,11 +390,7 @@ def run_ours(args, cfg, rank, world, local_rank):
                                                 ptr(rhoc_h), ptr(vf_h)))
         e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    t2 = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-    e2e_ms = float(t2.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1), world)
     if nu:
         phase_sum = np.append(phase_sum, nu_timed)
     cufft = None
@@ -808,8 +820,8 @@ def main():
     if world > 1:
         dist.barrier()
     r = run_ours(args, cfg, rank, world, local_rank)
-    value = r["npart"] * world * args.steps / (r["ms"] / 1e3)
-    e2e = r["npart"] * world * r["e2e_steps"] / (r["e2e_ms"] / 1e3)
+    value = job_rate(r["npart"], world, args.steps, r["ms"])
+    e2e = job_rate(r["npart"], world, r["e2e_steps"], r["e2e_ms"])
     peak, peak_kind = read_peaks()
     ab = algorithmic_bytes(cfg, r["npart"])
     names = PHASES + (["nu_fluid"] if cfg.get("nu") else [])
