@@ -515,11 +515,14 @@ def run_precision(args, cfg):
     """Precision study: the configuration's step run twice from the same seeded state,
     once in FP32 and once in the library's FP64 Poisson mode (FP64 meshes, FFT, Green
     and interpolation; the same integer deposit, codec and PP), in lockstep time steps
-    (the FP64 run takes the FP32 run's dt limits).  At checkpoint steps the FP64
-    context also computes the forces of the FP32 run's own state (the FP64 run of the
-    same step): the relative RMS difference of the fine and coarse force meshes.  At
-    z = 0 the power spectra of the two runs (the library's P(k), 4 log bins per octave)
-    give the P(k) ratio."""
+    (the FP64 run takes the FP32 run's dt limits).  Each run takes whole steps in the
+    order of Cube.step and is never read or reloaded in the middle of one.  At
+    checkpoint steps a third context, in the FP64 mode, takes the FP32 run's state
+    after its step and runs that step's particle_mesh on it: the kick moves no
+    particle, so its force meshes are the FP64 forces of the positions the FP32 run
+    just deposited, and the relative RMS difference of the fine and coarse force meshes
+    is the FP32 force error.  At z = 0 the power spectra of the two runs (the library's
+    P(k), 4 log bins per octave) give the P(k) ratio."""
     import torch
     from cube_nufluid_b200 import Cube, build, scalars_from_ic
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
@@ -541,40 +544,40 @@ def run_precision(args, cfg):
     rows = []
     n = 0
     pif = float(np.float32(4.0) * np.arctan(np.float32(1.0)))
+    gp = None  # the probe context, made at the first checkpoint
     for i, a_next in enumerate(targets):
         hit = False
         while not hit:
             for k in limits:
                 setattr(s64, k, getattr(s32, k))
-            hit = g32.timestep(s32, float(a_next))
-            g64.timestep(s64, float(a_next))
+            probe = None
             for g, sc in ((g32, s32), (g64, s64)):
+                h = g.timestep(sc, float(a_next))
                 g.update_x(sc)
                 if cfg["pp"]:
                     g.ext_pp_force(sc)
+                if g is g32:
+                    hit = h
+                    probe = s32.copy()  # the scalars particle_mesh starts from
+                g.particle_mesh(sc)
             if hit and i in checks:
-                # FP64 forces of the FP32 run's state: the FP64 context takes that state,
-                # runs the step's particle_mesh on a copy of the scalars, and gets its own back
-                keep = g64.store_state()
-                g64.load_state(*g32.store_state())
-                probe = s32.copy()
-                g64.particle_mesh(probe)
-                f64, c64 = g64.fetch(2), g64.fetch(3)
-                g64.load_state(*keep)
-                del keep
-                g32.particle_mesh(s32)
+                # FP64 forces of the positions the FP32 run deposited in this step
+                if gp is None:
+                    gp = Cube(p64, st.np)
+                gp.load_state(*g32.store_state())
+                gp.particle_mesh(probe)
+                f64, c64 = gp.fetch(2), gp.fetch(3)
                 f32, c32 = g32.fetch(2), g32.fetch(3)
                 # both meshes hold force * ((a_mid dt)/6)/pi: compare the forces
-                k32 = float(np.float32(np.float32(np.float32(s32.a_mid) * np.float32(s32.dt)) / np.float32(6.0))
+                k32 = float(np.float32(np.float32(np.float32(probe.a_mid) * np.float32(probe.dt)) / np.float32(6.0))
                             / np.float32(pif))
-                k64 = ((float(s32.a_mid) * float(s32.dt)) / 6.0) / pif
+                k64 = ((float(probe.a_mid) * float(probe.dt)) / 6.0) / pif
                 rows.append({"step": n, "a": float(s32.a), "fine": _rel_rms_chunked(f32, f64, k32, k64),
                              "coarse": _rel_rms_chunked(c32, c64, k32, k64)})
                 del f64, c64, f32, c32
-            else:
-                g32.particle_mesh(s32)
-            g64.particle_mesh(s64)
             n += 1
+    if gp is not None:
+        gp.close()
     # P(k) of both runs on the FP32 context (the FP64 mode's meshes are not FP32)
     pk32 = g32.power_spectrum(log_bins=True)
     g32.load_state(*g64.store_state())
