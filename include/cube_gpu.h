@@ -131,7 +131,10 @@ int32_t cube_abi_version(void);
 int32_t cube_create(const cube_params* params, int64_t np_capacity,
                     const float* fk_table, const float* ck_table, cube_ctx** out);
 
-/* Copies a checkpoint-layout state to the device (particle_initialization.f90:34-82). */
+/* Copies a checkpoint-layout state to the device (particle_initialization.f90:34-82).
+ * Load (and store) between steps, after cube_particle_mesh, where the reference
+ * reads and writes checkpoints: a state loaded between cube_update_x and
+ * cube_particle_mesh was measured to change the run that follows. */
 int32_t cube_load_state(cube_ctx* ctx, int64_t nplocal, const void* xp, const void* vp,
                         const int32_t* pid, const int32_t* rhoc, const float* vfield);
 
