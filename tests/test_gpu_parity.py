@@ -1,6 +1,6 @@
 """GPU parity tests: the CUDA library through its C-ABI against the CPU oracle.
 
-Bars (BASELINE north star): integer deposit, positions and velocity
+Bars: integer deposit, positions and velocity
 re-quantisation bit-exact; forces within FP32 tolerance of the FP64-FFT oracle
 (relative RMS <= 1e-5).  Sizes are small enough for the oracle to finish in
 seconds; crowded cells come from the clustered test state.
